@@ -1,0 +1,349 @@
+#!/usr/bin/env python3
+"""Benchmark: span-3 HRRT OP-OSEM subset-iterations per second on B200.
+
+Workload (the reference's span-3 configuration): HRRT model 999, span 3,
+maxdel 67 (45 segments, 6367 planes x 288 views x 256 bins), image 256x256x207
+at 1.21875 mm, 16 subsets, synthetic phantom study (seed 1 + rank, 3e8 counts,
+per-bin lognormal norm sigma 0.1, scatter 15% of trues, randoms 25%).
+
+One step = one OSEM subset-iteration: forward projection + OP ratio of the 9
+view pairs of a subset, their back projection, rotate-back and the
+multiplicative update (hrrt_osem3d_span3.cpp:4161-4260).
+
+  value : device-resident throughput (inputs, sensitivity and image in HBM).
+  e2e   : one full reconstruction through the C ABI from host buffers
+          (upload of prompts/randoms/norm/atten/scatter, sensitivity, 2
+          iterations x 16 subsets, image read back), subset-iterations per
+          second of wall time on the device (CUDA events).
+
+--impl reference times the reference's own CPU projector
+(oracle/_ref/libhrrt_ref.so: forward_proj3d_thread1 / back_proj3d_thread1 /
+rotate_image_buf and the -T thread grouping of CalculateOsem3d) on the host
+cores, one OSEM subset per step.
+With torchrun (N>1) every rank reconstructs its own frame (replicas, weak
+scaling); there is no data-path collective.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SPAN = 3
+SUBSETS = 16
+ITERATIONS = 2
+METRIC = "span-3 OSEM subset-iters/s"
+UNIT = "subset-iters/s"
+STUDY = dict(total_counts=3e8, randoms_frac=0.25, scatter_frac=0.15, norm_sigma=0.1)
+
+
+def geom_dict():
+    return dict(nrings=104, nelements=256, nangles=288, ring_radius=234.5, plane_sep=1.21875, binsize=1.21875,
+                span=SPAN, maxdel=67, subsets=SUBSETS)
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def init_dist(ws, backend):
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def barrier(dist, device=None):
+    if dist is not None:
+        if device is not None:
+            dist.barrier(device_ids=[device])
+        else:
+            dist.barrier()
+
+
+def max_over_ranks(dist, v, device=None):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{device}" if device is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_model(info):
+    """Per-launch algorithmic bytes and FLOPs of the subset kernels.
+
+    Bins per subset: 9 view pairs x 2 views x segmentsize x nbins.
+    fp_kernel : image read once (nx*ny*nz*4) + prompts (2 B) + additive term
+                (4 B) read + OP ratio (4 B) written per bin; FLOPs = 6 per
+                lerp sample (2 adds, 2 muls, 2 accumulating adds for a sample
+                pair, i.e. 3 per sample) x samples.
+    bp_kernel : ratio read (4 B/bin) + correction image written once
+                (nx*ny*nz*4).
+    rotback_kernel: correction read + image read/write + inverse sensitivity
+                read (4 image volumes).
+    """
+    nb = info.nbins
+    pairs = info.sviews // 2
+    bins = pairs * 2 * info.segmentsize * nb
+    vol = info.nx * info.ny * info.nz * 4
+    # lerp samples: every FOV column of every view contributes one sample to
+    # every plane of its ray's segments
+    samples = pairs * 2 * info.fov_columns * info.segmentsize
+    return {
+        "bins_per_subset": bins,
+        "fp_kernel": {"bytes": vol + bins * 10, "flops": samples * 3},
+        "bp_kernel": {"bytes": bins * 4 + vol, "flops": samples * 3},
+        "rotback_kernel": {"bytes": 4 * vol, "flops": info.fov_columns * info.zp * pairs * 16},
+        "subset_bytes": bins * (6 + 8) + 3 * vol,
+    }
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    dist = init_dist(ws, "nccl")
+    torch.cuda.set_device(local)
+    import hrrt_reconstruction_b200 as H
+    from hrrt_reconstruction_b200 import phantom
+
+    geom = H.hrrt_geometry(**geom_dict())
+    ctx = H.Context(geom, device=local)
+    storage = H.STORE_16 if args.storage == "16" else H.STORE_F32
+    t0 = time.time()
+    st = phantom.study(ctx, seed=1 + rank, **STUDY)
+    gen_s = time.time() - t0
+
+    # ---- end-to-end through the C ABI from host buffers ----
+    e2e_subsets = ITERATIONS * SUBSETS
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    cs = torch.cuda.ExternalStream(ctx.stream)
+    barrier(dist, local)
+    torch.cuda.synchronize()
+    ev[0].record(cs)
+    ctx.upload_inputs(st["prompts"], st["randoms"], st["norm"], st["atten"], st["scatter"], storage=storage)
+    ctx.sensitivity()
+    ctx.init_image()
+    stats = ctx.osem(ITERATIONS)
+    img = ctx.get_image()
+    ev[1].record(cs)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(dist, ev[0].elapsed_time(ev[1]), local)
+    h2d = sum(int(a.nbytes) for a in (st["prompts"], st["randoms"], st["norm"], st["atten"], st["scatter"])
+              if a is not None)
+    d2h = int(img.nbytes)
+    e2e = {"value": ws * e2e_subsets / (e2e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": h2d // e2e_subsets, "d2h_bytes_per_step": d2h // e2e_subsets,
+           "ms_total": e2e_ms, "subset_iterations": e2e_subsets, "sum_image": stats.sum_image}
+
+    # ---- device-resident steps ----
+    ctx.init_image()
+    ctx.osem_subsets(0, args.warmup)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    barrier(dist, local)
+    torch.cuda.synchronize()
+    clocks.start()
+    ctx.reset_kernel_stats()
+    ctx.set_profiling(True)
+    ev[0].record(cs)
+    ctx.osem_subsets(args.warmup, args.steps)
+    ev[1].record(cs)
+    torch.cuda.synchronize()
+    ctx.set_profiling(False)
+    clk = clocks.stop()
+    ms = max_over_ranks(dist, ev[0].elapsed_time(ev[1]), local)
+    barrier(dist, local)
+    kstats = {k: ctx.kernel_stats(k) for k in ("fp_kernel", "bp_kernel", "rotback_kernel")}
+    launches = sum(n for n, _ in kstats.values())
+    model = algorithmic_model(ctx.info)
+    dom = max(kstats, key=lambda k: kstats[k][1])
+    n, tot = kstats[dom]
+    avg_s = tot / max(n, 1) / 1e3
+    peak, peak_kind = measured_peaks()
+    achieved = model[dom]["bytes"] / avg_s / 1e9
+    out = {
+        "metric": METRIC, "value": ws * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if storage == H.STORE_F32 else "f32 compute, 16-bit stored inputs",
+        "data": "synthetic (seeded phantom study, Poisson prompts)",
+        "config": {"workload": "HRRT span 3 (45 segments, 6367 planes x 288 views x 256 bins), image 256x256x207, "
+                               "16 subsets, OP-OSEM (-W 3), 3e8 counts, lognormal norm 0.1, scatter 15%, randoms 25%",
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+                   "l2": "inputs larger than L2 (1.9 GB prompts+additive per frame; 117 MB ratio per subset)",
+                   "storage": args.storage},
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "kernels": {k: {"launches": v[0], "ms_total": v[1], "ms_avg": v[1] / max(v[0], 1)} for k, v in kstats.items()},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
+                     "fallback 6.65 TB/s", "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "bytes_per_launch": model[dom]["bytes"],
+                     "fp32_tflops": model[dom]["flops"] / avg_s / 1e12},
+        "clocks": clk,
+        "data_gen_s": gen_s,
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    del ctx
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def ref_inputs(R, seed=0):
+    """Cheap inputs for timing the reference CPU path: the phantom image and
+    Poisson prompts; the projector's cost does not depend on the values."""
+    rng = np.random.default_rng(seed)
+    shape = (R.P, R.views, R.nx)
+    prompts = rng.poisson(0.64, size=shape).astype(np.int16)
+    add = np.full(shape, 0.1, np.float32)
+    nf = np.ones(R.image_shape, np.float32)
+    img = R.init_image()
+    return img, nf, prompts, add
+
+
+def ref_threads():
+    return max(1, min(16, os.cpu_count() or 1))
+
+
+def cpu_baseline(args, subsets_in_sample=1):
+    from oracle import ref
+    if not ref.available():
+        return {"unavailable": "oracle/_ref/libhrrt_ref.so not built"}
+    T = ref_threads()
+    R = ref.RefProjector(nthreads=T, **geom_dict())
+    img, nf, prompts, add = ref_inputs(R)
+    order = R.order()
+    t0 = time.perf_counter()
+    for k in range(subsets_in_sample):
+        R.osem_subset(img, nf, prompts, add, int(order[k % SUBSETS]), T)
+    dt = time.perf_counter() - t0
+    return {"value": subsets_in_sample / dt, "unit": UNIT, "cores": T, "kind": "reference",
+            "sample": f"{subsets_in_sample} OP-OSEM subset(s) of the span-3 HRRT workload on the reference projector "
+                      f"(oracle/_ref/libhrrt_ref.so, -T {T} thread grouping of CalculateOsem3d)"}
+
+
+def run_reference(args, ws, rank, local):
+    if rank != 0:
+        return
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhrrt_ref.so not built"}))
+        return
+    T = ref_threads()
+    R = ref.RefProjector(nthreads=T, **geom_dict())
+    img, nf, prompts, add = ref_inputs(R)
+    order = R.order()
+    for k in range(args.warmup):
+        R.osem_subset(img, nf, prompts, add, int(order[k % SUBSETS]), T)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        R.osem_subset(img, nf, prompts, add, int(order[(args.warmup + k) % SUBSETS]), T)
+    dt = time.perf_counter() - t0
+    v = args.steps / dt
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": "HRRT span 3 OP-OSEM subset on the reference CPU projector", "threads": T},
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": T, "kind": "reference",
+                            "sample": "one OP-OSEM subset per step (9 view pairs), span-3 HRRT"},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=48)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--storage", default="f32", choices=["f32", "16"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, ws, rank, local)
+    else:
+        run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

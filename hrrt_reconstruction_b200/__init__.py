@@ -1,0 +1,295 @@
+"""hrrt_reconstruction_b200 -- B200 (sm_100a) OSEM hot path of hrrt_osem3d.
+
+Python binding of libhrrt_gpu.so (C ABI in include/hrrt_gpu.h).  It mirrors
+the reference's function-level projector interface
+(hrrt_osem3d/hrrt_osem3d.h:197-216: forward_proj3d_thread1,
+back_proj3d_thread1, rotate_image_buf) and its reconstruction steps
+(PrepareNormfac/PrepareOsem3dFiles, CalculateNormfac, Init_Image,
+CalculateOsem3d, SaveImage in hrrt_osem3d/hrrt_osem3d_span3.cpp).
+
+The library must be built (``python hrrt_reconstruction_b200/build.py`` or
+``__graft_entry__.build()``); importing the package without it raises.  There
+is no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["Geometry", "HrrtError", "Context", "lib", "LIB_PATH", "STORE_F32", "STORE_16", "BP_REF",
+           "geometry_table", "hrrt_geometry"]
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libhrrt_gpu.so")
+STORE_F32 = 0
+STORE_16 = 1
+BP_REF = 0
+
+
+class HrrtError(RuntimeError):
+    pass
+
+
+class Geometry(ctypes.Structure):
+    """hrrt_geom: scanner / sinogram / reconstruction parameters."""
+
+    _fields_ = [("nrings", ctypes.c_int), ("nelements", ctypes.c_int), ("nangles", ctypes.c_int),
+                ("ring_radius", ctypes.c_float), ("plane_sep", ctypes.c_float), ("binsize", ctypes.c_float),
+                ("span", ctypes.c_int), ("maxdel", ctypes.c_int), ("subsets", ctypes.c_int),
+                ("rel_fov", ctypes.c_float), ("z_min", ctypes.c_int), ("z_max", ctypes.c_int),
+                ("npskip", ctypes.c_int), ("epsilon1", ctypes.c_float), ("epsilon2", ctypes.c_float),
+                ("epsilon3", ctypes.c_float), ("image_max", ctypes.c_float)]
+
+
+class Info(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("zp", ctypes.c_int),
+                ("nbins", ctypes.c_int), ("nviews", ctypes.c_int), ("nseg", ctypes.c_int),
+                ("groupmax", ctypes.c_int), ("segmentsize", ctypes.c_int), ("subsets", ctypes.c_int),
+                ("sviews", ctypes.c_int), ("fov_columns", ctypes.c_int), ("sino_elems", ctypes.c_longlong),
+                ("image_elems", ctypes.c_longlong)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("sum_image", ctypes.c_double), ("subset_iterations", ctypes.c_int),
+                ("ms_total", ctypes.c_float)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run hrrt_reconstruction_b200/build.py")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, i, f, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double
+    G = ctypes.POINTER(Geometry)
+    sig = {
+        "hrrt_geom_default": (None, [G]),
+        "hrrt_ctx_create": (i, [G, i, ctypes.POINTER(vp)]),
+        "hrrt_ctx_destroy": (None, [vp]),
+        "hrrt_last_error": (ctypes.c_char_p, [vp]),
+        "hrrt_get_info": (i, [vp, ctypes.POINTER(Info)]),
+        "hrrt_get_stream": (vp, [vp]),
+        "hrrt_upload_inputs": (i, [vp, vp, vp, vp, vp, vp, i]),
+        "hrrt_sensitivity": (i, [vp]),
+        "hrrt_init_image": (i, [vp, vp]),
+        "hrrt_osem": (i, [vp, i, ctypes.POINTER(Stats)]),
+        "hrrt_osem_subsets": (i, [vp, i, i]),
+        "hrrt_get_image": (i, [vp, vp]),
+        "hrrt_get_image_xyz": (i, [vp, vp]),
+        "hrrt_set_image_xyz": (i, [vp, vp]),
+        "hrrt_get_sensitivity": (i, [vp, i, vp]),
+        "hrrt_get_norm_zero_mask": (i, [vp, vp]),
+        "hrrt_set_norm_zero_mask": (i, [vp, vp]),
+        "hrrt_fp_pair": (i, [vp, vp, i, vp]),
+        "hrrt_bp_pair": (i, [vp, vp, i, vp, i]),
+        "hrrt_forward_project": (i, [vp, vp, vp]),
+        "hrrt_rotate_add": (i, [vp, vp, i, vp]),
+        "hrrt_geometry_table": (ctypes.c_longlong, [G, ctypes.c_char_p, vp, ctypes.c_size_t]),
+        "hrrt_set_profiling": (i, [vp, i]),
+        "hrrt_kernel_stats": (i, [vp, ctypes.c_char_p, ctypes.POINTER(i), ctypes.POINTER(d)]),
+        "hrrt_reset_kernel_stats": (i, [vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    return L
+
+
+lib = _load()
+
+
+def hrrt_geometry(span=9, **kw):
+    """HRRT model 999 defaults (scanner_model.cpp:124) with overrides."""
+    g = Geometry()
+    lib.hrrt_geom_default(ctypes.byref(g))
+    g.span = span
+    for k, v in kw.items():
+        setattr(g, k, v)
+    return g
+
+
+_TABLE_DTYPES = {"cylwiny": np.int16, "segments": np.int32, "flookup_zzi": np.int32, "blookup": np.int32,
+                 "order": np.int16}
+
+
+def geometry_table(geom, name):
+    """One geometry table (host-only, no GPU needed) as a numpy array."""
+    n = lib.hrrt_geometry_table(ctypes.byref(geom), name.encode(), None, 0)
+    if n < 0:
+        raise HrrtError(f"geometry table {name!r}: status {n}")
+    dt = _TABLE_DTYPES.get(name, np.float32)
+    out = np.empty(n // np.dtype(dt).itemsize, dt)
+    lib.hrrt_geometry_table(ctypes.byref(geom), name.encode(), out.ctypes.data, n)
+    return out
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def _c(a, dtype):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=dtype)
+    return a
+
+
+class Context:
+    """One reconstruction context on one GPU (hrrt_ctx)."""
+
+    def __init__(self, geom=None, device=0):
+        self.geom = geom if geom is not None else hrrt_geometry()
+        h = ctypes.c_void_p()
+        rc = lib.hrrt_ctx_create(ctypes.byref(self.geom), device, ctypes.byref(h))
+        self._h = h
+        if rc != 0:
+            msg = lib.hrrt_last_error(h).decode() if h.value else "no context"
+            if h.value:
+                lib.hrrt_ctx_destroy(h)
+            self._h = ctypes.c_void_p()
+            raise HrrtError(f"hrrt_ctx_create: {rc}: {msg}")
+        info = Info()
+        lib.hrrt_get_info(self._h, ctypes.byref(info))
+        self.info = info
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.hrrt_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise HrrtError(f"{what}: {rc}: {lib.hrrt_last_error(self._h).decode()}")
+
+    # ---- shapes ----
+    @property
+    def image_shape(self):
+        i = self.info
+        return (i.nx, i.ny, i.zp)
+
+    @property
+    def sino_shape(self):
+        i = self.info
+        return (i.segmentsize, i.nviews, i.nbins)
+
+    @property
+    def rows_shape(self):
+        i = self.info
+        return (2 * i.segmentsize, i.nbins)
+
+    @property
+    def stream(self):
+        return lib.hrrt_get_stream(self._h)
+
+    # ---- reconstruction ----
+    def upload_inputs(self, prompts, randoms, norm=None, atten=None, scatter=None, storage=STORE_F32):
+        p = _c(prompts, np.int16)
+        r = _c(randoms, np.float32)
+        n = _c(norm, np.float32)
+        a = _c(atten, np.float32)
+        s = _c(scatter, np.float32)
+        need = int(np.prod(self.sino_shape))
+        for name, arr in (("prompts", p), ("randoms", r), ("norm", n), ("atten", a), ("scatter", s)):
+            if arr is not None and arr.size != need:
+                raise HrrtError(f"{name}: {arr.size} elements, expected {need}")
+        self._check(lib.hrrt_upload_inputs(self._h, _ptr(p), _ptr(r), _ptr(n), _ptr(a), _ptr(s), storage),
+                    "upload_inputs")
+
+    def sensitivity(self):
+        self._check(lib.hrrt_sensitivity(self._h), "sensitivity")
+
+    def init_image(self, image_zyx=None):
+        im = _c(image_zyx, np.float32)
+        self._check(lib.hrrt_init_image(self._h, _ptr(im)), "init_image")
+
+    def osem(self, iterations):
+        st = Stats()
+        self._check(lib.hrrt_osem(self._h, iterations, ctypes.byref(st)), "osem")
+        return st
+
+    def osem_subsets(self, first, count):
+        self._check(lib.hrrt_osem_subsets(self._h, first, count), "osem_subsets")
+
+    def get_image(self):
+        i = self.info
+        out = np.empty((i.nz, i.ny, i.nx), np.float32)
+        self._check(lib.hrrt_get_image(self._h, _ptr(out)), "get_image")
+        return out
+
+    def get_image_xyz(self):
+        out = np.empty(self.image_shape, np.float32)
+        self._check(lib.hrrt_get_image_xyz(self._h, _ptr(out)), "get_image_xyz")
+        return out
+
+    def set_image_xyz(self, img):
+        a = _c(img, np.float32)
+        assert a.shape == self.image_shape
+        self._check(lib.hrrt_set_image_xyz(self._h, _ptr(a)), "set_image_xyz")
+
+    def get_sensitivity(self, subset):
+        out = np.empty(self.image_shape, np.float32)
+        self._check(lib.hrrt_get_sensitivity(self._h, subset, _ptr(out)), "get_sensitivity")
+        return out
+
+    def norm_zero_mask(self):
+        i = self.info
+        out = np.empty((i.nviews // 2, i.nbins // 2 + 1), np.int16)
+        self._check(lib.hrrt_get_norm_zero_mask(self._h, _ptr(out)), "get_norm_zero_mask")
+        return out
+
+    def set_norm_zero_mask(self, mask):
+        m = _c(mask, np.int16)
+        self._check(lib.hrrt_set_norm_zero_mask(self._h, _ptr(m)), "set_norm_zero_mask")
+
+    # ---- projector entry points (reference function-level interface) ----
+    def fp_pair(self, image_xyz, view, prj=None):
+        img = _c(image_xyz, np.float32)
+        assert img.shape == self.image_shape
+        out = np.zeros(self.rows_shape, np.float32) if prj is None else _c(prj, np.float32).copy()
+        self._check(lib.hrrt_fp_pair(self._h, _ptr(img), view, _ptr(out)), "fp_pair")
+        return out
+
+    def forward_project(self, image_xyz):
+        """Full flat-file sinogram [segmentsize][nviews][nbins] of image_xyz."""
+        img = _c(image_xyz, np.float32)
+        assert img.shape == self.image_shape
+        out = np.empty(self.sino_shape, np.float32)
+        self._check(lib.hrrt_forward_project(self._h, _ptr(img), _ptr(out)), "forward_project")
+        return out
+
+    def bp_pair(self, prj, view, mode=BP_REF):
+        p = _c(prj, np.float32)
+        assert p.shape == self.rows_shape
+        out = np.zeros(self.image_shape, np.float32)
+        self._check(lib.hrrt_bp_pair(self._h, _ptr(p), view, _ptr(out), mode), "bp_pair")
+        return out
+
+    def rotate_add(self, imagebuf, view, corr):
+        ib = _c(imagebuf, np.float32)
+        co = _c(corr, np.float32).copy()
+        self._check(lib.hrrt_rotate_add(self._h, _ptr(ib), view, _ptr(co)), "rotate_add")
+        return co
+
+    # ---- timing ----
+    def set_profiling(self, on):
+        self._check(lib.hrrt_set_profiling(self._h, 1 if on else 0), "set_profiling")
+
+    def kernel_stats(self, name):
+        n = ctypes.c_int()
+        ms = ctypes.c_double()
+        self._check(lib.hrrt_kernel_stats(self._h, name.encode(), ctypes.byref(n), ctypes.byref(ms)),
+                    "kernel_stats")
+        return n.value, ms.value
+
+    def reset_kernel_stats(self):
+        self._check(lib.hrrt_reset_kernel_stats(self._h), "reset_kernel_stats")

@@ -1,0 +1,81 @@
+"""Builds libhrrt_gpu.so in-tree (sm_100a) with nvcc.
+
+The CUDA sources are compiled with -fmad=false: the reference projector is an
+x86-64 SSE2 build that never fuses multiply and add, and the kernels keep its
+expression order, so their results are bit-identical where the algorithm is.
+Host code (geometry tables) is compiled with -ffp-contract=off for the same
+reason.
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libhrrt_gpu.so")
+CLI = os.path.join(HERE, "hrrt_osem3d_gpu")
+
+SOURCES = ["kernels.cu", "hrrt_gpu.cu", "geometry.cpp"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc():
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(cand):
+        raise RuntimeError("nvcc not found")
+    return cand
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(d) <= t for d in deps)
+
+
+def build_library(force=False, verbose=False):
+    deps = [os.path.join(CSRC, s) for s in SOURCES]
+    deps += [os.path.join(CSRC, h) for h in ("kernels.cuh", "geometry.h")]
+    deps += [os.path.join(ROOT, "include", "hrrt_gpu.h"), __file__]
+    if not force and _newer(LIB, deps):
+        return LIB
+    cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-fmad=false", "--shared",
+           "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-I" + os.path.join(ROOT, "include"),
+           "-o", LIB + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lcudart"]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+    if verbose:
+        sys.stderr.write(r.stderr)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+def build_cli(force=False):
+    src = os.path.join(CSRC, "cli", "hrrt_osem3d_gpu.cpp")
+    if not os.path.exists(src):
+        return None
+    deps = [src, LIB]
+    if not force and _newer(CLI, deps):
+        return CLI
+    cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include"), src,
+           "-o", CLI + ".tmp", "-L" + HERE, "-lhrrt_gpu", "-Wl,-rpath,$ORIGIN", "-lpthread"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("g++ failed:\n" + r.stdout + r.stderr)
+    os.replace(CLI + ".tmp", CLI)
+    return CLI
+
+
+def build_all(force=False, verbose=False):
+    build_library(force=force, verbose=verbose)
+    build_cli(force=force)
+
+
+if __name__ == "__main__":
+    build_all(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(LIB)

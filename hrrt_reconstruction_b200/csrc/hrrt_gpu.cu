@@ -1,0 +1,940 @@
+// hrrt_gpu.cu -- the C ABI of libhrrt_gpu.so (declared in include/hrrt_gpu.h).
+//
+// A context owns the geometry tables, the device copies of the prepared
+// inputs (quad layout, every view pair), the image, the per-subset inverse
+// sensitivity images and the per-subset scratch (OP ratio and the two
+// back-projection partials of each view pair of a subset).  One OSEM subset
+// is three launches on the context stream:
+//   fp_kernel (forward projection + ratio) -> bp_kernel -> rotback_kernel
+//   (rotate-back of the nine view pairs fused with the multiplicative update).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/hrrt_gpu.h"
+#include "geometry.h"
+#include "kernels.cuh"
+
+using namespace hrrt;
+
+struct KernelTimer {
+  std::string name;
+  cudaEvent_t start, stop;
+};
+
+struct hrrt_ctx {
+  Geometry geo;
+  DevGeom dg{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::vector<void *> allocs;
+
+  int storage = -1;
+  void *q_prompts = nullptr, *q_add = nullptr, *q_mult = nullptr;
+  int16_t *d_nzmask = nullptr;
+  int *d_mask_accum = nullptr;
+  std::vector<int16_t> nzmask;
+
+  float *d_image = nullptr;
+  float *d_nfinv = nullptr;
+  float *d_ratio = nullptr, *d_bc = nullptr, *d_br = nullptr;
+  float *d_tmp_img = nullptr;  // test entry points
+  float *d_rows = nullptr;
+  double *d_partial = nullptr, *d_sum = nullptr;
+  int *d_pair_views = nullptr;  // [subsets][npairs]
+  QuadWork *d_work = nullptr;   // fp lists then bp lists, per subset
+  std::vector<int> fp_off, fp_cnt, bp_off, bp_cnt;
+  int *d_rowstart = nullptr;
+  int npairs = 0;               // view pairs per subset
+  long long vol = 0;            // nx*ny*zp
+  long long quad_pair = 0;      // floats per pair in quad layout
+  int tpt = 1;
+  bool have_inputs = false, have_sens = false, have_image = false;
+
+  bool prof = false;
+  std::vector<KernelTimer> pending;
+  std::map<std::string, std::pair<int, double>> kstats;
+
+  ~hrrt_ctx() {
+    for (auto &t : pending) {
+      cudaEventDestroy(t.start);
+      cudaEventDestroy(t.stop);
+    }
+    for (void *p : allocs) cudaFree(p);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+int fail(hrrt_ctx *ctx, int code, const std::string &msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+int cuda_fail(hrrt_ctx *ctx, cudaError_t e, const char *where) {
+  return fail(ctx, HRRT_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define CK(call, where)                                   \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
+  } while (0)
+
+template <typename T>
+T *dalloc(hrrt_ctx *ctx, size_t n, cudaError_t *e) {
+  void *p = nullptr;
+  *e = cudaMalloc(&p, n * sizeof(T) + 16);
+  if (*e != cudaSuccess) return nullptr;
+  *e = cudaMemsetAsync(p, 0, n * sizeof(T) + 16, ctx->stream);
+  ctx->allocs.push_back(p);
+  return (T *)p;
+}
+template <typename T>
+T *dupload(hrrt_ctx *ctx, const std::vector<T> &v, cudaError_t *e) {
+  T *p = dalloc<T>(ctx, std::max<size_t>(v.size(), 1), e);
+  if (!p) return nullptr;
+  if (!v.empty()) *e = cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
+  return p;
+}
+
+struct Launch {
+  hrrt_ctx *ctx;
+  KernelTimer t{};
+  Launch(hrrt_ctx *c, const char *name) : ctx(c) {
+    if (ctx->prof) {
+      t.name = name;
+      cudaEventCreate(&t.start);
+      cudaEventCreate(&t.stop);
+      cudaEventRecord(t.start, ctx->stream);
+    }
+  }
+  ~Launch() {
+    if (ctx->prof) {
+      cudaEventRecord(t.stop, ctx->stream);
+      ctx->pending.push_back(t);
+    }
+  }
+};
+
+void drain_timers(hrrt_ctx *ctx) {
+  for (auto &t : ctx->pending) {
+    cudaEventSynchronize(t.stop);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t.start, t.stop);
+    auto &s = ctx->kstats[t.name];
+    s.first += 1;
+    s.second += ms;
+    cudaEventDestroy(t.start);
+    cudaEventDestroy(t.stop);
+  }
+  ctx->pending.clear();
+}
+
+// Forward-projection tasks shared by every quad: (segment, plane run, kind).
+std::vector<FpTask> build_fp_tasks(const Geometry &g) {
+  std::vector<FpTask> mid, ends;
+  for (int p0 = 0; p0 < g.nz; p0 += kFpPlanes)
+    mid.push_back(FpTask{0, (int16_t)p0, (int16_t)std::min(kFpPlanes, g.nz - p0), 0});
+  for (int s = 1; s < g.nseg; s++) {
+    const int ns = g.yr_top[s] - g.yr_bottom[s] + 1;
+    for (int p0 = g.zshift; p0 < ns - g.zshift; p0 += kFpPlanes)
+      mid.push_back(FpTask{(int16_t)s, (int16_t)p0, (int16_t)std::min(kFpPlanes, ns - g.zshift - p0), 1});
+    for (int p0 = 0; p0 < g.zshift; p0 += kFpEndPlanes)
+      ends.push_back(FpTask{(int16_t)s, (int16_t)p0, (int16_t)std::min(kFpEndPlanes, g.zshift - p0), 2});
+    for (int p0 = ns - g.zshift; p0 < ns; p0 += kFpEndPlanes)
+      ends.push_back(FpTask{(int16_t)s, (int16_t)p0, (int16_t)std::min(kFpEndPlanes, ns - p0), 2});
+  }
+  mid.insert(mid.end(), ends.begin(), ends.end());
+  return mid;
+}
+
+// Every shared-memory index the forward projector can form for this geometry
+// must lie inside the staged column; checked once here so the kernel needs no
+// run-time guards.
+std::string validate_fp(const Geometry &g, const std::vector<FpMid> &mid, const std::vector<FpTask> &tasks) {
+  const int ZS = g.zp + kFpZPad, FS = g.flookup_stride();
+  int ymin = g.c;
+  for (int x = 1; x <= g.c; x++)
+    if (g.cyl0[x] != g.cyl1[x]) ymin = std::min<int>(ymin, g.cyl0[x]);
+  for (int y = ymin; y < g.c; y++) {
+    for (const FpTask &t : tasks) {
+      if (t.type == 0) {
+        if (t.p0 + kFpPlanes >= ZS) return "fp: segment-0 window out of range";
+        continue;
+      }
+      const int gg = (t.seg + 1) / 2 - 1;
+      const FpMid m = mid[(size_t)y * g.groupmax + gg];
+      if (m.z < 0) continue;
+      if (t.type == 1) {
+        const int za = m.z + t.p0 - g.zshift, zb = m.z2 + t.p0 - g.zshift;
+        if (za < 0 || zb < 0 || za + kFpPlanes >= ZS || zb + kFpPlanes >= ZS) return "fp: middle window out of range";
+      } else {
+        const int ns = g.yr_top[t.seg] - g.yr_bottom[t.seg] + 1;
+        for (int j = 0; j < t.n; j++) {
+          const int r = t.p0 + j;
+          const int yri = (r < g.zshift) ? r : r - ns + 2 * g.zshift;
+          const int li = gg * 2 * g.zshift + yri;
+          const int z = g.fl_zzi[(size_t)y * FS + li], z2 = g.fl_zzi[(size_t)(g.ny - y) * FS + li];
+          if (z < 0 || z2 < 0 || z + 1 >= ZS || z2 + 1 >= ZS) return "fp: end-plane index out of range";
+        }
+      }
+    }
+  }
+  return std::string();
+}
+
+// reads (and clears) the device status word after the stream has drained
+int device_status(hrrt_ctx *ctx) {
+  int v = 0;
+  cudaError_t e = cudaMemcpyAsync(&v, ctx->dg.err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "status");
+  if (v != 0) {
+    cudaMemsetAsync(ctx->dg.err, 0, sizeof(int), ctx->stream);
+    return fail(ctx, HRRT_ERR_DEVICE, "a device-side bounded wait timed out");
+  }
+  return HRRT_OK;
+}
+
+int build_work_lists(hrrt_ctx *ctx) {
+  const Geometry &g = ctx->geo;
+  const int S = g.sp.subsets;
+  std::vector<QuadWork> all;
+  std::vector<int> views;
+  ctx->fp_off.assign(S, 0);
+  ctx->fp_cnt.assign(S, 0);
+  ctx->bp_off.assign(S, 0);
+  ctx->bp_cnt.assign(S, 0);
+  // quads ordered by decreasing rotated-column length (longest work first)
+  std::vector<int> xs;
+  for (int x = 1; x <= g.c; x++)
+    if (g.cyl0[x] != g.cyl1[x]) xs.push_back(x);
+  std::stable_sort(xs.begin(), xs.end(), [&](int a, int b) { return g.cyl0[a] < g.cyl0[b]; });
+  const int nq = g.nx / 2 + 1;
+  for (int s = 0; s < S; s++) {
+    for (int k = 0; k < ctx->npairs; k++) views.push_back(g.vieworder[(size_t)s * g.sviews + k]);
+    for (int pass = 0; pass < 2; pass++) {
+      const int off = (int)all.size();
+      for (int x : xs)
+        for (int k = 0; k < ctx->npairs; k++) {
+          const int v = g.vieworder[(size_t)s * g.sviews + k];
+          if (pass == 0 && ctx->nzmask[(size_t)v * nq + x] == 0) continue;
+          all.push_back(QuadWork{(int16_t)k, (int16_t)x, (int16_t)v, 0});
+        }
+      if (pass == 0) {
+        ctx->fp_off[s] = off;
+        ctx->fp_cnt[s] = (int)all.size() - off;
+      } else {
+        ctx->bp_off[s] = off;
+        ctx->bp_cnt[s] = (int)all.size() - off;
+      }
+    }
+  }
+  cudaError_t e = cudaSuccess;
+  if (ctx->d_work) {
+    cudaFree(ctx->d_work);
+    ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)ctx->d_work));
+  }
+  ctx->d_work = dupload(ctx, all, &e);
+  if (!ctx->d_work) return cuda_fail(ctx, e, "work list");
+  if (!ctx->d_pair_views) {
+    ctx->d_pair_views = dupload(ctx, views, &e);
+    if (!ctx->d_pair_views) return cuda_fail(ctx, e, "pair views");
+  }
+  CK(e, "work list upload");
+  return HRRT_OK;
+}
+
+int run_subset(hrrt_ctx *ctx, int s) {
+  const DevGeom &g = ctx->dg;
+  const size_t in_stride = (size_t)ctx->quad_pair;
+  {
+    Launch L(ctx, "fp_kernel");
+    CK(launch_fp(g, ctx->d_image, ctx->d_work + ctx->fp_off[s], ctx->fp_cnt[s], 1, ctx->q_prompts, ctx->q_add,
+                 ctx->storage, ctx->d_ratio, ctx->quad_pair, ctx->tpt, ctx->stream),
+       "fp_kernel");
+  }
+  {
+    Launch L(ctx, "bp_kernel");
+    CK(launch_bp(g, ctx->d_ratio, in_stride, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s], ctx->d_bc, ctx->d_br,
+                 ctx->vol, ctx->stream),
+       "bp_kernel");
+  }
+  {
+    Launch L(ctx, "rotback_kernel");
+    CK(launch_rotback(g, ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_bc, ctx->d_br, ctx->vol,
+                      ctx->d_image, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 0, ctx->stream),
+       "rotback_kernel");
+  }
+  return HRRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void hrrt_geom_default(hrrt_geom *g) {
+  ScannerParams p;
+  g->nrings = p.nrings;
+  g->nelements = p.nelements;
+  g->nangles = p.nangles;
+  g->ring_radius = p.ring_radius;
+  g->plane_sep = p.plane_sep;
+  g->binsize = p.binsize;
+  g->span = p.span;
+  g->maxdel = p.maxdel;
+  g->subsets = p.subsets;
+  g->rel_fov = p.rel_fov;
+  g->z_min = p.z_min;
+  g->z_max = p.z_max;
+  g->npskip = p.npskip;
+  g->epsilon1 = p.epsilon1;
+  g->epsilon2 = p.epsilon2;
+  g->epsilon3 = p.epsilon3;
+  g->image_max = p.image_max;
+}
+
+const char *hrrt_last_error(const hrrt_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void *hrrt_get_stream(hrrt_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
+  if (!gp || !out) return HRRT_ERR_ARG;
+  *out = nullptr;
+  hrrt_ctx *ctx = new hrrt_ctx();
+  auto bail = [&](int code) {
+    // keep the context so the caller can read the message; destroy on request
+    *out = ctx;
+    return code;
+  };
+  ScannerParams p;
+  p.nrings = gp->nrings;
+  p.nelements = gp->nelements;
+  p.nangles = gp->nangles;
+  p.ring_radius = gp->ring_radius;
+  p.plane_sep = gp->plane_sep;
+  p.binsize = gp->binsize;
+  p.span = gp->span;
+  p.maxdel = gp->maxdel;
+  p.subsets = gp->subsets;
+  p.rel_fov = gp->rel_fov;
+  p.z_min = gp->z_min;
+  p.z_max = gp->z_max;
+  p.npskip = gp->npskip;
+  p.epsilon1 = gp->epsilon1;
+  p.epsilon2 = gp->epsilon2;
+  p.epsilon3 = gp->epsilon3;
+  p.image_max = gp->image_max;
+  // z range adjustments of GetScannerParameter (drv:3537-3540)
+  if (p.npskip > p.z_min) p.z_min = p.npskip;
+  if (p.z_max > (2 * p.nrings - 1) - p.npskip) p.z_max = (2 * p.nrings - 1) - p.npskip;
+  std::string m = ctx->geo.build(p);
+  if (!m.empty()) return bail(fail(ctx, HRRT_ERR_ARG, "geometry: " + m));
+  Geometry &g = ctx->geo;
+  if (g.nx > 32767 || g.segmentsize > 32767) return bail(fail(ctx, HRRT_ERR_ARG, "geometry too large"));
+  ctx->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "cudaSetDevice"));
+  e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "stream"));
+
+  ctx->npairs = g.sviews / 2;
+  ctx->vol = (long long)g.nx * g.ny * g.zp;
+  const int nq = g.nx / 2 + 1;
+  ctx->quad_pair = (long long)nq * g.padded_planes() * 4;
+
+  // derived device tables
+  std::vector<int> poff(g.nseg);
+  for (int s = 0; s < g.nseg; s++) poff[s] = g.padded_offset(s);
+  std::vector<FpMid> mid((size_t)g.c * g.groupmax);
+  const int FS = g.flookup_stride();
+  for (int y = 0; y < g.c; y++)
+    for (int th = 2, gg = 0; th < g.nseg; th += 2, gg++) {
+      const int yr = g.yr_bottom[th] + g.zshift;
+      const float t = g.tantheta[(size_t)gg * g.nz + yr];
+      float zz = yr + (y - g.c) * t;
+      const int z = (int)zz;
+      const float f = zz - z;
+      zz = yr + (g.c - y) * t;
+      const int z2 = (int)zz;
+      const float f2 = zz - z2;
+      // row 0 is never in the FOV (its mirror row ny is outside the tables)
+      const bool skip = y == 0 || g.fl_zzi[(size_t)y * FS + gg * g.zshift * 2] < 0 ||
+                        g.fl_zzi[(size_t)(g.ny - y) * FS + gg * g.zshift * 2 + g.zshift * 2 - 1] > g.nz - 1;
+      mid[(size_t)y * g.groupmax + gg] = FpMid{skip ? -1 : z, f, z2, f2};
+    }
+  // back-projection lookup, transposed to [group][row]
+  std::vector<BpLut> bpl((size_t)g.ny * g.groupmax);
+  for (int y = 0; y < g.ny; y++)
+    for (int gg = 0; gg < g.groupmax; gg++) {
+      const size_t i = (size_t)y * g.groupmax + gg;
+      bpl[(size_t)gg * g.ny + y] = BpLut{g.bl_zsa[i], g.bl_zea[i], g.bl_yra[i] - g.bl_zsa[i], g.bl_yr2a[i]};
+    }
+  std::vector<short2> fovxy;
+  std::vector<int> rowstart(g.nx + 1, 0);
+  for (int X = 0; X < g.nx; X++) {
+    rowstart[X] = (int)fovxy.size();
+    for (int Y = g.cyl0[X]; Y < g.cyl1[X]; Y++) fovxy.push_back(make_short2((short)X, (short)Y));
+  }
+  rowstart[g.nx] = (int)fovxy.size();
+  std::vector<int16_t> plane_seg(g.segmentsize);
+  for (int s = 0; s < g.nseg; s++)
+    for (int r = 0; r <= g.yr_top[s] - g.yr_bottom[s]; r++) plane_seg[g.segment_offset[s] + r] = (int16_t)s;
+  std::vector<FpTask> tasks = build_fp_tasks(g);
+  m = validate_fp(g, mid, tasks);
+  if (!m.empty()) return bail(fail(ctx, HRRT_ERR_ARG, m));
+  // one task per thread; a quad with more tasks than a CTA's launch bound is
+  // split over several CTAs (each samples the quad's rows itself)
+  ctx->tpt = 1;
+  if (tasks.size() > 8 * 448) return bail(fail(ctx, HRRT_ERR_ARG, "geometry has too many projection tasks"));
+  if (g.zp % kBpZ != 0) return bail(fail(ctx, HRRT_ERR_ARG, "padded z must be a multiple of 8"));
+  for (int x = 1; x <= g.c; x++)
+    if (g.cyl0[x] != g.cyl1[x] && g.cyl0[x] < 1) return bail(fail(ctx, HRRT_ERR_ARG, "FOV reaches the grid edge"));
+  if ((size_t)g.padded_planes() * 16 > 200 * 1024)
+    return bail(fail(ctx, HRRT_ERR_ARG, "sinogram quad exceeds shared memory"));
+
+  DevGeom &d = ctx->dg;
+  d.nx = g.nx;
+  d.nz = g.nz;
+  d.zp = g.zp;
+  d.c = g.c;
+  d.nseg = g.nseg;
+  d.groupmax = g.groupmax;
+  d.zshift = g.zshift;
+  d.segmentsize = g.segmentsize;
+  d.pplanes = g.padded_planes();
+  d.nviews = g.nviews;
+  d.nquads = nq;
+  d.fov_columns = (int)fovxy.size();
+  d.z_min = g.sp.z_min;
+  d.z_max = g.sp.z_max;
+  d.y_size = g.y_size;
+  d.eps1 = g.sp.epsilon1;
+  d.eps3 = g.sp.epsilon3;
+  d.image_max = g.sp.image_max;
+  d.cyl0 = dupload(ctx, g.cyl0, &e);
+  d.cyl1 = dupload(ctx, g.cyl1, &e);
+  d.ybot = dupload(ctx, g.yr_bottom, &e);
+  d.ytop = dupload(ctx, g.yr_top, &e);
+  d.poff = dupload(ctx, poff, &e);
+  d.rescale = dupload(ctx, g.rescale, &e);
+  d.bp_scale = dupload(ctx, g.bp_scale, &e);
+  d.fpmid = dupload(ctx, mid, &e);
+  d.fl_zzi = dupload(ctx, g.fl_zzi, &e);
+  d.fl_zzz0 = dupload(ctx, g.fl_zzz0, &e);
+  d.bplut = dupload(ctx, bpl, &e);
+  d.sin_psi = dupload(ctx, g.sin_psi, &e);
+  d.cos_psi = dupload(ctx, g.cos_psi, &e);
+  d.fov_xy = dupload(ctx, fovxy, &e);
+  d.fptasks = dupload(ctx, tasks, &e);
+  d.nfptasks = (int)tasks.size();
+  d.plane_seg = dupload(ctx, plane_seg, &e);
+  std::vector<int16_t> pplane_seg(g.padded_planes(), -1);
+  for (int s = 0; s < g.nseg; s++)
+    for (int r = 0; r <= g.yr_top[s] - g.yr_bottom[s]; r++) pplane_seg[g.padded_offset(s) + r] = (int16_t)s;
+  d.pplane_seg = dupload(ctx, pplane_seg, &e);
+  ctx->d_rowstart = dupload(ctx, rowstart, &e);
+  d.err = dalloc<int>(ctx, 1, &e);
+  ctx->nzmask = g.norm_zero_mask;
+  ctx->d_nzmask = dupload(ctx, ctx->nzmask, &e);
+  d.nzmask = ctx->d_nzmask;
+  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "table upload"));
+  float2 *rp = dalloc<float2>(ctx, (size_t)(g.nviews / 2) * d.fov_columns, &e);
+  if (!rp) return bail(cuda_fail(ctx, e, "rotpos"));
+  d.rotpos = rp;
+  e = launch_rotpos(d, rp, ctx->d_rowstart, ctx->stream);
+  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "rotpos kernel"));
+
+  // image, sensitivity, scratch
+  ctx->d_image = dalloc<float>(ctx, ctx->vol, &e);
+  ctx->d_nfinv = ctx->d_image ? dalloc<float>(ctx, (size_t)g.sp.subsets * ctx->vol, &e) : nullptr;
+  ctx->d_ratio = ctx->d_nfinv ? dalloc<float>(ctx, (size_t)ctx->npairs * ctx->quad_pair, &e) : nullptr;
+  ctx->d_bc = ctx->d_ratio ? dalloc<float>(ctx, (size_t)ctx->npairs * ctx->vol, &e) : nullptr;
+  ctx->d_br = ctx->d_bc ? dalloc<float>(ctx, (size_t)ctx->npairs * ctx->vol, &e) : nullptr;
+  const int pb = post_iteration_blocks(d);
+  ctx->d_partial = ctx->d_br ? dalloc<double>(ctx, pb, &e) : nullptr;
+  ctx->d_sum = ctx->d_partial ? dalloc<double>(ctx, 1, &e) : nullptr;
+  if (!ctx->d_sum) return bail(fail(ctx, HRRT_ERR_NOMEM, std::string("device allocation: ") + cudaGetErrorString(e)));
+  int rc = build_work_lists(ctx);
+  if (rc) return bail(rc);
+  e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "create"));
+  *out = ctx;
+  return HRRT_OK;
+}
+
+void hrrt_ctx_destroy(hrrt_ctx *ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  delete ctx;
+}
+
+int hrrt_get_info(const hrrt_ctx *ctx, hrrt_info *info) {
+  if (!ctx || !info) return HRRT_ERR_ARG;
+  const Geometry &g = ctx->geo;
+  info->nx = g.nx;
+  info->ny = g.ny;
+  info->nz = g.nz;
+  info->zp = g.zp;
+  info->nbins = g.nbins;
+  info->nviews = g.nviews;
+  info->nseg = g.nseg;
+  info->groupmax = g.groupmax;
+  info->segmentsize = g.segmentsize;
+  info->subsets = g.sp.subsets;
+  info->sviews = g.sviews;
+  info->fov_columns = g.fov_columns;
+  info->sino_elems = (long long)g.segmentsize * g.nviews * g.nbins;
+  info->image_elems = (long long)g.nx * g.ny * g.zp;
+  return HRRT_OK;
+}
+
+int hrrt_upload_inputs(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms, const float *norm,
+                       const float *atten, const float *scatter, int storage) {
+  if (!ctx) return HRRT_ERR_ARG;
+  if (!prompts || !randoms) return fail(ctx, HRRT_ERR_ARG, "prompts and randoms are required");
+  if (storage != HRRT_STORE_F32 && storage != HRRT_STORE_16) return fail(ctx, HRRT_ERR_ARG, "unknown storage");
+  const Geometry &g = ctx->geo;
+  const size_t n = (size_t)g.segmentsize * g.nviews * g.nbins;
+  cudaError_t e = cudaSuccess;
+  // quad-layout inputs for every view pair (allocated once per storage type)
+  if (ctx->storage != storage) {
+    for (void *p : {ctx->q_prompts, ctx->q_add, ctx->q_mult})
+      if (p) {
+        cudaFree(p);
+        ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), p));
+      }
+    const size_t nquad = (size_t)(g.nviews / 2) * ctx->quad_pair;
+    const size_t ab = storage == HRRT_STORE_F32 ? 4 : 2;
+    ctx->q_prompts = dalloc<char>(ctx, nquad * 2, &e);
+    ctx->q_add = ctx->q_prompts ? dalloc<char>(ctx, nquad * ab, &e) : nullptr;
+    ctx->q_mult = ctx->q_add ? dalloc<char>(ctx, nquad * ab, &e) : nullptr;
+    if (!ctx->q_mult) return fail(ctx, HRRT_ERR_NOMEM, "input allocation");
+    ctx->storage = storage;
+  }
+  if (!ctx->d_mask_accum) {
+    ctx->d_mask_accum = dalloc<int>(ctx, (size_t)(g.nviews / 2) * ctx->dg.nquads, &e);
+    if (!ctx->d_mask_accum) return fail(ctx, HRRT_ERR_NOMEM, "mask");
+  }
+  // staging of the raw flat-file arrays
+  const float *srcs[4] = {randoms, norm, atten, scatter};
+  float *stage[4] = {nullptr, nullptr, nullptr, nullptr};
+  int16_t *sp = nullptr;
+  std::vector<void *> tmp;
+  auto cleanup = [&]() {
+    cudaStreamSynchronize(ctx->stream);
+    for (void *p : tmp) cudaFree(p);
+  };
+  e = cudaMalloc(&sp, n * sizeof(int16_t));
+  if (e != cudaSuccess) return fail(ctx, HRRT_ERR_NOMEM, "staging");
+  tmp.push_back(sp);
+  for (int i = 0; i < 4; i++) {
+    if (!srcs[i]) continue;
+    e = cudaMalloc(&stage[i], n * sizeof(float));
+    if (e != cudaSuccess) {
+      cleanup();
+      return fail(ctx, HRRT_ERR_NOMEM, "staging");
+    }
+    tmp.push_back(stage[i]);
+  }
+  e = cudaMemcpyAsync(sp, prompts, n * sizeof(int16_t), cudaMemcpyHostToDevice, ctx->stream);
+  for (int i = 0; i < 4 && e == cudaSuccess; i++)
+    if (srcs[i]) e = cudaMemcpyAsync(stage[i], srcs[i], n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(ctx->d_mask_accum, 0, sizeof(int) * (size_t)(g.nviews / 2) * ctx->dg.nquads, ctx->stream);
+  if (e == cudaSuccess) {
+    Launch L(ctx, "prep_kernel");
+    e = launch_prep(ctx->dg, g.nbins, sp, stage[0], stage[1], stage[2], stage[3], g.sp.npskip, g.sp.epsilon2,
+                    storage, ctx->q_prompts, ctx->q_add, ctx->q_mult, ctx->d_mask_accum, ctx->stream);
+  }
+  if (e == cudaSuccess) e = launch_finish_mask(ctx->dg, ctx->d_mask_accum, ctx->d_nzmask, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->nzmask.data(), ctx->d_nzmask, ctx->nzmask.size() * sizeof(int16_t),
+                        cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cleanup();
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "upload_inputs");
+  int rc = build_work_lists(ctx);
+  if (rc) return rc;
+  ctx->have_inputs = true;
+  ctx->have_sens = false;
+  return HRRT_OK;
+}
+
+int hrrt_sensitivity(hrrt_ctx *ctx) {
+  if (!ctx) return HRRT_ERR_ARG;
+  if (!ctx->have_inputs) return fail(ctx, HRRT_ERR_STATE, "hrrt_upload_inputs must come first");
+  const Geometry &g = ctx->geo;
+  for (int s = 0; s < g.sp.subsets; s++) {
+    {
+      Launch L(ctx, "scale_pairs_kernel");
+      CK(launch_scale_pairs(ctx->dg, ctx->q_mult, ctx->storage, ctx->d_pair_views + (size_t)s * ctx->npairs,
+                            ctx->npairs, ctx->d_ratio, ctx->quad_pair, ctx->stream),
+         "scale_pairs");
+    }
+    {
+      Launch L(ctx, "bp_kernel");
+      CK(launch_bp(ctx->dg, ctx->d_ratio, ctx->quad_pair, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s], ctx->d_bc,
+                   ctx->d_br, ctx->vol, ctx->stream),
+         "bp_kernel");
+    }
+    {
+      Launch L(ctx, "rotback_kernel");
+      CK(launch_rotback(ctx->dg, ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_bc, ctx->d_br,
+                        ctx->vol, nullptr, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 1, ctx->stream),
+         "rotback_kernel");
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream), "sensitivity");
+  ctx->have_sens = true;
+  return HRRT_OK;
+}
+
+int hrrt_init_image(hrrt_ctx *ctx, const float *image_zyx) {
+  if (!ctx) return HRRT_ERR_ARG;
+  const Geometry &g = ctx->geo;
+  if (!image_zyx) {
+    CK(launch_init_image(ctx->dg, ctx->d_image, ctx->stream), "init_image");
+  } else {
+    // Init_Image with -i (drv:3970-3995): image[y][x][z] = file[z][y][x]
+    // restricted to FOV columns; the [z][y][x] file is read as tmp[x][y]
+    std::vector<float> h((size_t)ctx->vol, 0.f);
+    for (int z = 0; z < g.nz; z++)
+      for (int x = 0; x < g.nx; x++)
+        for (int y = g.cyl0[x]; y < g.cyl1[x]; y++)
+          h[((size_t)y * g.ny + x) * g.zp + z] = image_zyx[((size_t)z * g.nx + x) * g.ny + y];
+    CK(cudaMemcpyAsync(ctx->d_image, h.data(), h.size() * 4, cudaMemcpyHostToDevice, ctx->stream), "init_image");
+  }
+  CK(cudaStreamSynchronize(ctx->stream), "init_image");
+  ctx->have_image = true;
+  return HRRT_OK;
+}
+
+int hrrt_osem_subsets(hrrt_ctx *ctx, int first, int count) {
+  if (!ctx || count < 0) return HRRT_ERR_ARG;
+  if (!ctx->have_inputs || !ctx->have_sens || !ctx->have_image)
+    return fail(ctx, HRRT_ERR_STATE, "inputs, sensitivity and image must be set first");
+  const int S = ctx->geo.sp.subsets;
+  for (int i = 0; i < count; i++) {
+    const int s = ctx->geo.order[(size_t)(((first + i) % S) + S) % S];
+    int rc = run_subset(ctx, s);
+    if (rc) return rc;
+  }
+  return HRRT_OK;
+}
+
+int hrrt_osem(hrrt_ctx *ctx, int iterations, hrrt_stats *stats) {
+  if (!ctx || iterations < 0) return HRRT_ERR_ARG;
+  if (!ctx->have_inputs || !ctx->have_sens || !ctx->have_image)
+    return fail(ctx, HRRT_ERR_STATE, "inputs, sensitivity and image must be set first");
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a), "event");
+  CK(cudaEventCreate(&b), "event");
+  cudaEventRecord(a, ctx->stream);
+  double sum = 0.0;
+  int done = 0;
+  for (int it = 0; it < iterations; it++) {
+    for (int i = 0; i < ctx->geo.sp.subsets; i++) {
+      int rc = run_subset(ctx, ctx->geo.order[i]);
+      if (rc) {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        return rc;
+      }
+      done++;
+    }
+    {
+      Launch L(ctx, "post_iter_kernel");
+      CK(launch_post_iteration(ctx->dg, ctx->d_image, ctx->d_partial, ctx->d_sum, ctx->stream), "post_iteration");
+    }
+  }
+  cudaEventRecord(b, ctx->stream);
+  CK(cudaEventSynchronize(b), "osem");
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (iterations > 0) CK(cudaMemcpy(&sum, ctx->d_sum, sizeof(double), cudaMemcpyDeviceToHost), "sum");
+  if (int rc = device_status(ctx)) return rc;
+  if (stats) {
+    stats->sum_image = sum;
+    stats->subset_iterations = done;
+    stats->ms_total = ms;
+  }
+  return HRRT_OK;
+}
+
+int hrrt_get_image(hrrt_ctx *ctx, float *image_zyx) {
+  if (!ctx || !image_zyx) return HRRT_ERR_ARG;
+  const Geometry &g = ctx->geo;
+  std::vector<float> h((size_t)ctx->vol);
+  CK(cudaMemcpyAsync(h.data(), ctx->d_image, h.size() * 4, cudaMemcpyDeviceToHost, ctx->stream), "get_image");
+  CK(cudaStreamSynchronize(ctx->stream), "get_image");
+  // SaveImage (drv:4020-4043): tmpimage[z][y][x] = image[x][y][z] on FOV columns
+  std::memset(image_zyx, 0, sizeof(float) * (size_t)g.nz * g.ny * g.nx);
+  for (int x = 0; x < g.nx; x++)
+    for (int y = g.cyl0[x]; y < g.cyl1[x]; y++)
+      for (int z = 0; z < g.nz; z++)
+        image_zyx[((size_t)z * g.ny + y) * g.nx + x] = h[((size_t)x * g.ny + y) * g.zp + z];
+  return HRRT_OK;
+}
+
+int hrrt_get_image_xyz(hrrt_ctx *ctx, float *image_xyz) {
+  if (!ctx || !image_xyz) return HRRT_ERR_ARG;
+  CK(cudaMemcpyAsync(image_xyz, ctx->d_image, ctx->vol * 4, cudaMemcpyDeviceToHost, ctx->stream), "get_image");
+  CK(cudaStreamSynchronize(ctx->stream), "get_image");
+  return HRRT_OK;
+}
+
+int hrrt_set_image_xyz(hrrt_ctx *ctx, const float *image_xyz) {
+  if (!ctx || !image_xyz) return HRRT_ERR_ARG;
+  CK(cudaMemcpyAsync(ctx->d_image, image_xyz, ctx->vol * 4, cudaMemcpyHostToDevice, ctx->stream), "set_image");
+  CK(cudaStreamSynchronize(ctx->stream), "set_image");
+  ctx->have_image = true;
+  return HRRT_OK;
+}
+
+int hrrt_get_sensitivity(hrrt_ctx *ctx, int subset, float *nf_inv_xyz) {
+  if (!ctx || !nf_inv_xyz || subset < 0 || subset >= ctx->geo.sp.subsets) return HRRT_ERR_ARG;
+  if (!ctx->have_sens) return fail(ctx, HRRT_ERR_STATE, "no sensitivity");
+  CK(cudaMemcpyAsync(nf_inv_xyz, ctx->d_nfinv + (size_t)subset * ctx->vol, ctx->vol * 4, cudaMemcpyDeviceToHost,
+                     ctx->stream),
+     "get_sensitivity");
+  CK(cudaStreamSynchronize(ctx->stream), "get_sensitivity");
+  return HRRT_OK;
+}
+
+int hrrt_get_norm_zero_mask(hrrt_ctx *ctx, int16_t *mask) {
+  if (!ctx || !mask) return HRRT_ERR_ARG;
+  std::memcpy(mask, ctx->nzmask.data(), ctx->nzmask.size() * sizeof(int16_t));
+  return HRRT_OK;
+}
+
+int hrrt_set_norm_zero_mask(hrrt_ctx *ctx, const int16_t *mask) {
+  if (!ctx || !mask) return HRRT_ERR_ARG;
+  std::memcpy(ctx->nzmask.data(), mask, ctx->nzmask.size() * sizeof(int16_t));
+  CK(cudaMemcpyAsync(ctx->d_nzmask, ctx->nzmask.data(), ctx->nzmask.size() * 2, cudaMemcpyHostToDevice, ctx->stream),
+     "mask");
+  CK(cudaStreamSynchronize(ctx->stream), "mask");
+  return build_work_lists(ctx);
+}
+
+int hrrt_fp_pair(hrrt_ctx *ctx, const float *image_xyz, int view, float *prj) {
+  if (!ctx || !image_xyz || !prj) return HRRT_ERR_ARG;
+  const Geometry &g = ctx->geo;
+  if (view < 0 || view >= g.nviews / 2) return fail(ctx, HRRT_ERR_ARG, "view must be < nviews/2");
+  cudaError_t e = cudaSuccess;
+  const size_t rows = (size_t)2 * g.segmentsize * g.nbins;
+  if (!ctx->d_tmp_img) ctx->d_tmp_img = dalloc<float>(ctx, ctx->vol, &e);
+  if (!ctx->d_rows) ctx->d_rows = ctx->d_tmp_img ? dalloc<float>(ctx, rows, &e) : nullptr;
+  if (!ctx->d_rows) return fail(ctx, HRRT_ERR_NOMEM, "scratch");
+  std::vector<QuadWork> work;
+  const int nq = g.nx / 2 + 1;
+  for (int x = 1; x <= g.c; x++)
+    if (g.cyl0[x] != g.cyl1[x] && ctx->nzmask[(size_t)view * nq + x] != 0)
+      work.push_back(QuadWork{0, (int16_t)x, (int16_t)view, 0});
+  QuadWork *dw = dupload(ctx, work, &e);
+  if (!dw) return cuda_fail(ctx, e, "work");
+  CK(cudaMemcpyAsync(ctx->d_tmp_img, image_xyz, ctx->vol * 4, cudaMemcpyHostToDevice, ctx->stream), "fp_pair");
+  CK(cudaMemcpyAsync(ctx->d_rows, prj, rows * 4, cudaMemcpyHostToDevice, ctx->stream), "fp_pair");
+  {
+    Launch L(ctx, "fp_kernel");
+    CK(launch_fp(ctx->dg, ctx->d_tmp_img, dw, (int)work.size(), 0, nullptr, nullptr, 0, ctx->d_ratio, ctx->quad_pair,
+                 ctx->tpt, ctx->stream),
+       "fp_kernel");
+  }
+  CK(launch_quad_to_rows(ctx->dg, g.nbins, ctx->d_ratio, dw, (int)work.size(), ctx->d_rows, ctx->stream), "unpack");
+  CK(cudaMemcpyAsync(prj, ctx->d_rows, rows * 4, cudaMemcpyDeviceToHost, ctx->stream), "fp_pair");
+  CK(cudaStreamSynchronize(ctx->stream), "fp_pair");
+  cudaFree(dw);
+  ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)dw));
+  return device_status(ctx);
+}
+int hrrt_forward_project(hrrt_ctx *ctx, const float *image_xyz, float *sino) {
+  if (!ctx || !image_xyz || !sino) return HRRT_ERR_ARG;
+  const Geometry &g = ctx->geo;
+  cudaError_t e = cudaSuccess;
+  if (!ctx->d_tmp_img) ctx->d_tmp_img = dalloc<float>(ctx, ctx->vol, &e);
+  if (!ctx->d_tmp_img) return fail(ctx, HRRT_ERR_NOMEM, "scratch");
+  const size_t n = (size_t)g.segmentsize * g.nviews * g.nbins;
+  float *dsino = nullptr;
+  e = cudaMalloc(&dsino, n * sizeof(float));
+  if (e != cudaSuccess) return fail(ctx, HRRT_ERR_NOMEM, "sinogram");
+  QuadWork *dw = nullptr;
+  auto done = [&](int rc) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(dsino);
+    if (dw) cudaFree(dw);
+    return rc;
+  };
+  e = cudaMemsetAsync(dsino, 0, n * sizeof(float), ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->d_tmp_img, image_xyz, ctx->vol * 4, cudaMemcpyHostToDevice, ctx->stream);
+  // every active quad of every view pair, in batches of npairs pairs
+  const int nq = g.nx / 2 + 1, V2 = g.nviews / 2;
+  std::vector<QuadWork> work;
+  std::vector<int> off;
+  for (int b = 0; b < V2; b += ctx->npairs) {
+    off.push_back((int)work.size());
+    for (int x = 1; x <= g.c; x++)
+      for (int k = 0; k < ctx->npairs && b + k < V2; k++)
+        if (g.cyl0[x] != g.cyl1[x] && ctx->nzmask[(size_t)(b + k) * nq + x] != 0)
+          work.push_back(QuadWork{(int16_t)k, (int16_t)x, (int16_t)(b + k), 0});
+  }
+  off.push_back((int)work.size());
+  if (e == cudaSuccess) e = cudaMalloc(&dw, work.size() * sizeof(QuadWork) + 16);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dw, work.data(), work.size() * sizeof(QuadWork), cudaMemcpyHostToDevice, ctx->stream);
+  for (size_t b = 0; b + 1 < off.size() && e == cudaSuccess; b++) {
+    const int cnt = off[b + 1] - off[b];
+    {
+      Launch L(ctx, "fp_kernel");
+      e = launch_fp(ctx->dg, ctx->d_tmp_img, dw + off[b], cnt, 0, nullptr, nullptr, 0, ctx->d_ratio, ctx->quad_pair,
+                    ctx->tpt, ctx->stream);
+    }
+    if (e == cudaSuccess)
+      e = launch_quad_to_file(ctx->dg, g.nbins, ctx->d_ratio, ctx->quad_pair, dw + off[b], cnt, dsino, ctx->stream);
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sino, dsino, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return done(cuda_fail(ctx, e, "forward_project"));
+  return done(device_status(ctx));
+}
+
+int hrrt_bp_pair(hrrt_ctx *ctx, const float *prj, int view, float *imagebuf_xyz, int mode) {
+  if (!ctx || !prj || !imagebuf_xyz) return HRRT_ERR_ARG;
+  if (mode != HRRT_BP_REF) return fail(ctx, HRRT_ERR_ARG, "unknown back projector");
+  const Geometry &g = ctx->geo;
+  if (view < 0 || view >= g.nviews / 2) return fail(ctx, HRRT_ERR_ARG, "view must be < nviews/2");
+  cudaError_t e = cudaSuccess;
+  const size_t rows = (size_t)2 * g.segmentsize * g.nbins;
+  if (!ctx->d_tmp_img) ctx->d_tmp_img = dalloc<float>(ctx, ctx->vol, &e);
+  if (!ctx->d_rows) ctx->d_rows = ctx->d_tmp_img ? dalloc<float>(ctx, rows, &e) : nullptr;
+  if (!ctx->d_rows) return fail(ctx, HRRT_ERR_NOMEM, "scratch");
+  std::vector<QuadWork> work;
+  for (int x = 1; x <= g.c; x++)
+    if (g.cyl0[x] != g.cyl1[x]) work.push_back(QuadWork{0, (int16_t)x, (int16_t)view, 0});
+  QuadWork *dw = dupload(ctx, work, &e);
+  if (!dw) return cuda_fail(ctx, e, "work");
+  CK(cudaMemcpyAsync(ctx->d_rows, prj, rows * 4, cudaMemcpyHostToDevice, ctx->stream), "bp_pair");
+  CK(cudaMemsetAsync(ctx->d_ratio, 0, ctx->quad_pair * 4, ctx->stream), "bp_pair");
+  CK(launch_rows_to_quad(ctx->dg, g.nbins, ctx->d_rows, ctx->d_ratio, 1, ctx->stream), "pack");
+  {
+    Launch L(ctx, "bp_kernel");
+    CK(launch_bp(ctx->dg, ctx->d_ratio, ctx->quad_pair, dw, (int)work.size(), ctx->d_bc, ctx->d_br, ctx->vol,
+                 ctx->stream),
+       "bp_kernel");
+  }
+  CK(launch_add_partials(ctx->dg, ctx->d_bc, ctx->d_br, ctx->d_tmp_img, ctx->stream), "add");
+  CK(cudaMemcpyAsync(imagebuf_xyz, ctx->d_tmp_img, ctx->vol * 4, cudaMemcpyDeviceToHost, ctx->stream), "bp_pair");
+  CK(cudaStreamSynchronize(ctx->stream), "bp_pair");
+  cudaFree(dw);
+  ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)dw));
+  return HRRT_OK;
+}
+
+int hrrt_rotate_add(hrrt_ctx *ctx, const float *imagebuf_xyz, int view, float *corr_xyz) {
+  if (!ctx || !imagebuf_xyz || !corr_xyz) return HRRT_ERR_ARG;
+  const Geometry &g = ctx->geo;
+  if (view < 0 || view >= g.nviews / 2) return fail(ctx, HRRT_ERR_ARG, "view must be < nviews/2");
+  cudaError_t e = cudaSuccess;
+  if (!ctx->d_tmp_img) ctx->d_tmp_img = dalloc<float>(ctx, ctx->vol, &e);
+  if (!ctx->d_tmp_img) return fail(ctx, HRRT_ERR_NOMEM, "scratch");
+  int *dv = dupload(ctx, std::vector<int>{view}, &e);
+  if (!dv) return cuda_fail(ctx, e, "view");
+  // corr in d_bc[1], imagebuf in d_bc[0]
+  CK(cudaMemcpyAsync(ctx->d_bc, imagebuf_xyz, ctx->vol * 4, cudaMemcpyHostToDevice, ctx->stream), "rotate");
+  CK(cudaMemcpyAsync(ctx->d_tmp_img, corr_xyz, ctx->vol * 4, cudaMemcpyHostToDevice, ctx->stream), "rotate");
+  {
+    Launch L(ctx, "rotback_kernel");
+    CK(launch_rotback(ctx->dg, dv, 1, ctx->d_bc, nullptr, ctx->vol, nullptr, nullptr, ctx->d_tmp_img, 2, ctx->stream),
+       "rotback");
+  }
+  CK(cudaMemcpyAsync(corr_xyz, ctx->d_tmp_img, ctx->vol * 4, cudaMemcpyDeviceToHost, ctx->stream), "rotate");
+  CK(cudaStreamSynchronize(ctx->stream), "rotate");
+  cudaFree(dv);
+  ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)dv));
+  return HRRT_OK;
+}
+
+long long hrrt_geometry_table(const hrrt_geom *gp, const char *name, void *out, size_t bytes) {
+  if (!gp || !name) return HRRT_ERR_ARG;
+  ScannerParams p;
+  p.nrings = gp->nrings;
+  p.nelements = gp->nelements;
+  p.nangles = gp->nangles;
+  p.ring_radius = gp->ring_radius;
+  p.plane_sep = gp->plane_sep;
+  p.binsize = gp->binsize;
+  p.span = gp->span;
+  p.maxdel = gp->maxdel;
+  p.subsets = gp->subsets;
+  p.rel_fov = gp->rel_fov;
+  Geometry g;
+  if (!g.build(p).empty()) return HRRT_ERR_ARG;
+  std::vector<char> buf;
+  auto put = [&](const void *src, size_t n) {
+    const char *c = (const char *)src;
+    buf.insert(buf.end(), c, c + n);
+  };
+  const std::string n(name);
+  if (n == "cylwiny") {
+    for (int y = 0; y < g.ny; y++) {
+      put(&g.cyl0[y], 2);
+      put(&g.cyl1[y], 2);
+    }
+  } else if (n == "segments") {
+    put(g.yr_bottom.data(), 4 * g.nseg);
+    put(g.yr_top.data(), 4 * g.nseg);
+    put(g.segment_offset.data(), 4 * g.nseg);
+  } else if (n == "sin_theta") put(g.sin_theta.data(), 4 * g.nseg);
+  else if (n == "cos_theta") put(g.cos_theta.data(), 4 * g.nseg);
+  else if (n == "sin_psi") put(g.sin_psi.data(), 4 * g.nviews);
+  else if (n == "cos_psi") put(g.cos_psi.data(), 4 * g.nviews);
+  else if (n == "tantheta") put(g.tantheta.data(), 4 * g.tantheta.size());
+  else if (n == "rescale") put(g.rescale.data(), 4 * g.rescale.size());
+  else if (n == "flookup_zzi") put(g.fl_zzi.data(), 4 * g.fl_zzi.size());
+  else if (n == "flookup_zzz0") put(g.fl_zzz0.data(), 4 * g.fl_zzz0.size());
+  else if (n == "blookup") {
+    for (size_t i = 0; i < g.bl_zsa.size(); i++) {
+      put(&g.bl_zsa[i], 4);
+      put(&g.bl_zea[i], 4);
+      put(&g.bl_yra[i], 4);
+    }
+  } else if (n == "blookup_yr2a") put(g.bl_yr2a.data(), 4 * g.bl_yr2a.size());
+  else if (n == "bp_scale") put(g.bp_scale.data(), 4 * g.bp_scale.size());
+  else if (n == "order") put(g.order.data(), 2 * g.order.size());
+  else return HRRT_ERR_ARG;
+  if (out && bytes >= buf.size()) std::memcpy(out, buf.data(), buf.size());
+  return (long long)buf.size();
+}
+
+int hrrt_set_profiling(hrrt_ctx *ctx, int enable) {
+  if (!ctx) return HRRT_ERR_ARG;
+  ctx->prof = enable != 0;
+  return HRRT_OK;
+}
+
+int hrrt_kernel_stats(hrrt_ctx *ctx, const char *kernel, int *launches, double *total_ms) {
+  if (!ctx || !kernel) return HRRT_ERR_ARG;
+  drain_timers(ctx);
+  auto it = ctx->kstats.find(kernel);
+  if (launches) *launches = it == ctx->kstats.end() ? 0 : it->second.first;
+  if (total_ms) *total_ms = it == ctx->kstats.end() ? 0.0 : it->second.second;
+  return HRRT_OK;
+}
+
+int hrrt_reset_kernel_stats(hrrt_ctx *ctx) {
+  if (!ctx) return HRRT_ERR_ARG;
+  drain_timers(ctx);
+  ctx->kstats.clear();
+  return HRRT_OK;
+}
+
+}  // extern "C"

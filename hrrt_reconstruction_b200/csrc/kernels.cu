@@ -1,0 +1,975 @@
+// kernels.cu -- sm_100a kernels of the hrrt_osem3d OSEM hot path.
+//
+// Compiled with -fmad=false: the reference (x86-64 SSE2 build) never fuses a
+// multiply with an add, and every expression below keeps the reference's
+// association, so the forward projector, the rotate-back and the update are
+// bit-identical to the reference on the same inputs.
+#include "kernels.cuh"
+
+#include <cfloat>
+
+namespace hrrt {
+
+namespace {
+
+__device__ __forceinline__ float4 f4(float v) { return make_float4(v, v, v, v); }
+__device__ __forceinline__ float4 operator+(float4 a, float4 b) {
+  return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+__device__ __forceinline__ float4 operator-(float4 a, float4 b) {
+  return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
+}
+__device__ __forceinline__ float4 operator*(float4 a, float s) {
+  return make_float4(a.x * s, a.y * s, a.z * s, a.w * s);
+}
+__device__ __forceinline__ float lane(const float4 &v, int l) {
+  return l == 0 ? v.x : (l == 1 ? v.y : (l == 2 ? v.z : v.w));
+}
+
+// ---- storage-type helpers for the sinogram inputs ----
+struct P4 { float v[4]; };
+__device__ __forceinline__ P4 load_p4(const int16_t *p, size_t i) {
+  const short4 s = reinterpret_cast<const short4 *>(p)[i];
+  return P4{{(float)s.x, (float)s.y, (float)s.z, (float)s.w}};
+}
+__device__ __forceinline__ P4 load_p4(const __half *p, size_t i) {
+  const uint2 u = reinterpret_cast<const uint2 *>(p)[i];
+  const __half2 a = *reinterpret_cast<const __half2 *>(&u.x);
+  const __half2 b = *reinterpret_cast<const __half2 *>(&u.y);
+  return P4{{__low2float(a), __high2float(a), __low2float(b), __high2float(b)}};
+}
+__device__ __forceinline__ P4 load_p4(const float *p, size_t i) {
+  const float4 f = reinterpret_cast<const float4 *>(p)[i];
+  return P4{{f.x, f.y, f.z, f.w}};
+}
+__device__ __forceinline__ P4 load_p4(const __nv_bfloat16 *p, size_t i) {
+  const uint2 u = reinterpret_cast<const uint2 *>(p)[i];
+  const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162 *>(&u.x);
+  const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162 *>(&u.y);
+  return P4{{__low2float(a), __high2float(a), __low2float(b), __high2float(b)}};
+}
+__device__ __forceinline__ void store_p4(int16_t *p, size_t i, const float *v) {
+  reinterpret_cast<short4 *>(p)[i] = make_short4((short)v[0], (short)v[1], (short)v[2], (short)v[3]);
+}
+__device__ __forceinline__ void store_p4(__half *p, size_t i, const float *v) {
+  __half2 a = __floats2half2_rn(v[0], v[1]), b = __floats2half2_rn(v[2], v[3]);
+  uint2 u;
+  u.x = *reinterpret_cast<uint32_t *>(&a);
+  u.y = *reinterpret_cast<uint32_t *>(&b);
+  reinterpret_cast<uint2 *>(p)[i] = u;
+}
+__device__ __forceinline__ void store_p4(float *p, size_t i, const float *v) {
+  reinterpret_cast<float4 *>(p)[i] = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void store_p4(__nv_bfloat16 *p, size_t i, const float *v) {
+  __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]), b = __floats2bfloat162_rn(v[2], v[3]);
+  uint2 u;
+  u.x = *reinterpret_cast<uint32_t *>(&a);
+  u.y = *reinterpret_cast<uint32_t *>(&b);
+  reinterpret_cast<uint2 *>(p)[i] = u;
+}
+
+
+// ---- TMA bulk copies + mbarrier (sm_90+ async proxy) ----
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// bounded wait on an mbarrier phase; on timeout records the error and returns false
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
+  const uint32_t a = smem_u32(bar);
+  for (int i = 0; i < (1 << 22); i++) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  if (err) atomicExch(err, 1);
+  return false;
+}
+
+// Rotated-grid sample point (sbrt:1866-1871): position of rotated-frame voxel
+// (a,b) in the image, as flat column index of its (ix,iy) corner and the four
+// bilinear weights.  base < 0: outside (the reference zeroes that sample).
+struct SamplePt {
+  int base;
+  float c0, c1, c2, c3;
+};
+__device__ __forceinline__ SamplePt sample_point(int a, int b, int c, int N, int zp, float cosv, float sinv) {
+  SamplePt s;
+  const float fa = (float)(a - c), fb = (float)(b - c), fc = (float)c;
+  const float xx0 = fa * cosv - fb * sinv + fc;
+  const float yy0 = fa * sinv + fb * cosv + fc;
+  const float lim = (float)(N - 2);
+  // the reference tests xx0 against the upper limit twice and never yy0
+  if (xx0 < 0 || xx0 > lim || yy0 < 0 || xx0 > lim) {
+    s.base = -1;
+    s.c0 = s.c1 = s.c2 = s.c3 = 0.f;
+    return s;
+  }
+  const int ix = (int)xx0, iy = (int)yy0;
+  const float x1 = xx0 - ix, y1 = yy0 - iy;
+  s.c0 = (1 - x1) * (1 - y1);
+  s.c1 = x1 * (1 - y1);
+  s.c2 = y1 * (1 - x1);
+  s.c3 = y1 * x1;
+  // contiguous [x][y][zp] addressing, as the reference's matrix3dm128 image
+  if ((ix + 1) * N + iy + 1 >= N * N) {
+    s.base = -1;
+    return s;
+  }
+  s.base = (ix * N + iy) * zp;
+  return s;
+}
+__device__ __forceinline__ float bilinear(const float *__restrict__ img, const SamplePt &s, int N, int zp, int z) {
+  if (s.base < 0) return 0.f;
+  const float r1 = __ldg(img + s.base + z);
+  const float r2 = __ldg(img + s.base + N * zp + z);
+  const float r3 = __ldg(img + s.base + zp + z);
+  const float r4 = __ldg(img + s.base + N * zp + zp + z);
+  return (r1 * s.c0 + r2 * s.c1) + (r3 * s.c2 + r4 * s.c3);
+}
+
+// ============================================================================
+// Forward projection (+ fused OP ratio), one CTA per (view pair, quad x).
+// Restates forward_proj3d_view1_thread (sbrt:1728-1978) for one x: the eight
+// symmetric rotated-grid columns at row y are sampled once into shared memory
+// (pam: lanes (x,y),(N-x,y),(N-y,x),(N-y,N-x); pam2: (x,N-y),(N-x,N-y),(y,x),
+// (y,N-x)), then every thread accumulates its own (segment, plane-run) outputs
+// for all four lanes, row by row in the reference's order.
+// ============================================================================
+constexpr int fp_max_threads(int tpt) { return tpt == 1 ? 448 : (tpt == 2 ? 512 : 320); }
+constexpr int fp_min_blocks(int tpt) { return tpt == 1 ? 2 : 1; }
+
+template <int TPT, int MODE, typename PT, typename AT>
+__global__ void __launch_bounds__(fp_max_threads(TPT), fp_min_blocks(TPT)) fp_kernel(
+    DevGeom g, const float *__restrict__ image, const QuadWork *__restrict__ work, const PT *__restrict__ prompts,
+    const AT *__restrict__ add, float4 *__restrict__ out, long long out_pair_stride) {
+  // shared memory: [2 slots][8 points][2 column pairs][2*zp] corner columns,
+  // [2 slots][2 halves][ZS] sampled rows, [ZS] centre column
+  extern __shared__ float4 smem[];
+  const int ZS = g.zp + kFpZPad;
+  const int zp = g.zp;
+  float *corners = reinterpret_cast<float *>(smem);
+  const int cpair = 2 * zp;                       // floats per column pair
+  float4 *rows = smem + (size_t)(2 * 8 * 2 + 2) * cpair / 4;  // [2][2][ZS]
+  float4 *cen = rows + 4 * ZS;
+  // 2*cpair zeros after the corner slots: the corner pairs of outside points
+  const int zoff = 2 * 8 * 2 * cpair;
+  float *zcol = corners + zoff;
+  __shared__ float4 s_coef[2][8];
+  __shared__ int s_off[2][8];
+  __shared__ __align__(8) uint64_t s_bar[2];
+
+  const QuadWork w = work[blockIdx.x];
+  const int x = w.x, v = w.view;
+  const int N = g.nx, c = g.c;
+  const float cosv = g.cos_psi[v], sinv = g.sin_psi[v];
+  const int ystart = g.cyl0[x];
+  const int nrows = c - ystart;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+
+  // TMA producer (lanes 0-7 of warp 0, one sample point each): the two
+  // contiguous column pairs (ix, iy..iy+1) and (ix+1, iy..iy+1) of each inside
+  // point of row r; outside points read a zero column with zero weights
+  auto issue_row = [&](int r) {
+    const int sl = r & 1, y = ystart + r, l = tid;  // tid < 8
+    int a, b;
+    switch (l) {
+      case 0: a = x; b = y; break;
+      case 1: a = N - x; b = y; break;
+      case 2: a = N - y; b = x; break;
+      case 3: a = N - y; b = N - x; break;
+      case 4: a = x; b = N - y; break;
+      case 5: a = N - x; b = N - y; break;
+      case 6: a = y; b = x; break;
+      default: a = y; b = N - x; break;
+    }
+    const SamplePt pt = sample_point(a, b, c, N, zp, cosv, sinv);
+    const bool inside = pt.base >= 0;
+    s_coef[sl][l] = make_float4(pt.c0, pt.c1, pt.c2, pt.c3);
+    // outside points read the zero column (both pairs) of the corner area
+    s_off[sl][l] = inside ? (sl * 8 + l) * 2 * cpair : zoff;
+    const unsigned m = __ballot_sync(0xffu, inside);
+    if (l == 0) {
+      fence_proxy_async();
+      mbar_arrive_tx(&s_bar[sl], (uint32_t)__popc(m) * 2u * cpair * 4u);
+    }
+    __syncwarp(0xffu);
+    if (inside) {
+      float *dst = corners + ((size_t)(sl * 8 + l) * 2) * cpair;
+      bulk_g2s(dst, image + pt.base, cpair * 4u, &s_bar[sl]);
+      bulk_g2s(dst + cpair, image + pt.base + (size_t)N * zp, cpair * 4u, &s_bar[sl]);
+    }
+  };
+
+  if (tid == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    fence_mbar_init();
+  }
+  // zero the row pads once (sampling writes only [0, zp))
+  for (int i = tid; i < 5 * kFpZPad; i += nthr) {
+    const int col = i / kFpZPad, k = i % kFpZPad;
+    rows[col * ZS + zp + k] = f4(0.f);
+  }
+  for (int i = tid; i < 2 * cpair; i += nthr) zcol[i] = 0.f;
+  __syncthreads();
+  if (tid < 8 && nrows > 0) issue_row(0);
+
+  // centre column y = c (sbrt:1815-1853): lanes (x,c),(N-x,c),(c,x),(c,N-x)
+  {
+    SamplePt cp[4];
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      const int a = (l == 0) ? x : (l == 1) ? N - x : c;
+      const int b = (l == 0 || l == 1) ? c : (l == 2) ? x : N - x;
+      cp[l] = sample_point(a, b, c, N, zp, cosv, sinv);
+    }
+    for (int z = tid; z < zp; z += nthr)
+      cen[z] = make_float4(bilinear(image, cp[0], N, zp, z), bilinear(image, cp[1], N, zp, z),
+                           bilinear(image, cp[2], N, zp, z), bilinear(image, cp[3], N, zp, z));
+  }
+  for (int z = zp + tid; z < ZS; z += nthr) cen[z] = f4(0.f);
+  __syncthreads();
+
+  // accumulators start at the centre sample of their plane (the reference
+  // assigns the centre column before accumulating rows y < c)
+  float4 acc[TPT][kFpPlanes];
+  FpTask task[TPT];
+  // this CTA's share of the quad's tasks (blockIdx.y of gridDim.y)
+  const int t_begin = (int)(((long long)g.nfptasks * blockIdx.y) / gridDim.y);
+  const int t_end = (int)(((long long)g.nfptasks * (blockIdx.y + 1)) / gridDim.y);
+#pragma unroll
+  for (int t = 0; t < TPT; t++) {
+    const int ti = t_begin + tid + t * nthr;
+    task[t] = (ti < t_end) ? g.fptasks[ti] : FpTask{0, 0, 0, -1};
+    const int zb = (task[t].type < 0) ? 0 : g.ybot[task[t].seg] + task[t].p0;
+#pragma unroll
+    for (int j = 0; j < kFpPlanes; j++) acc[t][j] = cen[min(zb + j, ZS - 1)];
+  }
+
+  const int G = g.groupmax, FS = g.groupmax * 2 * g.zshift;
+  bool timed_out = false;
+  // bilinear work split: half the threads per sampled half-row
+  const int hsplit = nthr / 2;
+  const int h_mine = tid >= hsplit, z_mine = tid - h_mine * hsplit, z_step = hsplit;
+  for (int r = 0; r < nrows; r++) {
+    const int sl = r & 1, y = ystart + r;
+    // slot sl^1 was last read before the barrier of row r-1
+    if (tid < 8 && r + 1 < nrows) issue_row(r + 1);
+    if (!mbar_wait(&s_bar[sl], (uint32_t)((r >> 1) & 1), g.err)) timed_out = true;
+    // bilinear samples of row r from the staged corners (sbrt:1866-1905):
+    // threads [0, hsplit) build pam (lanes of points 0-3), the rest pam2
+    {
+      float4 *rw = rows + (size_t)sl * 2 * ZS + h_mine * ZS;
+      for (int z = z_mine; z < zp; z += z_step) {
+        float sv[4];
+#pragma unroll
+        for (int l = 0; l < 4; l++) {
+          // broadcast reads: every thread of this half uses the same point
+          const float4 k = s_coef[sl][h_mine * 4 + l];
+          const float *q0 = corners + s_off[sl][h_mine * 4 + l];
+          const float r1 = q0[z], r3 = q0[zp + z], r2 = q0[cpair + z], r4 = q0[cpair + zp + z];
+          sv[l] = (r1 * k.x + r2 * k.y) + (r3 * k.z + r4 * k.w);
+        }
+        rw[z] = make_float4(sv[0], sv[1], sv[2], sv[3]);
+      }
+    }
+    __syncthreads();
+    {
+      const float4 *pam = rows + (size_t)sl * 2 * ZS;
+      const float4 *pam2 = pam + ZS;
+#pragma unroll
+      for (int t = 0; t < TPT; t++) {
+        const FpTask tk = task[t];
+        if (tk.type == 0) {
+          // theta = 0 (sbrt:1907-1910)
+#pragma unroll
+          for (int j = 0; j < kFpPlanes; j++) acc[t][j] = acc[t][j] + (pam[tk.p0 + j] + pam2[tk.p0 + j]);
+        } else if (tk.type > 0) {
+          const int gg = (tk.seg + 1) / 2 - 1;
+          const FpMid m = g.fpmid[y * G + gg];
+          if (m.z < 0) continue;  // group skipped for this row (sbrt:1923-1924)
+          // segment 2k accumulates pam at z and pam2 at z2; segment 2k-1 the converse
+          const float4 *A = (tk.seg & 1) ? pam2 : pam;
+          const float4 *B = (tk.seg & 1) ? pam : pam2;
+          if (tk.type == 1) {
+            // middle planes: z, z2 advance with the plane (sbrt:1933-1947)
+            const int za = m.z + tk.p0 - g.zshift, zb2 = m.z2 + tk.p0 - g.zshift;
+            float4 a0 = A[za], b0 = B[zb2];
+#pragma unroll
+            for (int j = 0; j < kFpPlanes; j++) {
+              const float4 a1 = A[za + j + 1], b1 = B[zb2 + j + 1];
+              acc[t][j] = acc[t][j] + ((b1 + a0) * m.f2 + (a1 + b0) * m.f);
+              a0 = a1;
+              b0 = b1;
+            }
+          } else {
+            // end planes: per-plane flookup entries (sbrt:1925-1931, :1948-1952)
+            const int ns = g.ytop[tk.seg] - g.ybot[tk.seg] + 1;
+#pragma unroll
+            for (int j = 0; j < kFpPlanes; j++) {
+              if (j < tk.n) {
+                const int rr = tk.p0 + j;
+                const int yri = (rr < g.zshift) ? rr : rr - ns + 2 * g.zshift;
+                const int li = gg * 2 * g.zshift + yri;
+                const int z = __ldg(g.fl_zzi + y * FS + li), z2 = __ldg(g.fl_zzi + (N - y) * FS + li);
+                const float f = __ldg(g.fl_zzz0 + y * FS + li), f2 = __ldg(g.fl_zzz0 + (N - y) * FS + li);
+                acc[t][j] = acc[t][j] + ((B[z2 + 1] + A[z]) * f2 + (A[z + 1] + B[z2]) * f);
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+
+  if (timed_out) {
+    // results are void (the host reports the status word); give copies still
+    // in flight into this CTA's shared memory a bounded chance to land first
+    for (int sl = 0; sl < 2; sl++) {
+      const int last = (nrows - 1 - sl) >= 0 ? ((nrows - 1 - sl) | 0) : -1;
+      if (last >= 0) mbar_wait(&s_bar[(nrows - 1 - sl) & 1], (uint32_t)(((nrows - 1 - sl) >> 1) & 1), nullptr);
+    }
+    return;
+  }
+
+  // scale (sbrt:1953-1975), then either store the estimate or the OP ratio
+  // (pt_update_est_w3, drv:2474-2520) pre-multiplied by the back projector's
+  // segment weight (sbrt:1637-1649)
+  const size_t qbase = (size_t)x * g.pplanes;
+#pragma unroll
+  for (int t = 0; t < TPT; t++) {
+    const FpTask tk = task[t];
+    if (tk.type < 0) continue;
+    const int s = tk.seg, gg = (s + 1) / 2 - 1;
+#pragma unroll
+    for (int j = 0; j < kFpPlanes; j++) {
+      if (j >= tk.n) continue;
+      const int r = tk.p0 + j, yr = g.ybot[s] + r;
+      const float sc = (s == 0) ? g.y_size : g.rescale[gg * g.nz + yr];
+      const float4 est = acc[t][j] * sc;
+      const size_t qi = qbase + g.poff[s] + r;
+      if (MODE == 0) {
+        out[(size_t)w.slot * out_pair_stride + qi] = est;
+      } else {
+        const size_t ii = (size_t)v * g.nquads * g.pplanes + qi;
+        const P4 p = load_p4(prompts, ii);
+        const P4 ad = load_p4(add, ii);
+        const float bs = g.bp_scale[s];
+        float rr[4];
+#pragma unroll
+        for (int l = 0; l < 4; l++) {
+          const float den = lane(est, l) + ad.v[l];
+          float q;
+          if (p.v[l] == 0.f) q = 0.f;
+          else if (den > g.eps3) q = p.v[l] / den;
+          else q = 1.0f;
+          rr[l] = q * bs;
+        }
+        out[(size_t)w.slot * out_pair_stride + qi] = make_float4(rr[0], rr[1], rr[2], rr[3]);
+      }
+    }
+  }
+}
+
+// ============================================================================
+// Back projection, one CTA per (view pair, quad x).  Voxel-driven restatement
+// of back_proj3d_view_n1thread (sbrt:4162-4668): the quad's four sinogram
+// lanes sit in shared memory; each thread evaluates, for its rotated-grid row
+// y and a run of kBpZ planes, the two 4-lane sums the reference builds
+// incrementally (sumt1 for voxels (x,y),(N-x,y),(N-y,x),(N-y,N-x); sumt2 for
+// (x,N-y),(N-x,N-y),(y,x),(y,N-x)) as direct linear interpolations of the
+// zero-padded sinogram at yr = z + d.  Each voxel receives two partial sums,
+// one from the ray of view p (its column quad) and one from the ray of view
+// p+nviews/2 (its row quad); they go to Bc and Br and are added in the
+// rotate-back, which is the reference's assign-then-accumulate order.
+// ============================================================================
+template <int KB>
+__device__ __forceinline__ void bp_lerp(float4 (&s)[KB], const float4 *__restrict__ p, const BpLut &bl, int z0) {
+  if (bl.zs <= z0 && z0 + KB - 1 <= bl.ze) {
+    const int yr0 = z0 + bl.d;
+    float4 a = p[yr0];
+#pragma unroll
+    for (int j = 0; j < KB; j++) {
+      const float4 b = p[yr0 + j + 1];
+      s[j] = s[j] + (a + (b - a) * bl.f);
+      a = b;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < KB; j++) {
+      const int z = z0 + j;
+      if (z >= bl.zs && z <= bl.ze) {
+        const float4 a = p[z + bl.d], b = p[z + bl.d + 1];
+        s[j] = s[j] + (a + (b - a) * bl.f);
+      }
+    }
+  }
+}
+
+template <int KB>
+__device__ __forceinline__ void store_lane(float *__restrict__ dst, const float4 (&s)[KB], int l) {
+  float v[KB];
+#pragma unroll
+  for (int j = 0; j < KB; j++) v[j] = lane(s[j], l);
+#pragma unroll
+  for (int j = 0; j < KB; j += 4) *reinterpret_cast<float4 *>(dst + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+}
+
+template <int KB>
+__global__ void __launch_bounds__(256, 3) bp_kernel(DevGeom g, const float4 *__restrict__ in, long long in_pair_stride,
+                                                 const QuadWork *__restrict__ work, float *__restrict__ bc,
+                                                 float *__restrict__ br, long long vol) {
+  extern __shared__ float4 P[];  // [pplanes]
+  const QuadWork w = work[blockIdx.x];
+  const int x = w.x, N = g.nx, c = g.c, zp = g.zp, G = g.groupmax;
+  const bool masked = g.nzmask[w.view * g.nquads + x] == 0;
+  const float4 *src = in + (size_t)w.slot * in_pair_stride + (size_t)x * g.pplanes;
+  if (!masked)
+    for (int i = threadIdx.x; i < g.pplanes; i += blockDim.x) P[i] = src[i];
+  __syncthreads();
+
+  float *bcp = bc + (size_t)w.slot * vol;
+  float *brp = br + (size_t)w.slot * vol;
+  const int ystart = g.cyl0[x];
+  const int nyq = c - ystart + 1, nzc = zp / KB;
+  const float4 *P0 = P + g.poff[0];
+  // task = (half, plane run, row); half 0 builds sumt1 (voxels (x,y),(N-x,y),
+  // (N-y,x),(N-y,N-x)), half 1 sumt2 (voxels (x,N-y),(N-x,N-y),(y,x),(y,N-x)).
+  // Consecutive threads take consecutive rows at the same planes: their window
+  // starts z0 + d(y) differ by the slowly varying d(y), so the 16-byte shared
+  // loads of a warp fall in distinct banks or broadcast.
+  const int per_half = nyq * nzc;
+  for (int task = threadIdx.x; task < 2 * per_half; task += blockDim.x) {
+    const int half = task >= per_half;
+    const int t2 = task - half * per_half;
+    const int zc = t2 / nyq, yi = t2 - zc * nyq, z0 = zc * KB;
+    const int y = ystart + yi;
+    if (half && y == c) continue;  // the centre row has a single voxel set
+    float4 s[KB];
+    if (masked) {
+      // masked quads contribute zero (sbrt:4223-4258, :4595-4640)
+#pragma unroll
+      for (int j = 0; j < KB; j++) s[j] = f4(0.f);
+    } else if (y == c) {
+      // centre row (sbrt:4260-4284): rays pass plane yr = z exactly
+#pragma unroll
+      for (int j = 0; j < KB; j++) s[j] = P0[z0 + j];
+      for (int gg = 0; gg < G; gg++) {
+        const int se = 2 * gg + 2, so = 2 * gg + 1;
+        const int yb = g.ybot[se], yt = g.ytop[se];
+        const float4 *pe = P + g.poff[se] - yb, *po = P + g.poff[so] - yb;
+#pragma unroll
+        for (int j = 0; j < KB; j++) {
+          const int z = z0 + j;
+          if (z >= yb && z <= yt) s[j] = s[j] + (pe[z] + po[z]);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < KB; j++) s[j] = P0[z0 + j];
+      // bplut is [group][row]: the rows of a warp read consecutive entries
+      const BpLut *l1 = g.bplut + y, *l2 = g.bplut + (N - y);
+      BpLut b1 = l1[0], b2 = l2[0];
+      for (int gg = 0; gg < G; gg++) {
+        const int se = 2 * gg + 2, so = 2 * gg + 1;
+        const int yb = g.ybot[se];
+        const float4 *pe = P + g.poff[se] - yb, *po = P + g.poff[so] - yb;
+        const int gn = (gg + 1 < G) ? gg + 1 : gg;
+        const BpLut n1 = l1[(size_t)gn * N], n2 = l2[(size_t)gn * N];  // next group, in flight
+        // sumt1: segment 2k at +u and 2k-1 at -u; sumt2: the converse
+        bp_lerp<KB>(s, half ? po : pe, b1, z0);
+        bp_lerp<KB>(s, half ? pe : po, b2, z0);
+        b1 = n1;
+        b2 = n2;
+      }
+    }
+    // the reference writes planes z < nz only
+#pragma unroll
+    for (int j = 0; j < KB; j++)
+      if (z0 + j >= g.nz) s[j] = f4(0.f);
+    const size_t cz = (size_t)z0;
+    if (!half) {
+      store_lane<KB>(bcp + ((size_t)x * N + y) * zp + cz, s, 0);
+      store_lane<KB>(brp + ((size_t)(N - y) * N + x) * zp + cz, s, 2);
+      if (x != c) {
+        store_lane<KB>(bcp + ((size_t)(N - x) * N + y) * zp + cz, s, 1);
+        store_lane<KB>(brp + ((size_t)(N - y) * N + N - x) * zp + cz, s, 3);
+      }
+    } else {
+      store_lane<KB>(bcp + ((size_t)x * N + N - y) * zp + cz, s, 0);
+      store_lane<KB>(brp + ((size_t)y * N + x) * zp + cz, s, 2);
+      if (x != c) {
+        store_lane<KB>(bcp + ((size_t)(N - x) * N + N - y) * zp + cz, s, 1);
+        store_lane<KB>(brp + ((size_t)y * N + N - x) * zp + cz, s, 3);
+      }
+    }
+  }
+}
+
+// ============================================================================
+// Rotate-back of the summed partials of every pair (rotateimage2, sbrt:1137-
+// 1186) fused with what consumes the correction image:
+//   MODE 0: OSEM update pt_cal_updateimage (drv:2018-2059)
+//   MODE 1: inverse sensitivity pt_normfac_calculate (drv:1852-1894)
+//   MODE 2: corr_out += rotate-back (rotate_image_buf for one view)
+// One thread per (FOV column, 4 planes); pairs are added in subset order.
+// ============================================================================
+template <int MODE>
+__global__ void __launch_bounds__(256) rotback_kernel(DevGeom g, const int *__restrict__ pair_views, int npairs,
+                                                      const float *__restrict__ bc, const float *__restrict__ br,
+                                                      long long vol, float *__restrict__ image,
+                                                      float *__restrict__ nf_inv, float *__restrict__ corr_out) {
+  const int nq = g.zp / 4;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int col = (int)(t / nq), q = (int)(t - (long long)col * nq);
+  if (col >= g.fov_columns) return;
+  const short2 xy = g.fov_xy[col];
+  const int N = g.nx;
+  float4 acc = f4(0.f);
+  for (int p = 0; p < npairs; p++) {
+    const float2 pos = g.rotpos[(size_t)pair_views[p] * g.fov_columns + col];
+    const int ix = (int)pos.x, iy = (int)pos.y;
+    if (ix < 0 || ix > N - 2 || iy < 0 || iy > N - 2) continue;
+    const float x1 = pos.x - ix, y1 = pos.y - iy;
+    const float c1 = (1 - x1) * (1 - y1), c2 = x1 * (1 - y1), c3 = y1 * (1 - x1), c4 = y1 * x1;
+    const float4 *Bc = reinterpret_cast<const float4 *>(bc + (size_t)p * vol);
+    const size_t i1 = ((size_t)ix * N + iy) * nq + q, i2 = i1 + (size_t)N * nq, i3 = i1 + nq, i4 = i2 + nq;
+    float4 b1 = __ldg(Bc + i1), b2 = __ldg(Bc + i2), b3 = __ldg(Bc + i3), b4 = __ldg(Bc + i4);
+    if (br != nullptr) {
+      const float4 *Br = reinterpret_cast<const float4 *>(br + (size_t)p * vol);
+      b1 = b1 + __ldg(Br + i1);
+      b2 = b2 + __ldg(Br + i2);
+      b3 = b3 + __ldg(Br + i3);
+      b4 = b4 + __ldg(Br + i4);
+    }
+    acc = acc + ((b1 * c1 + b2 * c2) + (b3 * c3 + b4 * c4));
+  }
+  const size_t o = ((size_t)xy.x * N + xy.y) * nq + q;
+  if (MODE == 0) {
+    float4 *im = reinterpret_cast<float4 *>(image);
+    const float4 nf = reinterpret_cast<const float4 *>(nf_inv)[o];
+    float4 iv = im[o];
+    float a[4] = {acc.x, acc.y, acc.z, acc.w}, b[4] = {iv.x, iv.y, iv.z, iv.w}, n[4] = {nf.x, nf.y, nf.z, nf.w};
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      // _mm_max_ps(0.01, c), _mm_min_ps(100, .), _mm_min_ps(image_max, .):
+      // each returns its second operand when either is NaN
+      const float lo = (0.01f > a[l]) ? 0.01f : a[l];
+      const float cl = (100.0f < lo) ? 100.0f : lo;
+      const float u = b[l] * (cl * n[l]);
+      b[l] = (g.image_max < u) ? g.image_max : u;
+    }
+    im[o] = make_float4(b[0], b[1], b[2], b[3]);
+  } else if (MODE == 1) {
+    float a[4] = {acc.x, acc.y, acc.z, acc.w}, r[4];
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      const int z = q * 4 + l;
+      r[l] = (z < g.nz && fabsf(a[l]) > g.eps1) ? (1.0f / a[l]) : 0.f;
+    }
+    reinterpret_cast<float4 *>(nf_inv)[o] = make_float4(r[0], r[1], r[2], r[3]);
+  } else {
+    float4 *co = reinterpret_cast<float4 *>(corr_out);
+    co[o] = co[o] + acc;
+  }
+}
+
+// rotate-back sample positions, incremented along y exactly as rotateimage2
+// does (sbrt:1148-1184)
+__global__ void rotpos_kernel(DevGeom g, float2 *__restrict__ rotpos, const int *__restrict__ row_start) {
+  const int X = blockIdx.x * blockDim.x + threadIdx.x, vi = blockIdx.y;
+  if (X >= g.nx) return;
+  const int N = g.nx, h = N / 2;
+  const float cosv = g.cos_psi[vi] / 1.0f;
+  const float sinv = -g.sin_psi[vi] / 1.0f;
+  const float xxx0 = (float)(-N / 2) * cosv + (float)h * sinv + (float)h;
+  const float yyy0 = (float)(-N / 2) * sinv - (float)h * cosv + (float)h;
+  const int ys = g.cyl0[X], ye = g.cyl1[X];
+  float xx0 = xxx0 - (float)ys * sinv + (float)X * cosv;
+  float yy0 = yyy0 + (float)ys * cosv + (float)X * sinv;
+  float2 *dst = rotpos + (size_t)vi * g.fov_columns + row_start[X];
+  for (int y = ys; y < ye; y++) {
+    dst[y - ys] = make_float2(xx0, yy0);
+    xx0 -= sinv;
+    yy0 += cosv;
+  }
+}
+
+// ============================================================================
+// Input preparation + re-layout (prepare_norm/norm_ANW drv:796-1056,
+// prepare_osem3dw3 drv:1649-1818, mul/add projection simd_operation.cpp:4-58)
+// from the flat file layout into the quad layout.  One thread per (pair,
+// quad, run of planes).
+// ============================================================================
+template <typename PT, typename AT>
+__global__ void prep_kernel(DevGeom g, int nbins, const int16_t *__restrict__ prompts,
+                            const float *__restrict__ randoms, const float *__restrict__ norm,
+                            const float *__restrict__ atten, const float *__restrict__ scatter, int npskip,
+                            float eps2, PT *__restrict__ qp, AT *__restrict__ qadd, AT *__restrict__ qmult,
+                            int *__restrict__ mask_accum, int planes_per_thread) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;  // quad
+  const int vi = blockIdx.z;                            // pair
+  if (x >= g.nquads) return;
+  const int gp0 = blockIdx.y * planes_per_thread;
+  const int gp1 = min(gp0 + planes_per_thread, g.segmentsize);
+  const int V = g.nviews, half = V / 2;
+  int views[4] = {vi, vi, vi + half, vi + half};
+  int bins[4] = {x, nbins - x, x, nbins - x};
+  bool ok[4];
+  for (int l = 0; l < 4; l++) ok[l] = (bins[l] >= 0 && bins[l] < nbins && x > 0);
+  int any = 0;
+  for (int gp = gp0; gp < gp1; gp++) {
+    const int s = g.plane_seg[gp];
+    const int segoff = g.poff[s] - 2 * s - 1;
+    const int r = gp - segoff, ns = g.ytop[s] - g.ybot[s] + 1;
+    const bool kill = (r < npskip || r + npskip >= ns);
+    float pv[4], av[4], mv[4];
+    for (int l = 0; l < 4; l++) {
+      pv[l] = av[l] = mv[l] = 0.f;
+      if (!ok[l]) continue;
+      const size_t i = ((size_t)gp * V + views[l]) * nbins + bins[l];
+      const float nz = norm ? (kill ? 0.f : __ldg(norm + i)) : 1.0f;
+      const float araw = atten ? __ldg(atten + i) : 1.0f;
+      const float ac = (araw < 1.0f) ? 1.0f : araw;
+      float m;
+      if (nz > 0.0f) {
+        const float den = nz * ac;
+        m = (den > eps2) ? 1.0f / den : 0.0f;
+      } else {
+        m = nz;
+      }
+      float a = __ldg(randoms + i) * nz;
+      if (scatter) a = a + __ldg(scatter + i);
+      a = a * araw;
+      const float p = (nz == 0.0f) ? 0.f : (float)__ldg(prompts + i);
+      if (nz != 0.0f) any = 1;
+      pv[l] = p;
+      av[l] = a;
+      mv[l] = m;
+    }
+    const size_t o = ((size_t)vi * g.nquads + x) * g.pplanes + g.poff[s] + r;
+    store_p4(qp, o, pv);
+    store_p4(qadd, o, av);
+    store_p4(qmult, o, mv);
+  }
+  if (any) atomicOr(mask_accum + vi * g.nquads + x, 1);
+}
+
+__global__ void finish_mask_kernel(DevGeom g, const int *__restrict__ accum, int16_t *__restrict__ nzmask) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (g.nviews / 2) * g.nquads) return;
+  const int x = i % g.nquads;
+  nzmask[i] = (x == 0) ? 1 : (accum[i] ? 1 : 0);
+}
+
+__global__ void init_image_kernel(DevGeom g, float *__restrict__ image) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)g.nx * g.nx * g.zp;
+  if (t >= total) return;
+  const int z = (int)(t % g.zp);
+  const long long xy = t / g.zp;
+  const int X = (int)(xy / g.nx), Y = (int)(xy % g.nx);
+  const bool fov = g.cyl0[X] != g.cyl1[X] && Y >= g.cyl0[X] && Y < g.cyl1[X];
+  image[t] = (fov && z >= g.z_min && z < g.z_max) ? 1.0f : 0.0f;
+}
+
+// post-iteration pass (drv:4288-4297) with an FP64 sum, deterministic:
+// per-block partial sums, then one block adds them in order.
+__global__ void post_iter_kernel(DevGeom g, float *__restrict__ image, double *__restrict__ partial) {
+  __shared__ double red[256];
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int nz = g.z_max - g.z_min;
+  double s = 0.0;
+  if (t < (long long)g.fov_columns * nz) {
+    const int col = (int)(t / nz), z = g.z_min + (int)(t % nz);
+    const short2 xy = g.fov_xy[col];
+    float *p = image + ((size_t)xy.x * g.nx + xy.y) * g.zp + z;
+    const float v = *p;
+    s = (double)v;
+    if ((double)v < 1e-16) *p = 0.f;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if ((int)threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+__global__ void sum_partials_kernel(const double *__restrict__ partial, int n, double *__restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < n; i++) s += partial[i];
+    *out = s;
+  }
+}
+
+__global__ void rows_to_quad_kernel(DevGeom g, int nbins, const float *__restrict__ rows, float4 *__restrict__ quad,
+                                    int apply_bp_scale) {
+  const int gp = blockIdx.y, x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= g.nquads || gp >= g.segmentsize) return;
+  const int s = g.plane_seg[gp];
+  const int segoff = g.poff[s] - 2 * s - 1;
+  const int r = gp - segoff;
+  const size_t P = g.segmentsize;
+  const int xm = nbins - x;
+  float v[4] = {0.f, 0.f, 0.f, 0.f};
+  if (x > 0) {
+    v[0] = rows[(size_t)gp * nbins + x];
+    v[1] = rows[(size_t)gp * nbins + xm];
+    v[2] = rows[(P + gp) * nbins + x];
+    v[3] = rows[(P + gp) * nbins + xm];
+  }
+  if (apply_bp_scale) {
+    const float bs = g.bp_scale[s];
+    for (int l = 0; l < 4; l++) v[l] = v[l] * bs;
+  }
+  quad[(size_t)x * g.pplanes + g.poff[s] + r] = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+__global__ void quad_to_rows_kernel(DevGeom g, int nbins, const float4 *__restrict__ quad,
+                                    const QuadWork *__restrict__ work, float *__restrict__ rows) {
+  const int gp = blockIdx.x * blockDim.x + threadIdx.x;
+  const QuadWork w = work[blockIdx.y];
+  if (gp >= g.segmentsize) return;
+  const int s = g.plane_seg[gp];
+  const int segoff = g.poff[s] - 2 * s - 1;
+  const int r = gp - segoff;
+  const size_t P = g.segmentsize;
+  const int x = w.x, xm = nbins - x;
+  const float4 q = quad[(size_t)x * g.pplanes + g.poff[s] + r];
+  rows[(size_t)gp * nbins + x] = q.x;
+  rows[(size_t)gp * nbins + xm] = q.y;
+  rows[(P + gp) * nbins + x] = q.z;
+  rows[(P + gp) * nbins + xm] = q.w;
+}
+
+__global__ void quad_to_file_kernel(DevGeom g, int nbins, const float4 *__restrict__ quad, long long stride,
+                                    const QuadWork *__restrict__ work, float *__restrict__ sino) {
+  const int gp = blockIdx.x * blockDim.x + threadIdx.x;
+  const QuadWork w = work[blockIdx.y];
+  if (gp >= g.segmentsize) return;
+  const int s = g.plane_seg[gp];
+  const int r = gp - (g.poff[s] - 2 * s - 1);
+  const int x = w.x, xm = nbins - x, V = g.nviews;
+  const float4 q = quad[(size_t)w.slot * stride + (size_t)x * g.pplanes + g.poff[s] + r];
+  const size_t r0 = ((size_t)gp * V + w.view) * nbins, r1 = ((size_t)gp * V + w.view + V / 2) * nbins;
+  sino[r0 + x] = q.x;
+  sino[r0 + xm] = q.y;
+  sino[r1 + x] = q.z;
+  sino[r1 + xm] = q.w;
+}
+
+__global__ void add_partials_kernel(long long n4, const float4 *__restrict__ a, const float4 *__restrict__ b,
+                                    float4 *__restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n4) out[i] = a[i] + b[i];
+}
+
+template <typename T>
+__global__ void scale_pairs_kernel(DevGeom g, const T *__restrict__ src, const int *__restrict__ views,
+                                   float4 *__restrict__ dst, long long dst_pair_stride) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long per = (long long)g.nquads * g.pplanes;
+  if (i >= per) return;
+  const int slot = blockIdx.y;
+  const int pp = (int)(i % g.pplanes);
+  const int s = g.pplane_seg[pp];
+  const P4 m = load_p4(src, (size_t)views[slot] * per + i);
+  float4 o = f4(0.f);
+  if (s >= 0) {
+    const float bs = g.bp_scale[s];
+    o = make_float4(m.v[0] * bs, m.v[1] * bs, m.v[2] * bs, m.v[3] * bs);
+  }
+  dst[(size_t)slot * dst_pair_stride + i] = o;
+}
+
+template <int TPT, int MODE, typename PT, typename AT>
+cudaError_t launch_fp_t(const DevGeom &g, const float *image, const QuadWork *work, int nwork, const void *prompts,
+                        const void *add, float *out, long long out_pair_stride, cudaStream_t st) {
+  // split a quad's tasks over enough CTAs that each fits the launch bound
+  const int per_cta = fp_max_threads(TPT) * TPT;
+  const int nsplit = (g.nfptasks + per_cta - 1) / per_cta;
+  int threads = (g.nfptasks + nsplit * TPT - 1) / (nsplit * TPT);
+  threads = ((threads + 31) / 32) * 32;
+  if (threads > fp_max_threads(TPT) || nsplit > 8) return cudaErrorInvalidConfiguration;
+  const int ZS = g.zp + kFpZPad;
+  const size_t smem = (size_t)(2 * 8 * 2 + 2) * 2 * g.zp * sizeof(float) + (size_t)5 * ZS * sizeof(float4);
+  auto k = fp_kernel<TPT, MODE, PT, AT>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  k<<<dim3(nwork, nsplit), threads, smem, st>>>(g, image, work, (const PT *)prompts, (const AT *)add,
+                                    reinterpret_cast<float4 *>(out), out_pair_stride / 4);
+  return cudaGetLastError();
+}
+
+template <int TPT>
+cudaError_t launch_fp_tpt(const DevGeom &g, const float *image, const QuadWork *work, int nwork, int mode,
+                          const void *prompts, const void *add, int storage, float *out, long long stride,
+                          cudaStream_t st) {
+  if (mode == 0) return launch_fp_t<TPT, 0, int16_t, float>(g, image, work, nwork, nullptr, nullptr, out, stride, st);
+  if (storage == 0) return launch_fp_t<TPT, 1, int16_t, float>(g, image, work, nwork, prompts, add, out, stride, st);
+  return launch_fp_t<TPT, 1, __half, __nv_bfloat16>(g, image, work, nwork, prompts, add, out, stride, st);
+}
+
+}  // namespace
+
+cudaError_t launch_fp(const DevGeom &g, const float *image, const QuadWork *work, int nwork, int mode,
+                      const void *prompts, const void *add, int storage, float *out, long long out_pair_stride,
+                      int tasks_per_thread, cudaStream_t st) {
+  if (nwork <= 0) return cudaSuccess;
+  switch (tasks_per_thread) {
+    case 1: return launch_fp_tpt<1>(g, image, work, nwork, mode, prompts, add, storage, out, out_pair_stride, st);
+    case 2: return launch_fp_tpt<2>(g, image, work, nwork, mode, prompts, add, storage, out, out_pair_stride, st);
+    case 3: return launch_fp_tpt<3>(g, image, work, nwork, mode, prompts, add, storage, out, out_pair_stride, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
+                      float *bc, float *br, long long vol, cudaStream_t st) {
+  if (nwork <= 0) return cudaSuccess;
+  const size_t smem = (size_t)g.pplanes * sizeof(float4);
+  auto k = bp_kernel<kBpZ>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  k<<<nwork, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(in), in_pair_stride / 4, work, bc, br, vol);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rotback(const DevGeom &g, const int *pair_views, int npairs, const float *bc, const float *br,
+                           long long vol, float *image, float *nf_inv, float *corr_out, int mode, cudaStream_t st) {
+  const long long n = (long long)g.fov_columns * (g.zp / 4);
+  const int threads = 256;
+  const unsigned blocks = (unsigned)((n + threads - 1) / threads);
+  if (mode == 0)
+    rotback_kernel<0><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, corr_out);
+  else if (mode == 1)
+    rotback_kernel<1><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, corr_out);
+  else
+    rotback_kernel<2><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, corr_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rotpos(const DevGeom &g, float2 *rotpos, const int *row_start, cudaStream_t st) {
+  dim3 grid((g.nx + 127) / 128, g.nviews / 2);
+  rotpos_kernel<<<grid, 128, 0, st>>>(g, rotpos, row_start);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prep(const DevGeom &g, int nbins, const int16_t *prompts, const float *randoms, const float *norm,
+                        const float *atten, const float *scatter, int npskip, float eps2, int storage, void *q_prompts,
+                        void *q_add, void *q_mult, int *quad_mask_accum, cudaStream_t st) {
+  const int ppt = 32;
+  dim3 grid((g.nquads + 127) / 128, (g.segmentsize + ppt - 1) / ppt, g.nviews / 2);
+  if (storage == 0)
+    prep_kernel<int16_t, float><<<grid, 128, 0, st>>>(g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2,
+                                                      (int16_t *)q_prompts, (float *)q_add, (float *)q_mult,
+                                                      quad_mask_accum, ppt);
+  else
+    prep_kernel<__half, __nv_bfloat16><<<grid, 128, 0, st>>>(
+        g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (__half *)q_prompts, (__nv_bfloat16 *)q_add,
+        (__nv_bfloat16 *)q_mult, quad_mask_accum, ppt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale_pairs(const DevGeom &g, const void *src, int storage, const int *views, int npairs,
+                               float *dst, long long dst_pair_stride, cudaStream_t st) {
+  const long long per = (long long)g.nquads * g.pplanes;
+  dim3 grid((unsigned)((per + 255) / 256), npairs);
+  if (storage == 0)
+    scale_pairs_kernel<float><<<grid, 256, 0, st>>>(g, (const float *)src, views, reinterpret_cast<float4 *>(dst),
+                                                    dst_pair_stride / 4);
+  else
+    scale_pairs_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(g, (const __nv_bfloat16 *)src, views,
+                                                            reinterpret_cast<float4 *>(dst), dst_pair_stride / 4);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finish_mask(const DevGeom &g, const int *accum, int16_t *nzmask, cudaStream_t st) {
+  const int n = (g.nviews / 2) * g.nquads;
+  finish_mask_kernel<<<(n + 255) / 256, 256, 0, st>>>(g, accum, nzmask);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init_image(const DevGeom &g, float *image, cudaStream_t st) {
+  const long long n = (long long)g.nx * g.nx * g.zp;
+  init_image_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, image);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_post_iteration(const DevGeom &g, float *image, double *partial, double *sum, cudaStream_t st) {
+  const long long n = (long long)g.fov_columns * (g.z_max - g.z_min);
+  const int blocks = (int)((n + 255) / 256);
+  post_iter_kernel<<<blocks, 256, 0, st>>>(g, image, partial);
+  sum_partials_kernel<<<1, 32, 0, st>>>(partial, blocks, sum);
+  return cudaGetLastError();
+}
+
+int post_iteration_blocks(const DevGeom &g) {
+  const long long n = (long long)g.fov_columns * (g.z_max - g.z_min);
+  return (int)((n + 255) / 256);
+}
+
+cudaError_t launch_rows_to_quad(const DevGeom &g, int nbins, const float *rows, float *quad, int apply_bp_scale,
+                                cudaStream_t st) {
+  dim3 grid((g.nquads + 127) / 128, g.segmentsize);
+  rows_to_quad_kernel<<<grid, 128, 0, st>>>(g, nbins, rows, reinterpret_cast<float4 *>(quad), apply_bp_scale);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_quad_to_rows(const DevGeom &g, int nbins, const float *quad, const QuadWork *work, int nwork,
+                                float *rows, cudaStream_t st) {
+  if (nwork <= 0) return cudaSuccess;
+  dim3 grid((g.segmentsize + 255) / 256, nwork);
+  quad_to_rows_kernel<<<grid, 256, 0, st>>>(g, nbins, reinterpret_cast<const float4 *>(quad), work, rows);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_quad_to_file(const DevGeom &g, int nbins, const float *quad, long long quad_pair_stride,
+                                const QuadWork *work, int nwork, float *sino, cudaStream_t st) {
+  if (nwork <= 0) return cudaSuccess;
+  dim3 grid((g.segmentsize + 255) / 256, nwork);
+  quad_to_file_kernel<<<grid, 256, 0, st>>>(g, nbins, reinterpret_cast<const float4 *>(quad), quad_pair_stride / 4,
+                                            work, sino);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_add_partials(const DevGeom &g, const float *bc, const float *br, float *out, cudaStream_t st) {
+  const long long n4 = (long long)g.nx * g.nx * g.zp / 4;
+  add_partials_kernel<<<(unsigned)((n4 + 255) / 256), 256, 0, st>>>(n4, reinterpret_cast<const float4 *>(bc),
+                                                                     reinterpret_cast<const float4 *>(br),
+                                                                     reinterpret_cast<float4 *>(out));
+  return cudaGetLastError();
+}
+
+}  // namespace hrrt

@@ -1,0 +1,115 @@
+// kernels.cuh -- device tables and kernel launchers of the OSEM hot path.
+//
+// Data layouts on the device
+//   image, nf_inv, Bc, Br : [x][y][zp] float, z fastest (the reference's
+//                           image[x][y][z], z padded to a multiple of 4).
+//   "quad layout"         : one view pair p (views p and p+nviews/2) and one
+//                           radial "quad" x in [0, nbins/2] hold 4 lanes
+//                             lane 0 = (view p,           bin x)
+//                             lane 1 = (view p,           bin nbins-x)
+//                             lane 2 = (view p+nviews/2,  bin x)
+//                             lane 3 = (view p+nviews/2,  bin nbins-x)
+//                           stored as [pair][x][padded plane][lane] with every
+//                           segment padded by one zero plane on each side.
+//                           This is the reference's packed prjbuf[x][k][yr][4]
+//                           (hrrt_osem3dv_sbrt_span3.cpp:1397-1436, :1654-1693)
+//                           made contiguous per quad, so FP output, ratio and
+//                           BP input stream with 16-byte accesses.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <cstdint>
+
+namespace hrrt {
+
+constexpr int kFpPlanes = 9;    // planes per forward-projection task (odd: bank-conflict free)
+constexpr int kFpZPad = 16;     // zeroed entries after each sampled row
+constexpr int kFpEndPlanes = 4; // planes per end-plane task (they cost ~2x a middle plane)
+constexpr int kBpZ = 8;         // z per back-projection task
+
+struct FpTask {
+  int16_t seg;   // segment (internal = file order)
+  int16_t p0;    // first plane, relative to the segment's yr_bottom
+  int16_t n;     // planes in this task (<= kFpPlanes)
+  int16_t type;  // 0: segment 0, 1: oblique middle planes, 2: oblique end planes
+};
+
+struct FpMid {   // middle-plane sampling of group g at rotated row y < c (sbrt:1933-1947)
+  int z;         // int(yr_m + (y-c)*tan), yr_m = yr_bottom + zshift; < 0 => group skipped
+  float f;       // its fraction (coef1)
+  int z2;        // int(yr_m + (c-y)*tan)
+  float f2;      // its fraction (coef2)
+};
+
+struct BpLut {   // blookup (sbrt:672-700) in direct form: yr = z + d for z in [zs, ze]
+  int zs, ze, d;
+  float f;
+};
+
+struct DevGeom {
+  int nx, nz, zp, c, nseg, groupmax, zshift, segmentsize, pplanes, nviews, nquads;
+  int fov_columns, z_min, z_max;
+  float y_size, eps1, eps3, image_max;
+  const int16_t *cyl0, *cyl1;       // [ny]
+  const int *ybot, *ytop, *poff;    // [nseg]; poff = padded offset of plane yr_bottom
+  const float *rescale;             // [groupmax][nz]
+  const float *bp_scale;            // [nseg]
+  const FpMid *fpmid;               // [c][groupmax]
+  const int *fl_zzi;                // [ny][groupmax*2*zshift]
+  const float *fl_zzz0;
+  const BpLut *bplut;               // [groupmax][ny]
+  const int16_t *nzmask;            // [nviews/2][nquads]
+  const float *sin_psi, *cos_psi;   // [nviews]
+  const short2 *fov_xy;             // [fov_columns]
+  const float2 *rotpos;             // [nviews/2][fov_columns] rotate-back sample points
+  const FpTask *fptasks;
+  int nfptasks;
+  const int16_t *plane_seg;         // [segmentsize] segment of each global plane
+  const int16_t *pplane_seg;        // [pplanes] segment of each padded plane, -1 on pads
+  int *err;                         // device status word: non-zero after a bounded wait gave up
+};
+
+struct QuadWork {  // one (view pair slot, quad) work item
+  int16_t slot;    // pair slot within the batch
+  int16_t x;       // quad
+  int16_t view;    // first view of the pair
+  int16_t pad;
+};
+
+// ---- launchers (kernels.cu) ----
+// forward projection of the pairs listed in `work` (mode 0: write est*scale into
+// `out`; mode 1: write ratio*bp_scale using prompts/add at their global pair).
+cudaError_t launch_fp(const DevGeom &g, const float *image, const QuadWork *work, int nwork, int mode,
+                      const void *prompts, const void *add, int storage, float *out, long long out_pair_stride,
+                      int tasks_per_thread, cudaStream_t st);
+// back projection of quad-layout input into the column (Bc) / row (Br) partials
+cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
+                      float *bc, float *br, long long vol, cudaStream_t st);
+// corr = sum over pairs of rotate-back(Bc+Br); mode 0: OSEM update of image with
+// nf_inv; mode 1: write the inverse sensitivity into nf_inv; mode 2: corr_out += corr
+cudaError_t launch_rotback(const DevGeom &g, const int *pair_views, int npairs, const float *bc, const float *br,
+                           long long vol, float *image, float *nf_inv, float *corr_out, int mode, cudaStream_t st);
+cudaError_t launch_rotpos(const DevGeom &g, float2 *rotpos, const int *row_start, cudaStream_t st);
+cudaError_t launch_prep(const DevGeom &g, int nbins, const int16_t *prompts, const float *randoms, const float *norm,
+                        const float *atten, const float *scatter, int npskip, float eps2, int storage, void *q_prompts,
+                        void *q_add, void *q_mult, int *quad_mask_accum, cudaStream_t st);
+cudaError_t launch_finish_mask(const DevGeom &g, const int *accum, int16_t *nzmask, cudaStream_t st);
+cudaError_t launch_init_image(const DevGeom &g, float *image, cudaStream_t st);
+cudaError_t launch_post_iteration(const DevGeom &g, float *image, double *partial, double *sum, cudaStream_t st);
+int post_iteration_blocks(const DevGeom &g);
+// copy the quad-layout 1/(NA) of `npairs` view pairs into f32 scratch, times
+// the back projector's segment weight (sbrt:1637-1649 applied in place there)
+cudaError_t launch_scale_pairs(const DevGeom &g, const void *src, int storage, const int *views, int npairs,
+                               float *dst, long long dst_pair_stride, cudaStream_t st);
+// quad-layout <-> reference rows [2*segmentsize][nbins]
+cudaError_t launch_rows_to_quad(const DevGeom &g, int nbins, const float *rows, float *quad, int apply_bp_scale,
+                                cudaStream_t st);
+cudaError_t launch_quad_to_rows(const DevGeom &g, int nbins, const float *quad, const QuadWork *work, int nwork,
+                                float *rows, cudaStream_t st);
+// scatter the quad-layout estimates of a batch of pairs into a flat-file sinogram
+cudaError_t launch_quad_to_file(const DevGeom &g, int nbins, const float *quad, long long quad_pair_stride,
+                                const QuadWork *work, int nwork, float *sino, cudaStream_t st);
+cudaError_t launch_add_partials(const DevGeom &g, const float *bc, const float *br, float *out, cudaStream_t st);
+
+}  // namespace hrrt

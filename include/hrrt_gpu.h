@@ -1,0 +1,190 @@
+/*
+ * hrrt_gpu.h -- C ABI of libhrrt_gpu.so, the B200 (sm_100a) implementation of
+ * the 3D OSEM hot path of hrrt_osem3d (andrewcrabb/hrrt_reconstruction).
+ *
+ * Conventions
+ *   - Every call returns 0 (HRRT_OK) on success and a negative hrrt_status on
+ *     failure; hrrt_last_error() then describes the failure.  Nothing in the
+ *     library calls exit().
+ *   - Host buffers are owned by the caller and never retained.
+ *   - One context serves one host thread at a time.  All device work of a
+ *     context runs in order on that context's CUDA stream; calls that return
+ *     host data synchronise that stream.
+ *   - Sinogram arrays use the reference flat-file layout
+ *       [segment in file order][plane][view][radial bin]   (bins fastest),
+ *     i.e. what hrrt_osem3d reads with -p/-d/-n/-a/-s
+ *     (hrrt_osem3d/file_io_processor.cpp:144-294).
+ *   - Image arrays handed to the projector entry points use the reference's
+ *     in-memory layout image[x][y][z] with z padded to a multiple of 4
+ *     (hrrt_info.zp); hrrt_get_image returns the on-disk [z][y][x] layout of
+ *     SaveImage (hrrt_osem3d/hrrt_osem3d_span3.cpp:4020-4043).
+ *   - Sinogram rows handed to hrrt_fp_pair / hrrt_bp_pair use the reference's
+ *     per-view-pair layout prj[2*segmentsize][nbins]: rows [0,segmentsize) are
+ *     view v, rows [segmentsize,2*segmentsize) view v+nviews/2
+ *     (hrrt_osem3d_span3.cpp:2062-2095, :2145-2154).
+ */
+#ifndef HRRT_GPU_H
+#define HRRT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  HRRT_OK = 0,
+  HRRT_ERR_ARG = -1,      /* invalid argument or size */
+  HRRT_ERR_CUDA = -2,     /* CUDA runtime error */
+  HRRT_ERR_STATE = -3,    /* call made in the wrong order */
+  HRRT_ERR_NOMEM = -4,    /* device allocation failed */
+  HRRT_ERR_DEVICE = -5    /* a device-side check reported an error */
+} hrrt_status;
+
+/* storage types of the sinogram-shaped inputs on the device */
+enum {
+  HRRT_STORE_F32 = 0,     /* prompts int16, 1/(NA) and additive term float32 (the reference) */
+  HRRT_STORE_16 = 1       /* prompts fp16 (exact integers), 1/(NA) and additive term bf16 */
+};
+
+/* back projector variants */
+enum {
+  HRRT_BP_REF = 0         /* voxel-driven sinogram interpolation of the reference */
+};
+
+/*
+ * Scanner, sinogram and reconstruction parameters.  Field meanings follow the
+ * reference: ScannerModel (hrrt_osem3d/scanner_model.h:3-16), the -m span,maxdel
+ * -S subsets -f rel_fov,..,z_min,z_max -k npskip -e eps1,eps2,eps3 -u image_max
+ * flags (hrrt_osem3d_span3.cpp:3154-3355) and their defaults (:371-374).
+ */
+typedef struct hrrt_geom {
+  int nrings;          /* direct planes: 104 */
+  int nelements;       /* radial bins: 256 */
+  int nangles;         /* views: 288 */
+  float ring_radius;   /* mm: 234.5 */
+  float plane_sep;     /* mm: 1.21875 */
+  float binsize;       /* mm: 1.21875 */
+  int span;            /* 3 or 9 */
+  int maxdel;          /* 67 */
+  int subsets;         /* 16 */
+  float rel_fov;       /* 0.95 */
+  int z_min, z_max;    /* 6, 200 */
+  int npskip;          /* 3 */
+  float epsilon1, epsilon2, epsilon3, image_max;  /* 5e-2, 1e-2, 1e-10, 1e4 */
+} hrrt_geom;
+
+typedef struct hrrt_info {
+  int nx, ny, nz, zp;        /* image grid; zp = padded z */
+  int nbins, nviews;
+  int nseg, groupmax, segmentsize;
+  int subsets, sviews;
+  int fov_columns;
+  long long sino_elems;      /* segmentsize*nviews*nbins */
+  long long image_elems;     /* nx*ny*zp */
+} hrrt_info;
+
+typedef struct hrrt_stats {
+  double sum_image;          /* post-iteration sum over the FOV, z in [z_min,z_max), FP64 */
+  int subset_iterations;     /* completed */
+  float ms_total;            /* device time of the OSEM loop (CUDA events) */
+} hrrt_stats;
+
+typedef struct hrrt_ctx hrrt_ctx;
+
+/* HRRT model 999 (scanner_model.cpp:124) at span 9, maxdel 67, 16 subsets */
+void hrrt_geom_default(hrrt_geom *g);
+
+/* Replaces GetScannerParameter + dependencies (hrrt_osem3d_span3.cpp:3452-3551,
+ * hrrt_osem3dv_sbrt_span3.cpp:199-800): builds all tables on `device`. */
+int hrrt_ctx_create(const hrrt_geom *g, int device, hrrt_ctx **out);
+void hrrt_ctx_destroy(hrrt_ctx *ctx);
+const char *hrrt_last_error(const hrrt_ctx *ctx);
+int hrrt_get_info(const hrrt_ctx *ctx, hrrt_info *info);
+/* the context's CUDA stream (a cudaStream_t) for callers that time or order work */
+void *hrrt_get_stream(hrrt_ctx *ctx);
+
+/*
+ * Replaces PrepareNormfac + PrepareOsem3dFiles for OP-OSEM (-W 3): prepare_norm
+ * + norm_ANW (hrrt_osem3d_span3.cpp:796-1056) and prepare_osem3dw3 (:1649-1818)
+ * with 3D attenuation (Atten3D).  Builds on the device
+ *   1/(N*max(A,1)) (0 where N*A <= eps2),  (d*N + s)*A,  prompts zeroed where N==0,
+ *   and the norm-zero quad mask,
+ * with N's first/last npskip planes of each segment set to 0 when a norm is
+ * given (file_io_processor.cpp:168-172).  norm/atten/scatter may be NULL
+ * (N=1, A=1, s=0).  `storage` is HRRT_STORE_F32 or HRRT_STORE_16.
+ */
+int hrrt_upload_inputs(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms, const float *norm,
+                       const float *atten, const float *scatter, int storage);
+
+/* Replaces CalculateNormfac (hrrt_osem3d_span3.cpp:3760-3865) with -N: the
+ * per-subset inverse sensitivity images stay on the device. */
+int hrrt_sensitivity(hrrt_ctx *ctx);
+
+/* Replaces Init_Image (hrrt_osem3d_span3.cpp:3958-4006).  image_zyx NULL: 1 in
+ * the FOV for z in [z_min,z_max), else 0; otherwise a flat [z][y][x] image
+ * (the -i input, read without flip). */
+int hrrt_init_image(hrrt_ctx *ctx, const float *image_zyx);
+
+/* Replaces CalculateOsem3d (hrrt_osem3d_span3.cpp:4098-4341) for OP-OSEM:
+ * `iterations` full passes over the subsets in sequence() order. */
+int hrrt_osem(hrrt_ctx *ctx, int iterations, hrrt_stats *stats);
+
+/* Run `count` subset-iterations starting at position `first` of the subset
+ * order (wrapping), without the post-iteration pass; for benchmarking. */
+int hrrt_osem_subsets(hrrt_ctx *ctx, int first, int count);
+
+/* Image out in the SaveImage layout [z][y][x] (nz*ny*nx floats). */
+int hrrt_get_image(hrrt_ctx *ctx, float *image_zyx);
+/* Image in/out in the internal layout [x][y][zp]. */
+int hrrt_get_image_xyz(hrrt_ctx *ctx, float *image_xyz);
+int hrrt_set_image_xyz(hrrt_ctx *ctx, const float *image_xyz);
+/* Inverse sensitivity of one subset, [x][y][zp]. */
+int hrrt_get_sensitivity(hrrt_ctx *ctx, int subset, float *nf_inv_xyz);
+/* Quad mask [nviews/2][nbins/2+1] (norm_zero_mask, sbrt:333, drv:899-909). */
+int hrrt_get_norm_zero_mask(hrrt_ctx *ctx, int16_t *mask);
+int hrrt_set_norm_zero_mask(hrrt_ctx *ctx, const int16_t *mask);
+
+/* Replaces forward_proj3d_thread1 (hrrt_osem3dv_sbrt_span3.cpp:1373-1446):
+ * forward-projects image_xyz into the two views (view, view+nviews/2).  Rows
+ * and bins the reference leaves unwritten (bin 0, columns outside the FOV,
+ * masked quads) keep the caller's values. */
+int hrrt_fp_pair(hrrt_ctx *ctx, const float *image_xyz, int view, float *prj);
+
+/* Replaces the forward projection of Output_CorrectedScan
+ * (hrrt_osem3d_span3.cpp:3624-3723, the -I 0 -h mode): forward-projects
+ * image_xyz for every view pair into a full flat-file sinogram (zeros where the
+ * reference writes nothing). */
+int hrrt_forward_project(hrrt_ctx *ctx, const float *image_xyz, float *sino);
+
+/* Replaces back_proj3d_thread1 (sbrt:1622-1699): back-projects prj (not
+ * modified) for (view, view+nviews/2) into the rotated frame buffer
+ * imagebuf_xyz [x][y][zp] (overwritten). */
+int hrrt_bp_pair(hrrt_ctx *ctx, const float *prj, int view, float *imagebuf_xyz, int mode);
+
+/* Replaces rotate_image_buf (sbrt:1701-1725) for one view: corr_xyz +=
+ * rotate-back(imagebuf_xyz). */
+int hrrt_rotate_add(hrrt_ctx *ctx, const float *imagebuf_xyz, int view, float *corr_xyz);
+
+/* Host-only (no GPU needed): copy one geometry table built for `g` into `out`
+ * (capacity `bytes`); returns the table's size in bytes, or a negative status.
+ * Names: "cylwiny" (int16 [ny][2]), "segments" (int32 [3][nseg]: yr_bottom,
+ * yr_top, segment_offset), "sin_theta", "cos_theta", "sin_psi", "cos_psi",
+ * "tantheta", "rescale" (float [groupmax][nz]), "flookup_zzi" (int32),
+ * "flookup_zzz0" (float) [ny][groupmax*2*(span-1)], "blookup" (int32
+ * [ny][groupmax][3]: zsa, zea, yra), "blookup_yr2a" (float [ny][groupmax]),
+ * "bp_scale" (float [nseg]), "order" (int16 [subsets]).  Used to pin the
+ * tables against the reference's dependencies(). */
+long long hrrt_geometry_table(const hrrt_geom *g, const char *name, void *out, size_t bytes);
+
+/* Device kernel timing: enable per-kernel CUDA-event timing on the context
+ * stream, and read back launches / total milliseconds per kernel name. */
+int hrrt_set_profiling(hrrt_ctx *ctx, int enable);
+int hrrt_kernel_stats(hrrt_ctx *ctx, const char *kernel, int *launches, double *total_ms);
+int hrrt_reset_kernel_stats(hrrt_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HRRT_GPU_H */
