@@ -145,13 +145,23 @@ std::vector<FpTask> build_fp_tasks(const Geometry &g) {
     const int ns = g.yr_top[s] - g.yr_bottom[s] + 1;
     for (int p0 = g.zshift; p0 < ns - g.zshift; p0 += kFpPlanes)
       mid.push_back(FpTask{(int16_t)s, (int16_t)p0, (int16_t)std::min(kFpPlanes, ns - g.zshift - p0), 1});
+    // an end-plane run stays inside one end region, so its lookup entries are consecutive
     for (int p0 = 0; p0 < g.zshift; p0 += kFpEndPlanes)
       ends.push_back(FpTask{(int16_t)s, (int16_t)p0, (int16_t)std::min(kFpEndPlanes, g.zshift - p0), 2});
     for (int p0 = ns - g.zshift; p0 < ns; p0 += kFpEndPlanes)
       ends.push_back(FpTask{(int16_t)s, (int16_t)p0, (int16_t)std::min(kFpEndPlanes, ns - p0), 2});
   }
-  mid.insert(mid.end(), ends.begin(), ends.end());
-  return mid;
+  // one task kind per warp (the kinds cost different amounts per row, and a
+  // warp mixing them would set the pace of every row barrier): pad each kind
+  // to a multiple of 32 with empty tasks
+  std::vector<FpTask> t0, t1;
+  for (const FpTask &t : mid) (t.type == 0 ? t0 : t1).push_back(t);
+  std::vector<FpTask> out;
+  for (auto *lst : {&t0, &t1, &ends}) {
+    out.insert(out.end(), lst->begin(), lst->end());
+    while (out.size() % 32) out.push_back(FpTask{0, 0, 0, -1});
+  }
+  return out;
 }
 
 // Every shared-memory index the forward projector can form for this geometry
@@ -164,6 +174,7 @@ std::string validate_fp(const Geometry &g, const std::vector<FpMid> &mid, const 
     if (g.cyl0[x] != g.cyl1[x]) ymin = std::min<int>(ymin, g.cyl0[x]);
   for (int y = ymin; y < g.c; y++) {
     for (const FpTask &t : tasks) {
+      if (t.type < 0) continue;
       if (t.type == 0) {
         if (t.p0 + kFpPlanes >= ZS) return "fp: segment-0 window out of range";
         continue;
@@ -386,17 +397,37 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
   std::vector<int16_t> plane_seg(g.segmentsize);
   for (int s = 0; s < g.nseg; s++)
     for (int r = 0; r <= g.yr_top[s] - g.yr_bottom[s]; r++) plane_seg[g.segment_offset[s] + r] = (int16_t)s;
+  // back-projection shared-memory layout: every segment with kBpPad zero
+  // planes on each side; bp_src[i] = quad-layout plane of shared plane i or -1
+  std::vector<int> bp_soff(g.nseg), bp_src;
+  for (int s = 0; s < g.nseg; s++) {
+    const int ns = g.yr_top[s] - g.yr_bottom[s] + 1;
+    for (int k = 0; k < kBpPad; k++) bp_src.push_back(-1);
+    bp_soff[s] = (int)bp_src.size();
+    for (int r = 0; r < ns; r++) bp_src.push_back(g.padded_offset(s) + r);
+    for (int k = 0; k < kBpPad; k++) bp_src.push_back(-1);
+  }
+  // no back-projection window may run past its segment's zero planes
+  for (int y = 1; y < g.ny; y++)
+    for (int gg = 0; gg < g.groupmax; gg++) {
+      const size_t i = (size_t)y * g.groupmax + gg;
+      const int zs = g.bl_zsa[i], ze = g.bl_zea[i], d = g.bl_yra[i] - g.bl_zsa[i];
+      const int yb = g.yr_bottom[2 * gg + 2], yt = g.yr_top[2 * gg + 2];
+      if (ze < zs) return bail(fail(ctx, HRRT_ERR_ARG, "bp: empty plane range"));
+      const int z_lo = (zs / kBpZ) * kBpZ, z_hi = (ze / kBpZ) * kBpZ + kBpZ - 1;
+      if (z_lo + d < yb - kBpPad || z_hi + d + 1 > yt + kBpPad) return bail(fail(ctx, HRRT_ERR_ARG, "bp: padding"));
+    }
   std::vector<FpTask> tasks = build_fp_tasks(g);
   m = validate_fp(g, mid, tasks);
   if (!m.empty()) return bail(fail(ctx, HRRT_ERR_ARG, m));
   // one task per thread; a quad with more tasks than a CTA's launch bound is
   // split over several CTAs (each samples the quad's rows itself)
   ctx->tpt = 1;
-  if (tasks.size() > 8 * 448) return bail(fail(ctx, HRRT_ERR_ARG, "geometry has too many projection tasks"));
+  if (tasks.size() > 30 * 32) return bail(fail(ctx, HRRT_ERR_ARG, "geometry has too many projection tasks"));
   if (g.zp % kBpZ != 0) return bail(fail(ctx, HRRT_ERR_ARG, "padded z must be a multiple of 8"));
   for (int x = 1; x <= g.c; x++)
     if (g.cyl0[x] != g.cyl1[x] && g.cyl0[x] < 1) return bail(fail(ctx, HRRT_ERR_ARG, "FOV reaches the grid edge"));
-  if ((size_t)g.padded_planes() * 16 > 200 * 1024)
+  if ((size_t)bp_src.size() * 16 > 200 * 1024)
     return bail(fail(ctx, HRRT_ERR_ARG, "sinogram quad exceeds shared memory"));
 
   DevGeom &d = ctx->dg;
@@ -426,8 +457,13 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
   d.rescale = dupload(ctx, g.rescale, &e);
   d.bp_scale = dupload(ctx, g.bp_scale, &e);
   d.fpmid = dupload(ctx, mid, &e);
-  d.fl_zzi = dupload(ctx, g.fl_zzi, &e);
-  d.fl_zzz0 = dupload(ctx, g.fl_zzz0, &e);
+  std::vector<int2> flzf(g.fl_zzi.size());
+  for (size_t i = 0; i < flzf.size(); i++) {
+    int bits;
+    std::memcpy(&bits, &g.fl_zzz0[i], 4);
+    flzf[i] = make_int2(g.fl_zzi[i], bits);
+  }
+  d.fl_zf = dupload(ctx, flzf, &e);
   d.bplut = dupload(ctx, bpl, &e);
   d.sin_psi = dupload(ctx, g.sin_psi, &e);
   d.cos_psi = dupload(ctx, g.cos_psi, &e);
@@ -439,6 +475,9 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
   for (int s = 0; s < g.nseg; s++)
     for (int r = 0; r <= g.yr_top[s] - g.yr_bottom[s]; r++) pplane_seg[g.padded_offset(s) + r] = (int16_t)s;
   d.pplane_seg = dupload(ctx, pplane_seg, &e);
+  d.bp_soff = dupload(ctx, bp_soff, &e);
+  d.bp_src = dupload(ctx, bp_src, &e);
+  d.bp_splanes = (int)bp_src.size();
   ctx->d_rowstart = dupload(ctx, rowstart, &e);
   d.err = dalloc<int>(ctx, 1, &e);
   ctx->nzmask = g.norm_zero_mask;

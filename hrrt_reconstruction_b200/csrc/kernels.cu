@@ -16,9 +16,6 @@ __device__ __forceinline__ float4 f4(float v) { return make_float4(v, v, v, v); 
 __device__ __forceinline__ float4 operator+(float4 a, float4 b) {
   return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
 }
-__device__ __forceinline__ float4 operator-(float4 a, float4 b) {
-  return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
-}
 __device__ __forceinline__ float4 operator*(float4 a, float s) {
   return make_float4(a.x * s, a.y * s, a.z * s, a.w * s);
 }
@@ -69,6 +66,60 @@ __device__ __forceinline__ void store_p4(__nv_bfloat16 *p, size_t i, const float
   reinterpret_cast<uint2 *>(p)[i] = u;
 }
 
+
+
+// ---- packed pairs of IEEE single-precision values (sm_100 f32x2) ----
+// Each op is element-wise round-to-nearest, exactly the scalar add/sub/mul of
+// the reference, two values per instruction.  A quad value (4 lanes) is two
+// pairs: lanes (0,1) and (2,3).
+struct Q2 {
+  uint64_t lo, hi;
+};
+__device__ __forceinline__ uint64_t pk(float a, float b) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1,%2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ float2 upk(uint64_t v) {
+  float2 r;
+  asm("mov.b64 {%0,%1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+__device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+  uint64_t r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+// a + p where p is a packed product: done as two scalar adds.  The code
+// generator contracts a packed multiply that feeds a packed add into a fused
+// multiply-add (which rounds once instead of twice), even with -fmad=false and
+// explicit .rn; a scalar add of the product's halves is left alone.
+__device__ __forceinline__ uint64_t addp(uint64_t a, uint64_t p) {
+  const float2 x = upk(a), y = upk(p);
+  return pk(__fadd_rn(x.x, y.x), __fadd_rn(x.y, y.y));
+}
+__device__ __forceinline__ Q2 ldq(const float4 *p) {
+  const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(p);
+  return Q2{v.x, v.y};
+}
+__device__ __forceinline__ Q2 qadd(Q2 a, Q2 b) { return Q2{add2(a.lo, b.lo), add2(a.hi, b.hi)}; }
+__device__ __forceinline__ Q2 qsub(Q2 a, Q2 b) { return Q2{sub2(a.lo, b.lo), sub2(a.hi, b.hi)}; }
+__device__ __forceinline__ Q2 qmul(Q2 a, uint64_t s) { return Q2{mul2(a.lo, s), mul2(a.hi, s)}; }
+__device__ __forceinline__ Q2 qaddp(Q2 a, Q2 p) { return Q2{addp(a.lo, p.lo), addp(a.hi, p.hi)}; }
+__device__ __forceinline__ float4 q2f(Q2 q) {
+  const float2 a = upk(q.lo), b = upk(q.hi);
+  return make_float4(a.x, a.y, b.x, b.y);
+}
 
 // ---- TMA bulk copies + mbarrier (sm_90+ async proxy) ----
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -160,26 +211,56 @@ __device__ __forceinline__ float bilinear(const float *__restrict__ img, const S
 // (y,N-x)), then every thread accumulates its own (segment, plane-run) outputs
 // for all four lanes, row by row in the reference's order.
 // ============================================================================
-constexpr int fp_max_threads(int tpt) { return tpt == 1 ? 448 : (tpt == 2 ? 512 : 320); }
-constexpr int fp_min_blocks(int tpt) { return tpt == 1 ? 2 : 1; }
+// named barriers (id 0 is __syncthreads); ids are immediates so the kernel
+// reserves only the barriers it uses
+template <int ID>
+__device__ __forceinline__ void bar_sync_id(int count) {
+  asm volatile("bar.sync %0, %1;" ::"n"(ID), "r"(count) : "memory");
+}
+template <int ID>
+__device__ __forceinline__ void bar_arrive_id(int count) {
+  asm volatile("bar.arrive %0, %1;" ::"n"(ID), "r"(count) : "memory");
+}
+__device__ __forceinline__ void bar_sync(int id, int count) {
+  switch (id) {
+    case 1: bar_sync_id<1>(count); break;
+    case 2: bar_sync_id<2>(count); break;
+    case 3: bar_sync_id<3>(count); break;
+    case 4: bar_sync_id<4>(count); break;
+    default: bar_sync_id<5>(count); break;
+  }
+}
+__device__ __forceinline__ void bar_arrive(int id, int count) {
+  switch (id) {
+    case 1: bar_arrive_id<1>(count); break;
+    case 2: bar_arrive_id<2>(count); break;
+    case 3: bar_arrive_id<3>(count); break;
+    default: bar_arrive_id<4>(count); break;
+  }
+}
+constexpr int kBarFull = 1;   // + slot: sampled row ready (producers arrive, consumers wait)
+constexpr int kBarEmpty = 3;  // + slot: sampled row consumed (consumers arrive, producers wait)
+constexpr int kBarProd = 5;   // producers only: corner slot read by every producer
 
-template <int TPT, int MODE, typename PT, typename AT>
-__global__ void __launch_bounds__(fp_max_threads(TPT), fp_min_blocks(TPT)) fp_kernel(
-    DevGeom g, const float *__restrict__ image, const QuadWork *__restrict__ work, const PT *__restrict__ prompts,
-    const AT *__restrict__ add, float4 *__restrict__ out, long long out_pair_stride) {
-  // shared memory: [2 slots][8 points][2 column pairs][2*zp] corner columns,
-  // [2 slots][2 halves][ZS] sampled rows, [ZS] centre column
+template <int MODE, typename PT, typename AT>
+__global__ void __launch_bounds__(1024, 1) fp_kernel(DevGeom g, const float *__restrict__ image,
+                                                     const QuadWork *__restrict__ work,
+                                                     const PT *__restrict__ prompts, const AT *__restrict__ add,
+                                                     float4 *__restrict__ out, long long out_pair_stride,
+                                                     int nprod_warps) {
+  // shared memory: [2 slots][8 points][2 column pairs][2*zp] staged corner
+  // columns, 2*cpair zeros (the corners of outside points), [2 slots][2 halves]
+  // [ZS] sampled rows, [ZS] centre column
   extern __shared__ float4 smem[];
   const int ZS = g.zp + kFpZPad;
   const int zp = g.zp;
+  const int cpair = 2 * zp;  // floats per column pair
   float *corners = reinterpret_cast<float *>(smem);
-  const int cpair = 2 * zp;                       // floats per column pair
-  float4 *rows = smem + (size_t)(2 * 8 * 2 + 2) * cpair / 4;  // [2][2][ZS]
-  float4 *cen = rows + 4 * ZS;
-  // 2*cpair zeros after the corner slots: the corner pairs of outside points
   const int zoff = 2 * 8 * 2 * cpair;
   float *zcol = corners + zoff;
-  __shared__ float4 s_coef[2][8];
+  float4 *rows = smem + (size_t)(2 * 8 * 2 + 2) * cpair / 4;  // [2][2][ZS]
+  float4 *cen = rows + 4 * ZS;
+  __shared__ ulonglong2 s_w[2][4][2];
   __shared__ int s_off[2][8];
   __shared__ __align__(8) uint64_t s_bar[2];
 
@@ -190,12 +271,15 @@ __global__ void __launch_bounds__(fp_max_threads(TPT), fp_min_blocks(TPT)) fp_ke
   const int ystart = g.cyl0[x];
   const int nrows = c - ystart;
   const int tid = threadIdx.x, nthr = blockDim.x;
+  const int nprod = nprod_warps * 32;   // producer threads: [ncons, nthr)
+  const int ncons = nthr - nprod;        // consumer threads: one task each
+  const bool producer = tid >= ncons;
+  const int ptid = tid - ncons;
 
-  // TMA producer (lanes 0-7 of warp 0, one sample point each): the two
-  // contiguous column pairs (ix, iy..iy+1) and (ix+1, iy..iy+1) of each inside
-  // point of row r; outside points read a zero column with zero weights
+  // TMA issue (producer lanes 0-7, one sample point each): the two contiguous
+  // column pairs (ix, iy..iy+1) and (ix+1, iy..iy+1) of each inside point
   auto issue_row = [&](int r) {
-    const int sl = r & 1, y = ystart + r, l = tid;  // tid < 8
+    const int sl = r & 1, y = ystart + r, l = ptid;
     int a, b;
     switch (l) {
       case 0: a = x; b = y; break;
@@ -209,8 +293,14 @@ __global__ void __launch_bounds__(fp_max_threads(TPT), fp_min_blocks(TPT)) fp_ke
     }
     const SamplePt pt = sample_point(a, b, c, N, zp, cosv, sinv);
     const bool inside = pt.base >= 0;
-    s_coef[sl][l] = make_float4(pt.c0, pt.c1, pt.c2, pt.c3);
-    // outside points read the zero column (both pairs) of the corner area
+    // weights packed per lane pair: s_w[slot][point/2] = {(c0,c0'),(c1,c1')},{(c2,c2'),(c3,c3')}
+    float *wf = reinterpret_cast<float *>(&s_w[sl][l >> 1][0]);
+    const int e = l & 1;
+    wf[0 + e] = pt.c0;
+    wf[2 + e] = pt.c1;
+    wf[4 + e] = pt.c2;
+    wf[6 + e] = pt.c3;
+    // outside points read the zero column pairs
     s_off[sl][l] = inside ? (sl * 8 + l) * 2 * cpair : zoff;
     const unsigned m = __ballot_sync(0xffu, inside);
     if (l == 0) {
@@ -230,14 +320,16 @@ __global__ void __launch_bounds__(fp_max_threads(TPT), fp_min_blocks(TPT)) fp_ke
     mbar_init(&s_bar[1], 1);
     fence_mbar_init();
   }
-  // zero the row pads once (sampling writes only [0, zp))
   for (int i = tid; i < 5 * kFpZPad; i += nthr) {
     const int col = i / kFpZPad, k = i % kFpZPad;
     rows[col * ZS + zp + k] = f4(0.f);
   }
   for (int i = tid; i < 2 * cpair; i += nthr) zcol[i] = 0.f;
   __syncthreads();
-  if (tid < 8 && nrows > 0) issue_row(0);
+  if (producer && ptid < 8) {
+    if (nrows > 0) issue_row(0);
+    if (nrows > 1) issue_row(1);
+  }
 
   // centre column y = c (sbrt:1815-1853): lanes (x,c),(N-x,c),(c,x),(c,N-x)
   {
@@ -255,143 +347,142 @@ __global__ void __launch_bounds__(fp_max_threads(TPT), fp_min_blocks(TPT)) fp_ke
   for (int z = zp + tid; z < ZS; z += nthr) cen[z] = f4(0.f);
   __syncthreads();
 
-  // accumulators start at the centre sample of their plane (the reference
-  // assigns the centre column before accumulating rows y < c)
-  float4 acc[TPT][kFpPlanes];
-  FpTask task[TPT];
-  // this CTA's share of the quad's tasks (blockIdx.y of gridDim.y)
-  const int t_begin = (int)(((long long)g.nfptasks * blockIdx.y) / gridDim.y);
-  const int t_end = (int)(((long long)g.nfptasks * (blockIdx.y + 1)) / gridDim.y);
+  bool timed_out = false;
+  if (producer) {
+    // ---------------- producers: bilinear samples, two rows ahead ----------------
+    const int hsplit = nprod / 2;
+    const int h_mine = ptid >= hsplit, z_mine = ptid - h_mine * hsplit;
+    for (int r = 0; r < nrows; r++) {
+      const int sl = r & 1;
+      if (!mbar_wait(&s_bar[sl], (uint32_t)((r >> 1) & 1), g.err)) timed_out = true;
+      if (r >= 2) bar_sync(kBarEmpty + sl, nthr);  // consumers are done with row r-2
+      {
+        // lanes (0,1) and (2,3) of this half share nothing but the plane: each
+        // lane pair is evaluated with packed pairs, its weights pre-packed
+        float4 *rw = rows + (size_t)sl * 2 * ZS + h_mine * ZS;
+        for (int z = z_mine; z < zp; z += hsplit) {
+          uint64_t vv[2];
 #pragma unroll
-  for (int t = 0; t < TPT; t++) {
-    const int ti = t_begin + tid + t * nthr;
-    task[t] = (ti < t_end) ? g.fptasks[ti] : FpTask{0, 0, 0, -1};
-    const int zb = (task[t].type < 0) ? 0 : g.ybot[task[t].seg] + task[t].p0;
-#pragma unroll
-    for (int j = 0; j < kFpPlanes; j++) acc[t][j] = cen[min(zb + j, ZS - 1)];
+          for (int pp = 0; pp < 2; pp++) {
+            const int pt = h_mine * 4 + 2 * pp;
+            const ulonglong2 wa = s_w[sl][pt >> 1][0], wb = s_w[sl][pt >> 1][1];
+            const float *qa = corners + s_off[sl][pt], *qb = corners + s_off[sl][pt + 1];
+            // corner order of the reference: r1 (ix,iy), r2 (ix+1,iy), r3 (ix,iy+1), r4 (ix+1,iy+1)
+            const uint64_t r1 = pk(qa[z], qb[z]), r2 = pk(qa[cpair + z], qb[cpair + z]);
+            const uint64_t r3 = pk(qa[zp + z], qb[zp + z]), r4 = pk(qa[cpair + zp + z], qb[cpair + zp + z]);
+            vv[pp] = add2(addp(mul2(r1, wa.x), mul2(r2, wa.y)), addp(mul2(r3, wb.x), mul2(r4, wb.y)));
+          }
+          *reinterpret_cast<ulonglong2 *>(rw + z) = make_ulonglong2(vv[0], vv[1]);
+        }
+      }
+      bar_arrive(kBarFull + sl, nthr);
+      // every producer has finished reading corner slot sl: refill it with row r+2
+      bar_sync(kBarProd, nprod);
+      if (ptid < 8 && r + 2 < nrows) issue_row(r + 2);
+    }
+    if (timed_out) {
+      // results are void (the host reports the status word); give copies
+      // still in flight a bounded chance to land before the CTA exits
+      for (int r = max(0, nrows - 2); r < nrows; r++) mbar_wait(&s_bar[r & 1], (uint32_t)((r >> 1) & 1), nullptr);
+    }
+    return;
   }
 
+  // ---------------- consumers: one task (segment, plane run) each ----------------
+  // accumulators start at the centre sample of their plane (the reference
+  // assigns the centre column before accumulating rows y < c)
+  Q2 acc[kFpPlanes];
+  const FpTask tk = (tid < g.nfptasks) ? g.fptasks[tid] : FpTask{0, 0, 0, -1};
+  {
+    const int zb = (tk.type < 0) ? 0 : g.ybot[tk.seg] + tk.p0;
+#pragma unroll
+    for (int j = 0; j < kFpPlanes; j++) acc[j] = ldq(cen + min(zb + j, ZS - 1));
+  }
+  const int gg = (tk.seg + 1) / 2 - 1;
+  const bool odd = tk.seg & 1;  // segment 2k-1: pam2 at z, pam at z2
+  const int pofs = tk.p0 - g.zshift;
+  const FpMid *mrow = g.fpmid + (gg < 0 ? 0 : gg);
+  const int ns_t = (tk.type < 0) ? 0 : g.ytop[tk.seg] - g.ybot[tk.seg] + 1;
+  const int li0 = gg * 2 * g.zshift + ((tk.p0 < g.zshift) ? tk.p0 : tk.p0 - ns_t + 2 * g.zshift);
   const int G = g.groupmax, FS = g.groupmax * 2 * g.zshift;
-  bool timed_out = false;
-  // bilinear work split: half the threads per sampled half-row
-  const int hsplit = nthr / 2;
-  const int h_mine = tid >= hsplit, z_mine = tid - h_mine * hsplit, z_step = hsplit;
   for (int r = 0; r < nrows; r++) {
     const int sl = r & 1, y = ystart + r;
-    // slot sl^1 was last read before the barrier of row r-1
-    if (tid < 8 && r + 1 < nrows) issue_row(r + 1);
-    if (!mbar_wait(&s_bar[sl], (uint32_t)((r >> 1) & 1), g.err)) timed_out = true;
-    // bilinear samples of row r from the staged corners (sbrt:1866-1905):
-    // threads [0, hsplit) build pam (lanes of points 0-3), the rest pam2
-    {
-      float4 *rw = rows + (size_t)sl * 2 * ZS + h_mine * ZS;
-      for (int z = z_mine; z < zp; z += z_step) {
-        float sv[4];
+    bar_sync(kBarFull + sl, nthr);
+    const float4 *pam = rows + (size_t)sl * 2 * ZS;
+    const float4 *pam2 = pam + ZS;
+    if (tk.type == 0) {
+      // theta = 0 (sbrt:1907-1910)
 #pragma unroll
-        for (int l = 0; l < 4; l++) {
-          // broadcast reads: every thread of this half uses the same point
-          const float4 k = s_coef[sl][h_mine * 4 + l];
-          const float *q0 = corners + s_off[sl][h_mine * 4 + l];
-          const float r1 = q0[z], r3 = q0[zp + z], r2 = q0[cpair + z], r4 = q0[cpair + zp + z];
-          sv[l] = (r1 * k.x + r2 * k.y) + (r3 * k.z + r4 * k.w);
-        }
-        rw[z] = make_float4(sv[0], sv[1], sv[2], sv[3]);
-      }
-    }
-    __syncthreads();
-    {
-      const float4 *pam = rows + (size_t)sl * 2 * ZS;
-      const float4 *pam2 = pam + ZS;
+      for (int j = 0; j < kFpPlanes; j++) acc[j] = qadd(acc[j], qadd(ldq(pam + tk.p0 + j), ldq(pam2 + tk.p0 + j)));
+    } else if (tk.type > 0) {
+      const FpMid m = mrow[y * G];
+      if (m.z >= 0) {  // else the group is skipped for this row (sbrt:1923-1924)
+        // segment 2k accumulates pam at z and pam2 at z2; segment 2k-1 the converse
+        const float4 *A = odd ? pam2 : pam;
+        const float4 *B = odd ? pam : pam2;
+        if (tk.type == 1) {
+          // middle planes: z, z2 advance with the plane (sbrt:1933-1947)
+          const float4 *Aw = A + m.z + pofs, *Bw = B + m.z2 + pofs;
+          const uint64_t f = pk(m.f, m.f), f2 = pk(m.f2, m.f2);
+          Q2 a0 = ldq(Aw), b0 = ldq(Bw);
 #pragma unroll
-      for (int t = 0; t < TPT; t++) {
-        const FpTask tk = task[t];
-        if (tk.type == 0) {
-          // theta = 0 (sbrt:1907-1910)
+          for (int j = 0; j < kFpPlanes; j++) {
+            const Q2 a1 = ldq(Aw + j + 1), b1 = ldq(Bw + j + 1);
+            acc[j] = qadd(acc[j], qaddp(qmul(qadd(b1, a0), f2), qmul(qadd(a1, b0), f)));
+            a0 = a1;
+            b0 = b1;
+          }
+        } else {
+          // end planes: per-plane flookup entries (sbrt:1925-1931, :1948-1952)
+          const int2 *fy = g.fl_zf + y * FS + li0, *fm = g.fl_zf + (N - y) * FS + li0;
 #pragma unroll
-          for (int j = 0; j < kFpPlanes; j++) acc[t][j] = acc[t][j] + (pam[tk.p0 + j] + pam2[tk.p0 + j]);
-        } else if (tk.type > 0) {
-          const int gg = (tk.seg + 1) / 2 - 1;
-          const FpMid m = g.fpmid[y * G + gg];
-          if (m.z < 0) continue;  // group skipped for this row (sbrt:1923-1924)
-          // segment 2k accumulates pam at z and pam2 at z2; segment 2k-1 the converse
-          const float4 *A = (tk.seg & 1) ? pam2 : pam;
-          const float4 *B = (tk.seg & 1) ? pam : pam2;
-          if (tk.type == 1) {
-            // middle planes: z, z2 advance with the plane (sbrt:1933-1947)
-            const int za = m.z + tk.p0 - g.zshift, zb2 = m.z2 + tk.p0 - g.zshift;
-            float4 a0 = A[za], b0 = B[zb2];
-#pragma unroll
-            for (int j = 0; j < kFpPlanes; j++) {
-              const float4 a1 = A[za + j + 1], b1 = B[zb2 + j + 1];
-              acc[t][j] = acc[t][j] + ((b1 + a0) * m.f2 + (a1 + b0) * m.f);
-              a0 = a1;
-              b0 = b1;
-            }
-          } else {
-            // end planes: per-plane flookup entries (sbrt:1925-1931, :1948-1952)
-            const int ns = g.ytop[tk.seg] - g.ybot[tk.seg] + 1;
-#pragma unroll
-            for (int j = 0; j < kFpPlanes; j++) {
-              if (j < tk.n) {
-                const int rr = tk.p0 + j;
-                const int yri = (rr < g.zshift) ? rr : rr - ns + 2 * g.zshift;
-                const int li = gg * 2 * g.zshift + yri;
-                const int z = __ldg(g.fl_zzi + y * FS + li), z2 = __ldg(g.fl_zzi + (N - y) * FS + li);
-                const float f = __ldg(g.fl_zzz0 + y * FS + li), f2 = __ldg(g.fl_zzz0 + (N - y) * FS + li);
-                acc[t][j] = acc[t][j] + ((B[z2 + 1] + A[z]) * f2 + (A[z + 1] + B[z2]) * f);
-              }
+          for (int j = 0; j < kFpEndPlanes; j++) {
+            if (j < tk.n) {
+              const int2 e1 = __ldg(fy + j), e2 = __ldg(fm + j);
+              const int z = e1.x, z2 = e2.x;
+              const float f = __int_as_float(e1.y), f2 = __int_as_float(e2.y);
+              const uint64_t ff = pk(f, f), ff2 = pk(f2, f2);
+              acc[j] = qadd(acc[j], qaddp(qmul(qadd(ldq(B + z2 + 1), ldq(A + z)), ff2),
+                                          qmul(qadd(ldq(A + z + 1), ldq(B + z2)), ff)));
             }
           }
         }
       }
     }
-  }
-
-  if (timed_out) {
-    // results are void (the host reports the status word); give copies still
-    // in flight into this CTA's shared memory a bounded chance to land first
-    for (int sl = 0; sl < 2; sl++) {
-      const int last = (nrows - 1 - sl) >= 0 ? ((nrows - 1 - sl) | 0) : -1;
-      if (last >= 0) mbar_wait(&s_bar[(nrows - 1 - sl) & 1], (uint32_t)(((nrows - 1 - sl) >> 1) & 1), nullptr);
-    }
-    return;
+    if (r + 2 < nrows) bar_arrive(kBarEmpty + sl, nthr);
   }
 
   // scale (sbrt:1953-1975), then either store the estimate or the OP ratio
   // (pt_update_est_w3, drv:2474-2520) pre-multiplied by the back projector's
   // segment weight (sbrt:1637-1649)
+  if (tk.type < 0) return;
   const size_t qbase = (size_t)x * g.pplanes;
+  const int sg = tk.seg;
 #pragma unroll
-  for (int t = 0; t < TPT; t++) {
-    const FpTask tk = task[t];
-    if (tk.type < 0) continue;
-    const int s = tk.seg, gg = (s + 1) / 2 - 1;
+  for (int j = 0; j < kFpPlanes; j++) {
+    if (j >= tk.n) continue;
+    const int r = tk.p0 + j, yr = g.ybot[sg] + r;
+    const float sc = (sg == 0) ? g.y_size : g.rescale[gg * g.nz + yr];
+    const float4 est = q2f(qmul(acc[j], pk(sc, sc)));
+    const size_t qi = qbase + g.poff[sg] + r;
+    if (MODE == 0) {
+      out[(size_t)w.slot * out_pair_stride + qi] = est;
+    } else {
+      const size_t ii = (size_t)v * g.nquads * g.pplanes + qi;
+      const P4 p = load_p4(prompts, ii);
+      const P4 ad = load_p4(add, ii);
+      const float bs = g.bp_scale[sg];
+      float rr[4];
 #pragma unroll
-    for (int j = 0; j < kFpPlanes; j++) {
-      if (j >= tk.n) continue;
-      const int r = tk.p0 + j, yr = g.ybot[s] + r;
-      const float sc = (s == 0) ? g.y_size : g.rescale[gg * g.nz + yr];
-      const float4 est = acc[t][j] * sc;
-      const size_t qi = qbase + g.poff[s] + r;
-      if (MODE == 0) {
-        out[(size_t)w.slot * out_pair_stride + qi] = est;
-      } else {
-        const size_t ii = (size_t)v * g.nquads * g.pplanes + qi;
-        const P4 p = load_p4(prompts, ii);
-        const P4 ad = load_p4(add, ii);
-        const float bs = g.bp_scale[s];
-        float rr[4];
-#pragma unroll
-        for (int l = 0; l < 4; l++) {
-          const float den = lane(est, l) + ad.v[l];
-          float q;
-          if (p.v[l] == 0.f) q = 0.f;
-          else if (den > g.eps3) q = p.v[l] / den;
-          else q = 1.0f;
-          rr[l] = q * bs;
-        }
-        out[(size_t)w.slot * out_pair_stride + qi] = make_float4(rr[0], rr[1], rr[2], rr[3]);
+      for (int l = 0; l < 4; l++) {
+        const float den = lane(est, l) + ad.v[l];
+        float q;
+        if (p.v[l] == 0.f) q = 0.f;
+        else if (den > g.eps3) q = p.v[l] / den;
+        else q = 1.0f;
+        rr[l] = q * bs;
       }
+      out[(size_t)w.slot * out_pair_stride + qi] = make_float4(rr[0], rr[1], rr[2], rr[3]);
     }
   }
 }
@@ -409,33 +500,30 @@ __global__ void __launch_bounds__(fp_max_threads(TPT), fp_min_blocks(TPT)) fp_ke
 // rotate-back, which is the reference's assign-then-accumulate order.
 // ============================================================================
 template <int KB>
-__device__ __forceinline__ void bp_lerp(float4 (&s)[KB], const float4 *__restrict__ p, const BpLut &bl, int z0) {
-  if (bl.zs <= z0 && z0 + KB - 1 <= bl.ze) {
-    const int yr0 = z0 + bl.d;
-    float4 a = p[yr0];
+__device__ __forceinline__ void bp_lerp(Q2 (&s)[KB], const float4 *__restrict__ p, const BpLut &bl, int z0) {
+  // windows wholly outside [zs, ze] contribute nothing; a window that
+  // straddles an end reads the segment's zero planes for its outside planes
+  if (z0 + KB - 1 < bl.zs || z0 > bl.ze) return;
+  const float4 *pw = p + z0 + bl.d;
+  const uint64_t f = pk(bl.f, bl.f);
+  Q2 a = ldq(pw);
 #pragma unroll
-    for (int j = 0; j < KB; j++) {
-      const float4 b = p[yr0 + j + 1];
-      s[j] = s[j] + (a + (b - a) * bl.f);
-      a = b;
-    }
-  } else {
-#pragma unroll
-    for (int j = 0; j < KB; j++) {
-      const int z = z0 + j;
-      if (z >= bl.zs && z <= bl.ze) {
-        const float4 a = p[z + bl.d], b = p[z + bl.d + 1];
-        s[j] = s[j] + (a + (b - a) * bl.f);
-      }
-    }
+  for (int j = 0; j < KB; j++) {
+    const Q2 b = ldq(pw + j + 1);
+    // the reference's p[yr] + f*(p[yr+1]-p[yr]) (sbrt:4312-4315)
+    s[j] = qadd(s[j], qaddp(a, qmul(qsub(b, a), f)));
+    a = b;
   }
 }
 
 template <int KB>
-__device__ __forceinline__ void store_lane(float *__restrict__ dst, const float4 (&s)[KB], int l) {
+__device__ __forceinline__ void store_lane(float *__restrict__ dst, const Q2 (&s)[KB], int l) {
   float v[KB];
 #pragma unroll
-  for (int j = 0; j < KB; j++) v[j] = lane(s[j], l);
+  for (int j = 0; j < KB; j++) {
+    const float2 t = upk(l < 2 ? s[j].lo : s[j].hi);
+    v[j] = (l & 1) ? t.y : t.x;
+  }
 #pragma unroll
   for (int j = 0; j < KB; j += 4) *reinterpret_cast<float4 *>(dst + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
 }
@@ -444,20 +532,23 @@ template <int KB>
 __global__ void __launch_bounds__(256, 3) bp_kernel(DevGeom g, const float4 *__restrict__ in, long long in_pair_stride,
                                                  const QuadWork *__restrict__ work, float *__restrict__ bc,
                                                  float *__restrict__ br, long long vol) {
-  extern __shared__ float4 P[];  // [pplanes]
+  extern __shared__ float4 P[];  // [bp_splanes]: segments with kBpPad zero planes each side
   const QuadWork w = work[blockIdx.x];
   const int x = w.x, N = g.nx, c = g.c, zp = g.zp, G = g.groupmax;
   const bool masked = g.nzmask[w.view * g.nquads + x] == 0;
   const float4 *src = in + (size_t)w.slot * in_pair_stride + (size_t)x * g.pplanes;
   if (!masked)
-    for (int i = threadIdx.x; i < g.pplanes; i += blockDim.x) P[i] = src[i];
+    for (int i = threadIdx.x; i < g.bp_splanes; i += blockDim.x) {
+      const int q = __ldg(g.bp_src + i);
+      P[i] = (q >= 0) ? src[q] : f4(0.f);
+    }
   __syncthreads();
 
   float *bcp = bc + (size_t)w.slot * vol;
   float *brp = br + (size_t)w.slot * vol;
   const int ystart = g.cyl0[x];
   const int nyq = c - ystart + 1, nzc = zp / KB;
-  const float4 *P0 = P + g.poff[0];
+  const float4 *P0 = P + g.bp_soff[0];
   // task = (half, plane run, row); half 0 builds sumt1 (voxels (x,y),(N-x,y),
   // (N-y,x),(N-y,N-x)), half 1 sumt2 (voxels (x,N-y),(N-x,N-y),(y,x),(y,N-x)).
   // Consecutive threads take consecutive rows at the same planes: their window
@@ -470,35 +561,35 @@ __global__ void __launch_bounds__(256, 3) bp_kernel(DevGeom g, const float4 *__r
     const int zc = t2 / nyq, yi = t2 - zc * nyq, z0 = zc * KB;
     const int y = ystart + yi;
     if (half && y == c) continue;  // the centre row has a single voxel set
-    float4 s[KB];
+    Q2 s[KB];
     if (masked) {
       // masked quads contribute zero (sbrt:4223-4258, :4595-4640)
 #pragma unroll
-      for (int j = 0; j < KB; j++) s[j] = f4(0.f);
+      for (int j = 0; j < KB; j++) s[j] = Q2{0ull, 0ull};
     } else if (y == c) {
       // centre row (sbrt:4260-4284): rays pass plane yr = z exactly
 #pragma unroll
-      for (int j = 0; j < KB; j++) s[j] = P0[z0 + j];
+      for (int j = 0; j < KB; j++) s[j] = ldq(P0 + z0 + j);
       for (int gg = 0; gg < G; gg++) {
         const int se = 2 * gg + 2, so = 2 * gg + 1;
         const int yb = g.ybot[se], yt = g.ytop[se];
-        const float4 *pe = P + g.poff[se] - yb, *po = P + g.poff[so] - yb;
+        const float4 *pe = P + g.bp_soff[se] - yb, *po = P + g.bp_soff[so] - yb;
 #pragma unroll
         for (int j = 0; j < KB; j++) {
           const int z = z0 + j;
-          if (z >= yb && z <= yt) s[j] = s[j] + (pe[z] + po[z]);
+          if (z >= yb && z <= yt) s[j] = qadd(s[j], qadd(ldq(pe + z), ldq(po + z)));
         }
       }
     } else {
 #pragma unroll
-      for (int j = 0; j < KB; j++) s[j] = P0[z0 + j];
+      for (int j = 0; j < KB; j++) s[j] = ldq(P0 + z0 + j);
       // bplut is [group][row]: the rows of a warp read consecutive entries
       const BpLut *l1 = g.bplut + y, *l2 = g.bplut + (N - y);
       BpLut b1 = l1[0], b2 = l2[0];
       for (int gg = 0; gg < G; gg++) {
         const int se = 2 * gg + 2, so = 2 * gg + 1;
         const int yb = g.ybot[se];
-        const float4 *pe = P + g.poff[se] - yb, *po = P + g.poff[so] - yb;
+        const float4 *pe = P + g.bp_soff[se] - yb, *po = P + g.bp_soff[so] - yb;
         const int gn = (gg + 1 < G) ? gg + 1 : gg;
         const BpLut n1 = l1[(size_t)gn * N], n2 = l2[(size_t)gn * N];  // next group, in flight
         // sumt1: segment 2k at +u and 2k-1 at -u; sumt2: the converse
@@ -511,7 +602,7 @@ __global__ void __launch_bounds__(256, 3) bp_kernel(DevGeom g, const float4 *__r
     // the reference writes planes z < nz only
 #pragma unroll
     for (int j = 0; j < KB; j++)
-      if (z0 + j >= g.nz) s[j] = f4(0.f);
+      if (z0 + j >= g.nz) s[j] = Q2{0ull, 0ull};
     const size_t cz = (size_t)z0;
     if (!half) {
       store_lane<KB>(bcp + ((size_t)x * N + y) * zp + cz, s, 0);
@@ -809,34 +900,33 @@ __global__ void scale_pairs_kernel(DevGeom g, const T *__restrict__ src, const i
   dst[(size_t)slot * dst_pair_stride + i] = o;
 }
 
-template <int TPT, int MODE, typename PT, typename AT>
+template <int MODE, typename PT, typename AT>
 cudaError_t launch_fp_t(const DevGeom &g, const float *image, const QuadWork *work, int nwork, const void *prompts,
                         const void *add, float *out, long long out_pair_stride, cudaStream_t st) {
-  // split a quad's tasks over enough CTAs that each fits the launch bound
-  const int per_cta = fp_max_threads(TPT) * TPT;
-  const int nsplit = (g.nfptasks + per_cta - 1) / per_cta;
-  int threads = (g.nfptasks + nsplit * TPT - 1) / (nsplit * TPT);
-  threads = ((threads + 31) / 32) * 32;
-  if (threads > fp_max_threads(TPT) || nsplit > 8) return cudaErrorInvalidConfiguration;
+  // consumer warps: one task per thread; producer warps: enough to keep the
+  // sampled rows ahead of the consumers (a row is ~2*zp bilinear quads)
+  const int cwarps = (g.nfptasks + 31) / 32;
+  const int pwarps = min(6, max(2, 32 - cwarps));
+  if (cwarps + pwarps > 32) return cudaErrorInvalidConfiguration;
+  const int threads = (cwarps + pwarps) * 32;
   const int ZS = g.zp + kFpZPad;
   const size_t smem = (size_t)(2 * 8 * 2 + 2) * 2 * g.zp * sizeof(float) + (size_t)5 * ZS * sizeof(float4);
-  auto k = fp_kernel<TPT, MODE, PT, AT>;
+  auto k = fp_kernel<MODE, PT, AT>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  k<<<dim3(nwork, nsplit), threads, smem, st>>>(g, image, work, (const PT *)prompts, (const AT *)add,
-                                    reinterpret_cast<float4 *>(out), out_pair_stride / 4);
+  k<<<nwork, threads, smem, st>>>(g, image, work, (const PT *)prompts, (const AT *)add,
+                                  reinterpret_cast<float4 *>(out), out_pair_stride / 4, pwarps);
   return cudaGetLastError();
 }
 
-template <int TPT>
-cudaError_t launch_fp_tpt(const DevGeom &g, const float *image, const QuadWork *work, int nwork, int mode,
+cudaError_t launch_fp_any(const DevGeom &g, const float *image, const QuadWork *work, int nwork, int mode,
                           const void *prompts, const void *add, int storage, float *out, long long stride,
                           cudaStream_t st) {
-  if (mode == 0) return launch_fp_t<TPT, 0, int16_t, float>(g, image, work, nwork, nullptr, nullptr, out, stride, st);
-  if (storage == 0) return launch_fp_t<TPT, 1, int16_t, float>(g, image, work, nwork, prompts, add, out, stride, st);
-  return launch_fp_t<TPT, 1, __half, __nv_bfloat16>(g, image, work, nwork, prompts, add, out, stride, st);
+  if (mode == 0) return launch_fp_t<0, int16_t, float>(g, image, work, nwork, nullptr, nullptr, out, stride, st);
+  if (storage == 0) return launch_fp_t<1, int16_t, float>(g, image, work, nwork, prompts, add, out, stride, st);
+  return launch_fp_t<1, __half, __nv_bfloat16>(g, image, work, nwork, prompts, add, out, stride, st);
 }
 
 }  // namespace
@@ -845,18 +935,15 @@ cudaError_t launch_fp(const DevGeom &g, const float *image, const QuadWork *work
                       const void *prompts, const void *add, int storage, float *out, long long out_pair_stride,
                       int tasks_per_thread, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
-  switch (tasks_per_thread) {
-    case 1: return launch_fp_tpt<1>(g, image, work, nwork, mode, prompts, add, storage, out, out_pair_stride, st);
-    case 2: return launch_fp_tpt<2>(g, image, work, nwork, mode, prompts, add, storage, out, out_pair_stride, st);
-    case 3: return launch_fp_tpt<3>(g, image, work, nwork, mode, prompts, add, storage, out, out_pair_stride, st);
-    default: return cudaErrorInvalidValue;
-  }
+  (void)tasks_per_thread;
+  return launch_fp_any(g, image, work, nwork, mode, prompts, add, storage, out, out_pair_stride, st);
 }
 
 cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
                       float *bc, float *br, long long vol, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
-  const size_t smem = (size_t)g.pplanes * sizeof(float4);
+  static_assert(kBpPad >= kBpZ, "a straddling window must stay inside the zero planes");
+  const size_t smem = (size_t)g.bp_splanes * sizeof(float4);
   auto k = bp_kernel<kBpZ>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)

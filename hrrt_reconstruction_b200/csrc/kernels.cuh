@@ -27,6 +27,7 @@ constexpr int kFpPlanes = 9;    // planes per forward-projection task (odd: bank
 constexpr int kFpZPad = 16;     // zeroed entries after each sampled row
 constexpr int kFpEndPlanes = 4; // planes per end-plane task (they cost ~2x a middle plane)
 constexpr int kBpZ = 8;         // z per back-projection task
+constexpr int kBpPad = 8;       // zero planes on each side of a segment in the back projector (>= kBpZ)
 
 struct FpTask {
   int16_t seg;   // segment (internal = file order)
@@ -56,8 +57,7 @@ struct DevGeom {
   const float *rescale;             // [groupmax][nz]
   const float *bp_scale;            // [nseg]
   const FpMid *fpmid;               // [c][groupmax]
-  const int *fl_zzi;                // [ny][groupmax*2*zshift]
-  const float *fl_zzz0;
+  const int2 *fl_zf;                // [ny][groupmax*2*zshift]: (zzi, bits of zzz0)
   const BpLut *bplut;               // [groupmax][ny]
   const int16_t *nzmask;            // [nviews/2][nquads]
   const float *sin_psi, *cos_psi;   // [nviews]
@@ -68,6 +68,9 @@ struct DevGeom {
   const int16_t *plane_seg;         // [segmentsize] segment of each global plane
   const int16_t *pplane_seg;        // [pplanes] segment of each padded plane, -1 on pads
   int *err;                         // device status word: non-zero after a bounded wait gave up
+  const int *bp_soff;               // [nseg] back projector: shared-memory plane of yr_bottom
+  const int *bp_src;                // [bp_splanes] quad-layout plane of each shared plane, -1 = zero
+  int bp_splanes;
 };
 
 struct QuadWork {  // one (view pair slot, quad) work item
