@@ -80,6 +80,7 @@ def _load():
         "hrrt_fp_pair": (i, [vp, vp, i, vp]),
         "hrrt_bp_pair": (i, [vp, vp, i, vp, i]),
         "hrrt_forward_project": (i, [vp, vp, vp]),
+        "hrrt_bp_pair_noalloc": (i, [vp, vp, i, vp, vp]),
         "hrrt_rotate_add": (i, [vp, vp, i, vp]),
         "hrrt_geometry_table": (ctypes.c_longlong, [G, ctypes.c_char_p, vp, ctypes.c_size_t]),
         "hrrt_set_profiling": (i, [vp, i]),

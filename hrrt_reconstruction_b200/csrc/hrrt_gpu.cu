@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -875,6 +876,84 @@ int hrrt_bp_pair(hrrt_ctx *ctx, const float *prj, int view, float *imagebuf_xyz,
   CK(cudaStreamSynchronize(ctx->stream), "bp_pair");
   cudaFree(dw);
   ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)dw));
+  return HRRT_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Back projection without allocation.
+//
+// Some callers cannot allocate device memory while they run: an acquisition
+// loop that must not stall on cudaMalloc's implicit device synchronisation,
+// a host application that hands this library a fixed memory budget at start-up,
+// or code that issues its work into a stream another component is recording.
+// hrrt_bp_pair_noalloc serves them.  Its only scratch -- the quad-layout copy
+// of the input sinogram rows, scaled by the back projector's segment weights --
+// lives in the static device array below, so the call itself never allocates;
+// the input rows and the output buffer are the caller's.
+//
+// The array is kNoAllocScratchBytes (16 MiB: the quad layout of an HRRT span-3
+// view pair is 13.3 MB).  Every GPU on which the library is loaded holds it
+// until the process exits.  All calls share it and it keeps the last call's
+// contents, so calls that overlap on the GPU (other streams, other host
+// threads) race with each other.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchBytes / sizeof(float)];
+
+namespace {
+// device address of g_noalloc_scratch, resolved once per device (the host
+// symbol is only a stand-in for it)
+std::mutex g_noalloc_mu;
+std::map<int, float *> g_noalloc_ptr;
+
+cudaError_t noalloc_scratch(float **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  auto it = g_noalloc_ptr.find(dev);
+  if (it != g_noalloc_ptr.end()) {
+    *out = it->second;
+    return cudaSuccess;
+  }
+  float *p = nullptr;
+  e = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  g_noalloc_ptr[dev] = p;
+  *out = p;
+  return cudaSuccess;
+}
+}  // namespace
+
+extern "C" {
+
+int hrrt_bp_pair_noalloc(hrrt_ctx *ctx, const float *d_prj, int view, float *d_imagebuf, void *stream) {
+  if (!ctx || !d_prj || !d_imagebuf) return HRRT_ERR_ARG;
+  const Geometry &g = ctx->geo;
+  if (view < 0 || view >= g.nviews / 2) return fail(ctx, HRRT_ERR_ARG, "view must be < nviews/2");
+  const size_t need = (size_t)ctx->quad_pair * sizeof(float);
+  if (need > kNoAllocScratchBytes)
+    return fail(ctx, HRRT_ERR_ARG,
+                "hrrt_bp_pair_noalloc: this geometry needs " + std::to_string(need) +
+                    " bytes of scratch; the static scratch holds " + std::to_string(kNoAllocScratchBytes));
+  CK(cudaSetDevice(ctx->device), "hrrt_bp_pair_noalloc");
+  float *scratch = nullptr;
+  CK(noalloc_scratch(&scratch), "hrrt_bp_pair_noalloc: cudaGetSymbolAddress");
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  int x0 = 0, x1 = -1;  // the FOV quads are one run of x
+  for (int x = 1; x <= g.c; x++)
+    if (g.cyl0[x] != g.cyl1[x]) {
+      if (x0 == 0) x0 = x;
+      x1 = x;
+    }
+  // the segment pads of the quad layout must read as zero; the output
+  // collects two atomically added partial sums per voxel
+  CK(cudaMemsetAsync(scratch, 0, need, st), "hrrt_bp_pair_noalloc: clear scratch");
+  CK(cudaMemsetAsync(d_imagebuf, 0, (size_t)ctx->vol * sizeof(float), st), "hrrt_bp_pair_noalloc: clear output");
+  CK(launch_rows_to_quad(ctx->dg, g.nbins, d_prj, scratch, 1, st), "hrrt_bp_pair_noalloc: pack");
+  CK(launch_bp_sum(ctx->dg, scratch, view, x0, x1 - x0 + 1, d_imagebuf, st), "hrrt_bp_pair_noalloc: bp");
   return HRRT_OK;
 }
 

@@ -516,7 +516,7 @@ __device__ __forceinline__ void bp_lerp(Q2 (&s)[KB], const float4 *__restrict__ 
   }
 }
 
-template <int KB>
+template <int KB, bool ACC = false>
 __device__ __forceinline__ void store_lane(float *__restrict__ dst, const Q2 (&s)[KB], int l) {
   float v[KB];
 #pragma unroll
@@ -524,16 +524,25 @@ __device__ __forceinline__ void store_lane(float *__restrict__ dst, const Q2 (&s
     const float2 t = upk(l < 2 ? s[j].lo : s[j].hi);
     v[j] = (l & 1) ? t.y : t.x;
   }
+  if (ACC) {
 #pragma unroll
-  for (int j = 0; j < KB; j += 4) *reinterpret_cast<float4 *>(dst + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+    for (int j = 0; j < KB; j++) atomicAdd(dst + j, v[j]);
+  } else {
+#pragma unroll
+    for (int j = 0; j < KB; j += 4)
+      *reinterpret_cast<float4 *>(dst + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+  }
 }
 
-template <int KB>
+template <int KB, bool ACC = false>
 __global__ void __launch_bounds__(256, 3) bp_kernel(DevGeom g, const float4 *__restrict__ in, long long in_pair_stride,
                                                  const QuadWork *__restrict__ work, float *__restrict__ bc,
-                                                 float *__restrict__ br, long long vol) {
+                                                 float *__restrict__ br, long long vol, int view0 = 0, int x0 = 0) {
   extern __shared__ float4 P[];  // [bp_splanes]: segments with kBpPad zero planes each side
-  const QuadWork w = work[blockIdx.x];
+  // ACC: one view pair, quads x0 + blockIdx.x, both partial sums added into bc
+  // (each voxel receives exactly two terms, so the atomic adds onto a zeroed
+  // buffer give a + b whatever their order)
+  const QuadWork w = ACC ? QuadWork{0, (int16_t)(x0 + blockIdx.x), (int16_t)view0, 0} : work[blockIdx.x];
   const int x = w.x, N = g.nx, c = g.c, zp = g.zp, G = g.groupmax;
   const bool masked = g.nzmask[w.view * g.nquads + x] == 0;
   const float4 *src = in + (size_t)w.slot * in_pair_stride + (size_t)x * g.pplanes;
@@ -605,18 +614,18 @@ __global__ void __launch_bounds__(256, 3) bp_kernel(DevGeom g, const float4 *__r
       if (z0 + j >= g.nz) s[j] = Q2{0ull, 0ull};
     const size_t cz = (size_t)z0;
     if (!half) {
-      store_lane<KB>(bcp + ((size_t)x * N + y) * zp + cz, s, 0);
-      store_lane<KB>(brp + ((size_t)(N - y) * N + x) * zp + cz, s, 2);
+      store_lane<KB, ACC>(bcp + ((size_t)x * N + y) * zp + cz, s, 0);
+      store_lane<KB, ACC>(brp + ((size_t)(N - y) * N + x) * zp + cz, s, 2);
       if (x != c) {
-        store_lane<KB>(bcp + ((size_t)(N - x) * N + y) * zp + cz, s, 1);
-        store_lane<KB>(brp + ((size_t)(N - y) * N + N - x) * zp + cz, s, 3);
+        store_lane<KB, ACC>(bcp + ((size_t)(N - x) * N + y) * zp + cz, s, 1);
+        store_lane<KB, ACC>(brp + ((size_t)(N - y) * N + N - x) * zp + cz, s, 3);
       }
     } else {
-      store_lane<KB>(bcp + ((size_t)x * N + N - y) * zp + cz, s, 0);
-      store_lane<KB>(brp + ((size_t)y * N + x) * zp + cz, s, 2);
+      store_lane<KB, ACC>(bcp + ((size_t)x * N + N - y) * zp + cz, s, 0);
+      store_lane<KB, ACC>(brp + ((size_t)y * N + x) * zp + cz, s, 2);
       if (x != c) {
-        store_lane<KB>(bcp + ((size_t)(N - x) * N + N - y) * zp + cz, s, 1);
-        store_lane<KB>(brp + ((size_t)y * N + N - x) * zp + cz, s, 3);
+        store_lane<KB, ACC>(bcp + ((size_t)(N - x) * N + N - y) * zp + cz, s, 1);
+        store_lane<KB, ACC>(brp + ((size_t)y * N + N - x) * zp + cz, s, 3);
       }
     }
   }
@@ -949,7 +958,20 @@ cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_strid
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  k<<<nwork, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(in), in_pair_stride / 4, work, bc, br, vol);
+  k<<<nwork, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(in), in_pair_stride / 4, work, bc, br, vol, 0, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bp_sum(const DevGeom &g, const float *quad, int view, int x0, int nquads, float *out,
+                          cudaStream_t st) {
+  if (nquads <= 0) return cudaSuccess;
+  const size_t smem = (size_t)g.bp_splanes * sizeof(float4);
+  auto k = bp_kernel<kBpZ, true>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  k<<<nquads, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(quad), 0, nullptr, out, out, 0, view, x0);
   return cudaGetLastError();
 }
 

@@ -89,6 +89,10 @@ cudaError_t launch_fp(const DevGeom &g, const float *image, const QuadWork *work
 // back projection of quad-layout input into the column (Bc) / row (Br) partials
 cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
                       float *bc, float *br, long long vol, cudaStream_t st);
+// back projection of one view pair's quad-layout input (quads x0..x0+nquads-1)
+// with both partial sums added atomically into `out` (zeroed by the caller)
+cudaError_t launch_bp_sum(const DevGeom &g, const float *quad, int view, int x0, int nquads, float *out,
+                          cudaStream_t st);
 // corr = sum over pairs of rotate-back(Bc+Br); mode 0: OSEM update of image with
 // nf_inv; mode 1: write the inverse sensitivity into nf_inv; mode 2: corr_out += corr
 cudaError_t launch_rotback(const DevGeom &g, const int *pair_views, int npairs, const float *bc, const float *br,

@@ -163,6 +163,23 @@ int hrrt_forward_project(hrrt_ctx *ctx, const float *image_xyz, float *sino);
  * imagebuf_xyz [x][y][zp] (overwritten). */
 int hrrt_bp_pair(hrrt_ctx *ctx, const float *prj, int view, float *imagebuf_xyz, int mode);
 
+/*
+ * Back projection of one view pair that allocates no device memory (no
+ * counterpart in the reference, whose projector works on host arrays).  For
+ * callers that may not allocate while they run -- a real-time loop that cannot
+ * take cudaMalloc's device synchronisation, a host that grants the library a
+ * fixed memory budget at start-up, or work issued into a stream that is being
+ * recorded.  Same result as hrrt_bp_pair, with the caller's device buffers:
+ * d_prj rows [2*segmentsize][nbins] in, d_imagebuf [x][y][zp] out
+ * (overwritten), on `stream` (a cudaStream_t; NULL = the context's stream),
+ * asynchronously.  Its scratch is a static 16 MiB device array in the library
+ * (held on every GPU that loads it until exit); geometries whose quad-layout
+ * view pair exceeds it are rejected with HRRT_ERR_ARG.  The first call on a
+ * device resolves that array's address, so make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race.
+ */
+int hrrt_bp_pair_noalloc(hrrt_ctx *ctx, const float *d_prj, int view, float *d_imagebuf, void *stream);
+
 /* Replaces rotate_image_buf (sbrt:1701-1725) for one view: corr_xyz +=
  * rotate-back(imagebuf_xyz). */
 int hrrt_rotate_add(hrrt_ctx *ctx, const float *imagebuf_xyz, int view, float *corr_xyz);
