@@ -343,7 +343,8 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
   p.epsilon2 = gp->epsilon2;
   p.epsilon3 = gp->epsilon3;
   p.image_max = gp->image_max;
-  // z range adjustments of GetScannerParameter (drv:3537-3540)
+  // z range adjustments of GetScannerParameter (drv:3516, :3537-3540)
+  if (p.z_max == 0) p.z_max = (2 * p.nrings - 1) - p.z_min;
   if (p.npskip > p.z_min) p.z_min = p.npskip;
   if (p.z_max > (2 * p.nrings - 1) - p.npskip) p.z_max = (2 * p.nrings - 1) - p.npskip;
   std::string m = ctx->geo.build(p);

@@ -81,6 +81,14 @@ class RefProjector:
         self.subsets = subsets
         self.sviews = L.ref_sviews()
         self.span = span
+        # plane range after GetScannerParameter's adjustments (drv:3516,
+        # :3537-3540) for the default -f ...,6,200 and -k 3
+        z_min, z_max, npskip = 6, 200, 3
+        if npskip > z_min:
+            z_min = npskip
+        if z_max > self.nz - npskip:
+            z_max = self.nz - npskip
+        self.z_min, self.z_max = z_min, z_max
 
     @property
     def image_shape(self):
@@ -124,10 +132,16 @@ class RefProjector:
         self.L.ref_osem_subset(_p(image), _p(corr), _p(nf), _p(p), _p(a), isubset, nthreads or self.nthreads)
         return image
 
-    def post_iteration(self, image, zmin=6, zmax=200):
+    def post_iteration(self, image, zmin=None, zmax=None):
+        zmin = self.z_min if zmin is None else zmin
+        zmax = self.z_max if zmax is None else zmax
+        assert 0 <= zmin <= zmax <= self.zp and image.dtype == np.float32 and image.flags.c_contiguous
         return self.L.ref_post_iteration(_p(image), zmin, zmax)
 
-    def init_image(self, zmin=6, zmax=200):
+    def init_image(self, zmin=None, zmax=None):
+        zmin = self.z_min if zmin is None else zmin
+        zmax = self.z_max if zmax is None else zmax
+        assert 0 <= zmin <= zmax <= self.zp
         out = np.zeros(self.image_shape, np.float32)
         self.L.ref_init_image(_p(out), zmin, zmax)
         return out
