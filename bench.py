@@ -145,16 +145,38 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def algorithmic_model(info):
+FP32_TFLOPS_NOMINAL = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes (read + write) per launch of `kernel` at this workload, from
+    the committed ncu summary profiles/traffic.txt (lines
+    `<kernel> <bytes per launch> <source>`), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            parts = line.split(None, 2)
+            if len(parts) >= 2 and parts[0] == kernel and not line.startswith("#"):
+                try:
+                    return float(parts[1]), (parts[2].strip() if len(parts) > 2 else "profiles/traffic.txt")
+                except ValueError:
+                    return None
+    return None
+
+
+def algorithmic_model(info, add_bytes=4):
     """Per-launch algorithmic bytes and FLOPs of the subset kernels.
 
     Bins per subset: 9 view pairs x 2 views x segmentsize x nbins.
     fp_kernel : image read once (nx*ny*nz*4) + prompts (2 B) + additive term
-                (4 B) read + OP ratio (4 B) written per bin; FLOPs = 6 per
+                (4 B, or 2 B stored as bf16) read + OP ratio (4 B) written
+                per bin; FLOPs = 6 per
                 lerp sample (2 adds, 2 muls, 2 accumulating adds for a sample
                 pair, i.e. 3 per sample) x samples.
     bp_kernel : ratio read (4 B/bin) + correction image written once
-                (nx*ny*nz*4).
+                (nx*ny*nz*4); FLOPs = 4 per lerp sample (p + f*(q-p), summed).
     rotback_kernel: correction read + image read/write + inverse sensitivity
                 read (4 image volumes).
     """
@@ -167,11 +189,25 @@ def algorithmic_model(info):
     samples = pairs * 2 * info.fov_columns * info.segmentsize
     return {
         "bins_per_subset": bins,
-        "fp_kernel": {"bytes": vol + bins * 10, "flops": samples * 3},
-        "bp_kernel": {"bytes": bins * 4 + vol, "flops": samples * 3},
+        "fp_kernel": {"bytes": vol + bins * (6 + add_bytes), "flops": samples * 3},
+        "bp_kernel": {"bytes": bins * 4 + vol, "flops": samples * 4},
         "rotback_kernel": {"bytes": 4 * vol, "flops": info.fov_columns * info.zp * pairs * 16},
-        "subset_bytes": bins * (6 + 8) + 3 * vol,
+        # prompts + additive term read, ratio written and read back, image
+        # read, inverse sensitivity read, image written
+        "subset_bytes": bins * (2 + add_bytes + 8) + 3 * vol,
     }
+
+
+_PINNED = []  # page-locked tensors behind the numpy views handed to the C ABI
+
+
+def pinned_copy(torch, a):
+    """A numpy view of page-locked host memory holding a copy of `a`."""
+    t = torch.empty(a.shape, dtype=getattr(torch, a.dtype.name), pin_memory=True)
+    _PINNED.append(t)
+    out = t.numpy()
+    out[...] = a
+    return out
 
 
 def run_ours(args, ws, rank, local):
@@ -188,23 +224,26 @@ def run_ours(args, ws, rank, local):
     st = phantom.study(ctx, seed=1 + rank, **STUDY)
     gen_s = time.time() - t0
 
-    # ---- end-to-end through the C ABI from host buffers ----
+    # ---- end-to-end through the C ABI from pinned host buffers ----
     e2e_subsets = ITERATIONS * SUBSETS
+    names = ("prompts", "randoms", "norm", "atten", "scatter")
+    host = {k: pinned_copy(torch, st[k]) for k in names if st[k] is not None}
+    info = ctx.info
+    img = pinned_copy(torch, np.zeros((info.nz, info.ny, info.nx), np.float32))
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     cs = torch.cuda.ExternalStream(ctx.stream)
     barrier(dist, local)
     torch.cuda.synchronize()
     ev[0].record(cs)
-    ctx.upload_inputs(st["prompts"], st["randoms"], st["norm"], st["atten"], st["scatter"], storage=storage)
+    ctx.upload_inputs(*(host.get(k) for k in names), storage=storage)
     ctx.sensitivity()
     ctx.init_image()
     stats = ctx.osem(ITERATIONS)
-    img = ctx.get_image()
+    ctx.get_image(out=img)
     ev[1].record(cs)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(dist, ev[0].elapsed_time(ev[1]), local)
-    h2d = sum(int(a.nbytes) for a in (st["prompts"], st["randoms"], st["norm"], st["atten"], st["scatter"])
-              if a is not None)
+    h2d = sum(int(a.nbytes) for a in host.values())
     d2h = int(img.nbytes)
     e2e = {"value": ws * e2e_subsets / (e2e_ms / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": h2d // e2e_subsets, "d2h_bytes_per_step": d2h // e2e_subsets,
@@ -230,12 +269,14 @@ def run_ours(args, ws, rank, local):
     barrier(dist, local)
     kstats = {k: ctx.kernel_stats(k) for k in ("fp_kernel", "bp_kernel", "rotback_kernel")}
     launches = sum(n for n, _ in kstats.values())
-    model = algorithmic_model(ctx.info)
+    model = algorithmic_model(ctx.info, add_bytes=4 if storage == H.STORE_F32 else 2)
     dom = max(kstats, key=lambda k: kstats[k][1])
     n, tot = kstats[dom]
     avg_s = tot / max(n, 1) / 1e3
     peak, peak_kind = measured_peaks()
     achieved = model[dom]["bytes"] / avg_s / 1e9
+    traffic = ncu_traffic(dom)
+    sm_mhz = (clk or {}).get("sm_mhz") or 1965.0
     out = {
         "metric": METRIC, "value": ws * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -251,9 +292,26 @@ def run_ours(args, ws, rank, local):
         "kernels": {k: {"launches": v[0], "ms_total": v[1], "ms_avg": v[1] / max(v[0], 1)} for k, v in kstats.items()},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
-                     "fallback 6.65 TB/s", "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "fallback 6.65 TB/s", "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic[0] if traffic else None,
                      "bytes_per_launch": model[dom]["bytes"],
-                     "fp32_tflops": model[dom]["flops"] / avg_s / 1e12},
+                     "traffic_source": traffic[1] if traffic else None},
+        # the projectors are bound by the FP32 pipe, not by HBM: the same
+        # kernel against the FP32 CUDA-core peak (148 SMs x 128 lanes x 2 flop
+        # per clock; nominal at 1965 MHz, and at the median SM clock sampled
+        # during the timed region)
+        "roofline_alu": {"bound": "fp32", "kernel": dom, "unit": "TFLOP/s",
+                         "achieved": model[dom]["flops"] / avg_s / 1e12,
+                         "flops_per_launch": model[dom]["flops"],
+                         "peak_nominal": FP32_TFLOPS_NOMINAL,
+                         "peak_at_clock": FP32_TFLOPS_NOMINAL * sm_mhz / 1965.0,
+                         "frac_nominal": model[dom]["flops"] / avg_s / 1e12 / FP32_TFLOPS_NOMINAL,
+                         "frac_at_clock": model[dom]["flops"] / avg_s / 1e12 / (FP32_TFLOPS_NOMINAL * sm_mhz / 1965.0)},
+        # the whole subset-iteration against HBM: algorithmic bytes per subset
+        # (bins x (input bytes + 8) + 3 image volumes) over the step time
+        "roofline_subset": {"bound": "hbm", "unit": "GB/s", "bytes_per_step": model["subset_bytes"],
+                            "achieved": model["subset_bytes"] / (ms / args.steps / 1e3) / 1e9,
+                            "frac": model["subset_bytes"] / (ms / args.steps / 1e3) / 1e9 / peak},
         "clocks": clk,
         "data_gen_s": gen_s,
     }
@@ -285,7 +343,7 @@ def ref_threads():
 def cpu_baseline(args, subsets_in_sample=1):
     from oracle import ref
     if not ref.available():
-        return {"unavailable": "oracle/_ref/libhrrt_ref.so not built"}
+        return oracle_port_baseline(subsets_in_sample)
     T = ref_threads()
     R = ref.RefProjector(nthreads=T, **geom_dict())
     img, nf, prompts, add = ref_inputs(R)
@@ -297,6 +355,28 @@ def cpu_baseline(args, subsets_in_sample=1):
     return {"value": subsets_in_sample / dt, "unit": UNIT, "cores": T, "kind": "reference",
             "sample": f"{subsets_in_sample} OP-OSEM subset(s) of the span-3 HRRT workload on the reference projector "
                       f"(oracle/_ref/libhrrt_ref.so, -T {T} thread grouping of CalculateOsem3d)"}
+
+
+def oracle_port_baseline(subsets_in_sample=1):
+    """The C restatement (oracle/hrrt_oracle.c, f32 build) timed on the host
+    cores when the reference build is absent."""
+    from oracle.oracle import Oracle
+    T = ref_threads()
+    O = Oracle(precision="f32", nthreads=T, **geom_dict())
+    rng = np.random.default_rng(0)
+    shape = O.sino_shape
+    prompts = rng.poisson(0.64, size=shape).astype(np.int16)
+    add = np.full(shape, 0.1, np.float32)
+    nf = np.ones(O.image_shape, np.float32)
+    img = O.init_image()
+    order = O.order()
+    t0 = time.perf_counter()
+    for k in range(subsets_in_sample):
+        O.osem_subset(img, nf, prompts, add, int(order[k % SUBSETS]), T)
+    dt = time.perf_counter() - t0
+    return {"value": subsets_in_sample / dt, "unit": UNIT, "cores": min(T, O.sviews // 2), "kind": "port",
+            "sample": f"{subsets_in_sample} OP-OSEM subset(s) of the span-3 HRRT workload on the C restatement "
+                      f"(oracle/hrrt_oracle.c, {min(T, O.sviews // 2)} threads)"}
 
 
 def run_reference(args, ws, rank, local):

@@ -16,7 +16,7 @@ import os
 
 import numpy as np
 
-__all__ = ["Geometry", "HrrtError", "Context", "lib", "LIB_PATH", "STORE_F32", "STORE_16", "BP_REF",
+__all__ = ["Geometry", "HrrtError", "Context", "Listmode", "lib", "LIB_PATH", "STORE_F32", "STORE_16", "BP_REF",
            "geometry_table", "hrrt_geometry"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libhrrt_gpu.so")
@@ -53,6 +53,19 @@ class Stats(ctypes.Structure):
                 ("ms_total", ctypes.c_float)]
 
 
+class LmStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_longlong) for n in ("words_used", "prompts", "delayed", "timetags", "tags", "invalid",
+                                                  "unmapped", "doi_other", "doi7", "resyncs", "frame_start",
+                                                  "duration")] + [("terminated", ctypes.c_int), ("ms", ctypes.c_float)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+LM_TRUES, LM_PROMPTS_AND_DELAYED, LM_PROMPTS_ONLY = 0, 1, 2
+LM_IGNORE_BORDER_CRYSTAL, LM_NO_DOI, LM_TIME_FROM_COUNT = 1, 2, 4
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"{LIB_PATH} is not built; run hrrt_reconstruction_b200/build.py")
@@ -86,6 +99,13 @@ def _load():
         "hrrt_set_profiling": (i, [vp, i]),
         "hrrt_kernel_stats": (i, [vp, ctypes.c_char_p, ctypes.POINTER(i), ctypes.POINTER(d)]),
         "hrrt_reset_kernel_stats": (i, [vp]),
+        "hrrt_lm_create": (i, [i, i, i, ctypes.POINTER(vp)]),
+        "hrrt_lm_destroy": (None, [vp]),
+        "hrrt_lm_last_error": (ctypes.c_char_p, [vp]),
+        "hrrt_lm_sino_size": (ctypes.c_longlong, [vp]),
+        "hrrt_lm_reset_clock": (i, [vp]),
+        "hrrt_lm_histogram": (i, [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, ctypes.POINTER(LmStats)]),
+        "hrrt_lm_histogram_device": (i, [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, ctypes.POINTER(LmStats), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -221,9 +241,14 @@ class Context:
     def osem_subsets(self, first, count):
         self._check(lib.hrrt_osem_subsets(self._h, first, count), "osem_subsets")
 
-    def get_image(self):
+    def get_image(self, out=None):
+        """The [z][y][x] image the reference's SaveImage writes; `out`, when
+        given, is a C-contiguous float32 array of that shape to fill."""
         i = self.info
-        out = np.empty((i.nz, i.ny, i.nx), np.float32)
+        if out is None:
+            out = np.empty((i.nz, i.ny, i.nx), np.float32)
+        elif out.shape != (i.nz, i.ny, i.nx) or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise HrrtError("get_image: out must be C-contiguous float32 [nz][ny][nx]")
         self._check(lib.hrrt_get_image(self._h, _ptr(out)), "get_image")
         return out
 
@@ -294,3 +319,65 @@ class Context:
 
     def reset_kernel_stats(self):
         self._check(lib.hrrt_reset_kernel_stats(self._h), "reset_kernel_stats")
+
+
+class Listmode:
+    """64-bit HRRT listmode histogrammer on the device (hrrt_lm_* C ABI):
+    the rebinner LUT for output span 3 or 9, and the clock carried from one
+    frame to the next."""
+
+    def __init__(self, span=3, maxrd=67, device=0):
+        h = ctypes.c_void_p()
+        rc = lib.hrrt_lm_create(span, maxrd, device, ctypes.byref(h))
+        if rc != 0:
+            msg = lib.hrrt_lm_last_error(h).decode() if h.value else "hrrt_lm_create failed"
+            if h.value:
+                lib.hrrt_lm_destroy(h)
+            raise HrrtError(f"hrrt_lm_create: {msg} ({rc})")
+        self._h = h
+        self.span = span
+        self.sino_size = lib.hrrt_lm_sino_size(h)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib.hrrt_lm_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise HrrtError(f"{what}: {lib.hrrt_lm_last_error(self._h).decode()} ({rc})")
+
+    def reset_clock(self):
+        self._check(lib.hrrt_lm_reset_clock(self._h), "reset_clock")
+
+    def histogram(self, words, mode=LM_PROMPTS_AND_DELAYED, duration=0, flags=0):
+        """One frame from host words -> (sino, delayed or None, stats dict)."""
+        w = _c(words, np.uint32)
+        sino = np.empty(self.sino_size, np.uint16)
+        dly = np.empty(self.sino_size, np.uint16) if mode == LM_PROMPTS_AND_DELAYED else None
+        st = LmStats()
+        self._check(lib.hrrt_lm_histogram(self._h, _ptr(w), w.size, mode, duration, flags, _ptr(sino), _ptr(dly),
+                                          ctypes.byref(st)), "lm_histogram")
+        return sino, dly, st.as_dict()
+
+    def histogram_device(self, d_words, nwords, d_sino, d_delayed=None, mode=LM_PROMPTS_AND_DELAYED, duration=0,
+                         flags=0, stream=None):
+        """Device pointers (ints); adds into the sinograms; -> stats dict."""
+        st = LmStats()
+        self._check(lib.hrrt_lm_histogram_device(self._h, ctypes.c_void_p(d_words), nwords, mode, duration, flags,
+                                                 ctypes.c_void_p(d_sino),
+                                                 ctypes.c_void_p(d_delayed) if d_delayed else None, ctypes.byref(st),
+                                                 ctypes.c_void_p(stream) if stream else None), "lm_histogram_device")
+        return st.as_dict()

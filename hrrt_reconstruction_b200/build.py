@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhrrt_gpu.so")
 CLI = os.path.join(HERE, "hrrt_osem3d_gpu")
 
-SOURCES = ["kernels.cu", "hrrt_gpu.cu", "geometry.cpp"]
+SOURCES = ["kernels.cu", "hrrt_gpu.cu", "geometry.cpp", "listmode.cu", "lm_tables.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -37,7 +37,7 @@ def _newer(target, deps):
 
 def build_library(force=False, verbose=False):
     deps = [os.path.join(CSRC, s) for s in SOURCES]
-    deps += [os.path.join(CSRC, h) for h in ("kernels.cuh", "geometry.h")]
+    deps += [os.path.join(CSRC, h) for h in ("kernels.cuh", "geometry.h", "lm_tables.h")]
     deps += [os.path.join(ROOT, "include", "hrrt_gpu.h"), __file__]
     if not force and _newer(LIB, deps):
         return LIB

@@ -58,6 +58,13 @@ struct hrrt_ctx {
   int tpt = 1;
   bool have_inputs = false, have_sens = false, have_image = false;
 
+  // chunked upload: flat-file planes staged through two device buffers, the
+  // copy of one chunk overlapping the prep of the previous one
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+  char *stage[2] = {nullptr, nullptr};
+  size_t stage_bytes = 0;
+
   bool prof = false;
   std::vector<KernelTimer> pending;
   std::map<std::string, std::pair<int, double>> kstats;
@@ -68,11 +75,20 @@ struct hrrt_ctx {
       cudaEventDestroy(t.stop);
     }
     for (void *p : allocs) cudaFree(p);
+    for (int b = 0; b < 2; b++) {
+      if (ev_copied[b]) cudaEventDestroy(ev_copied[b]);
+      if (ev_free[b]) cudaEventDestroy(ev_free[b]);
+    }
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     if (stream) cudaStreamDestroy(stream);
   }
 };
 
 namespace {
+
+// flat-file planes per upload chunk (96 planes of 288 x 256 bins: 127 MB of
+// staging per buffer with all five inputs)
+constexpr int kUploadPlanes = 96;
 
 int fail(hrrt_ctx *ctx, int code, const std::string &msg) {
   if (ctx) ctx->err = msg;
@@ -542,7 +558,6 @@ int hrrt_upload_inputs(hrrt_ctx *ctx, const int16_t *prompts, const float *rando
   if (!prompts || !randoms) return fail(ctx, HRRT_ERR_ARG, "prompts and randoms are required");
   if (storage != HRRT_STORE_F32 && storage != HRRT_STORE_16) return fail(ctx, HRRT_ERR_ARG, "unknown storage");
   const Geometry &g = ctx->geo;
-  const size_t n = (size_t)g.segmentsize * g.nviews * g.nbins;
   cudaError_t e = cudaSuccess;
   // quad-layout inputs for every view pair (allocated once per storage type)
   if (ctx->storage != storage) {
@@ -563,44 +578,68 @@ int hrrt_upload_inputs(hrrt_ctx *ctx, const int16_t *prompts, const float *rando
     ctx->d_mask_accum = dalloc<int>(ctx, (size_t)(g.nviews / 2) * ctx->dg.nquads, &e);
     if (!ctx->d_mask_accum) return fail(ctx, HRRT_ERR_NOMEM, "mask");
   }
-  // staging of the raw flat-file arrays
+  // staging of the raw flat-file arrays, kUploadPlanes planes at a time
   const float *srcs[4] = {randoms, norm, atten, scatter};
-  float *stage[4] = {nullptr, nullptr, nullptr, nullptr};
-  int16_t *sp = nullptr;
-  std::vector<void *> tmp;
-  auto cleanup = [&]() {
-    cudaStreamSynchronize(ctx->stream);
-    for (void *p : tmp) cudaFree(p);
-  };
-  e = cudaMalloc(&sp, n * sizeof(int16_t));
-  if (e != cudaSuccess) return fail(ctx, HRRT_ERR_NOMEM, "staging");
-  tmp.push_back(sp);
-  for (int i = 0; i < 4; i++) {
-    if (!srcs[i]) continue;
-    e = cudaMalloc(&stage[i], n * sizeof(float));
-    if (e != cudaSuccess) {
-      cleanup();
-      return fail(ctx, HRRT_ERR_NOMEM, "staging");
+  const size_t plane_elems = (size_t)g.nviews * g.nbins;
+  const int CP = std::min(g.segmentsize, kUploadPlanes);
+  const size_t chunk = (size_t)CP * plane_elems;
+  const size_t need = chunk * (sizeof(int16_t) + 4 * sizeof(float));
+  if (ctx->stage_bytes < need) {
+    for (int b = 0; b < 2; b++)
+      if (ctx->stage[b]) {
+        cudaFree(ctx->stage[b]);
+        ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)ctx->stage[b]));
+        ctx->stage[b] = nullptr;
+      }
+    ctx->stage_bytes = 0;
+    for (int b = 0; b < 2; b++) {
+      ctx->stage[b] = dalloc<char>(ctx, need, &e);
+      if (!ctx->stage[b]) return fail(ctx, HRRT_ERR_NOMEM, "upload staging");
     }
-    tmp.push_back(stage[i]);
+    ctx->stage_bytes = need;
   }
-  e = cudaMemcpyAsync(sp, prompts, n * sizeof(int16_t), cudaMemcpyHostToDevice, ctx->stream);
-  for (int i = 0; i < 4 && e == cudaSuccess; i++)
-    if (srcs[i]) e = cudaMemcpyAsync(stage[i], srcs[i], n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
-  if (e == cudaSuccess)
-    e = cudaMemsetAsync(ctx->d_mask_accum, 0, sizeof(int) * (size_t)(g.nviews / 2) * ctx->dg.nquads, ctx->stream);
-  if (e == cudaSuccess) {
-    Launch L(ctx, "prep_kernel");
-    e = launch_prep(ctx->dg, g.nbins, sp, stage[0], stage[1], stage[2], stage[3], g.sp.npskip, g.sp.epsilon2,
-                    storage, ctx->q_prompts, ctx->q_add, ctx->q_mult, ctx->d_mask_accum, ctx->stream);
+  if (!ctx->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream");
+    for (int b = 0; b < 2; b++) {
+      CK(cudaEventCreateWithFlags(&ctx->ev_copied[b], cudaEventDisableTiming), "upload event");
+      CK(cudaEventCreateWithFlags(&ctx->ev_free[b], cudaEventDisableTiming), "upload event");
+    }
+  }
+  CK(cudaMemsetAsync(ctx->d_mask_accum, 0, sizeof(int) * (size_t)(g.nviews / 2) * ctx->dg.nquads, ctx->stream),
+     "upload_inputs");
+  for (int b = 0; b < 2; b++) CK(cudaEventRecord(ctx->ev_free[b], ctx->stream), "upload_inputs");
+  for (int p0 = 0, k = 0; p0 < g.segmentsize && e == cudaSuccess; p0 += CP, k++) {
+    const int b = k & 1, np = std::min(CP, g.segmentsize - p0);
+    const size_t off = (size_t)p0 * plane_elems, cnt = (size_t)np * plane_elems;
+    int16_t *sp = reinterpret_cast<int16_t *>(ctx->stage[b]);
+    float *stg[4] = {nullptr, nullptr, nullptr, nullptr};
+    e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_free[b], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(sp, prompts + off, cnt * sizeof(int16_t), cudaMemcpyHostToDevice, ctx->copy_stream);
+    for (int i = 0; i < 4 && e == cudaSuccess; i++) {
+      if (!srcs[i]) continue;
+      stg[i] = reinterpret_cast<float *>(ctx->stage[b] + chunk * sizeof(int16_t) + (size_t)i * chunk * sizeof(float));
+      e = cudaMemcpyAsync(stg[i], srcs[i] + off, cnt * sizeof(float), cudaMemcpyHostToDevice, ctx->copy_stream);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_copied[b], ctx->copy_stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_copied[b], 0);
+    if (e == cudaSuccess) {
+      Launch L(ctx, "prep_kernel");
+      e = launch_prep(ctx->dg, g.nbins, sp, stg[0], stg[1], stg[2], stg[3], g.sp.npskip, g.sp.epsilon2, storage,
+                      ctx->q_prompts, ctx->q_add, ctx->q_mult, ctx->d_mask_accum, p0, np, ctx->stream);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_free[b], ctx->stream);
   }
   if (e == cudaSuccess) e = launch_finish_mask(ctx->dg, ctx->d_mask_accum, ctx->d_nzmask, ctx->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(ctx->nzmask.data(), ctx->d_nzmask, ctx->nzmask.size() * sizeof(int16_t),
                         cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  cleanup();
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "upload_inputs");
+  if (e != cudaSuccess) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamSynchronize(ctx->stream);
+    return cuda_fail(ctx, e, "upload_inputs");
+  }
   int rc = build_work_lists(ctx);
   if (rc) return rc;
   ctx->have_inputs = true;

@@ -731,12 +731,13 @@ __global__ void prep_kernel(DevGeom g, int nbins, const int16_t *__restrict__ pr
                             const float *__restrict__ randoms, const float *__restrict__ norm,
                             const float *__restrict__ atten, const float *__restrict__ scatter, int npskip,
                             float eps2, PT *__restrict__ qp, AT *__restrict__ qadd, AT *__restrict__ qmult,
-                            int *__restrict__ mask_accum, int planes_per_thread) {
+                            int *__restrict__ mask_accum, int planes_per_thread, int plane0, int nplanes) {
+  // the inputs hold planes [plane0, plane0 + nplanes) of the flat-file arrays
   const int x = blockIdx.x * blockDim.x + threadIdx.x;  // quad
   const int vi = blockIdx.z;                            // pair
   if (x >= g.nquads) return;
-  const int gp0 = blockIdx.y * planes_per_thread;
-  const int gp1 = min(gp0 + planes_per_thread, g.segmentsize);
+  const int gp0 = plane0 + blockIdx.y * planes_per_thread;
+  const int gp1 = min(gp0 + planes_per_thread, plane0 + nplanes);
   const int V = g.nviews, half = V / 2;
   int views[4] = {vi, vi, vi + half, vi + half};
   int bins[4] = {x, nbins - x, x, nbins - x};
@@ -752,7 +753,7 @@ __global__ void prep_kernel(DevGeom g, int nbins, const int16_t *__restrict__ pr
     for (int l = 0; l < 4; l++) {
       pv[l] = av[l] = mv[l] = 0.f;
       if (!ok[l]) continue;
-      const size_t i = ((size_t)gp * V + views[l]) * nbins + bins[l];
+      const size_t i = ((size_t)(gp - plane0) * V + views[l]) * nbins + bins[l];
       const float nz = norm ? (kill ? 0.f : __ldg(norm + i)) : 1.0f;
       const float araw = atten ? __ldg(atten + i) : 1.0f;
       const float ac = (araw < 1.0f) ? 1.0f : araw;
@@ -821,12 +822,21 @@ __global__ void post_iter_kernel(DevGeom g, float *__restrict__ image, double *_
   }
   if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
 }
+// One block: each thread sums a contiguous run of partials, then a fixed
+// tree adds the runs -- the same order on every call (deterministic).
 __global__ void sum_partials_kernel(const double *__restrict__ partial, int n, double *__restrict__ out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    double s = 0.0;
-    for (int i = 0; i < n; i++) s += partial[i];
-    *out = s;
+  __shared__ double red[1024];
+  const int t = threadIdx.x, T = blockDim.x;
+  const int per = (n + T - 1) / T, b = t * per, e = min(b + per, n);
+  double s = 0.0;
+  for (int i = b; i < e; i++) s += partial[i];
+  red[t] = s;
+  __syncthreads();
+  for (int k = T / 2; k > 0; k >>= 1) {
+    if (t < k) red[t] += red[t + k];
+    __syncthreads();
   }
+  if (t == 0) *out = red[0];
 }
 
 __global__ void rows_to_quad_kernel(DevGeom g, int nbins, const float *__restrict__ rows, float4 *__restrict__ quad,
@@ -997,17 +1007,18 @@ cudaError_t launch_rotpos(const DevGeom &g, float2 *rotpos, const int *row_start
 
 cudaError_t launch_prep(const DevGeom &g, int nbins, const int16_t *prompts, const float *randoms, const float *norm,
                         const float *atten, const float *scatter, int npskip, float eps2, int storage, void *q_prompts,
-                        void *q_add, void *q_mult, int *quad_mask_accum, cudaStream_t st) {
-  const int ppt = 32;
-  dim3 grid((g.nquads + 127) / 128, (g.segmentsize + ppt - 1) / ppt, g.nviews / 2);
+                        void *q_add, void *q_mult, int *quad_mask_accum, int plane0, int nplanes,
+                        cudaStream_t st) {
+  const int ppt = 16;
+  dim3 grid((g.nquads + 127) / 128, (nplanes + ppt - 1) / ppt, g.nviews / 2);
   if (storage == 0)
     prep_kernel<int16_t, float><<<grid, 128, 0, st>>>(g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2,
                                                       (int16_t *)q_prompts, (float *)q_add, (float *)q_mult,
-                                                      quad_mask_accum, ppt);
+                                                      quad_mask_accum, ppt, plane0, nplanes);
   else
     prep_kernel<__half, __nv_bfloat16><<<grid, 128, 0, st>>>(
         g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (__half *)q_prompts, (__nv_bfloat16 *)q_add,
-        (__nv_bfloat16 *)q_mult, quad_mask_accum, ppt);
+        (__nv_bfloat16 *)q_mult, quad_mask_accum, ppt, plane0, nplanes);
   return cudaGetLastError();
 }
 
@@ -1040,7 +1051,7 @@ cudaError_t launch_post_iteration(const DevGeom &g, float *image, double *partia
   const long long n = (long long)g.fov_columns * (g.z_max - g.z_min);
   const int blocks = (int)((n + 255) / 256);
   post_iter_kernel<<<blocks, 256, 0, st>>>(g, image, partial);
-  sum_partials_kernel<<<1, 32, 0, st>>>(partial, blocks, sum);
+  sum_partials_kernel<<<1, 1024, 0, st>>>(partial, blocks, sum);
   return cudaGetLastError();
 }
 

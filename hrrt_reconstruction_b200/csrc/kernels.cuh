@@ -100,7 +100,8 @@ cudaError_t launch_rotback(const DevGeom &g, const int *pair_views, int npairs, 
 cudaError_t launch_rotpos(const DevGeom &g, float2 *rotpos, const int *row_start, cudaStream_t st);
 cudaError_t launch_prep(const DevGeom &g, int nbins, const int16_t *prompts, const float *randoms, const float *norm,
                         const float *atten, const float *scatter, int npskip, float eps2, int storage, void *q_prompts,
-                        void *q_add, void *q_mult, int *quad_mask_accum, cudaStream_t st);
+                        void *q_add, void *q_mult, int *quad_mask_accum, int plane0, int nplanes,
+                        cudaStream_t st);
 cudaError_t launch_finish_mask(const DevGeom &g, const int *accum, int16_t *nzmask, cudaStream_t st);
 cudaError_t launch_init_image(const DevGeom &g, float *image, cudaStream_t st);
 cudaError_t launch_post_iteration(const DevGeom &g, float *image, double *partial, double *sum, cudaStream_t st);

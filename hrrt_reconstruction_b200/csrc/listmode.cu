@@ -1,0 +1,661 @@
+// listmode.cu -- HRRT 64-bit listmode histogramming on the device.
+//
+// The reference (lmhistogram_mp/histogram_mp.cpp, LM_Rebinner_mp.cpp) reads
+// the stream in packets of 1 Mi 64-bit events (LM_Reader_mp.hpp:39), decodes
+// each packet from its first word -- an out-of-sync word pair advances the
+// parse by one word, anything else by two (histogram_mp.cpp:1055-1066) --
+// rebins events through a crystal-pair LUT, and increments 16-bit bins in
+// stream order until a time tag ends the frame.
+//
+// Device design.  The word stream is cut into tiles of kTileWords words (a
+// tile never straddles a packet); a block of 256 threads owns a tile, each
+// thread 16 consecutive words.  Where a thread's parse starts depends on the
+// words before it, but only through one bit: whether the previous event
+// ended on the thread's first word or ran one word into it.  Each thread
+// therefore parses its words twice (entering at offset 0 and at offset 1),
+// which yields a 2-state map (entry -> exit) plus the number of time tags
+// seen for each entry.  Maps compose associatively, so
+//   lm_map_kernel   : block scan -> one composed map per tile;
+//   lm_entry_kernel : one thread per packet walks its tiles -> tile entry
+//                     offsets and per-tile time-tag offsets;
+//   lm_scan_kernel  : exclusive scan of the per-packet tag counts;
+//   lm_hist_kernel  : re-derives each thread's entry with the same block
+//                     scan, parses its words once, writes the time tags in
+//                     stream order and (below the frame limit) adds the
+//                     events to the sinograms.
+// The frame end is found on the host from the ordered time tags (the clock
+// logic of process_tagword, histogram_mp.cpp:225-260); when a frame length
+// is given the histogram pass runs after it with the limit.
+//
+// Bins are 16-bit and wrap (the reference's short sinogram).  Two bins share
+// a 32-bit word; an increment of the low half that wraps carries into the
+// high half, which the thread that caused it takes back with a second atomic
+// -- the sum of all updates is exact modulo 2^16 per bin whatever the order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/hrrt_gpu.h"
+#include "lm_tables.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kSub = 16;                       // words per thread
+constexpr int kTileWords = kThreads * kSub;    // 4096
+constexpr long long kPacketWords = 2LL << 20;  // 1 Mi 64-bit events
+static_assert(kPacketWords % kTileWords == 0, "tiles must not straddle packets");
+constexpr int kSinoPlane = 256 * 288;
+// EWTYPES (geometry_info.h:76) packed two bits per entry: index =
+// (ew1 >> 30) << 2 | (ew2 >> 30); 0 prompt, 1 delayed, 2 tag, 3 out of sync
+constexpr uint32_t kEwTypes = (3u << 0) | (3u << 2) | (1u << 4) | (0u << 6) | (3u << 8) | (3u << 10) | (2u << 12) |
+                              (2u << 14) | 0xFFFF0000u;
+
+struct LmDev {
+  const hrrt::LmSol *sol;   // [21][144][144]
+  const float *zpos, *zpos2;  // [104]
+  const int *segz0, *segzmax, *segzoff;  // [nsegs]
+  int nsegs;
+  long long sino_size;
+};
+
+enum : int { kStPrompts, kStDelayed, kStTimetags, kStTags, kStInvalid, kStUnmapped, kStDoiOther, kStDoi7, kStResync,
+             kStCount };
+
+__device__ __forceinline__ int ewtype(uint32_t ew1, uint32_t ew2) {
+  return (kEwTypes >> (2 * (((ew1 >> 30) << 2) | (ew2 >> 30)))) & 3;
+}
+
+// A thread's parse summary: bit e of `map` = exit offset when entering at e;
+// c0 / c1 = time tags seen when entering at 0 / 1.
+struct Sub {
+  uint32_t map, c0, c1;
+};
+__device__ __forceinline__ Sub compose(const Sub &a, const Sub &b) {  // a then b
+  const uint32_t a0 = a.map & 1, a1 = (a.map >> 1) & 1;
+  Sub h;
+  h.map = ((b.map >> a0) & 1) | (((b.map >> a1) & 1) << 1);
+  h.c0 = a.c0 + (a0 ? b.c1 : b.c0);
+  h.c1 = a.c1 + (a1 ? b.c1 : b.c0);
+  return h;
+}
+__device__ __forceinline__ bool is_timetag(uint32_t ew1, uint32_t ew2) {
+  const uint32_t tag = (ew1 & 0xffff) | ((ew2 & 0xffff) << 16);
+  return (tag & 0xE0000000u) == 0x80000000u;
+}
+
+// Parse positions [s + e, s + kSub) of the staged tile; `pend` is where the
+// packet (or the stream) ends, relative to the tile.
+__device__ __forceinline__ void sub_parse(const uint32_t *w, int s, int e, int pend, uint32_t &exit_off,
+                                          uint32_t &ntags) {
+  int pos = s + e;
+  ntags = 0;
+  while (pos < s + kSub) {
+    if (pos + 1 >= pend) {  // the packet's last word has no partner
+      exit_off = 0;
+      return;
+    }
+    const uint32_t a = w[pos], b = w[pos + 1];
+    const int t = ewtype(a, b);
+    if (t == 2 && is_timetag(a, b)) ntags++;
+    pos += (t == 3) ? 1 : 2;
+  }
+  exit_off = (uint32_t)(pos - (s + kSub));
+}
+
+__device__ __forceinline__ Sub sub_summary(const uint32_t *w, int s, int pend) {
+  Sub r;
+  uint32_t x0, x1;
+  sub_parse(w, s, 0, pend, x0, r.c0);
+  sub_parse(w, s, 1, pend, x1, r.c1);
+  r.map = x0 | (x1 << 1);
+  return r;
+}
+
+__device__ __forceinline__ Sub shfl_up_sub(const Sub &v, int d) {
+  Sub o;
+  o.map = __shfl_up_sync(0xffffffffu, v.map, d);
+  o.c0 = __shfl_up_sync(0xffffffffu, v.c0, d);
+  o.c1 = __shfl_up_sync(0xffffffffu, v.c1, d);
+  return o;
+}
+
+// Inclusive block scan of Sub (composition in thread order); also returns
+// the exclusive prefix of this thread.  Identity: map 0b10 (0->0, 1->1).
+__device__ void block_scan(Sub v, Sub &incl, Sub &excl, Sub *warp_tot) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  Sub x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const Sub o = shfl_up_sub(x, d);
+    if (lane >= d) x = compose(o, x);
+  }
+  if (lane == 31) warp_tot[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    Sub t = lane < kThreads / 32 ? warp_tot[lane] : Sub{2u, 0u, 0u};
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const Sub o = shfl_up_sub(t, d);
+      if (lane >= d) t = compose(o, t);
+    }
+    if (lane < kThreads / 32) warp_tot[lane] = t;  // inclusive over warps
+  }
+  __syncthreads();
+  incl = (wid > 0) ? compose(warp_tot[wid - 1], x) : x;
+  const Sub prev_lane = shfl_up_sub(x, 1);
+  const Sub in_warp = (lane > 0) ? prev_lane : Sub{2u, 0u, 0u};
+  excl = (wid > 0) ? compose(warp_tot[wid - 1], in_warp) : in_warp;
+}
+
+// Stage the tile (plus one halo word) in shared memory; returns `pend`.
+__device__ __forceinline__ int stage_tile(const uint32_t *__restrict__ words, long long n, long long t0, uint32_t *w) {
+  const long long pkt_end = (t0 / kPacketWords + 1) * kPacketWords;
+  const long long lim = pkt_end < n ? pkt_end : n;
+  const long long avail = lim - t0;
+  const int pend = (int)(avail < kTileWords + 1 ? avail : (long long)kTileWords + 1);
+  const uint4 *src = reinterpret_cast<const uint4 *>(words + t0);
+  const int nvec = (pend >= kTileWords) ? kTileWords / 4 : pend / 4;
+  for (int i = threadIdx.x; i < nvec; i += kThreads) reinterpret_cast<uint4 *>(w)[i] = __ldg(src + i);
+  for (int i = nvec * 4 + threadIdx.x; i < pend; i += kThreads) w[i] = __ldg(words + t0 + i);
+  for (int i = pend + threadIdx.x; i < kTileWords + 1; i += kThreads) w[i] = 0u;
+  __syncthreads();
+  return pend;
+}
+
+__global__ void __launch_bounds__(kThreads) lm_map_kernel(const uint32_t *__restrict__ words, long long n,
+                                                          unsigned long long *__restrict__ tile_sum) {
+  __shared__ __align__(16) uint32_t w[kTileWords + 4];
+  __shared__ Sub wt[32];
+  const long long t0 = (long long)blockIdx.x * kTileWords;
+  const int pend = stage_tile(words, n, t0, w);
+  const Sub v = sub_summary(w, threadIdx.x * kSub, pend);
+  Sub incl, excl;
+  block_scan(v, incl, excl, wt);
+  if (threadIdx.x == kThreads - 1)
+    tile_sum[blockIdx.x] = (unsigned long long)incl.map | ((unsigned long long)incl.c0 << 16) |
+                           ((unsigned long long)incl.c1 << 40);
+}
+
+// One thread per packet: tile entries and tag offsets within the packet.
+__global__ void lm_entry_kernel(const unsigned long long *__restrict__ tile_sum, long long ntiles, int tiles_per_packet,
+                                long long npackets, uint8_t *__restrict__ tile_entry,
+                                unsigned int *__restrict__ tile_tagoff, unsigned long long *__restrict__ packet_tags) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npackets) return;
+  const long long t_begin = p * tiles_per_packet;
+  const long long t_end = min(t_begin + tiles_per_packet, ntiles);
+  uint32_t e = 0;
+  unsigned long long off = 0;
+  for (long long t = t_begin; t < t_end; t++) {
+    const unsigned long long s = tile_sum[t];
+    tile_entry[t] = (uint8_t)e;
+    tile_tagoff[t] = (unsigned int)off;
+    off += e ? ((s >> 40) & 0xFFFFFF) : ((s >> 16) & 0xFFFFFF);
+    e = (uint32_t)((s >> e) & 1);
+  }
+  packet_tags[p] = off;
+}
+
+// Exclusive scan of the per-packet tag counts (one block).
+__global__ void lm_scan_kernel(unsigned long long *__restrict__ v, long long n, unsigned long long *__restrict__ total) {
+  __shared__ unsigned long long part[1024];
+  const int t = threadIdx.x, T = blockDim.x;
+  const long long per = (n + T - 1) / T, b = t * per, e = min(b + per, n);
+  unsigned long long s = 0;
+  for (long long i = b; i < e; i++) s += v[i];
+  part[t] = s;
+  __syncthreads();
+  if (t == 0) {
+    unsigned long long run = 0;
+    for (int i = 0; i < T; i++) {
+      const unsigned long long x = part[i];
+      part[i] = run;
+      run += x;
+    }
+    *total = run;
+  }
+  __syncthreads();
+  unsigned long long run = part[t];
+  for (long long i = b; i < e; i++) {
+    const unsigned long long x = v[i];
+    v[i] = run;
+    run += x;
+  }
+}
+
+__device__ __forceinline__ void bump16(uint32_t *__restrict__ bins, long long addr, bool minus) {
+  uint32_t *w = bins + (addr >> 1);
+  const uint32_t hi = (uint32_t)(addr & 1);
+  const uint32_t inc = minus ? 0xFFFFu : 1u;
+  const uint32_t old = atomicAdd(w, inc << (16 * hi));
+  if (!hi && (old & 0xFFFFu) + inc > 0xFFFFu) atomicSub(w, 0x10000u);  // undo the carry into the high bin
+}
+
+// rebin_event (LM_Rebinner_mp.cpp:188-219): address or -1
+__device__ __forceinline__ long long rebin(const LmDev &g, const float *zp, const float *zp2, int mp, int al, int ax,
+                                           int ay, int bl, int bx, int by) {
+  const hrrt::LmSol s = g.sol[((size_t)mp * 144 + ax + 72 * al) * 144 + bx + 72 * bl];
+  if (s.nsino == -1) return -1;
+  const float cay = zp2[ay];
+  const float dz2 = __fsub_rn(zp[by], zp[ay]);
+  const int plane = (int)__fadd_rn(cay, __fmul_rn(s.z, dz2));
+  const float seg = (float)(0.5 + (double)__fmul_rn(dz2, s.d));
+  int segnum = (int)seg;
+  segnum = (seg < 0) ? 1 - 2 * segnum : 2 * segnum;
+  if (segnum >= g.nsegs) return -1;
+  if (plane < 0 || plane > 206) return -1;
+  if (plane < g.segz0[segnum] || plane > g.segzmax[segnum]) return -1;
+  return (long long)(plane + g.segzoff[segnum]) * kSinoPlane + s.nsino;
+}
+
+template <bool kHist>
+__global__ void __launch_bounds__(kThreads) lm_hist_kernel(
+    LmDev g, const uint32_t *__restrict__ words, long long n, const uint8_t *__restrict__ tile_entry,
+    const unsigned int *__restrict__ tile_tagoff, const unsigned long long *__restrict__ packet_tagoff,
+    int tiles_per_packet, long long limit, int mode, int flags, long long tag_cap, longlong2 *__restrict__ tags,
+    uint32_t *__restrict__ sino, uint32_t *__restrict__ dly, unsigned long long *__restrict__ stats) {
+  __shared__ __align__(16) uint32_t w[kTileWords + 4];
+  __shared__ Sub wt[32];
+  __shared__ float zp[104], zp2[104];
+  __shared__ unsigned long long st[kStCount];
+  if (threadIdx.x < 104) {
+    zp[threadIdx.x] = g.zpos[threadIdx.x];
+    zp2[threadIdx.x] = g.zpos2[threadIdx.x];
+  }
+  if (threadIdx.x < kStCount) st[threadIdx.x] = 0;
+  const long long tile = blockIdx.x;
+  const long long t0 = tile * kTileWords;
+  const int pend = stage_tile(words, n, t0, w);
+  const int s = threadIdx.x * kSub;
+  const Sub v = sub_summary(w, s, pend);
+  Sub incl, excl;
+  block_scan(v, incl, excl, wt);
+  const uint32_t te = tile_entry[tile];
+  const int e = (int)((excl.map >> te) & 1);
+  unsigned long long tagpos = packet_tagoff[tile / tiles_per_packet] + tile_tagoff[tile] + (te ? excl.c1 : excl.c0);
+
+  const bool doi = (flags & HRRT_LM_NO_DOI) == 0;
+  const bool border = (flags & HRRT_LM_IGNORE_BORDER_CRYSTAL) != 0;
+  const int xhigh = border ? 71 : 72;
+  uint32_t c[kStCount] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  int pos = s + e;
+  while (pos < s + kSub) {
+    if (pos + 1 >= pend) break;
+    const long long gp = t0 + pos;
+    const uint32_t ew1 = w[pos], ew2 = w[pos + 1];
+    const int type = ewtype(ew1, ew2);
+    if (type == 3) {
+      if (gp < limit) c[kStResync]++;
+      pos += 1;
+      continue;
+    }
+    pos += 2;
+    if (type == 2) {
+      const uint32_t tag = (ew1 & 0xffff) | ((ew2 & 0xffff) << 16);
+      const bool timetag = (tag & 0xE0000000u) == 0x80000000u;
+      if (timetag) {
+        if (tag_cap > 0 && (long long)tagpos < tag_cap) tags[tagpos] = make_longlong2(gp, (long long)tag);
+        tagpos++;
+      }
+      if (gp >= limit) continue;
+      c[kStTags]++;
+      if (timetag) c[kStTimetags]++;
+      if (tag & 0x80000000u) continue;
+      // a tag value with bit 31 clear reads as an event word
+      const bool prompt = (tag & 0x40000000u) != 0;
+      c[prompt ? kStPrompts : kStDelayed]++;
+      const long long addr = tag & 0x3fffffff;
+      if (kHist && addr < g.sino_size) {
+        if (mode == HRRT_LM_PROMPTS_AND_DELAYED)
+          bump16(prompt ? sino : dly, addr, false);
+        else
+          bump16(sino, addr, !prompt);
+      }
+      continue;
+    }
+    if (gp >= limit) continue;
+    // coincidence event (rebin_packet, histogram_mp.cpp:1114-1225)
+    const int mpe = ((ew1 >> 16) & 7) | (((ew2 >> 16) & 7) << 3);
+    const int ax = ew1 & 0xff, ay = (ew1 >> 8) & 0xff, bx = ew2 & 0xff, by = (ew2 >> 8) & 0xff;
+    const int doia = doi ? (int)((ew1 >> 22) & 7) : 1, doib = doi ? (int)((ew2 >> 22) & 7) : 1;
+    if (mpe < 1 || mpe > 20 || ax >= 72 || ay >= 104 || bx >= 72 || by >= 104) {
+      c[kStInvalid]++;
+      continue;
+    }
+    if (doia == 7 || doib == 7) {
+      c[kStDoi7]++;
+      continue;
+    }
+    if (doia > 1 || doib > 1) {
+      c[kStDoiOther]++;
+      continue;
+    }
+    long long addr = -1;
+    if (!(border && (ax * bx == 0 || ax == xhigh || bx == xhigh)) && !(mode == HRRT_LM_PROMPTS_ONLY && type != 0))
+      addr = rebin(g, zp, zp2, mpe, doia, ax, ay, doib, bx, by);
+    if (addr < 0) {
+      c[kStUnmapped]++;
+      continue;
+    }
+    c[type == 0 ? kStPrompts : kStDelayed]++;
+    if (kHist) {
+      if (mode == HRRT_LM_PROMPTS_AND_DELAYED)
+        bump16(type == 0 ? sino : dly, addr, false);
+      else
+        bump16(sino, addr, type != 0);
+    }
+  }
+  // block reduction of the counters
+#pragma unroll
+  for (int k = 0; k < kStCount; k++) {
+    uint32_t x = c[k];
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(&st[k], (unsigned long long)x);
+  }
+  __syncthreads();
+  if (threadIdx.x < kStCount && st[threadIdx.x]) atomicAdd(&stats[threadIdx.x], st[threadIdx.x]);
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+struct hrrt_lm {
+  hrrt::LmTables tab;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  LmDev dev{};
+  std::vector<void *> allocs;
+  // scratch grown on demand
+  void *scratch = nullptr;
+  size_t scratch_bytes = 0;
+  uint32_t *h_words_dev = nullptr;  // host-API staging
+  size_t h_words_cap = 0;
+  uint16_t *h_sino_dev = nullptr;   // host-API sinograms (prompts, delayed)
+  // clock carried across frames (process_tagword's statics)
+  long long current_time = -1, current_time_msec = -1, prev_time = 0;
+  int clock_reset = 0;
+  ~hrrt_lm() {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(device);
+    for (void *p : allocs) cudaFree(p);
+    if (scratch) cudaFree(scratch);
+    if (h_words_dev) cudaFree(h_words_dev);
+    if (h_sino_dev) cudaFree(h_sino_dev);
+    if (stream) cudaStreamDestroy(stream);
+    cudaSetDevice(cur);
+  }
+};
+
+namespace {
+
+int lm_fail(hrrt_lm *h, int code, const std::string &m) {
+  if (h) h->err = m;
+  return code;
+}
+int lm_cuda(hrrt_lm *h, cudaError_t e, const char *where) {
+  return lm_fail(h, HRRT_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+T *lm_upload(hrrt_lm *h, const std::vector<T> &v, cudaError_t *e) {
+  T *p = nullptr;
+  *e = cudaMalloc(&p, sizeof(T) * std::max<size_t>(v.size(), 1));
+  if (*e != cudaSuccess) return nullptr;
+  h->allocs.push_back(p);
+  *e = cudaMemcpy(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice);
+  return p;
+}
+
+// process_tagword's time-tag branch (histogram_mp.cpp:225-260) over the
+// ordered time tags; returns the index of the tag that ends the frame or -1.
+long long replay_clock(hrrt_lm *h, const longlong2 *tags, long long ntags, int duration, int flags,
+                       long long *frame_start) {
+  for (long long i = 0; i < ntags; i++) {
+    const uint32_t tag = (uint32_t)tags[i].y;
+    if (flags & HRRT_LM_TIME_FROM_COUNT)
+      h->current_time_msec++;
+    else
+      h->current_time_msec = tag & 0x3fffffff;
+    if (h->prev_time > h->current_time_msec && !h->clock_reset) {
+      h->current_time = h->current_time_msec / 1000;
+      h->clock_reset = 1;
+      continue;
+    }
+    h->prev_time = h->current_time_msec;
+    if (h->current_time != h->current_time_msec / 1000) {
+      h->current_time = h->current_time_msec / 1000;
+      if (*frame_start < 0) *frame_start = h->current_time;
+      if (duration > 0 && h->current_time - *frame_start >= duration) return i;
+    }
+  }
+  return -1;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hrrt_lm_create(int span, int maxrd, int device, hrrt_lm **out) {
+  if (!out) return HRRT_ERR_ARG;
+  *out = nullptr;
+  std::unique_ptr<hrrt_lm> h(new hrrt_lm());
+  std::string m = h->tab.build(span, maxrd);
+  if (!m.empty()) {
+    hrrt_lm *raw = h.release();
+    raw->err = m;
+    *out = raw;
+    return HRRT_ERR_ARG;
+  }
+  h->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  LmDev &d = h->dev;
+  if (e == cudaSuccess) d.sol = lm_upload(h.get(), h->tab.sol, &e);
+  if (e == cudaSuccess) d.zpos = lm_upload(h.get(), h->tab.zpos, &e);
+  if (e == cudaSuccess) d.zpos2 = lm_upload(h.get(), h->tab.zpos2, &e);
+  if (e == cudaSuccess) d.segz0 = lm_upload(h.get(), h->tab.segz0, &e);
+  if (e == cudaSuccess) d.segzmax = lm_upload(h.get(), h->tab.segzmax, &e);
+  if (e == cudaSuccess) d.segzoff = lm_upload(h.get(), h->tab.segzoffset, &e);
+  d.nsegs = h->tab.nsegs;
+  d.sino_size = h->tab.sino_size();
+  if (e != cudaSuccess) {
+    hrrt_lm *raw = h.release();
+    lm_cuda(raw, e, "hrrt_lm_create");
+    *out = raw;
+    return HRRT_ERR_CUDA;
+  }
+  *out = h.release();
+  return HRRT_OK;
+}
+
+void hrrt_lm_destroy(hrrt_lm *h) { delete h; }
+
+const char *hrrt_lm_last_error(const hrrt_lm *h) { return h ? h->err.c_str() : "null listmode context"; }
+
+long long hrrt_lm_sino_size(const hrrt_lm *h) { return h ? h->tab.sino_size() : -1; }
+
+int hrrt_lm_reset_clock(hrrt_lm *h) {
+  if (!h) return HRRT_ERR_ARG;
+  h->current_time = -1;
+  h->current_time_msec = -1;
+  h->prev_time = 0;
+  h->clock_reset = 0;
+  return HRRT_OK;
+}
+
+int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwords, int mode, int duration, int flags,
+                             uint16_t *d_sino, uint16_t *d_delayed, hrrt_lm_stats *out, void *stream) {
+  if (!h) return HRRT_ERR_ARG;
+  if (nwords < 0 || (nwords > 0 && !d_words) || !d_sino || !out)
+    return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_histogram: null buffer or negative length");
+  if (mode != HRRT_LM_TRUES && mode != HRRT_LM_PROMPTS_AND_DELAYED && mode != HRRT_LM_PROMPTS_ONLY)
+    return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_histogram: unknown mode");
+  if (mode == HRRT_LM_PROMPTS_AND_DELAYED && !d_delayed)
+    return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_histogram: the delayed sinogram is required in this mode");
+  if (((uintptr_t)d_words & 15) || ((uintptr_t)d_sino & 3) || ((uintptr_t)d_delayed & 3))
+    return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_histogram: words need 16-byte, sinograms 4-byte alignment");
+  memset(out, 0, sizeof(*out));
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_histogram");
+  long long frame_start = h->current_time >= 0 ? h->current_time : -1;
+  if (nwords == 0) {
+    out->frame_start = frame_start;
+    return HRRT_OK;
+  }
+  const long long ntiles = (nwords + kTileWords - 1) / kTileWords;
+  const int tpp = (int)(kPacketWords / kTileWords);
+  const long long npackets = (nwords + kPacketWords - 1) / kPacketWords;
+  // time tags: at most one per two words
+  const long long tag_cap = nwords / 2 + 1;
+  // scratch: tile sums (8), entries (1), tag offsets (4) per tile; packet
+  // offsets (8) per packet; stats; tags (16 each)
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t b_sum = al(8 * ntiles), b_ent = al(ntiles), b_off = al(4 * ntiles), b_pk = al(8 * (npackets + 1)),
+               b_st = al(8 * (kStCount + 1)), b_tags = al(16 * tag_cap);
+  const size_t need = b_sum + b_ent + b_off + b_pk + b_st + b_tags;
+  if (h->scratch_bytes < need) {
+    if (h->scratch) cudaFree(h->scratch);
+    h->scratch = nullptr;
+    h->scratch_bytes = 0;
+    e = cudaMalloc(&h->scratch, need);
+    if (e != cudaSuccess) return lm_fail(h, HRRT_ERR_NOMEM, "hrrt_lm_histogram: scratch");
+    h->scratch_bytes = need;
+  }
+  char *p = (char *)h->scratch;
+  auto *tile_sum = (unsigned long long *)p;
+  auto *tile_entry = (uint8_t *)(p + b_sum);
+  auto *tile_tagoff = (unsigned int *)(p + b_sum + b_ent);
+  auto *pk = (unsigned long long *)(p + b_sum + b_ent + b_off);
+  auto *stats = (unsigned long long *)(p + b_sum + b_ent + b_off + b_pk);
+  auto *tags = (longlong2 *)(p + b_sum + b_ent + b_off + b_pk + b_st);
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEventCreate(&ev0);
+  cudaEventCreate(&ev1);
+  cudaEventRecord(ev0, st);
+  e = cudaMemsetAsync(stats, 0, 8 * (kStCount + 1), st);
+  if (e == cudaSuccess) {
+    lm_map_kernel<<<(unsigned)ntiles, kThreads, 0, st>>>(d_words, nwords, tile_sum);
+    lm_entry_kernel<<<(unsigned)((npackets + 127) / 128), 128, 0, st>>>(tile_sum, ntiles, tpp, npackets, tile_entry,
+                                                                       tile_tagoff, pk);
+    lm_scan_kernel<<<1, 1024, 0, st>>>(pk, npackets, stats + kStCount);
+    e = cudaGetLastError();
+  }
+  // pass 1: ordered time tags (and, without a frame length, the histogram)
+  const bool one_pass = duration <= 0;
+  if (e == cudaSuccess) {
+    const long long lim = one_pass ? nwords : -1;
+    if (one_pass)
+      lm_hist_kernel<true><<<(unsigned)ntiles, kThreads, 0, st>>>(
+          h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim, mode, flags, tag_cap, tags,
+          (uint32_t *)d_sino, (uint32_t *)d_delayed, stats);
+    else
+      lm_hist_kernel<false><<<(unsigned)ntiles, kThreads, 0, st>>>(
+          h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim, mode, flags, tag_cap, tags,
+          (uint32_t *)d_sino, (uint32_t *)d_delayed, stats);
+    e = cudaGetLastError();
+  }
+  unsigned long long ntags = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&ntags, stats + kStCount, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  std::vector<longlong2> htags;
+  if (e == cudaSuccess && ntags > 0) {
+    htags.resize(ntags);
+    e = cudaMemcpyAsync(htags.data(), tags, 16 * ntags, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  }
+  if (e != cudaSuccess) {
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    return lm_cuda(h, e, "hrrt_lm_histogram");
+  }
+  const long long end_tag = replay_clock(h, htags.data(), (long long)ntags, duration, flags, &frame_start);
+  long long limit = nwords;
+  if (end_tag >= 0) limit = htags[end_tag].x;
+  if (!one_pass) {
+    lm_hist_kernel<true><<<(unsigned)ntiles, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk,
+                                                                tpp, limit, mode, flags, 0, tags, (uint32_t *)d_sino,
+                                                                (uint32_t *)d_delayed, stats);
+    e = cudaGetLastError();
+  }
+  unsigned long long hs[kStCount] = {};
+  cudaEventRecord(ev1, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hs, stats, 8 * kStCount, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_histogram");
+  // the time tags below the limit, and the tag that ends the frame itself
+  out->prompts = (long long)hs[kStPrompts];
+  out->delayed = (long long)hs[kStDelayed];
+  out->timetags = (long long)hs[kStTimetags] + (end_tag >= 0 ? 1 : 0);
+  out->tags = (long long)hs[kStTags] + (end_tag >= 0 ? 1 : 0);
+  out->invalid = (long long)hs[kStInvalid];
+  out->unmapped = (long long)hs[kStUnmapped];
+  out->doi_other = (long long)hs[kStDoiOther];
+  out->doi7 = (long long)hs[kStDoi7];
+  out->resyncs = (long long)hs[kStResync];
+  out->terminated = end_tag >= 0;
+  out->words_used = end_tag >= 0 ? limit + 2 : nwords;
+  if (end_tag < 0) h->current_time = (h->current_time_msec + 500) / 1000;
+  out->frame_start = frame_start;
+  out->duration = h->current_time - frame_start;
+  out->ms = ms;
+  return HRRT_OK;
+}
+
+int hrrt_lm_histogram(hrrt_lm *h, const uint32_t *words, long long nwords, int mode, int duration, int flags,
+                      uint16_t *sino, uint16_t *delayed, hrrt_lm_stats *out) {
+  if (!h) return HRRT_ERR_ARG;
+  if (nwords < 0 || (nwords > 0 && !words) || !sino || !out)
+    return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_histogram: null buffer or negative length");
+  if (mode == HRRT_LM_PROMPTS_AND_DELAYED && !delayed)
+    return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_histogram: the delayed sinogram is required in this mode");
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_histogram");
+  const long long S = h->tab.sino_size();
+  if (!h->h_sino_dev) {
+    e = cudaMalloc(&h->h_sino_dev, sizeof(uint16_t) * 2 * (size_t)S);
+    if (e != cudaSuccess) {
+      h->h_sino_dev = nullptr;
+      return lm_fail(h, HRRT_ERR_NOMEM, "hrrt_lm_histogram: sinograms");
+    }
+  }
+  if ((size_t)nwords > h->h_words_cap) {
+    if (h->h_words_dev) cudaFree(h->h_words_dev);
+    h->h_words_dev = nullptr;
+    h->h_words_cap = 0;
+    e = cudaMalloc(&h->h_words_dev, sizeof(uint32_t) * std::max<long long>(nwords, 4));
+    if (e != cudaSuccess) return lm_fail(h, HRRT_ERR_NOMEM, "hrrt_lm_histogram: event staging");
+    h->h_words_cap = (size_t)nwords;
+  }
+  cudaStream_t st = h->stream;
+  e = cudaMemsetAsync(h->h_sino_dev, 0, sizeof(uint16_t) * 2 * (size_t)S, st);
+  if (e == cudaSuccess && nwords > 0)
+    e = cudaMemcpyAsync(h->h_words_dev, words, sizeof(uint32_t) * nwords, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_histogram");
+  int rc = hrrt_lm_histogram_device(h, h->h_words_dev, nwords, mode, duration, flags, h->h_sino_dev,
+                                    h->h_sino_dev + S, out, st);
+  if (rc != HRRT_OK) return rc;
+  e = cudaMemcpyAsync(sino, h->h_sino_dev, sizeof(uint16_t) * S, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && delayed && mode == HRRT_LM_PROMPTS_AND_DELAYED)
+    e = cudaMemcpyAsync(delayed, h->h_sino_dev + S, sizeof(uint16_t) * S, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_histogram");
+  return HRRT_OK;
+}
+
+}  // extern "C"

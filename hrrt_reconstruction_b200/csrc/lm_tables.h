@@ -1,0 +1,38 @@
+// lm_tables.h -- HRRT listmode rebinning tables (host).
+//
+// The crystal-pair lookup the reference's hrrt_rebinner_lut writes and
+// lmhistogram_mp reads (lor_sinogram_map.cpp:99-221), the axial crystal
+// positions, and the span-3 segment tables with the output span's plane
+// offsets (segment_info_fromarchive.cpp:35-141).  Computed with the same
+// float/double operand types and order as the reference so that every
+// event lands in the reference's bin.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace hrrt {
+
+struct LmSol {
+  int32_t nsino;  // bin + view * 256, -1 outside the sinogram
+  float d;        // 1 / (transaxial length * d_tan_theta), signed by orientation
+  float z;        // axial parameter / plane separation
+};
+
+struct LmTables {
+  static constexpr int kHeads = 8, kLayers = 2, kXCrys = 72, kYCrys = 104, kPairs = 20;
+  static constexpr int kXD = kXCrys * kLayers;  // crystal x index with layer
+  static constexpr int kBins = 256, kViews = 288;
+  int span = 3, maxrd = 67;
+  int nsegs = 0;         // span-3 segments (45 at maxrd 67)
+  int nplanes = 0;       // planes of the output sinogram (6367 / 2209)
+  double d_tan_theta = 0;
+  std::vector<LmSol> sol;        // [21][144][144], head pair 0 unused
+  std::vector<float> zpos, zpos2;  // [104]: z (cm) and z / plane_sep + 0.5
+  std::vector<int> segz0, segzmax, segzoffset;  // [nsegs]
+  long long sino_size() const { return (long long)nplanes * kBins * kViews; }
+  // empty string on success
+  std::string build(int span, int maxrd);
+};
+
+}  // namespace hrrt

@@ -201,6 +201,69 @@ int hrrt_set_profiling(hrrt_ctx *ctx, int enable);
 int hrrt_kernel_stats(hrrt_ctx *ctx, const char *kernel, int *launches, double *total_ms);
 int hrrt_reset_kernel_stats(hrrt_ctx *ctx);
 
+/* ------------------------------------------------------------------------ */
+/* Listmode (64-bit HRRT events) to span-3 / span-9 sinograms               */
+/* ------------------------------------------------------------------------ */
+
+/* Histogram modes of lmhistogram_mp (histogram_mp.cpp:1301-1398): trues =
+ * prompts minus delayed in one sinogram; prompts and delayed in two; prompts
+ * only. */
+#define HRRT_LM_TRUES 0
+#define HRRT_LM_PROMPTS_AND_DELAYED 1
+#define HRRT_LM_PROMPTS_ONLY 2
+/* flags: the rebinner's border-crystal option (histogram_mp.cpp:1190), no DOI
+ * decoding (every event layer 1), time from the count of time tags instead
+ * of their value (timetag_processing = 0) */
+#define HRRT_LM_IGNORE_BORDER_CRYSTAL 1
+#define HRRT_LM_NO_DOI 2
+#define HRRT_LM_TIME_FROM_COUNT 4
+
+typedef struct hrrt_lm_stats {
+  long long words_used;  /* words consumed: through the tag that ended the frame, or all */
+  long long prompts;     /* prompt events histogrammed (next_event_32's count) */
+  long long delayed;     /* delayed events */
+  long long timetags;    /* time tags processed */
+  long long tags;        /* tag words of every kind */
+  long long invalid;     /* events failing the head-pair / crystal checks */
+  long long unmapped;    /* valid events without a sinogram address */
+  long long doi_other;   /* events with a DOI value other than 0, 1 and 7 */
+  long long doi7;        /* transmission-flagged events in an emission stream (not histogrammed) */
+  long long resyncs;     /* out-of-sync words skipped */
+  long long frame_start; /* s, from the time tags */
+  long long duration;    /* s histogrammed */
+  int terminated;        /* 1 when a time tag ended the frame */
+  float ms;              /* device time of the call (CUDA events) */
+} hrrt_lm_stats;
+
+typedef struct hrrt_lm hrrt_lm;
+
+/* Replaces LM_Rebinner::init_rebinner (LM_Rebinner_mp.cpp:56-146) with the
+ * LUT that hrrt_rebinner_lut writes (lor_sinogram_map.cpp:141-221, depth
+ * 1.0 cm): output span 3 or 9, maximum ring difference (67). */
+int hrrt_lm_create(int span, int maxrd, int device, hrrt_lm **out);
+void hrrt_lm_destroy(hrrt_lm *lm);
+const char *hrrt_lm_last_error(const hrrt_lm *lm);
+/* bins of one sinogram: planes x 288 views x 256 bins */
+long long hrrt_lm_sino_size(const hrrt_lm *lm);
+/* forget the clock carried from the previous frame (a new stream) */
+int hrrt_lm_reset_clock(hrrt_lm *lm);
+
+/* Replaces the reader / rebinner / histogram threads of lmhistogram_mp for
+ * one frame (histogram_mp.cpp:1026-1398; rebin_event, LM_Rebinner_mp.cpp:
+ * 188-219): `words` is the raw l64 stream as 32-bit words (ew1, ew2 pairs),
+ * packets of 1 Mi events parsed from their own first word; `duration` > 0
+ * ends the frame on the first time tag that reaches it (seconds), else the
+ * whole stream is one frame.  Host buffers; `sino` / `delayed` (16-bit
+ * bins, wrapping like the reference's short sinogram) are overwritten.
+ * The clock carries into the next call: pass the remaining words
+ * (from stats.words_used) for the next frame. */
+int hrrt_lm_histogram(hrrt_lm *lm, const uint32_t *words, long long nwords, int mode, int duration, int flags,
+                      uint16_t *sino, uint16_t *delayed, hrrt_lm_stats *stats);
+/* The same on device buffers (words 16-byte aligned, sinograms 4-byte
+ * aligned), ADDING into sino / delayed, on `stream` (NULL: the library's). */
+int hrrt_lm_histogram_device(hrrt_lm *lm, const uint32_t *d_words, long long nwords, int mode, int duration,
+                             int flags, uint16_t *d_sino, uint16_t *d_delayed, hrrt_lm_stats *stats, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

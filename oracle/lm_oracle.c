@@ -1,0 +1,396 @@
+/*
+ * lm_oracle.c -- CPU restatement of HRRT listmode histogramming.
+ *
+ * TEST INFRASTRUCTURE ONLY (see lm_oracle.h).  Plain C99, -ffp-contract=off:
+ * every float and double expression below has the operand types and the
+ * order of the reference's C++ (x86-64 SSE2, no fused multiply-add).
+ *
+ * Reference files cited, within the reference project:
+ *   gi   = gen_delays_lib/geometry_info.{h,cpp}      crystal positions
+ *   si   = gen_delays_lib/segment_info_fromarchive.cpp  segment tables
+ *   lsm  = gen_delays_lib/lor_sinogram_map.cpp       LUT (init_sol)
+ *   lut  = hrrt_rebinner_lut/hrrt_rebinner_lut.cpp   how the LUT file is made
+ *   reb  = lmhistogram_mp/LM_Rebinner_mp.cpp         rebin_event
+ *   hist = lmhistogram_mp/histogram_mp.cpp           decode, tags, histogram
+ *   rdr  = lmhistogram_mp/LM_Reader_mp.{hpp,cpp}     packets
+ */
+#include "lm_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+/* gi.h:31-66 */
+#define NDOIS 2
+#define NXCRYS 72
+#define NYCRYS 104
+#define NHEADS 8
+#define NMPAIRS 20
+#define NPROJS 256
+#define NVIEWS 288
+#define NXD (NXCRYS * NDOIS)
+/* rdr.hpp:39: 1024*1024 64-bit events per packet */
+#define PACKET_WORDS (2 * 1024 * 1024)
+
+static const int HRRT_MPAIRS[21][2] = {{-1, -1}, {0, 2}, {0, 3}, {0, 4}, {0, 5}, {0, 6}, {1, 3}, {1, 4}, {1, 5}, {1, 6},
+                                       {1, 7},   {2, 4}, {2, 5}, {2, 6}, {2, 7}, {3, 5}, {3, 6}, {3, 7}, {4, 6}, {4, 7},
+                                       {5, 7}};
+static const int EWTYPES[16] = {3, 3, 1, 0, 3, 3, 2, 2, 3, 3, 3, 3, 3, 3, 3, 3};
+/* span-3 to span-9 segment map (si:23-26) */
+static const int CONVERSION[45] = {0, 0,  0,  1,  2,  1,  2,  1,  2,  3,  4,  3,  4,  3,  4,  5,  6,  5,  6,  5,  6,  7,  8,
+                                   7, 8,  7,  8,  9,  10, 9,  10, 9,  10, 11, 12, 11, 12, 11, 12, 13, 14, 13, 14, 13, 14};
+
+struct lm_tables {
+  int span, nsegs, nplanes_out;
+  double d_tan_theta, plane_sep, binsize, crystal_radius;
+  float xyz[NHEADS][NDOIS][NXCRYS][NYCRYS][3];
+  float c_zpos[NYCRYS], c_zpos2[NYCRYS];
+  int segz0[63], segzmax[63], segzoffset[63];
+  short segplane[63][2 * NYCRYS - 1];
+  lm_sol *sol; /* [21][NXD][NXD], entry 0 unused */
+};
+
+/* gi.h:50-66 constants, evaluated with the reference's types */
+static float c_csize(void) { return 0.22f; }
+static float c_cgap(void) { return 0.02f; }
+static float c_bsize(void) { return (float)(8.0 * c_csize() + 7 * c_cgap()); }
+static float c_bgap(void) { return 0.05f; }
+static float c_xhsize(void) { return (float)(9.0 * c_bsize() + 8 * c_bgap()); }
+
+/* calc_det_to_phy (gi.cpp:137-163), head_crystal_depth = 1.0 */
+static void det_to_phy(const double *sin_head, const double *cos_head, double crystal_radius, int head, int layer,
+                       int detx, int dety, float pos[3]) {
+  const float BSIZE = c_bsize(), BGAP = c_bgap(), CSIZE = c_csize(), CGAP = c_cgap(), XHSIZE = c_xhsize();
+  const float depth = 1.0f;
+  const double sint = sin_head[head], cost = cos_head[head];
+  int bcrys = detx % 8, blk = detx / 8;
+  const float xf = blk * (BSIZE + BGAP) + bcrys * (CSIZE + CGAP);
+  const double x = xf - XHSIZE / 2.0 + CSIZE / 2.0;
+  const double y = crystal_radius + depth * (1 - layer) + 0.5 * depth;
+  bcrys = dety % 8;
+  blk = dety / 8;
+  const float zf = blk * (BSIZE + BGAP) + bcrys * (CSIZE + CGAP);
+  const double z = zf;
+  const double xpos = x * cost + y * sint;
+  const double ypos = -x * sint + y * cost;
+  pos[0] = (float)xpos;
+  pos[1] = (float)ypos;
+  pos[2] = (float)z;
+}
+
+/* init_phy_to_pro (lsm:99-138) */
+static void phy_to_pro(const lm_tables *t, const float deta[3], const float detb[3], lm_sol *sol) {
+  const float pi = (float)M_PI;
+  double dy = deta[1] - detb[1];
+  double dx = deta[0] - detb[0];
+  double d = sqrt(dx * dx + dy * dy);
+  float r = (float)((deta[1] * detb[0] - deta[0] * detb[1]) / d);
+  float phi = (float)(atan2(dx, dy));
+  if (phi < 0.0) {
+    phi += pi;
+    r = -r;
+    d = -d;
+  }
+  if (phi >= M_PI) {
+    phi = 0.0;
+    r = -r;
+    d = -d;
+  }
+  int view = (int)(NVIEWS * phi / M_PI);
+  if (view >= 288) view = 0;
+  if (view <= -1) view = 0;
+  const float z = (float)((deta[0] * dx + deta[1] * dy) / (d * d));
+  const int bin = (int)(NPROJS / 2 + (r / t->binsize + 0.5));
+  if (bin < 0 || bin > NPROJS - 1)
+    sol->nsino = -1;
+  else
+    sol->nsino = bin + view * NPROJS;
+  sol->d = (float)(1.0 / d / t->d_tan_theta);
+  sol->z = (float)(z / t->plane_sep);
+}
+
+lm_tables *lm_create(int span, int maxrd) {
+  if ((span != 3 && span != 9) || maxrd < span || maxrd > 103) return NULL;
+  lm_tables *t = (lm_tables *)calloc(1, sizeof(lm_tables));
+  if (!t) return NULL;
+  t->span = span;
+  /* init_geometry_hrrt (gi.cpp:168-218), LR_0, loop counter from 0 */
+  const float pitch = 0.24375f, rdiam = 46.9f;
+  double sin_head[NHEADS], cos_head[NHEADS];
+  for (int i = 0; i < NHEADS; i++) {
+    sin_head[i] = sin(i * 2.0 * M_PI / NHEADS);
+    cos_head[i] = cos(i * 2.0 * M_PI / NHEADS);
+  }
+  t->crystal_radius = rdiam / 2.0;
+  t->binsize = pitch / 2.0;
+  t->plane_sep = pitch / 2.0;
+  for (int h = 0; h < NHEADS; h++)
+    for (int l = 0; l < NDOIS; l++)
+      for (int x = 0; x < NXCRYS; x++)
+        for (int y = 0; y < NYCRYS; y++) det_to_phy(sin_head, cos_head, t->crystal_radius, h, l, x, y, t->xyz[h][l][x][y]);
+
+  /* init_segment_info (si:113-141): span-3 segment planes; offsets of the
+   * output span (span 9 through the conversion table) */
+  const int np = 2 * NYCRYS - 1;
+  int seg9off[63] = {0};
+  {
+    const int maxseg = maxrd / span, nsegs = 2 * maxseg + 1, sp2 = (span + 1) / 2;
+    int segz0 = 0, segnz = 0, segzoff = 0, prev_nz = 0;
+    for (int i = 0; i < nsegs; i++) {
+      segz0 = (i == 0) ? 0 : sp2 + span * ((i - 1) / 2);
+      segnz = np - 2 * segz0;
+      segzoff = (i == 0) ? 0 : segzoff + prev_nz;
+      prev_nz = segnz;
+      seg9off[i] = -segz0 + segzoff;
+      t->nplanes_out = segzoff + segnz;
+    }
+    t->d_tan_theta = span * t->plane_sep / t->crystal_radius;
+  }
+  {
+    const int maxseg = maxrd / 3, sp2 = 2;
+    t->nsegs = 2 * maxseg + 1;
+    int segzoff = 0, prev_nz = 0, total = 0;
+    for (int i = 0; i < t->nsegs; i++) {
+      t->segz0[i] = (i == 0) ? 0 : sp2 + 3 * ((i - 1) / 2);
+      const int segnz = np - 2 * t->segz0[i];
+      segzoff = (i == 0) ? 0 : segzoff + prev_nz;
+      prev_nz = segnz;
+      t->segzmax[i] = t->segz0[i] + segnz - 1;
+      t->segzoffset[i] = -t->segz0[i] + segzoff;
+      total = segzoff + segnz;
+    }
+    t->d_tan_theta = 3 * t->plane_sep / t->crystal_radius;
+    if (span == 3) t->nplanes_out = total;
+    if (span == 9)
+      for (int i = 0; i < t->nsegs && i < 45; i++) t->segzoffset[i] = seg9off[CONVERSION[i]];
+  }
+
+  /* init_sol (lsm:141-221) */
+  t->sol = (lm_sol *)calloc((size_t)21 * NXD * NXD, sizeof(lm_sol));
+  if (!t->sol) {
+    free(t);
+    return NULL;
+  }
+  for (int i = 1; i <= NMPAIRS; i++) {
+    const int ahead = HRRT_MPAIRS[i][0], bhead = HRRT_MPAIRS[i][1];
+    for (int al = 0; al < NDOIS; al++)
+      for (int ax = 0; ax < NXCRYS; ax++) {
+        const int axx = ax + NXCRYS * al;
+        for (int bl = 0; bl < NDOIS; bl++)
+          for (int bx = 0; bx < NXCRYS; bx++) {
+            const int bxx = bx + NXCRYS * bl;
+            phy_to_pro(t, t->xyz[ahead][al][ax][0], t->xyz[bhead][bl][bx][0],
+                       &t->sol[((size_t)i * NXD + axx) * NXD + bxx]);
+          }
+      }
+  }
+  for (int i = 0; i < NYCRYS; i++) {
+    const float *p = t->xyz[0][0][0][i];
+    t->c_zpos[i] = p[2];
+    t->c_zpos2[i] = (float)(p[2] / t->plane_sep + 0.5);
+  }
+  for (int i = 0; i < 63; i++)
+    for (int plane = 0; plane < np; plane++) {
+      short v = 0;
+      if (i > t->nsegs - 1 || plane < t->segz0[i] || plane > t->segzmax[i])
+        v = -1;
+      else
+        v = (short)(plane + t->segzoffset[i]);
+      t->segplane[i][plane] = v;
+    }
+  return t;
+}
+
+void lm_destroy(lm_tables *t) {
+  if (!t) return;
+  free(t->sol);
+  free(t);
+}
+
+long long lm_sino_size(const lm_tables *t) { return (long long)t->nplanes_out * NPROJS * NVIEWS; }
+int lm_nplanes(const lm_tables *t) { return t->nplanes_out; }
+double lm_d_tan_theta(const lm_tables *t) { return t->d_tan_theta; }
+void lm_get_sol(const lm_tables *t, lm_sol *sol) { memcpy(sol, t->sol, sizeof(lm_sol) * 21 * NXD * NXD); }
+void lm_get_zpos(const lm_tables *t, float *a, float *b) {
+  memcpy(a, t->c_zpos, sizeof(t->c_zpos));
+  memcpy(b, t->c_zpos2, sizeof(t->c_zpos2));
+}
+void lm_get_seg(const lm_tables *t, int *z0, int *zmax, int *off, int *nsegs) {
+  memcpy(z0, t->segz0, sizeof(int) * t->nsegs);
+  memcpy(zmax, t->segzmax, sizeof(int) * t->nsegs);
+  memcpy(off, t->segzoffset, sizeof(int) * t->nsegs);
+  *nsegs = t->nsegs;
+}
+void lm_get_crystals(const lm_tables *t, float *xyz) { memcpy(xyz, t->xyz, sizeof(t->xyz)); }
+
+/* rebin_event (reb:188-219).  A plane outside [0, 2*104-2] would index
+ * m_segplane outside its row in the reference; here it has no address. */
+int lm_rebin_event(const lm_tables *t, int mp, int alayer, int ax, int ay, int blayer, int bx, int by) {
+  const int axx = ax + NXCRYS * alayer, bxx = bx + NXCRYS * blayer;
+  const lm_sol *s = &t->sol[((size_t)mp * NXD + axx) * NXD + bxx];
+  const int sino_addr = s->nsino;
+  if (sino_addr == -1) return -1;
+  const float cay = t->c_zpos2[ay];
+  const float dz2 = t->c_zpos[by] - t->c_zpos[ay];
+  const float z = s->z, d = s->d;
+  const int plane = (int)(cay + z * dz2);
+  const float seg = (float)(0.5 + dz2 * d);
+  int segnum = (int)seg;
+  if (seg < 0)
+    segnum = 1 - 2 * segnum;
+  else
+    segnum = 2 * segnum;
+  if (segnum >= t->nsegs) return -1;
+  if (plane < 0 || plane > 2 * NYCRYS - 2) return -1;
+  if (t->segplane[segnum][plane] == -1) return -1;
+  return (plane + t->segzoffset[segnum]) * NPROJS * NVIEWS + sino_addr;
+}
+
+void lm_clock_init(lm_clock *c) {
+  c->current_time = -1;
+  c->current_time_msec = -1;
+  c->prev_time = 0;
+  c->clock_reset = 0;
+  c->pad = 0;
+}
+
+/* process_tagword time-tag branch (hist:225-260); returns 1 when the frame
+ * ends at this tag */
+static int time_tag(lm_clock *c, unsigned tag, int duration, int flags, long long *frame_start) {
+  if ((tag & 0xE0000000u) != 0x80000000u) return 0;
+  if (flags & LM_TIME_FROM_COUNT)
+    c->current_time_msec++;
+  else
+    c->current_time_msec = tag & 0x3fffffff;
+  if (c->prev_time > c->current_time_msec) {
+    if (!c->clock_reset) {
+      c->current_time = c->current_time_msec / 1000;
+      c->clock_reset = 1;
+      return 0;
+    }
+  }
+  c->prev_time = c->current_time_msec;
+  if (c->current_time != c->current_time_msec / 1000) {
+    c->current_time = c->current_time_msec / 1000;
+    if (*frame_start < 0) *frame_start = c->current_time;
+    if (duration > 0 && (c->current_time - *frame_start) >= duration) return 1;
+  }
+  return 0;
+}
+
+static void bump(uint16_t *h, long long a, int delta) { h[a] = (uint16_t)(h[a] + delta); }
+
+/* Emission decode (rebin_packet, hist:1026-1233) and histogram (hist:1301-
+ * 1372), in stream order.  Packets of PACKET_WORDS words are parsed from
+ * their own first word: a word left over at a packet end is dropped
+ * (`(src_pos + 1) < count`).  The reference's reader exits on a short last
+ * packet; here the last packet is parsed like the others. */
+int lm_histogram(const lm_tables *t, const uint32_t *w, long long n, int mode, int duration, int flags, lm_clock *clk,
+                 uint16_t *sino, uint16_t *delayed, lm_stats *st) {
+  memset(st, 0, sizeof(*st));
+  const long long sino_size = lm_sino_size(t);
+  const int ignore_border = flags & LM_IGNORE_BORDER_CRYSTAL;
+  const int doi_processing = (flags & LM_NO_DOI) == 0;
+  const int xhigh = ignore_border ? NXCRYS - 1 : NXCRYS;
+  /* reset_statistics (hist:196-216) */
+  long long frame_start = (clk->current_time >= 0) ? clk->current_time : -1;
+  int terminated = 0;
+  long long pos = 0;
+  for (long long p0 = 0; p0 < n && !terminated; p0 += PACKET_WORDS) {
+    const long long count = (n - p0 < PACKET_WORDS) ? n - p0 : PACKET_WORDS;
+    long long sp = 0;
+    while (sp + 1 < count && !terminated) {
+      const unsigned ew1 = w[p0 + sp], ew2 = w[p0 + sp + 1];
+      const int type = EWTYPES[((ew2 & 0xc0000000u) >> 30) | ((ew1 & 0xc0000000u) >> 28)];
+      long long address = -1;
+      unsigned word32 = 0;
+      int have = 0;
+      if (type == 3) {
+        sp++;
+        st->resyncs++;
+        continue;
+      }
+      if (type == 2) {
+        sp += 2;
+        st->tags++;
+        word32 = (ew1 & 0xffff) | ((ew2 & 0xffff) << 16);
+        have = 1;
+      } else {
+        sp += 2;
+        int doia = 1, doib = 1, err = 0;
+        const int mpe = ((ew1 & 0x00070000) >> 16) | ((ew2 & 0x00070000) >> 13);
+        const int ax = ew1 & 0xff, ay = (ew1 & 0xff00) >> 8, bx = ew2 & 0xff, by = (ew2 & 0xff00) >> 8;
+        if (doi_processing) {
+          doia = (ew1 & 0x01C00000) >> 22;
+          doib = (ew2 & 0x01C00000) >> 22;
+        }
+        if (mpe < 1 || mpe > NMPAIRS) err++;
+        if (ax >= NXCRYS || ay >= NYCRYS) err++;
+        if (bx >= NXCRYS || by >= NYCRYS) err++;
+        if (err) {
+          st->invalid++;
+          continue;
+        }
+        if (doia == 7 || doib == 7) {
+          /* the transmission branch: in an emission stream the reference
+           * looks the event up in a TX table that only a transmission run
+           * builds; such events are not histogrammed */
+          st->doi7++;
+          continue;
+        }
+        if ((doia == 1 || doia == 0) && (doib == 1 || doib == 0)) {
+          if (ignore_border && (ax * bx == 0 || ax == xhigh || bx == xhigh)) {
+            address = -1;
+          } else if (mode == LM_PROMPTS_ONLY && type != 0) {
+            address = -1;
+          } else {
+            address = lm_rebin_event(t, mpe, doia, ax, ay, doib, bx, by);
+            if (address >= 0 && type == 0) address |= 0x40000000;
+          }
+        } else {
+          st->doi_other++;
+        }
+        if (address < 0) {
+          if ((doia == 1 || doia == 0) && (doib == 1 || doib == 0)) st->unmapped++;
+          continue;
+        }
+        word32 = (unsigned)address;
+        have = 1;
+      }
+      if (!have) continue;
+      /* next_event_32 (hist:334-382) and histogram (hist:1316-1362) */
+      if (word32 & 0x80000000u) {
+        st->timetags += ((word32 & 0xE0000000u) == 0x80000000u);
+        if (time_tag(clk, word32, duration, flags, &frame_start)) terminated = 1;
+        continue;
+      }
+      const int prompt = (word32 & 0x40000000u) != 0;
+      const long long value = word32 & 0x3fffffff;
+      if (prompt)
+        st->prompts++;
+      else
+        st->delayed++;
+      if (value >= 0 && value < sino_size) {
+        if (mode == LM_PROMPTS_AND_DELAYED) {
+          if (prompt)
+            bump(sino, value, 1);
+          else if (delayed)
+            bump(delayed, value, 1);
+        } else {
+          bump(sino, value, prompt ? 1 : -1);
+        }
+      }
+    }
+    pos = p0 + sp;
+  }
+  st->words_used = terminated ? pos : n;
+  st->terminated = terminated;
+  if (!terminated) clk->current_time = (clk->current_time_msec + 500) / 1000;
+  st->frame_start = frame_start;
+  st->duration = clk->current_time - frame_start;
+  return 0;
+}

@@ -1,0 +1,146 @@
+"""Device listmode histogrammer (hrrt_lm_* through the C ABI) against the CPU
+restatement oracle/lm_oracle.c: sinograms bit-identical, statistics equal,
+on the known-answer streams and on seeded random streams that mix every word
+class, several packets, a partial last packet and frame ends."""
+import numpy as np
+import pytest
+
+from oracle import lm
+from oracle.lm import LMOracle, event_words, interleave, tag_words
+
+pytestmark = pytest.mark.gpu
+
+STAT_KEYS = ("words_used", "prompts", "delayed", "timetags", "tags", "invalid", "unmapped", "doi_other", "doi7",
+             "resyncs", "frame_start", "duration", "terminated")
+
+
+def random_stream(seed, nevents, tag_every=1000, p_resync=1e-4, p_bad=0.01, p_delayed=0.1):
+    """Seeded l64 words: coincidences (10 % delayed) with random head pairs,
+    crystals and DOI (mostly valid), a time tag every `tag_every` events
+    counting milliseconds from 5 s, block-singles tags, lone out-of-sync
+    words."""
+    rng = np.random.default_rng(seed)
+    mp = rng.integers(1, 21, nevents)
+    ax, bx = rng.integers(0, 72, nevents), rng.integers(0, 72, nevents)
+    ay, by = rng.integers(0, 104, nevents), rng.integers(0, 104, nevents)
+    doia = rng.choice([0, 1], nevents)
+    doib = rng.choice([0, 1], nevents)
+    bad = rng.random(nevents) < p_bad
+    kind = rng.integers(0, 5, nevents)
+    mp = np.where(bad & (kind == 0), rng.choice([0, 21, 40], nevents), mp)
+    ax = np.where(bad & (kind == 1), rng.integers(72, 256, nevents), ax)
+    by = np.where(bad & (kind == 2), rng.integers(104, 256, nevents), by)
+    doia = np.where(bad & (kind == 3), rng.integers(2, 8, nevents), doia)
+    doib = np.where(bad & (kind == 4), 7, doib)
+    prompt = rng.random(nevents) >= p_delayed
+    ew1, ew2 = event_words(mp, ax, ay, bx, by, doia, doib, prompt)
+    ev = interleave(ew1, ew2).reshape(-1, 2)
+    # insert tags and lone words
+    chunks = []
+    ms = 5000
+    for i in range(0, nevents, tag_every):
+        t1, t2 = tag_words(np.uint32(0x80000000 | ms))
+        chunks.append(np.array([[t1, t2]], np.uint32).reshape(-1))
+        ms += 1
+        if (i // tag_every) % 7 == 3:
+            s1, s2 = tag_words(np.uint32(0xA0000000 | (i & 0x7ffff)))
+            chunks.append(np.array([s1, s2], np.uint32))
+        block = ev[i:i + tag_every].reshape(-1).copy()
+        chunks.append(block)
+        if rng.random() < p_resync * tag_every:
+            chunks.append(np.array([0x00000000], np.uint32))
+    return np.concatenate(chunks).astype(np.uint32)
+
+
+def compare(O, D, words, mode, duration=0, flags=0):
+    O.reset_clock()
+    D.reset_clock()
+    so, do, sto = O.histogram(words, mode=mode, duration=duration, flags=flags)
+    sd, dd, std = D.histogram(words, mode=mode, duration=duration, flags=flags)
+    assert np.array_equal(so, sd), np.flatnonzero(so != sd)[:10]
+    if mode == lm.PROMPTS_AND_DELAYED:
+        assert np.array_equal(do, dd), np.flatnonzero(do != dd)[:10]
+    for k in STAT_KEYS:
+        assert sto[k] == std[k], (k, sto[k], std[k])
+    return sto
+
+
+@pytest.fixture(scope="module", params=[3, 9])
+def pair(request):
+    import hrrt_reconstruction_b200 as H
+    O = LMOracle(request.param)
+    D = H.Listmode(request.param)
+    yield O, D
+    D.close()
+
+
+def test_known_answer_streams(pair):
+    O, D = pair
+    good = event_words(3, 35, 50, 35, 50)
+    dly = event_words(3, 35, 50, 35, 50, prompt=False)
+    w = np.concatenate([interleave(np.atleast_1d(a), np.atleast_1d(b)) for a, b in (
+        good, dly, (np.uint32(0), np.uint32(0)), event_words(0, 35, 50, 35, 50), event_words(3, 72, 50, 35, 50),
+        event_words(3, 35, 50, 35, 50, doia=3), event_words(3, 35, 50, 35, 50, doib=7), tag_words(0xA0000005),
+        tag_words(0x40000000 | 12345), tag_words(777), good)]).astype(np.uint32)
+    for mode in (lm.TRUES, lm.PROMPTS_AND_DELAYED, lm.PROMPTS_ONLY):
+        compare(O, D, w, mode)
+
+
+def test_wrap_and_trues(pair):
+    O, D = pair
+    n = 70000
+    ew1, ew2 = event_words(np.full(n, 3), np.full(n, 20), np.full(n, 60), np.full(n, 50), np.full(n, 61),
+                           prompt=np.arange(n) % 3 != 0)
+    w = interleave(ew1, ew2)
+    for mode in (lm.TRUES, lm.PROMPTS_AND_DELAYED):
+        compare(O, D, w, mode)
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_random_stream_packets(pair, seed):
+    """About 2.6 packets of mixed words; whole stream and 2-s frames."""
+    O, D = pair
+    w = random_stream(seed, 2_700_000)
+    assert w.size > 2 * lm.PACKET_WORDS
+    st = compare(O, D, w, lm.PROMPTS_AND_DELAYED)
+    assert st["prompts"] > 0 and st["resyncs"] > 0 and st["invalid"] > 0 and st["doi7"] > 0
+    compare(O, D, w, lm.TRUES, flags=lm.IGNORE_BORDER_CRYSTAL)
+    compare(O, D, w, lm.PROMPTS_ONLY, flags=lm.NO_DOI)
+
+
+def test_frames_follow_the_clock(pair):
+    """Consecutive 1-s frames (1000 tags each): every frame bit-identical and
+    the clock carried from one call to the next."""
+    O, D = pair
+    w = random_stream(3, 2_500_000, tag_every=800)
+    O.reset_clock()
+    D.reset_clock()
+    pos_o = pos_d = 0
+    for _ in range(3):
+        so, do, sto = O.histogram(w[pos_o:], duration=1)
+        sd, dd, std = D.histogram(w[pos_d:], duration=1)
+        assert np.array_equal(so, sd) and np.array_equal(do, dd)
+        for k in STAT_KEYS:
+            assert sto[k] == std[k], (k, sto[k], std[k])
+        assert sto["terminated"] == 1
+        pos_o += sto["words_used"]
+        pos_d += std["words_used"]
+
+
+def test_device_entry_adds_into_buffers(pair):
+    import torch
+    O, D = pair
+    w = random_stream(4, 300_000)
+    O.reset_clock()
+    so, do, _ = O.histogram(w)
+    dw = torch.from_numpy(w.view(np.int32)).cuda()
+    ds = torch.zeros(D.sino_size, dtype=torch.int16, device="cuda")
+    dd = torch.zeros(D.sino_size, dtype=torch.int16, device="cuda")
+    for _ in range(2):
+        D.reset_clock()
+        D.histogram_device(dw.data_ptr(), w.size, ds.data_ptr(), dd.data_ptr())
+    torch.cuda.synchronize()
+    got_s = ds.cpu().numpy().view(np.uint16)
+    got_d = dd.cpu().numpy().view(np.uint16)
+    assert np.array_equal(got_s, (2 * so.astype(np.uint32)).astype(np.uint16))
+    assert np.array_equal(got_d, (2 * do.astype(np.uint32)).astype(np.uint16))
