@@ -16,13 +16,14 @@ import os
 
 import numpy as np
 
-__all__ = ["Geometry", "HrrtError", "Context", "Listmode", "lib", "LIB_PATH", "STORE_F32", "STORE_16", "BP_REF",
+__all__ = ["Geometry", "HrrtError", "Context", "Listmode", "lib", "LIB_PATH", "STORE_F32", "STORE_16", "BP_REF", "BP_ADJOINT",
            "geometry_table", "hrrt_geometry"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libhrrt_gpu.so")
 STORE_F32 = 0
 STORE_16 = 1
 BP_REF = 0
+BP_ADJOINT = 1
 
 
 class HrrtError(RuntimeError):
@@ -94,6 +95,7 @@ def _load():
         "hrrt_bp_pair": (i, [vp, vp, i, vp, i]),
         "hrrt_forward_project": (i, [vp, vp, vp]),
         "hrrt_bp_pair_noalloc": (i, [vp, vp, i, vp, vp]),
+        "hrrt_set_backprojector": (i, [vp, i]),
         "hrrt_rotate_add": (i, [vp, vp, i, vp]),
         "hrrt_geometry_table": (ctypes.c_longlong, [G, ctypes.c_char_p, vp, ctypes.c_size_t]),
         "hrrt_set_profiling": (i, [vp, i]),
@@ -299,6 +301,11 @@ class Context:
         out = np.zeros(self.image_shape, np.float32)
         self._check(lib.hrrt_bp_pair(self._h, _ptr(p), view, _ptr(out), mode), "bp_pair")
         return out
+
+    def set_backprojector(self, mode):
+        """BP_REF (the reference's back projector) or BP_ADJOINT (the forward
+        projector's exact transpose) for sensitivity() and osem()."""
+        self._check(lib.hrrt_set_backprojector(self._h, mode), "set_backprojector")
 
     def rotate_add(self, imagebuf, view, corr):
         ib = _c(imagebuf, np.float32)

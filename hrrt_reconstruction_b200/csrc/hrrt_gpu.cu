@@ -65,6 +65,12 @@ struct hrrt_ctx {
   char *stage[2] = {nullptr, nullptr};
   size_t stage_bytes = 0;
 
+  // back projector of the OSEM loop, and the device geometry it runs with
+  // (for the adjoint: segment weights of 1, the forward projector's scaling)
+  int bp_mode = HRRT_BP_REF;
+  DevGeom dg_adj{};
+  int *d_view1 = nullptr;       // one view index, for single-pair entry points
+
   bool prof = false;
   std::vector<KernelTimer> pending;
   std::map<std::string, std::pair<int, double>> kstats;
@@ -282,6 +288,28 @@ int build_work_lists(hrrt_ctx *ctx) {
 int run_subset(hrrt_ctx *ctx, int s) {
   const DevGeom &g = ctx->dg;
   const size_t in_stride = (size_t)ctx->quad_pair;
+  if (ctx->bp_mode == HRRT_BP_ADJOINT) {
+    const DevGeom &ga = ctx->dg_adj;
+    {
+      Launch L(ctx, "fp_kernel");
+      CK(launch_fp(ga, ctx->d_image, ctx->d_work + ctx->fp_off[s], ctx->fp_cnt[s], 1, ctx->q_prompts, ctx->q_add,
+                   ctx->storage, ctx->d_ratio, ctx->quad_pair, ctx->tpt, ctx->stream),
+         "fp_kernel");
+    }
+    {
+      Launch L(ctx, "adj_kernel");
+      CK(launch_adj(ga, ctx->d_ratio, in_stride, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s], ctx->d_bc, ctx->d_br,
+                    ctx->vol, ctx->stream),
+         "adj_kernel");
+    }
+    {
+      Launch L(ctx, "adj_rotate_kernel");
+      CK(launch_adj_rotate(ga, ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_bc, ctx->d_br,
+                           ctx->vol, ctx->d_image, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 0, ctx->stream),
+         "adj_rotate_kernel");
+    }
+    return HRRT_OK;
+  }
   {
     Launch L(ctx, "fp_kernel");
     CK(launch_fp(g, ctx->d_image, ctx->d_work + ctx->fp_off[s], ctx->fp_cnt[s], 1, ctx->q_prompts, ctx->q_add,
@@ -518,6 +546,12 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
   ctx->d_partial = ctx->d_br ? dalloc<double>(ctx, pb, &e) : nullptr;
   ctx->d_sum = ctx->d_partial ? dalloc<double>(ctx, 1, &e) : nullptr;
   if (!ctx->d_sum) return bail(fail(ctx, HRRT_ERR_NOMEM, std::string("device allocation: ") + cudaGetErrorString(e)));
+  // the adjoint runs with segment weights of 1 (its rows carry the forward
+  // projector's own scaling)
+  ctx->dg_adj = d;
+  ctx->dg_adj.bp_scale = dupload(ctx, std::vector<float>(g.nseg, 1.0f), &e);
+  ctx->d_view1 = dalloc<int>(ctx, 1, &e);
+  if (!ctx->dg_adj.bp_scale || !ctx->d_view1) return bail(cuda_fail(ctx, e, "adjoint tables"));
   int rc = build_work_lists(ctx);
   if (rc) return bail(rc);
   e = cudaStreamSynchronize(ctx->stream);
@@ -651,12 +685,30 @@ int hrrt_sensitivity(hrrt_ctx *ctx) {
   if (!ctx) return HRRT_ERR_ARG;
   if (!ctx->have_inputs) return fail(ctx, HRRT_ERR_STATE, "hrrt_upload_inputs must come first");
   const Geometry &g = ctx->geo;
+  const bool adj = ctx->bp_mode == HRRT_BP_ADJOINT;
   for (int s = 0; s < g.sp.subsets; s++) {
     {
       Launch L(ctx, "scale_pairs_kernel");
-      CK(launch_scale_pairs(ctx->dg, ctx->q_mult, ctx->storage, ctx->d_pair_views + (size_t)s * ctx->npairs,
-                            ctx->npairs, ctx->d_ratio, ctx->quad_pair, ctx->stream),
+      CK(launch_scale_pairs(adj ? ctx->dg_adj : ctx->dg, ctx->q_mult, ctx->storage,
+                            ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_ratio, ctx->quad_pair,
+                            ctx->stream),
          "scale_pairs");
+    }
+    if (adj) {
+      {
+        Launch L(ctx, "adj_kernel");
+        CK(launch_adj(ctx->dg_adj, ctx->d_ratio, ctx->quad_pair, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s],
+                      ctx->d_bc, ctx->d_br, ctx->vol, ctx->stream),
+           "adj_kernel");
+      }
+      {
+        Launch L(ctx, "adj_rotate_kernel");
+        CK(launch_adj_rotate(ctx->dg_adj, ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_bc,
+                             ctx->d_br, ctx->vol, nullptr, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 1,
+                             ctx->stream),
+           "adj_rotate_kernel");
+      }
+      continue;
     }
     {
       Launch L(ctx, "bp_kernel");
@@ -887,9 +939,17 @@ int hrrt_forward_project(hrrt_ctx *ctx, const float *image_xyz, float *sino) {
   return done(device_status(ctx));
 }
 
+int hrrt_set_backprojector(hrrt_ctx *ctx, int mode) {
+  if (!ctx) return HRRT_ERR_ARG;
+  if (mode != HRRT_BP_REF && mode != HRRT_BP_ADJOINT) return fail(ctx, HRRT_ERR_ARG, "unknown back projector");
+  if (mode != ctx->bp_mode) ctx->have_sens = false;
+  ctx->bp_mode = mode;
+  return HRRT_OK;
+}
+
 int hrrt_bp_pair(hrrt_ctx *ctx, const float *prj, int view, float *imagebuf_xyz, int mode) {
   if (!ctx || !prj || !imagebuf_xyz) return HRRT_ERR_ARG;
-  if (mode != HRRT_BP_REF) return fail(ctx, HRRT_ERR_ARG, "unknown back projector");
+  if (mode != HRRT_BP_REF && mode != HRRT_BP_ADJOINT) return fail(ctx, HRRT_ERR_ARG, "unknown back projector");
   const Geometry &g = ctx->geo;
   if (view < 0 || view >= g.nviews / 2) return fail(ctx, HRRT_ERR_ARG, "view must be < nviews/2");
   cudaError_t e = cudaSuccess;
@@ -904,6 +964,31 @@ int hrrt_bp_pair(hrrt_ctx *ctx, const float *prj, int view, float *imagebuf_xyz,
   if (!dw) return cuda_fail(ctx, e, "work");
   CK(cudaMemcpyAsync(ctx->d_rows, prj, rows * 4, cudaMemcpyHostToDevice, ctx->stream), "bp_pair");
   CK(cudaMemsetAsync(ctx->d_ratio, 0, ctx->quad_pair * 4, ctx->stream), "bp_pair");
+  if (mode == HRRT_BP_ADJOINT) {
+    CK(launch_rows_to_quad(ctx->dg, g.nbins, ctx->d_rows, ctx->d_ratio, 0, ctx->stream), "pack");
+    CK(cudaMemsetAsync(ctx->d_bc, 0, ctx->vol * 4, ctx->stream), "bp_pair");
+    CK(cudaMemsetAsync(ctx->d_br, 0, ctx->vol * 4, ctx->stream), "bp_pair");
+    {
+      Launch L(ctx, "adj_kernel");
+      CK(launch_adj(ctx->dg, ctx->d_ratio, ctx->quad_pair, dw, (int)work.size(), ctx->d_bc, ctx->d_br, ctx->vol,
+                    ctx->stream),
+         "adj_kernel");
+    }
+    CK(cudaMemsetAsync(ctx->d_tmp_img, 0, ctx->vol * 4, ctx->stream), "bp_pair");
+    CK(cudaMemcpyAsync(ctx->d_view1, &view, sizeof(int), cudaMemcpyHostToDevice, ctx->stream), "bp_pair");
+    CK(cudaStreamSynchronize(ctx->stream), "bp_pair");
+    {
+      Launch L(ctx, "adj_rotate_kernel");
+      CK(launch_adj_rotate(ctx->dg, ctx->d_view1, 1, ctx->d_bc, ctx->d_br, ctx->vol, nullptr, nullptr,
+                           ctx->d_tmp_img, 2, ctx->stream),
+         "adj_rotate_kernel");
+    }
+    CK(cudaMemcpyAsync(imagebuf_xyz, ctx->d_tmp_img, ctx->vol * 4, cudaMemcpyDeviceToHost, ctx->stream), "bp_pair");
+    CK(cudaStreamSynchronize(ctx->stream), "bp_pair");
+    cudaFree(dw);
+    ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)dw));
+    return device_status(ctx);
+  }
   CK(launch_rows_to_quad(ctx->dg, g.nbins, ctx->d_rows, ctx->d_ratio, 1, ctx->stream), "pack");
   {
     Launch L(ctx, "bp_kernel");

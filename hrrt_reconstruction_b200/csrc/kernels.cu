@@ -632,6 +632,223 @@ __global__ void __launch_bounds__(256, 3) bp_kernel(DevGeom g, const float4 *__r
 }
 
 // ============================================================================
+// Exact adjoint of the forward projector (no counterpart in the reference,
+// whose back projector is not the transpose of its forward projector).
+//
+// adj_kernel: per (pair, quad x) the forward projector's z interpolation
+// transposed -- every rotated-frame sample of the forward projection receives
+// the rows it fed, weighted as it was weighted (sbrt:1914-1951 read backwards:
+// the middle planes are two windows of the segment, the end planes one
+// position each), with the rows first scaled as the forward projector scales
+// them (sbrt:1953-1976).  The samples are the back projector's voxel roles, so
+// the lanes go to the same column / row partials.
+// adj_rotate_kernel: the bilinear sampling transposed as a gather: an image
+// voxel collects from the <= 16 rotated-frame points around its inverse
+// rotation whose sample footprint (recomputed with the forward projector's own
+// float expressions) holds it, with that footprint's weight.
+// ============================================================================
+template <int KB>
+__global__ void __launch_bounds__(256, 2) adj_kernel(DevGeom g, const float4 *__restrict__ in, long long in_pair_stride,
+                                                  const QuadWork *__restrict__ work, float *__restrict__ bc,
+                                                  float *__restrict__ br, long long vol) {
+  extern __shared__ float4 P[];
+  const QuadWork w = work[blockIdx.x];
+  const int x = w.x, N = g.nx, c = g.c, zp = g.zp, G = g.groupmax, ZS = g.zshift, nz = g.nz;
+  const int FS = G * 2 * ZS;
+  const bool masked = g.nzmask[w.view * g.nquads + x] == 0 || g.cyl0[x] == g.cyl1[x];
+  const float4 *src = in + (size_t)w.slot * in_pair_stride + (size_t)x * g.pplanes;
+  if (!masked)
+    for (int i = threadIdx.x; i < g.bp_splanes; i += blockDim.x) {
+      const int q = __ldg(g.bp_src + i);
+      float4 v = f4(0.f);
+      if (q >= 0) {
+        const int sg = g.pplane_seg[q];
+        const int yb = g.ybot[sg], yr = yb + (q - g.poff[sg]);
+        float sc = g.y_size;
+        if (sg > 0) {
+          int zs = yr - yb;
+          if (zs >= ZS) zs = g.ytop[sg] - yr;
+          sc = g.rescale[((sg - 1) >> 1) * nz + (zs < ZS ? yr : yb + ZS)];
+        }
+        v = src[q] * sc;
+      }
+      P[i] = v;
+    }
+  __syncthreads();
+  float *bcp = bc + (size_t)w.slot * vol;
+  float *brp = br + (size_t)w.slot * vol;
+  const int ystart = g.cyl0[x];
+  const int nyq = c - ystart + 1, nzc = zp / KB;
+  const float4 *P0 = P + g.bp_soff[0];
+  const int per_half = nyq * nzc;
+  for (int task = threadIdx.x; task < 2 * per_half; task += blockDim.x) {
+    const int half = task >= per_half;
+    const int t2 = task - half * per_half;
+    const int zc = t2 / nyq, yi = t2 - zc * nyq, z0 = zc * KB;
+    const int y = ystart + yi;
+    if (half && y == c) continue;
+    float4 s[KB];
+#pragma unroll
+    for (int j = 0; j < KB; j++) s[j] = f4(0.f);
+    if (!masked) {
+#pragma unroll
+      for (int j = 0; j < KB; j++) s[j] = P0[z0 + j];
+      if (y == c) {
+        // centre row: every plane of every segment took the centre samples
+        for (int gg = 0; gg < G; gg++) {
+          const int se = 2 * gg + 2, so = 2 * gg + 1;
+          const int yb = g.ybot[se], yt = g.ytop[se];
+          const float4 *pe = P + g.bp_soff[se] - yb, *po = P + g.bp_soff[so] - yb;
+#pragma unroll
+          for (int j = 0; j < KB; j++) {
+            const int z = z0 + j;
+            if (z >= yb && z <= yt) s[j] = s[j] + (pe[z] + po[z]);
+          }
+        }
+      } else {
+        for (int gg = 0; gg < G; gg++) {
+          const FpMid m = g.fpmid[y * G + gg];
+          if (m.z < 0) continue;  // the forward projector skipped this group for this row
+          const int se = 2 * gg + 2, so = 2 * gg + 1;
+          const int yb = g.ybot[se], yt = g.ytop[se], ym = yb + ZS, ye = yt - ZS;
+          // A: the rows that read this sample at (z, z+1) with (f2, f); B:
+          // the rows that read it at (z2+1, z2) with (f2, f)
+          const float4 *A = P + g.bp_soff[half ? so : se] - yb, *B = P + g.bp_soff[half ? se : so] - yb;
+          const int a0 = z0 - m.z + ym, b0 = z0 - m.z2 + ym;
+#pragma unroll
+          for (int j = 0; j < KB; j++) {
+            const int ya = a0 + j, yb2 = b0 + j;
+            float4 t = f4(0.f);
+            if (ya >= ym && ya <= ye) t = t + A[ya] * m.f2;
+            if (ya - 1 >= ym && ya - 1 <= ye) t = t + A[ya - 1] * m.f;
+            if (yb2 - 1 >= ym && yb2 - 1 <= ye) t = t + B[yb2 - 1] * m.f2;
+            if (yb2 >= ym && yb2 <= ye) t = t + B[yb2] * m.f;
+            s[j] = s[j] + t;
+          }
+          // end planes: one position per plane
+          const int2 *e1 = g.fl_zf + (size_t)y * FS + gg * 2 * ZS, *e2 = g.fl_zf + (size_t)(N - y) * FS + gg * 2 * ZS;
+          for (int i = 0; i < 2 * ZS; i++) {
+            const int yr = (i < ZS) ? yb + i : yt - 2 * ZS + 1 + i;
+            const int2 u = e1[i], v = e2[i];
+            const int za = u.x, zb = v.x;
+            if ((za + 1 < z0 || za >= z0 + KB) && (zb + 1 < z0 || zb >= z0 + KB)) continue;
+            const float fa = __int_as_float(u.y), fb = __int_as_float(v.y);
+            const float4 a = A[yr], b = B[yr];
+#pragma unroll
+            for (int j = 0; j < KB; j++) {
+              const int z = z0 + j;
+              if (z == za) s[j] = s[j] + a * fb;
+              if (z == za + 1) s[j] = s[j] + a * fa;
+              if (z == zb + 1) s[j] = s[j] + b * fb;
+              if (z == zb) s[j] = s[j] + b * fa;
+            }
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < KB; j++)
+      if (z0 + j >= nz) s[j] = f4(0.f);
+    const size_t cz = (size_t)z0;
+    auto put = [&](float *dst, int l) {
+      float v[KB];
+#pragma unroll
+      for (int j = 0; j < KB; j++) v[j] = l == 0 ? s[j].x : l == 1 ? s[j].y : l == 2 ? s[j].z : s[j].w;
+#pragma unroll
+      for (int j = 0; j < KB; j += 4) *reinterpret_cast<float4 *>(dst + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+    };
+    if (!half) {
+      put(bcp + ((size_t)x * N + y) * zp + cz, 0);
+      put(brp + ((size_t)(N - y) * N + x) * zp + cz, 2);
+      if (x != c) {
+        put(bcp + ((size_t)(N - x) * N + y) * zp + cz, 1);
+        put(brp + ((size_t)(N - y) * N + N - x) * zp + cz, 3);
+      }
+    } else {
+      put(bcp + ((size_t)x * N + N - y) * zp + cz, 0);
+      put(brp + ((size_t)y * N + x) * zp + cz, 2);
+      if (x != c) {
+        put(bcp + ((size_t)(N - x) * N + N - y) * zp + cz, 1);
+        put(brp + ((size_t)y * N + N - x) * zp + cz, 3);
+      }
+    }
+  }
+}
+
+// MODE 0: OSEM update, 1: inverse sensitivity (both over the FOV columns, as
+// the rotate-back), 2: out += adjoint over every image column.
+template <int MODE>
+__global__ void __launch_bounds__(256) adj_rotate_kernel(DevGeom g, const int *__restrict__ pair_views, int npairs,
+                                                         const float *__restrict__ bc, const float *__restrict__ br,
+                                                         long long vol, float *__restrict__ image,
+                                                         float *__restrict__ nf_inv, float *__restrict__ out) {
+  const int nq = g.zp / 4, N = g.nx, c = g.c;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int col = (int)(t / nq), q = (int)(t - (long long)col * nq);
+  int i, j;
+  if (MODE == 2) {
+    if (col >= N * N) return;
+    i = col / N;
+    j = col - i * N;
+  } else {
+    if (col >= g.fov_columns) return;
+    const short2 xy = g.fov_xy[col];
+    i = xy.x;
+    j = xy.y;
+  }
+  float4 acc = f4(0.f);
+  for (int p = 0; p < npairs; p++) {
+    const int view = pair_views[p];
+    const float cosv = g.cos_psi[view], sinv = g.sin_psi[view];
+    const float di = (float)(i - c), dj = (float)(j - c);
+    const int qx0 = (int)floorf(di * cosv + dj * sinv + (float)c) - 1;
+    const int qy0 = (int)floorf(-di * sinv + dj * cosv + (float)c) - 1;
+    const float4 *Bc = reinterpret_cast<const float4 *>(bc + (size_t)p * vol);
+    const float4 *Br = reinterpret_cast<const float4 *>(br + (size_t)p * vol);
+    for (int a = qx0; a < qx0 + 4; a++) {
+      if (a < 0 || a >= N) continue;
+      for (int b = qy0; b < qy0 + 4; b++) {
+        if (b < 0 || b >= N) continue;
+        const SamplePt pt = sample_point(a, b, c, N, g.zp, cosv, sinv);
+        if (pt.base < 0) continue;
+        const int ix = pt.base / (N * g.zp), iy = (pt.base / g.zp) - ix * N;
+        const int dx = i - ix, dy = j - iy;
+        if (dx < 0 || dx > 1 || dy < 0 || dy > 1) continue;
+        const float wgt = dx ? (dy ? pt.c3 : pt.c1) : (dy ? pt.c2 : pt.c0);
+        const size_t o = ((size_t)a * N + b) * nq + q;
+        acc = acc + (__ldg(Bc + o) + __ldg(Br + o)) * wgt;
+      }
+    }
+  }
+  const size_t o = ((size_t)i * N + j) * nq + q;
+  if (MODE == 0) {
+    float4 *im = reinterpret_cast<float4 *>(image);
+    const float4 nf = reinterpret_cast<const float4 *>(nf_inv)[o];
+    float4 iv = im[o];
+    float a[4] = {acc.x, acc.y, acc.z, acc.w}, b[4] = {iv.x, iv.y, iv.z, iv.w}, n[4] = {nf.x, nf.y, nf.z, nf.w};
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      const float lo = (0.01f > a[l]) ? 0.01f : a[l];
+      const float cl = (100.0f < lo) ? 100.0f : lo;
+      const float u = b[l] * (cl * n[l]);
+      b[l] = (g.image_max < u) ? g.image_max : u;
+    }
+    im[o] = make_float4(b[0], b[1], b[2], b[3]);
+  } else if (MODE == 1) {
+    float a[4] = {acc.x, acc.y, acc.z, acc.w}, r[4];
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      const int z = q * 4 + l;
+      r[l] = (z < g.nz && fabsf(a[l]) > g.eps1) ? (1.0f / a[l]) : 0.f;
+    }
+    reinterpret_cast<float4 *>(nf_inv)[o] = make_float4(r[0], r[1], r[2], r[3]);
+  } else {
+    float4 *dst = reinterpret_cast<float4 *>(out);
+    dst[o] = dst[o] + acc;
+  }
+}
+
+// ============================================================================
 // Rotate-back of the summed partials of every pair (rotateimage2, sbrt:1137-
 // 1186) fused with what consumes the correction image:
 //   MODE 0: OSEM update pt_cal_updateimage (drv:2018-2059)
@@ -969,6 +1186,34 @@ cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_strid
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   k<<<nwork, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(in), in_pair_stride / 4, work, bc, br, vol, 0, 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adj(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
+                       float *bc, float *br, long long vol, cudaStream_t st) {
+  if (nwork <= 0) return cudaSuccess;
+  const size_t smem = (size_t)g.bp_splanes * sizeof(float4);
+  auto k = adj_kernel<kBpZ>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  if (e != cudaSuccess) return e;
+  k<<<nwork, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(in), in_pair_stride / 4, work, bc, br, vol);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adj_rotate(const DevGeom &g, const int *pair_views, int npairs, const float *bc, const float *br,
+                              long long vol, float *image, float *nf_inv, float *out, int mode, cudaStream_t st) {
+  const long long cols = (mode == 2) ? (long long)g.nx * g.nx : (long long)g.fov_columns;
+  const long long n = cols * (g.zp / 4);
+  const int threads = 256;
+  const unsigned blocks = (unsigned)((n + threads - 1) / threads);
+  if (mode == 0)
+    adj_rotate_kernel<0><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, out);
+  else if (mode == 1)
+    adj_rotate_kernel<1><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, out);
+  else
+    adj_rotate_kernel<2><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, out);
   return cudaGetLastError();
 }
 

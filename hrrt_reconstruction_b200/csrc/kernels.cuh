@@ -89,6 +89,14 @@ cudaError_t launch_fp(const DevGeom &g, const float *image, const QuadWork *work
 // back projection of quad-layout input into the column (Bc) / row (Br) partials
 cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
                       float *bc, float *br, long long vol, cudaStream_t st);
+// exact adjoint of the forward projector: z-transpose into the column / row
+// partials (rows scaled as the forward projector scales them)
+cudaError_t launch_adj(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
+                       float *bc, float *br, long long vol, cudaStream_t st);
+// bilinear-sampling transpose of the partials of every pair; mode 0: OSEM
+// update, 1: inverse sensitivity (FOV columns), 2: out += (every column)
+cudaError_t launch_adj_rotate(const DevGeom &g, const int *pair_views, int npairs, const float *bc, const float *br,
+                              long long vol, float *image, float *nf_inv, float *out, int mode, cudaStream_t st);
 // back projection of one view pair's quad-layout input (quads x0..x0+nquads-1)
 // with both partial sums added atomically into `out` (zeroed by the caller)
 cudaError_t launch_bp_sum(const DevGeom &g, const float *quad, int view, int x0, int nquads, float *out,

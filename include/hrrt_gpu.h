@@ -50,7 +50,8 @@ enum {
 
 /* back projector variants */
 enum {
-  HRRT_BP_REF = 0         /* voxel-driven sinogram interpolation of the reference */
+  HRRT_BP_REF = 0,        /* voxel-driven sinogram interpolation of the reference */
+  HRRT_BP_ADJOINT = 1     /* the exact transpose of the forward projector (no counterpart in the reference) */
 };
 
 /*
@@ -160,8 +161,17 @@ int hrrt_forward_project(hrrt_ctx *ctx, const float *image_xyz, float *sino);
 
 /* Replaces back_proj3d_thread1 (sbrt:1622-1699): back-projects prj (not
  * modified) for (view, view+nviews/2) into the rotated frame buffer
- * imagebuf_xyz [x][y][zp] (overwritten). */
+ * imagebuf_xyz [x][y][zp] (overwritten).
+ * mode HRRT_BP_ADJOINT instead writes FP^T prj in the image frame (every
+ * column, overwritten): the exact transpose of hrrt_fp_pair, so that
+ * <fp(x), y> = <x, bp(y)> to rounding.  No counterpart in the reference. */
 int hrrt_bp_pair(hrrt_ctx *ctx, const float *prj, int view, float *imagebuf_xyz, int mode);
+
+/* The back projector of hrrt_sensitivity / hrrt_osem: HRRT_BP_REF (default,
+ * the reference's) or HRRT_BP_ADJOINT (the forward projector's transpose; the
+ * ratio is then not weighted by the reference's cos^3 segment factor).
+ * Clears the sensitivity images.  No counterpart in the reference. */
+int hrrt_set_backprojector(hrrt_ctx *ctx, int mode);
 
 /*
  * Back projection of one view pair that allocates no device memory (no

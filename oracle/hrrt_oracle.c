@@ -549,6 +549,176 @@ void orc_fp_pair(const orc_geom *g, const R *img, int view, R *rows) {
   free(p2);
 }
 
+/* Sample position of voxel (xx, yy) in the forward projector (as sample()):
+ * the four corner offsets into the image and their weights; 0 when outside. */
+static int sample_taps(const orc_geom *g, int xx, int yy, float cosv, float sinv, size_t b[4], float w[4]) {
+  const int nx = g->nx, c = g->c, zp = g->zp;
+  const float xx0 = (xx - c) * cosv - (yy - c) * sinv + c;
+  const float yy0 = (xx - c) * sinv + (yy - c) * cosv + c;
+  if (xx0 < 0 || xx0 > nx - 2 || yy0 < 0 || xx0 > nx - 2) return 0;
+  const int ix = (int)xx0, iy = (int)yy0;
+  const float x1 = xx0 - ix, y1 = yy0 - iy;
+  b[0] = ((size_t)ix * g->ny + iy) * zp;
+  b[1] = b[0] + (size_t)g->ny * zp;
+  b[2] = b[0] + zp;
+  b[3] = b[1] + zp;
+  if (b[3] + zp > (size_t)nx * g->ny * zp) return 0;
+  w[0] = (1 - x1) * (1 - y1);
+  w[1] = x1 * (1 - y1);
+  w[2] = y1 * (1 - x1);
+  w[3] = y1 * x1;
+  return 1;
+}
+
+/* Exact adjoint of orc_fp_pair: image += FP^T rows for one view pair.  Every
+ * step of the forward projection is transposed: the copy into the rows (for
+ * quad x = c the bins of lanes 1 and 3 are the ones written), the scaling,
+ * the z interpolation of each segment (end planes with their own positions,
+ * middle planes advancing one plane per plane, the same skipped groups), the
+ * centre-row initialisation and the bilinear samples.  No counterpart in the
+ * reference, whose back projector is not the transpose of its forward
+ * projector; <FP x, y> = <x, FP^T y> holds to rounding. */
+void orc_fp_adjoint(const orc_geom *g, const R *rows, int view, R *img) {
+  const int nx = g->nx, c = g->c, nz = g->nz, zp = g->zp, G = g->groupmax, ZS = g->zshift, N = g->nbins;
+  const int ss = g->segmentsize, FS = G * 2 * ZS;
+  const float cosv = g->cos_psi[view], sinv = g->sin_psi[view];
+  R *q0 = NEW(R, nz * 4);
+  R *q1 = NEW(R, (size_t)(G + 1) * nz * 4);
+  R *q2 = NEW(R, (size_t)(G + 1) * nz * 4);
+  R *gp = NEW(R, (size_t)(nz + 2) * 4), *gp2 = NEW(R, (size_t)(nz + 2) * 4);
+#define L(a, k, z, l) a[(((size_t)(k)) * nz + (z)) * 4 + (l)]
+  for (int x = 1; x <= c; x++) {
+    const int *cy = g->cyl + 2 * x;
+    if (cy[0] == 0) continue;                     /* no rows written */
+    if (cy[0] == cy[1]) continue;                 /* never projected */
+    if (g->nzmask[view * (nx / 2 + 1) + x] == 0) continue;
+    const int xri = N - x;
+    /* transpose of the copy-out: lane values from the rows */
+    memset(q0, 0, sizeof(R) * nz * 4);
+    memset(q1, 0, sizeof(R) * (G + 1) * nz * 4);
+    memset(q2, 0, sizeof(R) * (G + 1) * nz * 4);
+    const int l0 = (x == c) ? 1 : 0, l2 = (x == c) ? 3 : 2;  /* for x = c the later lane wins */
+    for (int yr = 0; yr < nz; yr++) {
+      L(q0, 0, yr, l0) += rows[(size_t)yr * N + x];
+      if (x != c) L(q0, 0, yr, 1) += rows[(size_t)yr * N + xri];
+      L(q0, 0, yr, l2) += rows[(size_t)(yr + ss) * N + x];
+      if (x != c) L(q0, 0, yr, 3) += rows[(size_t)(yr + ss) * N + xri];
+      for (int l = 0; l < 4; l++) L(q0, 0, yr, l) *= g->y_size;
+    }
+    for (int k = 1; k <= G; k++) {
+      const int th = 2 * k, gr = k - 1, yb = g->yb[th];
+      for (int yr = yb; yr <= g->yt[th]; yr++) {
+        const size_t a = (size_t)(g->soff[th] + yr - yb), b = (size_t)(g->soff[th - 1] + yr - yb);
+        int zs = yr - yb;
+        if (zs >= ZS) zs = g->yt[th] - yr;
+        const float sc = (zs < ZS) ? g->rescale[gr * nz + yr] : g->rescale[gr * nz + yb + ZS];
+        L(q1, k, yr, l0) += rows[a * N + x];
+        L(q1, k, yr, l2) += rows[(a + ss) * N + x];
+        L(q2, k, yr, l0) += rows[b * N + x];
+        L(q2, k, yr, l2) += rows[(b + ss) * N + x];
+        if (x != c) {
+          L(q1, k, yr, 1) += rows[a * N + xri];
+          L(q1, k, yr, 3) += rows[(a + ss) * N + xri];
+          L(q2, k, yr, 1) += rows[b * N + xri];
+          L(q2, k, yr, 3) += rows[(b + ss) * N + xri];
+        }
+        for (int l = 0; l < 4; l++) {
+          L(q1, k, yr, l) *= sc;
+          L(q2, k, yr, l) *= sc;
+        }
+      }
+    }
+    size_t tb[4];
+    float tw[4];
+    /* centre row: every plane of every segment took the four centre samples */
+    {
+      const int cx[4] = {x, nx - x, c, c}, cyy[4] = {c, c, x, nx - x};
+      for (int i = 0; i < 4; i++) {
+        if (!sample_taps(g, cx[i], cyy[i], cosv, sinv, tb, tw)) continue;
+        for (int z = 0; z < nz; z++) {
+          R v = L(q0, 0, z, i);
+          for (int k = 1; k <= G; k++)
+            if (z >= g->yb[2 * k] && z <= g->yt[2 * k]) v += L(q1, k, z, i) + L(q2, k, z, i);
+          for (int t = 0; t < 4; t++) img[tb[t] + z] += tw[t] * v;
+        }
+      }
+    }
+    for (int y = cy[0]; y < c; y++) {
+      memset(gp, 0, sizeof(R) * (nz + 2) * 4);
+      memset(gp2, 0, sizeof(R) * (nz + 2) * 4);
+      for (int z = 0; z < nz; z++)
+        for (int l = 0; l < 4; l++) {
+          gp[z * 4 + l] += L(q0, 0, z, l);
+          gp2[z * 4 + l] += L(q0, 0, z, l);
+        }
+      const int *zi1 = g->fl_zzi + y * FS, *zi2 = g->fl_zzi + (nx - y) * FS;
+      const float *f1a = g->fl_zzz0 + y * FS, *f2a = g->fl_zzz0 + (nx - y) * FS;
+      for (int th = 2, gr = 0; th < g->nseg; th += 2, gr++) {
+        const int k = th / 2;
+        int yri = gr * ZS * 2;
+        if (zi1[yri] < 0) continue;
+        if (zi2[yri + ZS * 2 - 1] > nz - 1) continue;
+        int yr;
+        for (yr = g->yb[th]; yr < g->yb[th] + ZS; yr++, yri++) {
+          const int z = zi1[yri], z2 = zi2[yri];
+          const float f1 = f1a[yri], f2 = f2a[yri];
+          for (int l = 0; l < 4; l++) {
+            const R r1 = L(q1, k, yr, l), r2 = L(q2, k, yr, l);
+            gp2[(z2 + 1) * 4 + l] += f2 * r1; gp[z * 4 + l] += f2 * r1;
+            gp[(z + 1) * 4 + l] += f1 * r1;   gp2[z2 * 4 + l] += f1 * r1;
+            gp[(z2 + 1) * 4 + l] += f2 * r2;  gp2[z * 4 + l] += f2 * r2;
+            gp2[(z + 1) * 4 + l] += f1 * r2;  gp[z2 * 4 + l] += f1 * r2;
+          }
+        }
+        float zz0 = yr + (y - c) * g->tantheta[gr * nz + yr];
+        int z = (int)zz0;
+        const float c1 = zz0 - z;
+        zz0 = yr + (c - y) * g->tantheta[gr * nz + yr];
+        int z2 = (int)zz0;
+        const float c2 = zz0 - z2;
+        for (; yr <= g->yt[th] - ZS; yr++, z++, z2++)
+          for (int l = 0; l < 4; l++) {
+            const R r1 = L(q1, k, yr, l), r2 = L(q2, k, yr, l);
+            gp2[(z2 + 1) * 4 + l] += c2 * r1; gp[z * 4 + l] += c2 * r1;
+            gp[(z + 1) * 4 + l] += c1 * r1;   gp2[z2 * 4 + l] += c1 * r1;
+            gp[(z2 + 1) * 4 + l] += c2 * r2;  gp2[z * 4 + l] += c2 * r2;
+            gp2[(z + 1) * 4 + l] += c1 * r2;  gp[z2 * 4 + l] += c1 * r2;
+          }
+        for (yr = g->yt[th] - ZS + 1; yr <= g->yt[th]; yr++, yri++) {
+          const int ze = zi1[yri], ze2 = zi2[yri];
+          const float f1 = f1a[yri], f2 = f2a[yri];
+          for (int l = 0; l < 4; l++) {
+            const R r1 = L(q1, k, yr, l), r2 = L(q2, k, yr, l);
+            gp2[(ze2 + 1) * 4 + l] += f2 * r1; gp[ze * 4 + l] += f2 * r1;
+            gp[(ze + 1) * 4 + l] += f1 * r1;   gp2[ze2 * 4 + l] += f1 * r1;
+            gp[(ze2 + 1) * 4 + l] += f2 * r2;  gp2[ze * 4 + l] += f2 * r2;
+            gp2[(ze + 1) * 4 + l] += f1 * r2;  gp[ze2 * 4 + l] += f1 * r2;
+          }
+        }
+      }
+      /* the eight samples of this row; planes >= nz of pam/pam2 are zero in
+       * the forward projection, so their gradient is dropped */
+      const int px[8] = {x, nx - x, nx - y, nx - y, x, nx - x, y, y};
+      const int py[8] = {y, y, x, nx - x, nx - y, nx - y, x, nx - x};
+      for (int i = 0; i < 8; i++) {
+        if (!sample_taps(g, px[i], py[i], cosv, sinv, tb, tw)) continue;
+        const R *src = (i < 4) ? gp : gp2;
+        const int l = i & 3;
+        for (int z = 0; z < nz; z++) {
+          const R v = src[z * 4 + l];
+          for (int t = 0; t < 4; t++) img[tb[t] + z] += tw[t] * v;
+        }
+      }
+    }
+  }
+#undef L
+  free(q0);
+  free(q1);
+  free(q2);
+  free(gp);
+  free(gp2);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Back projection                                                          */
 /* ------------------------------------------------------------------------ */

@@ -70,6 +70,8 @@ void orc_get_norm_zero_mask(const orc_geom *g, int16_t *mask);
 void orc_fp_pair(const orc_geom *g, const orc_real *img, int view, orc_real *rows);
 /* back projection of one view pair into the rotated frame (overwritten) */
 void orc_bp_pair(const orc_geom *g, const orc_real *rows, int view, orc_real *imagebuf);
+/* image += FP^T rows: the exact transpose of orc_fp_pair (image frame) */
+void orc_fp_adjoint(const orc_geom *g, const orc_real *rows, int view, orc_real *image);
 /* corr += rotate-back(imagebuf) for one view */
 void orc_rotate_add(const orc_geom *g, const orc_real *imagebuf, int view, orc_real *corr);
 

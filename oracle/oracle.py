@@ -52,7 +52,7 @@ def lib(precision="f64"):
             sigs = {
                 "orc_order": [vp, vp], "orc_z_range": [vp, i, i, vp], "orc_cylwiny": [vp, vp], "orc_trig": [vp, vp, vp, vp, vp],
                 "orc_tantheta": [vp, vp, vp], "orc_flookup": [vp, vp, vp], "orc_blookup": [vp, vp, vp, vp, vp],
-                "orc_set_norm_zero_mask": [vp, vp], "orc_get_norm_zero_mask": [vp, vp], "orc_fp_pair": [vp, vp, i, vp], "orc_bp_pair": [vp, vp, i, vp],
+                "orc_set_norm_zero_mask": [vp, vp], "orc_get_norm_zero_mask": [vp, vp], "orc_fp_pair": [vp, vp, i, vp], "orc_bp_pair": [vp, vp, i, vp], "orc_fp_adjoint": [vp, vp, i, vp],
                 "orc_rotate_add": [vp, vp, i, vp], "orc_prep": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
                 "orc_sensitivity": [vp, vp, vp, i], "orc_init_image": [vp, vp, i, i],
                 "orc_osem_subset": [vp, vp, vp, vp, vp, i, i],
@@ -134,6 +134,13 @@ class Oracle:
         rows = self._r(rows)
         out = np.zeros(self.image_shape, self.dtype)
         self.L.orc_bp_pair(self.g, _p(rows), view, _p(out))
+        return out
+
+    def fp_adjoint(self, rows, view, image=None):
+        """image + FP^T rows (the exact transpose of fp_pair), image frame."""
+        rows = self._r(rows)
+        out = np.zeros(self.image_shape, self.dtype) if image is None else np.array(image, self.dtype, copy=True)
+        self.L.orc_fp_adjoint(self.g, _p(rows), view, _p(out))
         return out
 
     def rotate_add(self, imagebuf, view, corr):
