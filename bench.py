@@ -44,7 +44,15 @@ UNIT = "subset-iters/s"
 STUDY = dict(total_counts=3e8, randoms_frac=0.25, scatter_frac=0.15, norm_sigma=0.1)
 
 
+GEOMETRY = "hrrt"
+
+
 def geom_dict():
+    """HRRT model 999 at span 3; `--geometry small` selects a 24-ring test
+    scanner that only the multi-process plumbing tests use."""
+    if GEOMETRY == "small":
+        return dict(nrings=24, nelements=64, nangles=96, ring_radius=58.625, plane_sep=1.21875, binsize=1.21875,
+                    span=3, maxdel=13, subsets=SUBSETS)
     return dict(nrings=104, nelements=256, nangles=288, ring_radius=234.5, plane_sep=1.21875, binsize=1.21875,
                 span=SPAN, maxdel=67, subsets=SUBSETS)
 
@@ -317,11 +325,108 @@ def run_ours(args, ws, rank, local):
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
+    ctx.close()
+    del ctx
+    if args.lm_events > 0:
+        out["listmode"] = run_listmode(args, torch, H, local, dist, ws, cpu=(rank == 0 and ws == 1 and
+                                                                             not args.no_cpu_baseline))
     if rank == 0:
         print(json.dumps(out), flush=True)
-    del ctx
     if dist is not None:
         dist.destroy_process_group()
+
+
+def run_listmode(args, torch, H, local, dist, ws, cpu=True):
+    """l64 listmode -> span-3 prompt and delayed sinograms (16-bit), the
+    config-5 workload: synthetic events from the config-1 phantom's LOR
+    distribution, 10 % delayed, a time tag every 1000 events (1 ms)."""
+    from hrrt_reconstruction_b200 import listmode_synth as LS
+    n = args.lm_events
+    t0 = time.time()
+    with H.Context(H.hrrt_geometry(span=3), device=local) as c3:
+        E = LS.expected_prompts(c3, seed=0)
+    words = LS.synth_words(n, E, seed=0, device=f"cuda:{local}")
+    del E
+    gen_s = time.time() - t0
+    nwords = words.numel()
+    lm = H.Listmode(3, device=local)
+    S = lm.sino_size
+    ds = torch.zeros(S, dtype=torch.int16, device=f"cuda:{local}")
+    dd = torch.zeros(S, dtype=torch.int16, device=f"cuda:{local}")
+    cs = torch.cuda.current_stream()
+    for _ in range(2):
+        lm.reset_clock()
+        lm.histogram_device(words.data_ptr(), nwords, ds.data_ptr(), dd.data_ptr(), stream=cs.cuda_stream)
+    torch.cuda.synchronize()
+    reps = 3
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    barrier(dist, local)
+    ev[0].record(cs)
+    dev_ms = []
+    for _ in range(reps):
+        lm.reset_clock()
+        st = lm.histogram_device(words.data_ptr(), nwords, ds.data_ptr(), dd.data_ptr(), stream=cs.cuda_stream)
+        dev_ms.append(st["ms"])
+    ev[1].record(cs)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(dist, ev[0].elapsed_time(ev[1]) / reps, local)
+    # end to end: words from pinned host memory, sinograms back to pinned host memory
+    hw = torch.empty(nwords, dtype=torch.int32, pin_memory=True)
+    hw.copy_(words)
+    del words, ds, dd
+    torch.cuda.empty_cache()
+    hs = torch.empty(S, dtype=torch.int16, pin_memory=True)
+    hd = torch.empty(S, dtype=torch.int16, pin_memory=True)
+    hwn = hw.numpy().view(np.uint32)
+    out = (hs.numpy().view(np.uint16), hd.numpy().view(np.uint16))
+    lm.reset_clock()
+    lm.histogram(hwn, out=out)  # warm: grows the library's staging buffers
+    ls = torch.cuda.ExternalStream(lm.stream)
+    torch.cuda.synchronize()
+    barrier(dist, local)
+    ev[0].record(ls)
+    lm.reset_clock()
+    st = lm.histogram(hwn, out=out)[2]
+    ev[1].record(ls)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(dist, ev[0].elapsed_time(ev[1]), local)
+    peak, peak_kind = measured_peaks()
+    algo = nwords * 4 + 2 * S * 2  # events read once + both 16-bit sinograms written once
+    res = {
+        "metric": "listmode events/s (l64 -> span-3 prompt + delayed sinograms, 16-bit)", "unit": "events/s",
+        "value": ws * n / (ms / 1e3), "ms_per_frame": ms, "events": n, "words": nwords,
+        "workload": "1 frame of synthetic l64 events (config-1 phantom LORs, 10 % delayed, 1 time tag / 1000 "
+                    "events), histogram modes prompts + delayed, span 3",
+        "stats": {k: st[k] for k in ("prompts", "delayed", "timetags", "unmapped", "invalid")},
+        "e2e": {"value": ws * n / (e2e_ms / 1e3), "unit": "events/s", "ms": e2e_ms,
+                "h2d_bytes_per_step": nwords * 4, "d2h_bytes_per_step": 2 * S * 2},
+        "roofline": {"bound": "hbm", "kernel": "lm_map + lm_hist passes (whole call)", "unit": "GB/s",
+                     "achieved": algo / (ms / 1e3) / 1e9, "peak": peak, "frac": algo / (ms / 1e3) / 1e9 / peak,
+                     "bytes_per_launch": algo,
+                     "note": "algorithmic bytes: the event words read once and both sinograms written once"},
+        "device_ms_per_call": float(np.mean(dev_ms)),
+        "data_gen_s": gen_s,
+    }
+    if cpu:
+        res["cpu_baseline"] = listmode_cpu_baseline(hwn)
+    lm.close()
+    return res
+
+
+def listmode_cpu_baseline(words, n_sample_words=8_000_000):
+    """The listmode restatement (oracle/lm_oracle.c, one thread) on the first
+    `n_sample_words` words of the same stream."""
+    from oracle.lm import LMOracle
+    O = LMOracle(3)
+    w = np.ascontiguousarray(words[:n_sample_words])
+    s = np.zeros(O.sino_size, np.uint16)
+    d = np.zeros(O.sino_size, np.uint16)
+    t0 = time.perf_counter()
+    _, _, st = O.histogram(w, sino=s, delayed=d)
+    dt = time.perf_counter() - t0
+    ev = st["prompts"] + st["delayed"]
+    return {"value": ev / dt, "unit": "events/s", "cores": 1, "kind": "port",
+            "sample": f"first {n_sample_words} words ({ev} events) of the stream on oracle/lm_oracle.c"}
 
 
 def ref_inputs(R, seed=0):
@@ -415,8 +520,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--storage", default="f32", choices=["f32", "16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--lm-events", type=int, default=1_000_000_000,
+                    help="listmode events of the l64 leg (0: skip it)")
+    ap.add_argument("--geometry", default="hrrt", choices=["hrrt", "small"])
     args = ap.parse_args()
-    if args.warmup < 3:
+    global GEOMETRY
+    GEOMETRY = args.geometry
+    if args.warmup < 3 and args.impl != "reference":
         args.warmup = 3
     ws, rank, local = dist_env()
     if args.impl == "reference":

@@ -106,6 +106,8 @@ def _load():
         "hrrt_lm_last_error": (ctypes.c_char_p, [vp]),
         "hrrt_lm_sino_size": (ctypes.c_longlong, [vp]),
         "hrrt_lm_reset_clock": (i, [vp]),
+        "hrrt_lm_get_stream": (vp, [vp]),
+        "hrrt_lm_table": (ctypes.c_longlong, [i, i, ctypes.c_char_p, vp, ctypes.c_size_t]),
         "hrrt_lm_histogram": (i, [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, ctypes.POINTER(LmStats)]),
         "hrrt_lm_histogram_device": (i, [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, ctypes.POINTER(LmStats), vp]),
     }
@@ -328,6 +330,25 @@ class Context:
         self._check(lib.hrrt_reset_kernel_stats(self._h), "reset_kernel_stats")
 
 
+LM_SOL = np.dtype([("nsino", np.int32), ("d", np.float32), ("z", np.float32)])
+
+
+def lm_table(name, span=3, maxrd=67):
+    """One listmode rebinning table (host-only): "sol" [21][144][144] LM_SOL,
+    "zpos"/"zpos2" float [104], "segz0"/"segzmax"/"segzoffset" int32."""
+    n = lib.hrrt_lm_table(span, maxrd, name.encode(), None, 0)
+    if n < 0:
+        raise HrrtError(f"lm_table({name!r}): {n}")
+    if name == "sol":
+        out = np.empty((21, 144, 144), LM_SOL)
+    elif name.startswith("zpos"):
+        out = np.empty(n // 4, np.float32)
+    else:
+        out = np.empty(n // 4, np.int32)
+    lib.hrrt_lm_table(span, maxrd, name.encode(), out.ctypes.data, out.nbytes)
+    return out
+
+
 class Listmode:
     """64-bit HRRT listmode histogrammer on the device (hrrt_lm_* C ABI):
     the rebinner LUT for output span 3 or 9, and the clock carried from one
@@ -369,11 +390,20 @@ class Listmode:
     def reset_clock(self):
         self._check(lib.hrrt_lm_reset_clock(self._h), "reset_clock")
 
-    def histogram(self, words, mode=LM_PROMPTS_AND_DELAYED, duration=0, flags=0):
-        """One frame from host words -> (sino, delayed or None, stats dict)."""
+    @property
+    def stream(self):
+        """cudaStream_t (int) of the host-buffer entry point."""
+        return lib.hrrt_lm_get_stream(self._h)
+
+    def histogram(self, words, mode=LM_PROMPTS_AND_DELAYED, duration=0, flags=0, out=None):
+        """One frame from host words -> (sino, delayed or None, stats dict);
+        `out` = (sino, delayed) uint16 host arrays to fill."""
         w = _c(words, np.uint32)
-        sino = np.empty(self.sino_size, np.uint16)
-        dly = np.empty(self.sino_size, np.uint16) if mode == LM_PROMPTS_AND_DELAYED else None
+        if out is None:
+            sino = np.empty(self.sino_size, np.uint16)
+            dly = np.empty(self.sino_size, np.uint16) if mode == LM_PROMPTS_AND_DELAYED else None
+        else:
+            sino, dly = out
         st = LmStats()
         self._check(lib.hrrt_lm_histogram(self._h, _ptr(w), w.size, mode, duration, flags, _ptr(sino), _ptr(dly),
                                           ctypes.byref(st)), "lm_histogram")

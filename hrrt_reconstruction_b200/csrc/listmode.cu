@@ -381,6 +381,8 @@ struct hrrt_lm {
   uint32_t *h_words_dev = nullptr;  // host-API staging
   size_t h_words_cap = 0;
   uint16_t *h_sino_dev = nullptr;   // host-API sinograms (prompts, delayed)
+  longlong2 *tagbuf = nullptr;      // ordered time tags (position, value)
+  long long tag_cap = 0;
   // clock carried across frames (process_tagword's statics)
   long long current_time = -1, current_time_msec = -1, prev_time = 0;
   int clock_reset = 0;
@@ -390,6 +392,7 @@ struct hrrt_lm {
     cudaSetDevice(device);
     for (void *p : allocs) cudaFree(p);
     if (scratch) cudaFree(scratch);
+    if (tagbuf) cudaFree(tagbuf);
     if (h_words_dev) cudaFree(h_words_dev);
     if (h_sino_dev) cudaFree(h_sino_dev);
     if (stream) cudaStreamDestroy(stream);
@@ -485,6 +488,8 @@ const char *hrrt_lm_last_error(const hrrt_lm *h) { return h ? h->err.c_str() : "
 
 long long hrrt_lm_sino_size(const hrrt_lm *h) { return h ? h->tab.sino_size() : -1; }
 
+void *hrrt_lm_get_stream(const hrrt_lm *h) { return h ? (void *)h->stream : nullptr; }
+
 int hrrt_lm_reset_clock(hrrt_lm *h) {
   if (!h) return HRRT_ERR_ARG;
   h->current_time = -1;
@@ -517,14 +522,13 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
   const long long ntiles = (nwords + kTileWords - 1) / kTileWords;
   const int tpp = (int)(kPacketWords / kTileWords);
   const long long npackets = (nwords + kPacketWords - 1) / kPacketWords;
-  // time tags: at most one per two words
-  const long long tag_cap = nwords / 2 + 1;
   // scratch: tile sums (8), entries (1), tag offsets (4) per tile; packet
-  // offsets (8) per packet; stats; tags (16 each)
+  // offsets (8) per packet; stats.  The time tags get their own buffer once
+  // the scan has counted them.
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t b_sum = al(8 * ntiles), b_ent = al(ntiles), b_off = al(4 * ntiles), b_pk = al(8 * (npackets + 1)),
-               b_st = al(8 * (kStCount + 1)), b_tags = al(16 * tag_cap);
-  const size_t need = b_sum + b_ent + b_off + b_pk + b_st + b_tags;
+               b_st = al(8 * (kStCount + 1));
+  const size_t need = b_sum + b_ent + b_off + b_pk + b_st;
   if (h->scratch_bytes < need) {
     if (h->scratch) cudaFree(h->scratch);
     h->scratch = nullptr;
@@ -539,7 +543,6 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
   auto *tile_tagoff = (unsigned int *)(p + b_sum + b_ent);
   auto *pk = (unsigned long long *)(p + b_sum + b_ent + b_off);
   auto *stats = (unsigned long long *)(p + b_sum + b_ent + b_off + b_pk);
-  auto *tags = (longlong2 *)(p + b_sum + b_ent + b_off + b_pk + b_st);
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
@@ -552,6 +555,25 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
     lm_scan_kernel<<<1, 1024, 0, st>>>(pk, npackets, stats + kStCount);
     e = cudaGetLastError();
   }
+  unsigned long long ntags = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&ntags, stats + kStCount, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && (long long)ntags > h->tag_cap) {
+    if (h->tagbuf) cudaFree(h->tagbuf);
+    h->tagbuf = nullptr;
+    h->tag_cap = 0;
+    const long long cap = std::max<long long>((long long)ntags, 1024);
+    e = cudaMalloc(&h->tagbuf, sizeof(longlong2) * (size_t)cap);
+    if (e != cudaSuccess) {
+      h->tagbuf = nullptr;
+      cudaEventDestroy(ev0);
+      cudaEventDestroy(ev1);
+      return lm_fail(h, HRRT_ERR_NOMEM, "hrrt_lm_histogram: time tags");
+    }
+    h->tag_cap = cap;
+  }
+  longlong2 *tags = h->tagbuf;
+  const long long tag_cap = h->tag_cap;
   // pass 1: ordered time tags (and, without a frame length, the histogram)
   const bool one_pass = duration <= 0;
   if (e == cudaSuccess) {
@@ -566,8 +588,6 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
           (uint32_t *)d_sino, (uint32_t *)d_delayed, stats);
     e = cudaGetLastError();
   }
-  unsigned long long ntags = 0;
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&ntags, stats + kStCount, 8, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   std::vector<longlong2> htags;
   if (e == cudaSuccess && ntags > 0) {
@@ -615,6 +635,38 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
   out->duration = h->current_time - frame_start;
   out->ms = ms;
   return HRRT_OK;
+}
+
+long long hrrt_lm_table(int span, int maxrd, const char *name, void *out, size_t bytes) {
+  if (!name) return HRRT_ERR_ARG;
+  hrrt::LmTables t;
+  if (!t.build(span, maxrd).empty()) return HRRT_ERR_ARG;
+  const void *src = nullptr;
+  size_t n = 0;
+  const std::string k(name);
+  if (k == "sol") {
+    src = t.sol.data();
+    n = t.sol.size() * sizeof(hrrt::LmSol);
+  } else if (k == "zpos") {
+    src = t.zpos.data();
+    n = t.zpos.size() * sizeof(float);
+  } else if (k == "zpos2") {
+    src = t.zpos2.data();
+    n = t.zpos2.size() * sizeof(float);
+  } else if (k == "segz0") {
+    src = t.segz0.data();
+    n = t.segz0.size() * sizeof(int);
+  } else if (k == "segzmax") {
+    src = t.segzmax.data();
+    n = t.segzmax.size() * sizeof(int);
+  } else if (k == "segzoffset") {
+    src = t.segzoffset.data();
+    n = t.segzoffset.size() * sizeof(int);
+  } else {
+    return HRRT_ERR_ARG;
+  }
+  if (out && bytes >= n) std::memcpy(out, src, n);
+  return (long long)n;
 }
 
 int hrrt_lm_histogram(hrrt_lm *h, const uint32_t *words, long long nwords, int mode, int duration, int flags,

@@ -255,6 +255,14 @@ void hrrt_lm_destroy(hrrt_lm *lm);
 const char *hrrt_lm_last_error(const hrrt_lm *lm);
 /* bins of one sinogram: planes x 288 views x 256 bins */
 long long hrrt_lm_sino_size(const hrrt_lm *lm);
+/* the stream the host-buffer entry point runs on (cudaStream_t) */
+void *hrrt_lm_get_stream(const hrrt_lm *lm);
+/* Host-only (no GPU needed): copy one rebinning table for (span, maxrd) into
+ * `out` (capacity `bytes`); returns its size in bytes or a negative status.
+ * Names: "sol" ({int32 nsino; float d; float z} [21][144][144], the LUT
+ * hrrt_rebinner_lut writes), "zpos", "zpos2" (float [104]), "segz0",
+ * "segzmax", "segzoffset" (int32 [45]). */
+long long hrrt_lm_table(int span, int maxrd, const char *name, void *out, size_t bytes);
 /* forget the clock carried from the previous frame (a new stream) */
 int hrrt_lm_reset_clock(hrrt_lm *lm);
 

@@ -189,3 +189,20 @@ def test_crystals_and_segments_match_reference_build():
         k = n.value
         assert np.array_equal(z0[:k], oz0) and np.array_equal(zm[:k], ozm) and np.array_equal(off[:k], ooff)
         assert npl.value == O.nplanes and dt.value == O.L.lm_d_tan_theta(O.t)
+
+
+def test_device_lut_matches_oracle():
+    """The library's host-built LUT (hrrt_lm_table, no GPU needed) equals the
+    restatement's bit for bit."""
+    import hrrt_reconstruction_b200 as H
+    for span in (3, 9):
+        O = LMOracle(span)
+        sol = H.lm_table("sol", span)
+        assert np.array_equal(sol.view(np.uint8), O.sol().view(np.uint8))
+        zp, zp2 = O.zpos()
+        assert np.array_equal(H.lm_table("zpos", span).view(np.uint32), zp.view(np.uint32))
+        assert np.array_equal(H.lm_table("zpos2", span).view(np.uint32), zp2.view(np.uint32))
+        z0, zm, off = O.segments()
+        assert np.array_equal(H.lm_table("segz0", span), z0)
+        assert np.array_equal(H.lm_table("segzmax", span), zm)
+        assert np.array_equal(H.lm_table("segzoffset", span), off)
