@@ -82,6 +82,7 @@ def _load():
         "hrrt_get_stream": (vp, [vp]),
         "hrrt_upload_inputs": (i, [vp, vp, vp, vp, vp, vp, i]),
         "hrrt_sensitivity": (i, [vp]),
+        "hrrt_reconstruct": (i, [vp, vp, vp, vp, vp, vp, i, vp, i, vp, ctypes.POINTER(Stats)]),
         "hrrt_init_image": (i, [vp, vp]),
         "hrrt_osem": (i, [vp, i, ctypes.POINTER(Stats)]),
         "hrrt_osem_subsets": (i, [vp, i, i]),
@@ -232,6 +233,31 @@ class Context:
 
     def sensitivity(self):
         self._check(lib.hrrt_sensitivity(self._h), "sensitivity")
+
+    def reconstruct(self, prompts, randoms, norm=None, atten=None, scatter=None, storage=STORE_F32, iterations=1,
+                    init_image_zyx=None, out=None):
+        """upload + sensitivity + init + osem + get_image in one pipelined
+        call -> (image [z][y][x], Stats).  Host arrays in pinned memory let
+        the uploads overlap the first iteration."""
+        p = _c(prompts, np.int16)
+        r = _c(randoms, np.float32)
+        n = _c(norm, np.float32)
+        a = _c(atten, np.float32)
+        s = _c(scatter, np.float32)
+        need = int(np.prod(self.sino_shape))
+        for name, arr in (("prompts", p), ("randoms", r), ("norm", n), ("atten", a), ("scatter", s)):
+            if arr is not None and arr.size != need:
+                raise HrrtError(f"{name}: {arr.size} elements, expected {need}")
+        i = self.info
+        if out is None:
+            out = np.empty((i.nz, i.ny, i.nx), np.float32)
+        elif out.shape != (i.nz, i.ny, i.nx) or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise HrrtError("reconstruct: out must be C-contiguous float32 [nz][ny][nx]")
+        im = _c(init_image_zyx, np.float32)
+        st = Stats()
+        self._check(lib.hrrt_reconstruct(self._h, _ptr(p), _ptr(r), _ptr(n), _ptr(a), _ptr(s), storage, _ptr(im),
+                                         iterations, _ptr(out), ctypes.byref(st)), "reconstruct")
+        return out, st
 
     def init_image(self, image_zyx=None):
         im = _c(image_zyx, np.float32)

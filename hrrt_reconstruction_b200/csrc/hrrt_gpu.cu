@@ -64,6 +64,9 @@ struct hrrt_ctx {
   cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
   char *stage[2] = {nullptr, nullptr};
   size_t stage_bytes = 0;
+  // pipelined reconstruction: the view pairs of one subset staged pair-major
+  char *pstage[2] = {nullptr, nullptr};
+  size_t pstage_bytes = 0;
 
   // back projector of the OSEM loop, and the device geometry it runs with
   // (for the adjoint: segment weights of 1, the forward projector's scaling)
@@ -331,6 +334,69 @@ int run_subset(hrrt_ctx *ctx, int s) {
   return HRRT_OK;
 }
 
+// quad-layout input buffers for `storage` (allocated once per storage type)
+int ensure_input_buffers(hrrt_ctx *ctx, int storage) {
+  const Geometry &g = ctx->geo;
+  cudaError_t e = cudaSuccess;
+  if (ctx->storage != storage) {
+    for (void *p : {ctx->q_prompts, ctx->q_add, ctx->q_mult})
+      if (p) {
+        cudaFree(p);
+        ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), p));
+      }
+    ctx->q_prompts = ctx->q_add = ctx->q_mult = nullptr;
+    ctx->storage = -1;
+    const size_t nquad = (size_t)(g.nviews / 2) * ctx->quad_pair;
+    const size_t ab = storage == HRRT_STORE_F32 ? 4 : 2;
+    ctx->q_prompts = dalloc<char>(ctx, nquad * 2, &e);
+    ctx->q_add = ctx->q_prompts ? dalloc<char>(ctx, nquad * ab, &e) : nullptr;
+    ctx->q_mult = ctx->q_add ? dalloc<char>(ctx, nquad * ab, &e) : nullptr;
+    if (!ctx->q_mult) return fail(ctx, HRRT_ERR_NOMEM, "input allocation");
+    ctx->storage = storage;
+  }
+  if (!ctx->d_mask_accum) {
+    ctx->d_mask_accum = dalloc<int>(ctx, (size_t)(g.nviews / 2) * ctx->dg.nquads, &e);
+    if (!ctx->d_mask_accum) return fail(ctx, HRRT_ERR_NOMEM, "mask");
+  }
+  return HRRT_OK;
+}
+
+// inverse sensitivity of subset s (CalculateNormfac's subset body)
+int sens_subset(hrrt_ctx *ctx, int s) {
+  const bool adj = ctx->bp_mode == HRRT_BP_ADJOINT;
+  {
+    Launch L(ctx, "scale_pairs_kernel");
+    CK(launch_scale_pairs(adj ? ctx->dg_adj : ctx->dg, ctx->q_mult, ctx->storage,
+                          ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_ratio, ctx->quad_pair,
+                          ctx->stream),
+       "scale_pairs");
+  }
+  if (adj) {
+    {
+      Launch L(ctx, "adj_kernel");
+      CK(launch_adj(ctx->dg_adj, ctx->d_ratio, ctx->quad_pair, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s],
+                    ctx->d_bc, ctx->d_br, ctx->vol, ctx->stream),
+         "adj_kernel");
+    }
+    Launch L(ctx, "adj_rotate_kernel");
+    CK(launch_adj_rotate(ctx->dg_adj, ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_bc, ctx->d_br,
+                         ctx->vol, nullptr, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 1, ctx->stream),
+       "adj_rotate_kernel");
+    return HRRT_OK;
+  }
+  {
+    Launch L(ctx, "bp_kernel");
+    CK(launch_bp(ctx->dg, ctx->d_ratio, ctx->quad_pair, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s], ctx->d_bc,
+                 ctx->d_br, ctx->vol, ctx->stream),
+       "bp_kernel");
+  }
+  Launch L(ctx, "rotback_kernel");
+  CK(launch_rotback(ctx->dg, ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_bc, ctx->d_br, ctx->vol,
+                    nullptr, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 1, ctx->stream),
+     "rotback_kernel");
+  return HRRT_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -465,6 +531,7 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
     }
   std::vector<FpTask> tasks = build_fp_tasks(g);
   m = validate_fp(g, mid, tasks);
+  if (m.empty() && ((int)tasks.size() + 31) / 32 + 2 > kFpMaxWarps) m = "fp: too many projection tasks for one CTA";
   if (!m.empty()) return bail(fail(ctx, HRRT_ERR_ARG, m));
   // one task per thread; a quad with more tasks than a CTA's launch bound is
   // split over several CTAs (each samples the quad's rows itself)
@@ -593,25 +660,7 @@ int hrrt_upload_inputs(hrrt_ctx *ctx, const int16_t *prompts, const float *rando
   if (storage != HRRT_STORE_F32 && storage != HRRT_STORE_16) return fail(ctx, HRRT_ERR_ARG, "unknown storage");
   const Geometry &g = ctx->geo;
   cudaError_t e = cudaSuccess;
-  // quad-layout inputs for every view pair (allocated once per storage type)
-  if (ctx->storage != storage) {
-    for (void *p : {ctx->q_prompts, ctx->q_add, ctx->q_mult})
-      if (p) {
-        cudaFree(p);
-        ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), p));
-      }
-    const size_t nquad = (size_t)(g.nviews / 2) * ctx->quad_pair;
-    const size_t ab = storage == HRRT_STORE_F32 ? 4 : 2;
-    ctx->q_prompts = dalloc<char>(ctx, nquad * 2, &e);
-    ctx->q_add = ctx->q_prompts ? dalloc<char>(ctx, nquad * ab, &e) : nullptr;
-    ctx->q_mult = ctx->q_add ? dalloc<char>(ctx, nquad * ab, &e) : nullptr;
-    if (!ctx->q_mult) return fail(ctx, HRRT_ERR_NOMEM, "input allocation");
-    ctx->storage = storage;
-  }
-  if (!ctx->d_mask_accum) {
-    ctx->d_mask_accum = dalloc<int>(ctx, (size_t)(g.nviews / 2) * ctx->dg.nquads, &e);
-    if (!ctx->d_mask_accum) return fail(ctx, HRRT_ERR_NOMEM, "mask");
-  }
+  if (int rc = ensure_input_buffers(ctx, storage)) return rc;
   // staging of the raw flat-file arrays, kUploadPlanes planes at a time
   const float *srcs[4] = {randoms, norm, atten, scatter};
   const size_t plane_elems = (size_t)g.nviews * g.nbins;
@@ -685,44 +734,8 @@ int hrrt_sensitivity(hrrt_ctx *ctx) {
   if (!ctx) return HRRT_ERR_ARG;
   if (!ctx->have_inputs) return fail(ctx, HRRT_ERR_STATE, "hrrt_upload_inputs must come first");
   const Geometry &g = ctx->geo;
-  const bool adj = ctx->bp_mode == HRRT_BP_ADJOINT;
-  for (int s = 0; s < g.sp.subsets; s++) {
-    {
-      Launch L(ctx, "scale_pairs_kernel");
-      CK(launch_scale_pairs(adj ? ctx->dg_adj : ctx->dg, ctx->q_mult, ctx->storage,
-                            ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_ratio, ctx->quad_pair,
-                            ctx->stream),
-         "scale_pairs");
-    }
-    if (adj) {
-      {
-        Launch L(ctx, "adj_kernel");
-        CK(launch_adj(ctx->dg_adj, ctx->d_ratio, ctx->quad_pair, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s],
-                      ctx->d_bc, ctx->d_br, ctx->vol, ctx->stream),
-           "adj_kernel");
-      }
-      {
-        Launch L(ctx, "adj_rotate_kernel");
-        CK(launch_adj_rotate(ctx->dg_adj, ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_bc,
-                             ctx->d_br, ctx->vol, nullptr, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 1,
-                             ctx->stream),
-           "adj_rotate_kernel");
-      }
-      continue;
-    }
-    {
-      Launch L(ctx, "bp_kernel");
-      CK(launch_bp(ctx->dg, ctx->d_ratio, ctx->quad_pair, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s], ctx->d_bc,
-                   ctx->d_br, ctx->vol, ctx->stream),
-         "bp_kernel");
-    }
-    {
-      Launch L(ctx, "rotback_kernel");
-      CK(launch_rotback(ctx->dg, ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_bc, ctx->d_br,
-                        ctx->vol, nullptr, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 1, ctx->stream),
-         "rotback_kernel");
-    }
-  }
+  for (int s = 0; s < g.sp.subsets; s++)
+    if (int rc = sens_subset(ctx, s)) return rc;
   CK(cudaStreamSynchronize(ctx->stream), "sensitivity");
   ctx->have_sens = true;
   return HRRT_OK;
@@ -802,18 +815,152 @@ int hrrt_osem(hrrt_ctx *ctx, int iterations, hrrt_stats *stats) {
   return HRRT_OK;
 }
 
+int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms, const float *norm,
+                     const float *atten, const float *scatter, int storage, const float *init_image_zyx,
+                     int iterations, float *image_zyx, hrrt_stats *stats) {
+  if (!ctx) return HRRT_ERR_ARG;
+  if (!prompts || !randoms || !image_zyx || iterations < 1)
+    return fail(ctx, HRRT_ERR_ARG, "prompts, randoms, an output image and iterations >= 1 are required");
+  if (storage != HRRT_STORE_F32 && storage != HRRT_STORE_16) return fail(ctx, HRRT_ERR_ARG, "unknown storage");
+  const Geometry &g = ctx->geo;
+  if (int rc = ensure_input_buffers(ctx, storage)) return rc;
+  // pair-major staging of one subset's view pairs, two buffers
+  const float *srcs[4] = {randoms, norm, atten, scatter};
+  const size_t P = g.segmentsize, N = g.nbins, V = g.nviews;
+  const size_t pair_elems = 2 * P * N, set_elems = (size_t)ctx->npairs * pair_elems;
+  const size_t need = set_elems * (sizeof(int16_t) + 4 * sizeof(float));
+  cudaError_t e = cudaSuccess;
+  if (ctx->pstage_bytes < need) {
+    for (int b = 0; b < 2; b++)
+      if (ctx->pstage[b]) {
+        cudaFree(ctx->pstage[b]);
+        ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)ctx->pstage[b]));
+        ctx->pstage[b] = nullptr;
+      }
+    ctx->pstage_bytes = 0;
+    for (int b = 0; b < 2; b++) {
+      ctx->pstage[b] = dalloc<char>(ctx, need, &e);
+      if (!ctx->pstage[b]) return fail(ctx, HRRT_ERR_NOMEM, "reconstruct staging");
+    }
+    ctx->pstage_bytes = need;
+  }
+  if (!ctx->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream");
+    for (int b = 0; b < 2; b++) {
+      CK(cudaEventCreateWithFlags(&ctx->ev_copied[b], cudaEventDisableTiming), "event");
+      CK(cudaEventCreateWithFlags(&ctx->ev_free[b], cudaEventDisableTiming), "event");
+    }
+  }
+  // the norm-zero mask is not known until every pair is prepared: the first
+  // iteration projects every FOV quad (a masked quad's prompts are zero, so
+  // its ratio is zero, and the back projector skips it by the mask)
+  std::fill(ctx->nzmask.begin(), ctx->nzmask.end(), (int16_t)1);
+  if (int rc = build_work_lists(ctx)) return rc;
+  if (int rc = hrrt_init_image(ctx, init_image_zyx)) return rc;
+  CK(cudaMemsetAsync(ctx->d_mask_accum, 0, sizeof(int) * (size_t)(g.nviews / 2) * ctx->dg.nquads, ctx->stream),
+     "reconstruct");
+  cudaEvent_t ta, tb;
+  CK(cudaEventCreate(&ta), "event");
+  CK(cudaEventCreate(&tb), "event");
+  auto bail = [&](int rc) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamSynchronize(ctx->stream);
+    cudaEventDestroy(ta);
+    cudaEventDestroy(tb);
+    return rc;
+  };
+  cudaEventRecord(ta, ctx->stream);
+  for (int b = 0; b < 2; b++) CK(cudaEventRecord(ctx->ev_free[b], ctx->stream), "reconstruct");
+  const int S = g.sp.subsets;
+  for (int k = 0; k < S; k++) {
+    const int s = g.order[k], b = k & 1;
+    int16_t *sp = reinterpret_cast<int16_t *>(ctx->pstage[b]);
+    float *stg[4] = {nullptr, nullptr, nullptr, nullptr};
+    e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_free[b], 0);
+    for (int j = 0; j < ctx->npairs && e == cudaSuccess; j++) {
+      const int v = g.vieworder[(size_t)s * g.sviews + j];
+      for (int h = 0; h < 2 && e == cudaSuccess; h++) {
+        const size_t view = v + h * (V / 2), doff = j * pair_elems + h * P * N;
+        e = cudaMemcpy2DAsync(sp + doff, N * sizeof(int16_t), prompts + view * N, V * N * sizeof(int16_t),
+                              N * sizeof(int16_t), P, cudaMemcpyHostToDevice, ctx->copy_stream);
+        for (int i = 0; i < 4 && e == cudaSuccess; i++) {
+          if (!srcs[i]) continue;
+          stg[i] = reinterpret_cast<float *>(ctx->pstage[b] + set_elems * sizeof(int16_t) +
+                                             (size_t)i * set_elems * sizeof(float));
+          e = cudaMemcpy2DAsync(stg[i] + doff, N * sizeof(float), srcs[i] + view * N, V * N * sizeof(float),
+                                N * sizeof(float), P, cudaMemcpyHostToDevice, ctx->copy_stream);
+        }
+      }
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_copied[b], ctx->copy_stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_copied[b], 0);
+    if (e == cudaSuccess) {
+      Launch L(ctx, "prep_kernel");
+      e = launch_prep_pairs(ctx->dg, g.nbins, sp, stg[0], stg[1], stg[2], stg[3], g.sp.npskip, g.sp.epsilon2,
+                            storage, ctx->q_prompts, ctx->q_add, ctx->q_mult, ctx->d_mask_accum,
+                            ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->stream);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_free[b], ctx->stream);
+    if (e == cudaSuccess) e = launch_finish_mask(ctx->dg, ctx->d_mask_accum, ctx->d_nzmask, ctx->stream);
+    if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "reconstruct upload"));
+    if (int rc = sens_subset(ctx, s)) return bail(rc);
+    if (int rc = run_subset(ctx, s)) return bail(rc);
+  }
+  {
+    Launch L(ctx, "post_iter_kernel");
+    e = launch_post_iteration(ctx->dg, ctx->d_image, ctx->d_partial, ctx->d_sum, ctx->stream);
+    if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "post_iteration"));
+  }
+  // the mask is complete: the remaining iterations skip masked quads
+  e = cudaMemcpyAsync(ctx->nzmask.data(), ctx->d_nzmask, ctx->nzmask.size() * sizeof(int16_t),
+                      cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "reconstruct"));
+  if (int rc = build_work_lists(ctx)) return bail(rc);
+  ctx->have_inputs = ctx->have_sens = ctx->have_image = true;
+  int done = S;
+  for (int it = 1; it < iterations; it++) {
+    for (int i = 0; i < S; i++, done++)
+      if (int rc = run_subset(ctx, g.order[i])) return bail(rc);
+    Launch L(ctx, "post_iter_kernel");
+    e = launch_post_iteration(ctx->dg, ctx->d_image, ctx->d_partial, ctx->d_sum, ctx->stream);
+    if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "post_iteration"));
+  }
+  double sum = 0.0;
+  e = launch_image_zyx(ctx->dg, ctx->d_image, ctx->d_tmp_img ? ctx->d_tmp_img : ctx->d_bc, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(image_zyx, ctx->d_tmp_img ? ctx->d_tmp_img : ctx->d_bc,
+                        sizeof(float) * (size_t)g.nz * g.ny * g.nx, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&sum, ctx->d_sum, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(tb, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "reconstruct"));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ta, tb);
+  cudaEventDestroy(ta);
+  cudaEventDestroy(tb);
+  if (int rc = device_status(ctx)) return rc;
+  if (stats) {
+    stats->sum_image = sum;
+    stats->subset_iterations = done;
+    stats->ms_total = ms;
+  }
+  return HRRT_OK;
+}
+
 int hrrt_get_image(hrrt_ctx *ctx, float *image_zyx) {
   if (!ctx || !image_zyx) return HRRT_ERR_ARG;
   const Geometry &g = ctx->geo;
-  std::vector<float> h((size_t)ctx->vol);
-  CK(cudaMemcpyAsync(h.data(), ctx->d_image, h.size() * 4, cudaMemcpyDeviceToHost, ctx->stream), "get_image");
+  // SaveImage (drv:4020-4043): tmpimage[z][y][x] = image[x][y][z] on FOV
+  // columns, transposed on the device
+  cudaError_t e = cudaSuccess;
+  if (!ctx->d_tmp_img) ctx->d_tmp_img = dalloc<float>(ctx, ctx->vol, &e);
+  if (!ctx->d_tmp_img) return fail(ctx, HRRT_ERR_NOMEM, "scratch");
+  CK(launch_image_zyx(ctx->dg, ctx->d_image, ctx->d_tmp_img, ctx->stream), "get_image");
+  CK(cudaMemcpyAsync(image_zyx, ctx->d_tmp_img, sizeof(float) * (size_t)g.nz * g.ny * g.nx, cudaMemcpyDeviceToHost,
+                     ctx->stream),
+     "get_image");
   CK(cudaStreamSynchronize(ctx->stream), "get_image");
-  // SaveImage (drv:4020-4043): tmpimage[z][y][x] = image[x][y][z] on FOV columns
-  std::memset(image_zyx, 0, sizeof(float) * (size_t)g.nz * g.ny * g.nx);
-  for (int x = 0; x < g.nx; x++)
-    for (int y = g.cyl0[x]; y < g.cyl1[x]; y++)
-      for (int z = 0; z < g.nz; z++)
-        image_zyx[((size_t)z * g.ny + y) * g.nx + x] = h[((size_t)x * g.ny + y) * g.zp + z];
   return HRRT_OK;
 }
 

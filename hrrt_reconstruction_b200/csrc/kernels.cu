@@ -243,7 +243,7 @@ constexpr int kBarEmpty = 3;  // + slot: sampled row consumed (consumers arrive,
 constexpr int kBarProd = 5;   // producers only: corner slot read by every producer
 
 template <int MODE, typename PT, typename AT>
-__global__ void __launch_bounds__(1024, 1) fp_kernel(DevGeom g, const float *__restrict__ image,
+__global__ void __launch_bounds__(kFpMaxWarps * 32, 1) fp_kernel(DevGeom g, const float *__restrict__ image,
                                                      const QuadWork *__restrict__ work,
                                                      const PT *__restrict__ prompts, const AT *__restrict__ add,
                                                      float4 *__restrict__ out, long long out_pair_stride,
@@ -948,15 +948,20 @@ __global__ void prep_kernel(DevGeom g, int nbins, const int16_t *__restrict__ pr
                             const float *__restrict__ randoms, const float *__restrict__ norm,
                             const float *__restrict__ atten, const float *__restrict__ scatter, int npskip,
                             float eps2, PT *__restrict__ qp, AT *__restrict__ qadd, AT *__restrict__ qmult,
-                            int *__restrict__ mask_accum, int planes_per_thread, int plane0, int nplanes) {
-  // the inputs hold planes [plane0, plane0 + nplanes) of the flat-file arrays
+                            int *__restrict__ mask_accum, int planes_per_thread, int plane0, int nplanes,
+                            const int *__restrict__ pair_views, long long s_plane, long long s_half,
+                            long long s_slot) {
+  // Input element of plane gp, lane l: base + (gp - plane0)*s_plane + h*s_half
+  // + bin.  Flat-file chunk (pair_views null): pair = blockIdx.z, base =
+  // pair*nbins, planes [plane0, plane0 + nplanes).  Pair-major staging: pair =
+  // pair_views[blockIdx.z], base = blockIdx.z*s_slot, all planes.
   const int x = blockIdx.x * blockDim.x + threadIdx.x;  // quad
-  const int vi = blockIdx.z;                            // pair
+  const int vi = pair_views ? pair_views[blockIdx.z] : (int)blockIdx.z;
+  const long long base = pair_views ? (long long)blockIdx.z * s_slot : (long long)vi * nbins;
   if (x >= g.nquads) return;
   const int gp0 = plane0 + blockIdx.y * planes_per_thread;
   const int gp1 = min(gp0 + planes_per_thread, plane0 + nplanes);
-  const int V = g.nviews, half = V / 2;
-  int views[4] = {vi, vi, vi + half, vi + half};
+  const int hl[4] = {0, 0, 1, 1};
   int bins[4] = {x, nbins - x, x, nbins - x};
   bool ok[4];
   for (int l = 0; l < 4; l++) ok[l] = (bins[l] >= 0 && bins[l] < nbins && x > 0);
@@ -970,7 +975,7 @@ __global__ void prep_kernel(DevGeom g, int nbins, const int16_t *__restrict__ pr
     for (int l = 0; l < 4; l++) {
       pv[l] = av[l] = mv[l] = 0.f;
       if (!ok[l]) continue;
-      const size_t i = ((size_t)(gp - plane0) * V + views[l]) * nbins + bins[l];
+      const size_t i = (size_t)(base + (long long)(gp - plane0) * s_plane + hl[l] * s_half + bins[l]);
       const float nz = norm ? (kill ? 0.f : __ldg(norm + i)) : 1.0f;
       const float araw = atten ? __ldg(atten + i) : 1.0f;
       const float ac = (araw < 1.0f) ? 1.0f : araw;
@@ -1142,8 +1147,8 @@ cudaError_t launch_fp_t(const DevGeom &g, const float *image, const QuadWork *wo
   // consumer warps: one task per thread; producer warps: enough to keep the
   // sampled rows ahead of the consumers (a row is ~2*zp bilinear quads)
   const int cwarps = (g.nfptasks + 31) / 32;
-  const int pwarps = min(6, max(2, 32 - cwarps));
-  if (cwarps + pwarps > 32) return cudaErrorInvalidConfiguration;
+  const int pwarps = min(6, max(2, kFpMaxWarps - cwarps));
+  if (cwarps + pwarps > kFpMaxWarps) return cudaErrorInvalidConfiguration;
   const int threads = (cwarps + pwarps) * 32;
   const int ZS = g.zp + kFpZPad;
   const size_t smem = (size_t)(2 * 8 * 2 + 2) * 2 * g.zp * sizeof(float) + (size_t)5 * ZS * sizeof(float4);
@@ -1256,14 +1261,50 @@ cudaError_t launch_prep(const DevGeom &g, int nbins, const int16_t *prompts, con
                         cudaStream_t st) {
   const int ppt = 16;
   dim3 grid((g.nquads + 127) / 128, (nplanes + ppt - 1) / ppt, g.nviews / 2);
+  const long long sp = (long long)g.nviews * nbins, sh = (long long)(g.nviews / 2) * nbins;
   if (storage == 0)
     prep_kernel<int16_t, float><<<grid, 128, 0, st>>>(g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2,
                                                       (int16_t *)q_prompts, (float *)q_add, (float *)q_mult,
-                                                      quad_mask_accum, ppt, plane0, nplanes);
+                                                      quad_mask_accum, ppt, plane0, nplanes, nullptr, sp, sh, 0);
   else
     prep_kernel<__half, __nv_bfloat16><<<grid, 128, 0, st>>>(
         g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (__half *)q_prompts, (__nv_bfloat16 *)q_add,
-        (__nv_bfloat16 *)q_mult, quad_mask_accum, ppt, plane0, nplanes);
+        (__nv_bfloat16 *)q_mult, quad_mask_accum, ppt, plane0, nplanes, nullptr, sp, sh, 0);
+  return cudaGetLastError();
+}
+
+// SaveImage's layout (drv:4020-4043): out[z][y][x] = image[x][y][z] on FOV
+// columns, planes < nz; zero elsewhere.  One thread per (z, y, x), x fastest.
+__global__ void image_zyx_kernel(DevGeom g, const float *__restrict__ image, float *__restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = (long long)g.nz * g.nx * g.nx;
+  if (t >= n) return;
+  const int x = (int)(t % g.nx), y = (int)((t / g.nx) % g.nx), z = (int)(t / ((long long)g.nx * g.nx));
+  const bool in = y >= g.cyl0[x] && y < g.cyl1[x];
+  out[t] = in ? __ldg(image + ((size_t)x * g.nx + y) * g.zp + z) : 0.f;
+}
+
+cudaError_t launch_image_zyx(const DevGeom &g, const float *image, float *out, cudaStream_t st) {
+  const long long n = (long long)g.nz * g.nx * g.nx;
+  image_zyx_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, image, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prep_pairs(const DevGeom &g, int nbins, const int16_t *prompts, const float *randoms,
+                              const float *norm, const float *atten, const float *scatter, int npskip, float eps2,
+                              int storage, void *q_prompts, void *q_add, void *q_mult, int *quad_mask_accum,
+                              const int *pair_views, int npairs, cudaStream_t st) {
+  const int ppt = 16;
+  dim3 grid((g.nquads + 127) / 128, (g.segmentsize + ppt - 1) / ppt, npairs);
+  const long long P = g.segmentsize, sp = nbins, sh = P * nbins, ss = 2 * P * nbins;
+  if (storage == 0)
+    prep_kernel<int16_t, float><<<grid, 128, 0, st>>>(g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2,
+                                                      (int16_t *)q_prompts, (float *)q_add, (float *)q_mult,
+                                                      quad_mask_accum, ppt, 0, g.segmentsize, pair_views, sp, sh, ss);
+  else
+    prep_kernel<__half, __nv_bfloat16><<<grid, 128, 0, st>>>(
+        g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (__half *)q_prompts, (__nv_bfloat16 *)q_add,
+        (__nv_bfloat16 *)q_mult, quad_mask_accum, ppt, 0, g.segmentsize, pair_views, sp, sh, ss);
   return cudaGetLastError();
 }
 

@@ -23,7 +23,14 @@
 
 namespace hrrt {
 
-constexpr int kFpPlanes = 9;    // planes per forward-projection task (odd: bank-conflict free)
+#ifndef HRRT_FP_PLANES
+#define HRRT_FP_PLANES 9
+#endif
+#ifndef HRRT_FP_MAX_WARPS
+#define HRRT_FP_MAX_WARPS 32
+#endif
+constexpr int kFpPlanes = HRRT_FP_PLANES;     // planes per forward-projection task (odd: bank-conflict free)
+constexpr int kFpMaxWarps = HRRT_FP_MAX_WARPS;  // warps per forward-projection CTA (consumers + producers)
 constexpr int kFpZPad = 16;     // zeroed entries after each sampled row
 constexpr int kFpEndPlanes = 4; // planes per end-plane task (they cost ~2x a middle plane)
 constexpr int kBpZ = 8;         // z per back-projection task
@@ -110,7 +117,15 @@ cudaError_t launch_prep(const DevGeom &g, int nbins, const int16_t *prompts, con
                         const float *atten, const float *scatter, int npskip, float eps2, int storage, void *q_prompts,
                         void *q_add, void *q_mult, int *quad_mask_accum, int plane0, int nplanes,
                         cudaStream_t st);
+// the same from pair-major staging: for each of `npairs` slots, the rows of
+// view pair_views[slot] and its partner, [2 views][segmentsize][nbins]
+cudaError_t launch_prep_pairs(const DevGeom &g, int nbins, const int16_t *prompts, const float *randoms,
+                              const float *norm, const float *atten, const float *scatter, int npskip, float eps2,
+                              int storage, void *q_prompts, void *q_add, void *q_mult, int *quad_mask_accum,
+                              const int *pair_views, int npairs, cudaStream_t st);
 cudaError_t launch_finish_mask(const DevGeom &g, const int *accum, int16_t *nzmask, cudaStream_t st);
+// [z][y][x] image of SaveImage (FOV columns, planes < nz) from [x][y][zp]
+cudaError_t launch_image_zyx(const DevGeom &g, const float *image, float *out, cudaStream_t st);
 cudaError_t launch_init_image(const DevGeom &g, float *image, cudaStream_t st);
 cudaError_t launch_post_iteration(const DevGeom &g, float *image, double *partial, double *sum, cudaStream_t st);
 int post_iteration_blocks(const DevGeom &g);

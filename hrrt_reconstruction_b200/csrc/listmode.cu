@@ -51,6 +51,8 @@ constexpr int kTileWords = kThreads * kSub;    // 4096
 constexpr long long kPacketWords = 2LL << 20;  // 1 Mi 64-bit events
 static_assert(kPacketWords % kTileWords == 0, "tiles must not straddle packets");
 constexpr int kSinoPlane = 256 * 288;
+// streams of at least this many words take the partitioned histogram path
+constexpr long long kPartitionMinWords = 1LL << 24;
 // EWTYPES (geometry_info.h:76) packed two bits per entry: index =
 // (ew1 >> 30) << 2 | (ew2 >> 30); 0 prompt, 1 delayed, 2 tag, 3 out of sync
 constexpr uint32_t kEwTypes = (3u << 0) | (3u << 2) | (1u << 4) | (0u << 6) | (3u << 8) | (3u << 10) | (2u << 12) |
@@ -254,36 +256,22 @@ __device__ __forceinline__ long long rebin(const LmDev &g, const float *zp, cons
   return (long long)(plane + g.segzoff[segnum]) * kSinoPlane + s.nsino;
 }
 
-template <bool kHist>
-__global__ void __launch_bounds__(kThreads) lm_hist_kernel(
-    LmDev g, const uint32_t *__restrict__ words, long long n, const uint8_t *__restrict__ tile_entry,
-    const unsigned int *__restrict__ tile_tagoff, const unsigned long long *__restrict__ packet_tagoff,
-    int tiles_per_packet, long long limit, int mode, int flags, long long tag_cap, longlong2 *__restrict__ tags,
-    uint32_t *__restrict__ sino, uint32_t *__restrict__ dly, unsigned long long *__restrict__ stats) {
-  __shared__ __align__(16) uint32_t w[kTileWords + 4];
-  __shared__ Sub wt[32];
-  __shared__ float zp[104], zp2[104];
-  __shared__ unsigned long long st[kStCount];
-  if (threadIdx.x < 104) {
-    zp[threadIdx.x] = g.zpos[threadIdx.x];
-    zp2[threadIdx.x] = g.zpos2[threadIdx.x];
-  }
-  if (threadIdx.x < kStCount) st[threadIdx.x] = 0;
-  const long long tile = blockIdx.x;
-  const long long t0 = tile * kTileWords;
-  const int pend = stage_tile(words, n, t0, w);
-  const int s = threadIdx.x * kSub;
-  const Sub v = sub_summary(w, s, pend);
-  Sub incl, excl;
-  block_scan(v, incl, excl, wt);
-  const uint32_t te = tile_entry[tile];
-  const int e = (int)((excl.map >> te) & 1);
-  unsigned long long tagpos = packet_tagoff[tile / tiles_per_packet] + tile_tagoff[tile] + (te ? excl.c1 : excl.c0);
+// Partitions of the histogram for the L2-resident pass: 32 Mi bins (64 MB of
+// 16-bit bins) each, prompts-side partitions first.
+constexpr int kPartShift = 25;
+constexpr int kMaxParts = 64;
 
+// Walk one thread's words from its entry offset: count the statistics (kStats),
+// record time tags in stream order (when tags != null), and hand every
+// histogrammed event to emit(address, sinogram 0/1, subtract).
+template <bool kStats, typename Emit>
+__device__ __forceinline__ void walk_events(const LmDev &g, const float *zp, const float *zp2, const uint32_t *w,
+                                            int s, int e, int pend, long long t0, long long limit, int mode,
+                                            int flags, uint32_t (&c)[kStCount], unsigned long long tagpos,
+                                            long long tag_cap, longlong2 *__restrict__ tags, Emit emit) {
   const bool doi = (flags & HRRT_LM_NO_DOI) == 0;
   const bool border = (flags & HRRT_LM_IGNORE_BORDER_CRYSTAL) != 0;
   const int xhigh = border ? 71 : 72;
-  uint32_t c[kStCount] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   int pos = s + e;
   while (pos < s + kSub) {
     if (pos + 1 >= pend) break;
@@ -291,7 +279,7 @@ __global__ void __launch_bounds__(kThreads) lm_hist_kernel(
     const uint32_t ew1 = w[pos], ew2 = w[pos + 1];
     const int type = ewtype(ew1, ew2);
     if (type == 3) {
-      if (gp < limit) c[kStResync]++;
+      if (kStats && gp < limit) c[kStResync]++;
       pos += 1;
       continue;
     }
@@ -300,22 +288,24 @@ __global__ void __launch_bounds__(kThreads) lm_hist_kernel(
       const uint32_t tag = (ew1 & 0xffff) | ((ew2 & 0xffff) << 16);
       const bool timetag = (tag & 0xE0000000u) == 0x80000000u;
       if (timetag) {
-        if (tag_cap > 0 && (long long)tagpos < tag_cap) tags[tagpos] = make_longlong2(gp, (long long)tag);
+        if (tags && (long long)tagpos < tag_cap) tags[tagpos] = make_longlong2(gp, (long long)tag);
         tagpos++;
       }
       if (gp >= limit) continue;
-      c[kStTags]++;
-      if (timetag) c[kStTimetags]++;
+      if (kStats) {
+        c[kStTags]++;
+        if (timetag) c[kStTimetags]++;
+      }
       if (tag & 0x80000000u) continue;
       // a tag value with bit 31 clear reads as an event word
       const bool prompt = (tag & 0x40000000u) != 0;
-      c[prompt ? kStPrompts : kStDelayed]++;
+      if (kStats) c[prompt ? kStPrompts : kStDelayed]++;
       const long long addr = tag & 0x3fffffff;
-      if (kHist && addr < g.sino_size) {
+      if (addr < g.sino_size) {
         if (mode == HRRT_LM_PROMPTS_AND_DELAYED)
-          bump16(prompt ? sino : dly, addr, false);
+          emit(addr, prompt ? 0 : 1, false);
         else
-          bump16(sino, addr, !prompt);
+          emit(addr, 0, !prompt);
       }
       continue;
     }
@@ -325,42 +315,141 @@ __global__ void __launch_bounds__(kThreads) lm_hist_kernel(
     const int ax = ew1 & 0xff, ay = (ew1 >> 8) & 0xff, bx = ew2 & 0xff, by = (ew2 >> 8) & 0xff;
     const int doia = doi ? (int)((ew1 >> 22) & 7) : 1, doib = doi ? (int)((ew2 >> 22) & 7) : 1;
     if (mpe < 1 || mpe > 20 || ax >= 72 || ay >= 104 || bx >= 72 || by >= 104) {
-      c[kStInvalid]++;
+      if (kStats) c[kStInvalid]++;
       continue;
     }
     if (doia == 7 || doib == 7) {
-      c[kStDoi7]++;
+      if (kStats) c[kStDoi7]++;
       continue;
     }
     if (doia > 1 || doib > 1) {
-      c[kStDoiOther]++;
+      if (kStats) c[kStDoiOther]++;
       continue;
     }
     long long addr = -1;
     if (!(border && (ax * bx == 0 || ax == xhigh || bx == xhigh)) && !(mode == HRRT_LM_PROMPTS_ONLY && type != 0))
       addr = rebin(g, zp, zp2, mpe, doia, ax, ay, doib, bx, by);
     if (addr < 0) {
-      c[kStUnmapped]++;
+      if (kStats) c[kStUnmapped]++;
       continue;
     }
-    c[type == 0 ? kStPrompts : kStDelayed]++;
-    if (kHist) {
-      if (mode == HRRT_LM_PROMPTS_AND_DELAYED)
-        bump16(type == 0 ? sino : dly, addr, false);
-      else
-        bump16(sino, addr, type != 0);
+    if (kStats) c[type == 0 ? kStPrompts : kStDelayed]++;
+    if (mode == HRRT_LM_PROMPTS_AND_DELAYED)
+      emit(addr, type == 0 ? 0 : 1, false);
+    else
+      emit(addr, 0, type != 0);
+  }
+}
+
+// kMode 0: time tags only; 1: histogram directly (atomics into the 16-bit
+// bins); 2: count events per histogram partition; 3: scatter packed event
+// records (address | sinogram << 29 | subtract << 30) partition-major.
+// Statistics are counted by modes 1 and 2.
+template <int kMode>
+__global__ void __launch_bounds__(kThreads) lm_hist_kernel(
+    LmDev g, const uint32_t *__restrict__ words, long long n, const uint8_t *__restrict__ tile_entry,
+    const unsigned int *__restrict__ tile_tagoff, const unsigned long long *__restrict__ packet_tagoff,
+    int tiles_per_packet, long long limit, int mode, int flags, long long tag_cap, longlong2 *__restrict__ tags,
+    uint32_t *__restrict__ sino, uint32_t *__restrict__ dly, unsigned long long *__restrict__ stats,
+    unsigned long long *__restrict__ part_cursor, uint32_t *__restrict__ records, int parts_per_sino) {
+  __shared__ __align__(16) uint32_t w[kTileWords + 4];
+  __shared__ Sub wt[32];
+  __shared__ float zp[104], zp2[104];
+  __shared__ unsigned long long st[kStCount];
+  __shared__ unsigned int pcount[kMaxParts];
+  __shared__ unsigned long long pbase[kMaxParts];
+  if (threadIdx.x < 104) {
+    zp[threadIdx.x] = g.zpos[threadIdx.x];
+    zp2[threadIdx.x] = g.zpos2[threadIdx.x];
+  }
+  if (threadIdx.x < kStCount) st[threadIdx.x] = 0;
+  if (threadIdx.x < kMaxParts) pcount[threadIdx.x] = 0;
+  const long long tile = blockIdx.x;
+  const long long t0 = tile * kTileWords;
+  const int pend = stage_tile(words, n, t0, w);
+  const int s = threadIdx.x * kSub;
+  const Sub v = sub_summary(w, s, pend);
+  Sub incl, excl;
+  block_scan(v, incl, excl, wt);
+  const uint32_t te = tile_entry[tile];
+  const int e = (int)((excl.map >> te) & 1);
+  const unsigned long long tagpos =
+      packet_tagoff[tile / tiles_per_packet] + tile_tagoff[tile] + (te ? excl.c1 : excl.c0);
+  longlong2 *tg = tag_cap > 0 ? tags : nullptr;
+  uint32_t c[kStCount] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  auto part_of = [&](long long addr, int sel) { return sel * parts_per_sino + (int)(addr >> kPartShift); };
+  if (kMode == 0) {
+    walk_events<false>(g, zp, zp2, w, s, e, pend, t0, limit, mode, flags, c, tagpos, tag_cap, tg,
+                       [](long long, int, bool) {});
+  } else if (kMode == 1) {
+    walk_events<true>(g, zp, zp2, w, s, e, pend, t0, limit, mode, flags, c, tagpos, tag_cap, tg,
+                      [&](long long addr, int sel, bool minus) { bump16(sel ? dly : sino, addr, minus); });
+  } else if (kMode == 2) {
+    walk_events<true>(g, zp, zp2, w, s, e, pend, t0, limit, mode, flags, c, tagpos, tag_cap, tg,
+                      [&](long long addr, int sel, bool) { atomicAdd(&pcount[part_of(addr, sel)], 1u); });
+    __syncthreads();
+    if (threadIdx.x < 2 * parts_per_sino && pcount[threadIdx.x])
+      atomicAdd(&part_cursor[threadIdx.x], (unsigned long long)pcount[threadIdx.x]);
+  } else {
+    walk_events<false>(g, zp, zp2, w, s, e, pend, t0, limit, mode, flags, c, tagpos, 0, nullptr,
+                       [&](long long addr, int sel, bool) { atomicAdd(&pcount[part_of(addr, sel)], 1u); });
+    __syncthreads();
+    if (threadIdx.x < 2 * parts_per_sino) {
+      const unsigned int k = pcount[threadIdx.x];
+      pbase[threadIdx.x] = k ? atomicAdd(&part_cursor[threadIdx.x], (unsigned long long)k) : 0ull;
+      pcount[threadIdx.x] = 0;
     }
+    __syncthreads();
+    walk_events<false>(g, zp, zp2, w, s, e, pend, t0, limit, mode, flags, c, tagpos, 0, nullptr,
+                       [&](long long addr, int sel, bool minus) {
+                         const int p = part_of(addr, sel);
+                         const unsigned int k = atomicAdd(&pcount[p], 1u);
+                         records[pbase[p] + k] = (uint32_t)addr | ((uint32_t)sel << 29) | ((uint32_t)minus << 30);
+                       });
   }
-  // block reduction of the counters
+  if (kMode == 1 || kMode == 2) {
+    // block reduction of the counters
 #pragma unroll
-  for (int k = 0; k < kStCount; k++) {
-    uint32_t x = c[k];
+    for (int k = 0; k < kStCount; k++) {
+      uint32_t x = c[k];
 #pragma unroll
-    for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
-    if ((threadIdx.x & 31) == 0 && x) atomicAdd(&st[k], (unsigned long long)x);
+      for (int d = 16; d > 0; d >>= 1) x += __shfl_down_sync(0xffffffffu, x, d);
+      if ((threadIdx.x & 31) == 0 && x) atomicAdd(&st[k], (unsigned long long)x);
+    }
+    __syncthreads();
+    if (threadIdx.x < kStCount && st[threadIdx.x]) atomicAdd(&stats[threadIdx.x], st[threadIdx.x]);
   }
-  __syncthreads();
-  if (threadIdx.x < kStCount && st[threadIdx.x]) atomicAdd(&stats[threadIdx.x], st[threadIdx.x]);
+}
+
+// Partition counts -> start offsets (exclusive scan; one thread, <= 64 entries).
+__global__ void lm_part_scan_kernel(unsigned long long *__restrict__ cursor, int nparts,
+                                    unsigned long long *__restrict__ starts) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  unsigned long long run = 0;
+  for (int p = 0; p < nparts; p++) {
+    const unsigned long long k = cursor[p];
+    starts[p] = run;
+    cursor[p] = run;
+    run += k;
+  }
+  starts[nparts] = run;
+}
+
+// The records in partition order, contiguous chunks per block: the blocks
+// resident at any moment touch one or two 64 MB partitions, which stay in L2.
+constexpr int kRecPerThread = 16;
+__global__ void __launch_bounds__(kThreads) lm_part_hist_kernel(const uint32_t *__restrict__ records,
+                                                                const unsigned long long *__restrict__ total,
+                                                                uint32_t *__restrict__ sino, uint32_t *__restrict__ dly) {
+  const unsigned long long n = *total;
+  const unsigned long long b0 = (unsigned long long)blockIdx.x * kThreads * kRecPerThread;
+#pragma unroll 4
+  for (int k = 0; k < kRecPerThread; k++) {
+    const unsigned long long i = b0 + (unsigned long long)k * kThreads + threadIdx.x;
+    if (i >= n) break;
+    const uint32_t r = __ldg(records + i);
+    bump16(((r >> 29) & 1) ? dly : sino, r & 0x1FFFFFFFu, ((r >> 30) & 1) != 0);
+  }
 }
 
 }  // namespace
@@ -383,6 +472,8 @@ struct hrrt_lm {
   uint16_t *h_sino_dev = nullptr;   // host-API sinograms (prompts, delayed)
   longlong2 *tagbuf = nullptr;      // ordered time tags (position, value)
   long long tag_cap = 0;
+  uint32_t *records = nullptr;      // partitioned path: packed event records
+  long long rec_cap = 0;
   // clock carried across frames (process_tagword's statics)
   long long current_time = -1, current_time_msec = -1, prev_time = 0;
   int clock_reset = 0;
@@ -393,6 +484,7 @@ struct hrrt_lm {
     for (void *p : allocs) cudaFree(p);
     if (scratch) cudaFree(scratch);
     if (tagbuf) cudaFree(tagbuf);
+    if (records) cudaFree(records);
     if (h_words_dev) cudaFree(h_words_dev);
     if (h_sino_dev) cudaFree(h_sino_dev);
     if (stream) cudaStreamDestroy(stream);
@@ -527,7 +619,7 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
   // the scan has counted them.
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t b_sum = al(8 * ntiles), b_ent = al(ntiles), b_off = al(4 * ntiles), b_pk = al(8 * (npackets + 1)),
-               b_st = al(8 * (kStCount + 1));
+               b_st = al(8 * (kStCount + 1 + 2 * kMaxParts + 1));
   const size_t need = b_sum + b_ent + b_off + b_pk + b_st;
   if (h->scratch_bytes < need) {
     if (h->scratch) cudaFree(h->scratch);
@@ -574,20 +666,60 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
   }
   longlong2 *tags = h->tagbuf;
   const long long tag_cap = h->tag_cap;
-  // pass 1: ordered time tags (and, without a frame length, the histogram)
-  const bool one_pass = duration <= 0;
-  if (e == cudaSuccess) {
-    const long long lim = one_pass ? nwords : -1;
-    if (one_pass)
-      lm_hist_kernel<true><<<(unsigned)ntiles, kThreads, 0, st>>>(
-          h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim, mode, flags, tag_cap, tags,
-          (uint32_t *)d_sino, (uint32_t *)d_delayed, stats);
-    else
-      lm_hist_kernel<false><<<(unsigned)ntiles, kThreads, 0, st>>>(
-          h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim, mode, flags, tag_cap, tags,
-          (uint32_t *)d_sino, (uint32_t *)d_delayed, stats);
-    e = cudaGetLastError();
+  // Histogram path: directly (atomics into the full sinograms) for short
+  // streams, partitioned (events scattered by 64 MB partition, then
+  // histogrammed partition by partition in L2) for long ones.
+  const int pps = (int)((h->dev.sino_size + (1LL << kPartShift) - 1) >> kPartShift);
+  bool partitioned = nwords >= kPartitionMinWords;
+  if (flags & HRRT_LM_FORCE_DIRECT) partitioned = false;
+  if (flags & HRRT_LM_FORCE_PARTITIONED) partitioned = true;
+  if (2 * pps > kMaxParts) partitioned = false;
+  unsigned long long *cursor = stats + kStCount + 1;          // [kMaxParts]
+  unsigned long long *starts = cursor + kMaxParts;            // [kMaxParts + 1]
+  if (partitioned && e == cudaSuccess) {
+    const long long cap = nwords / 2 + 1;
+    if (cap > h->rec_cap) {
+      if (h->records) cudaFree(h->records);
+      h->records = nullptr;
+      h->rec_cap = 0;
+      e = cudaMalloc(&h->records, sizeof(uint32_t) * (size_t)cap);
+      if (e != cudaSuccess) {
+        h->records = nullptr;
+        partitioned = false;  // not enough memory: fall back to the direct path
+        e = cudaSuccess;
+        cudaGetLastError();
+      } else {
+        h->rec_cap = cap;
+      }
+    }
   }
+  if (partitioned && e == cudaSuccess) e = cudaMemsetAsync(cursor, 0, 8 * kMaxParts, st);
+  auto launch = [&](int kmode, long long lim, long long tcap) {
+    const unsigned nb = (unsigned)ntiles;
+    uint32_t *sn = (uint32_t *)d_sino, *dl = (uint32_t *)d_delayed;
+    switch (kmode) {
+      case 0:
+        lm_hist_kernel<0><<<nb, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
+                                                   mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
+        break;
+      case 1:
+        lm_hist_kernel<1><<<nb, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
+                                                   mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
+        break;
+      case 2:
+        lm_hist_kernel<2><<<nb, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
+                                                   mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
+        break;
+      default:
+        lm_hist_kernel<3><<<nb, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
+                                                   mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
+    }
+    return cudaGetLastError();
+  };
+  // pass 1: the ordered time tags (and, without a frame length, the counts
+  // or the histogram itself)
+  const bool one_pass = duration <= 0;
+  if (e == cudaSuccess) e = launch(one_pass ? (partitioned ? 2 : 1) : 0, one_pass ? nwords : -1, tag_cap);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   std::vector<longlong2> htags;
   if (e == cudaSuccess && ntags > 0) {
@@ -603,11 +735,16 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
   const long long end_tag = replay_clock(h, htags.data(), (long long)ntags, duration, flags, &frame_start);
   long long limit = nwords;
   if (end_tag >= 0) limit = htags[end_tag].x;
-  if (!one_pass) {
-    lm_hist_kernel<true><<<(unsigned)ntiles, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk,
-                                                                tpp, limit, mode, flags, 0, tags, (uint32_t *)d_sino,
-                                                                (uint32_t *)d_delayed, stats);
-    e = cudaGetLastError();
+  if (!one_pass) e = launch(partitioned ? 2 : 1, limit, 0);
+  if (partitioned && e == cudaSuccess) {
+    lm_part_scan_kernel<<<1, 32, 0, st>>>(cursor, 2 * pps, starts);
+    e = launch(3, limit, 0);
+    if (e == cudaSuccess) {
+      const long long blocks = (nwords / 2 + 1 + (long long)kThreads * kRecPerThread - 1) / ((long long)kThreads * kRecPerThread);
+      lm_part_hist_kernel<<<(unsigned)blocks, kThreads, 0, st>>>(h->records, starts + 2 * pps, (uint32_t *)d_sino,
+                                                                 (uint32_t *)d_delayed);
+      e = cudaGetLastError();
+    }
   }
   unsigned long long hs[kStCount] = {};
   cudaEventRecord(ev1, st);

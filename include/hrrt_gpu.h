@@ -153,6 +153,17 @@ int hrrt_set_norm_zero_mask(hrrt_ctx *ctx, const int16_t *mask);
  * masked quads) keep the caller's values. */
 int hrrt_fp_pair(hrrt_ctx *ctx, const float *image_xyz, int view, float *prj);
 
+/* The reconstruction of main (drv:4487-4560: PrepareNormfac, CalculateNormfac,
+ * PrepareOsem3dFiles, Init_Image, CalculateOsem3d, SaveImage) in one call,
+ * pipelined: the inputs stream in subset order (each view pair's rows as 2D
+ * copies; pinned host memory lets them overlap) while the first iteration's
+ * sensitivity images and subsets run behind them.  Same arguments and result
+ * as hrrt_upload_inputs + hrrt_sensitivity + hrrt_init_image + hrrt_osem +
+ * hrrt_get_image; image_zyx receives SaveImage's [z][y][x] image. */
+int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms, const float *norm,
+                     const float *atten, const float *scatter, int storage, const float *init_image_zyx,
+                     int iterations, float *image_zyx, hrrt_stats *stats);
+
 /* Replaces the forward projection of Output_CorrectedScan
  * (hrrt_osem3d_span3.cpp:3624-3723, the -I 0 -h mode): forward-projects
  * image_xyz for every view pair into a full flat-file sinogram (zeros where the
@@ -227,6 +238,11 @@ int hrrt_reset_kernel_stats(hrrt_ctx *ctx);
 #define HRRT_LM_IGNORE_BORDER_CRYSTAL 1
 #define HRRT_LM_NO_DOI 2
 #define HRRT_LM_TIME_FROM_COUNT 4
+/* implementation choice (same result): streams of 16 Mi words or more are
+ * histogrammed through 64 MB partitions that stay in L2, shorter ones with
+ * atomics straight into the sinograms; these flags force one or the other */
+#define HRRT_LM_FORCE_DIRECT 16
+#define HRRT_LM_FORCE_PARTITIONED 32
 
 typedef struct hrrt_lm_stats {
   long long words_used;  /* words consumed: through the tag that ended the frame, or all */

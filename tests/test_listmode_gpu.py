@@ -52,11 +52,14 @@ def random_stream(seed, nevents, tag_every=1000, p_resync=1e-4, p_bad=0.01, p_de
     return np.concatenate(chunks).astype(np.uint32)
 
 
-def compare(O, D, words, mode, duration=0, flags=0):
+FORCE_DIRECT, FORCE_PARTITIONED = 16, 32  # device path selection (same result)
+
+
+def compare(O, D, words, mode, duration=0, flags=0, path=0):
     O.reset_clock()
     D.reset_clock()
     so, do, sto = O.histogram(words, mode=mode, duration=duration, flags=flags)
-    sd, dd, std = D.histogram(words, mode=mode, duration=duration, flags=flags)
+    sd, dd, std = D.histogram(words, mode=mode, duration=duration, flags=flags | path)
     assert np.array_equal(so, sd), np.flatnonzero(so != sd)[:10]
     if mode == lm.PROMPTS_AND_DELAYED:
         assert np.array_equal(do, dd), np.flatnonzero(do != dd)[:10]
@@ -83,7 +86,8 @@ def test_known_answer_streams(pair):
         event_words(3, 35, 50, 35, 50, doia=3), event_words(3, 35, 50, 35, 50, doib=7), tag_words(0xA0000005),
         tag_words(0x40000000 | 12345), tag_words(777), good)]).astype(np.uint32)
     for mode in (lm.TRUES, lm.PROMPTS_AND_DELAYED, lm.PROMPTS_ONLY):
-        compare(O, D, w, mode)
+        for path in (FORCE_DIRECT, FORCE_PARTITIONED):
+            compare(O, D, w, mode, path=path)
 
 
 def test_wrap_and_trues(pair):
@@ -93,7 +97,8 @@ def test_wrap_and_trues(pair):
                            prompt=np.arange(n) % 3 != 0)
     w = interleave(ew1, ew2)
     for mode in (lm.TRUES, lm.PROMPTS_AND_DELAYED):
-        compare(O, D, w, mode)
+        for path in (FORCE_DIRECT, FORCE_PARTITIONED):
+            compare(O, D, w, mode, path=path)
 
 
 @pytest.mark.parametrize("seed", [1, 2])
@@ -102,10 +107,11 @@ def test_random_stream_packets(pair, seed):
     O, D = pair
     w = random_stream(seed, 2_700_000)
     assert w.size > 2 * lm.PACKET_WORDS
-    st = compare(O, D, w, lm.PROMPTS_AND_DELAYED)
+    st = compare(O, D, w, lm.PROMPTS_AND_DELAYED, path=FORCE_DIRECT)
     assert st["prompts"] > 0 and st["resyncs"] > 0 and st["invalid"] > 0 and st["doi7"] > 0
-    compare(O, D, w, lm.TRUES, flags=lm.IGNORE_BORDER_CRYSTAL)
-    compare(O, D, w, lm.PROMPTS_ONLY, flags=lm.NO_DOI)
+    compare(O, D, w, lm.PROMPTS_AND_DELAYED, path=FORCE_PARTITIONED)
+    compare(O, D, w, lm.TRUES, flags=lm.IGNORE_BORDER_CRYSTAL, path=FORCE_PARTITIONED)
+    compare(O, D, w, lm.PROMPTS_ONLY, flags=lm.NO_DOI, path=FORCE_PARTITIONED)
 
 
 def test_frames_follow_the_clock(pair):
@@ -116,12 +122,12 @@ def test_frames_follow_the_clock(pair):
     O.reset_clock()
     D.reset_clock()
     pos_o = pos_d = 0
-    for _ in range(3):
+    for k in range(3):
         so, do, sto = O.histogram(w[pos_o:], duration=1)
-        sd, dd, std = D.histogram(w[pos_d:], duration=1)
+        sd, dd, std = D.histogram(w[pos_d:], duration=1, flags=FORCE_PARTITIONED if k % 2 else FORCE_DIRECT)
         assert np.array_equal(so, sd) and np.array_equal(do, dd)
-        for k in STAT_KEYS:
-            assert sto[k] == std[k], (k, sto[k], std[k])
+        for key in STAT_KEYS:
+            assert sto[key] == std[key], (key, sto[key], std[key])
         assert sto["terminated"] == 1
         pos_o += sto["words_used"]
         pos_d += std["words_used"]
