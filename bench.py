@@ -321,10 +321,15 @@ def run_ours(args, ws, rank, local):
         "clocks": clk,
         "data_gen_s": gen_s,
     }
+    if args.storage == "f32" and args.compare_16:
+        out["storage16"] = run_storage16(args, torch, H, ctx, st, host, names, img, cs, dist, local, ws, ms)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     ctx.close()
-    del ctx
+    del ctx, host, st
+    _PINNED.clear()
+    if args.dyn_frames > 0:
+        out["dynamic"] = run_dynamic(args, torch, H, local, dist, ws)
     if args.lm_events > 0:
         out["listmode"] = run_listmode(args, torch, H, local, dist, ws, cpu=(rank == 0 and ws == 1 and
                                                                              not args.no_cpu_baseline))
@@ -332,6 +337,163 @@ def run_ours(args, ws, rank, local):
         print(json.dumps(out), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+def run_storage16(args, torch, H, ctx, st, host, names, img_f32, cs, dist, local, ws, ms_f32):
+    """The same study with the sinogram-shaped inputs stored in 16 bits (prompts
+    fp16, 1/(NA) and the additive term bf16; FP32 arithmetic): device-resident
+    subset-iterations/s over the same steps, and the rel-L2 of its image after
+    the e2e reconstruction against the f32-stored image."""
+    img16 = pinned_copy(torch, np.zeros_like(img_f32))
+    ctx.reconstruct(*(host.get(k) for k in names), storage=H.STORE_16, iterations=ITERATIONS, out=img16)
+    a = img16.astype(np.float64)
+    b = img_f32.astype(np.float64)
+    rel = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+    ctx.init_image()
+    ctx.osem_subsets(0, args.warmup)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    barrier(dist, local)
+    torch.cuda.synchronize()
+    ev[0].record(cs)
+    ctx.osem_subsets(args.warmup, args.steps)
+    ev[1].record(cs)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(dist, ev[0].elapsed_time(ev[1]), local)
+    return {"value": ws * args.steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / args.steps,
+            "speedup_vs_f32": ms_f32 / ms, "rel_l2_vs_f32_image": rel,
+            "rel_l2_note": f"image after {ITERATIONS} iterations x {SUBSETS} subsets (hrrt_reconstruct), "
+                           "16-bit-stored vs f32-stored inputs, same prompts",
+            "storage": "prompts fp16, 1/(NA) and additive term bf16; FP32 accumulation, FP64 image sum"}
+
+
+# Dynamic study: 24 span-9 frames of the config-0 phantom, sphere activity
+# varying with time, counts log-uniform in [2e6, 2e8], 1-4 iterations each
+# (seeded), 16-bit-stored inputs, one batch (hrrt_batch_*).
+DYN = dict(seed=4, counts=(2e6, 2e8), iterations=(1, 4), randoms_frac=0.20)
+
+
+def dynamic_frames(nframes, seed):
+    """Per frame: total counts, iterations, sphere activities (6 curves: uptake
+    with time constant tau_k, washout over the study)."""
+    rng = np.random.default_rng(seed)
+    lo, hi = DYN["counts"]
+    counts = np.exp(rng.uniform(np.log(lo), np.log(hi), nframes))
+    iters = rng.integers(DYN["iterations"][0], DYN["iterations"][1] + 1, nframes)
+    t = (np.arange(nframes) + 0.5) / nframes
+    tau = np.linspace(0.05, 0.5, 6)
+    act = 1.0 + 5.0 * (1.0 - np.exp(-t[:, None] / tau[None, :])) * np.exp(-t[:, None] / 1.5)
+    return counts, iters, act
+
+
+def run_dynamic(args, torch, H, local, dist, ws):
+    from hrrt_reconstruction_b200 import phantom
+    dev = f"cuda:{local}"
+    nf = args.dyn_frames
+    t0 = time.time()
+    geom = H.hrrt_geometry(nrings=104, nelements=256, nangles=288, ring_radius=234.5, plane_sep=1.21875,
+                           binsize=1.21875, span=9, maxdel=67, subsets=SUBSETS)
+    ctx = H.Context(geom, device=local)
+    counts, iters, act = dynamic_frames(nf, DYN["seed"] + 1000 * int(os.environ.get("RANK", "0")))
+    # the frame images are linear in the sphere activities: forward-project
+    # the cylinder and the six sphere indicators once
+    base = phantom.phantom(ctx, seed=0, sphere_activity=1.0)
+    parts = [ctx.forward_project(base)]
+    for k in range(6):
+        sc = np.zeros(6)
+        sc[k] = 1.0
+        ind = phantom.phantom(ctx, seed=0, activity=0.0, sphere_activity=1.0, sphere_scale=sc)
+        parts.append(ctx.forward_project(ind))
+    atten = np.exp(ctx.forward_project(phantom.mu_map(ctx)), dtype=np.float32)
+    fps = torch.stack([torch.from_numpy(p) for p in parts]).to(dev)
+    del parts
+    atten_d = torch.from_numpy(atten).to(dev)
+    valid = fps[0] > 0
+    nvalid = int(valid.sum())
+    g = torch.Generator(device=dev)
+    g.manual_seed(DYN["seed"])
+    host_p, host_r = [], []
+    for f in range(nf):
+        w = torch.tensor(np.concatenate([[1.0], act[f] - 1.0]), dtype=torch.float32, device=dev)
+        t = torch.tensordot(w, fps, dims=1) / atten_d
+        t_sum = float(t.sum(dtype=torch.float64))
+        r_total = DYN["randoms_frac"] / (1.0 - DYN["randoms_frac"]) * t_sum
+        scale = counts[f] / (t_sum + r_total)
+        r_level = r_total * scale / nvalid
+        mean = t * scale + valid * r_level
+        pr = torch.poisson(mean, generator=g).clamp_(max=32767).to(torch.int16)
+        hp = torch.empty(pr.shape, dtype=torch.int16, pin_memory=True)
+        hp.copy_(pr)
+        hr = torch.empty(pr.shape, dtype=torch.float32, pin_memory=True)
+        hr.copy_(valid.float() * float(r_level))
+        host_p.append(hp.numpy())
+        host_r.append(hr.numpy())
+        del t, mean, pr
+    del fps, atten_d, valid
+    torch.cuda.empty_cache()
+    gen_s = time.time() - t0
+    info = ctx.info
+    imgs = [pinned_copy(torch, np.zeros((info.nz, info.ny, info.nx), np.float32)) for _ in range(nf)]
+    cs = torch.cuda.ExternalStream(ctx.stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    b = ctx.batch(nf, atten=atten, storage=H.STORE_16)
+    # untimed: prepare every frame, tune the launch shapes, capture the graphs
+    for f in range(nf):
+        b.set_frame(f, host_p[f], host_r[f], iterations=int(iters[f]))
+    tune = b.autotune(repeats=3)
+    b.run()
+    torch.cuda.synchronize()
+    # device-resident: every frame reconstructed from the uniform image
+    clocks = ClockSampler(local)
+    barrier(dist, local)
+    clocks.start()
+    bst = b.run()
+    clk = clocks.stop()
+    run_ms = max_over_ranks(dist, bst.ms_total, local)
+    # end to end through the C ABI: every frame's inputs from pinned memory,
+    # the reconstruction, every image back into pinned memory
+    barrier(dist, local)
+    torch.cuda.synchronize()
+    ev[0].record(cs)
+    for f in range(nf):
+        b.set_frame(f, host_p[f], host_r[f], iterations=int(iters[f]))
+    est = b.run()
+    for f in range(nf):
+        b.get_image(f, out=imgs[f])
+    ev[1].record(cs)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(dist, ev[0].elapsed_time(ev[1]), local)
+    sums = [b.get_image(f, out=imgs[f])[1] for f in range(nf)]
+    # precision: two frames reconstructed alone with f32-stored inputs
+    rel = {}
+    for f in (int(np.argmin(counts)), int(np.argmax(counts))):
+        ctx2 = H.Context(geom, device=local)
+        want, _ = ctx2.reconstruct(host_p[f], host_r[f], atten=atten, storage=H.STORE_F32,
+                                   iterations=int(iters[f]))
+        ctx2.close()
+        a = imgs[f].astype(np.float64)
+        rel[f"frame{f} ({counts[f]:.3g} counts, {int(iters[f])} it)"] = float(
+            np.linalg.norm(a - want) / max(np.linalg.norm(want.astype(np.float64)), 1e-30))
+    h2d = sum(int(a.nbytes) for a in host_p) + sum(int(a.nbytes) for a in host_r)
+    d2h = sum(int(a.nbytes) for a in imgs)
+    b.close()
+    ctx.close()
+    si = bst.subset_iterations
+    return {
+        "metric": "dynamic-study subset-iters/s (span 9, 24 frames, 16-bit-stored inputs)",
+        "unit": UNIT, "value": ws * si / (run_ms / 1e3), "ms_run": run_ms, "subset_iterations": si,
+        "workload": f"{nf} span-9 HRRT frames (2209 planes x 288 views x 256 bins), image 256x256x207, phantom "
+                    "seed 0 with time-varying sphere activity, counts log-uniform 2e6..2e8, 16 subsets x 1-4 "
+                    "iterations per frame (seeded), randoms 20 %, water attenuation, norm 1",
+        "frames": {"counts": [float(c) for c in counts], "iterations": [int(i) for i in iters],
+                   "sum_image": sums},
+        "batch": bst.as_dict(), "tuning": tune.as_dict(), "gpu_launches": bst.kernel_launches,
+        "e2e": {"value": ws * est.subset_iterations / (e2e_ms / 1e3), "unit": UNIT, "ms": e2e_ms,
+                "h2d_bytes_per_step": h2d // max(est.subset_iterations, 1),
+                "d2h_bytes_per_step": d2h // max(est.subset_iterations, 1)},
+        "rel_l2_vs_f32_stored": rel,
+        "clocks": clk, "data_gen_s": gen_s,
+    }
 
 
 def run_listmode(args, torch, H, local, dist, ws, cpu=True):
@@ -521,6 +683,9 @@ def main():
     ap.add_argument("--lm-events", type=int, default=1_000_000_000,
                     help="listmode events of the l64 leg (0: skip it)")
     ap.add_argument("--geometry", default="hrrt", choices=["hrrt", "small"])
+    ap.add_argument("--dyn-frames", type=int, default=24, help="frames of the dynamic-study leg (0: skip it)")
+    ap.add_argument("--no-compare-16", dest="compare_16", action="store_false",
+                    help="skip the 16-bit-storage leg of the span-3 workload")
     args = ap.parse_args()
     global GEOMETRY
     GEOMETRY = args.geometry

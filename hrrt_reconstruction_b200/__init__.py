@@ -16,7 +16,7 @@ import os
 
 import numpy as np
 
-__all__ = ["Geometry", "HrrtError", "Context", "Listmode", "lib", "LIB_PATH", "STORE_F32", "STORE_16", "BP_REF", "BP_ADJOINT",
+__all__ = ["Geometry", "HrrtError", "Context", "Batch", "Tuning", "Listmode", "lib", "LIB_PATH", "STORE_F32", "STORE_16", "BP_REF", "BP_ADJOINT",
            "geometry_table", "hrrt_geometry"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libhrrt_gpu.so")
@@ -63,6 +63,23 @@ class LmStats(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class Tuning(ctypes.Structure):
+    """hrrt_tuning: launch shape of the projectors (results do not depend on it)."""
+    _fields_ = [("fp_planes", ctypes.c_int), ("fp_producer_warps", ctypes.c_int), ("bp_planes", ctypes.c_int),
+                ("fp_ms", ctypes.c_double), ("bp_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [("ms_total", ctypes.c_double), ("subset_iterations", ctypes.c_int), ("groups", ctypes.c_int),
+                ("graphs", ctypes.c_int), ("graph_launches", ctypes.c_int), ("kernel_launches", ctypes.c_longlong)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 LM_TRUES, LM_PROMPTS_AND_DELAYED, LM_PROMPTS_ONLY = 0, 1, 2
 LM_IGNORE_BORDER_CRYSTAL, LM_NO_DOI, LM_TIME_FROM_COUNT = 1, 2, 4
 
@@ -102,6 +119,15 @@ def _load():
         "hrrt_set_profiling": (i, [vp, i]),
         "hrrt_kernel_stats": (i, [vp, ctypes.c_char_p, ctypes.POINTER(i), ctypes.POINTER(d)]),
         "hrrt_reset_kernel_stats": (i, [vp]),
+        "hrrt_set_tuning": (i, [vp, ctypes.POINTER(Tuning)]),
+        "hrrt_get_tuning": (i, [vp, ctypes.POINTER(Tuning)]),
+        "hrrt_autotune": (i, [vp, i, ctypes.POINTER(Tuning)]),
+        "hrrt_batch_create": (i, [vp, i, i, vp, vp, ctypes.POINTER(vp)]),
+        "hrrt_batch_destroy": (None, [vp]),
+        "hrrt_batch_set_frame": (i, [vp, i, vp, vp, vp, i]),
+        "hrrt_batch_autotune": (i, [vp, i, ctypes.POINTER(Tuning)]),
+        "hrrt_batch_run": (i, [vp, ctypes.POINTER(BatchStats)]),
+        "hrrt_batch_get_image": (i, [vp, i, vp, ctypes.POINTER(d)]),
         "hrrt_lm_create": (i, [i, i, i, ctypes.POINTER(vp)]),
         "hrrt_lm_destroy": (None, [vp]),
         "hrrt_lm_last_error": (ctypes.c_char_p, [vp]),
@@ -342,6 +368,26 @@ class Context:
         return co
 
     # ---- timing ----
+    def set_tuning(self, fp_planes=0, fp_producer_warps=0, bp_planes=0):
+        t = Tuning(fp_planes, fp_producer_warps, bp_planes, 0.0, 0.0)
+        self._check(lib.hrrt_set_tuning(self._h, ctypes.byref(t)), "set_tuning")
+
+    def get_tuning(self):
+        t = Tuning()
+        self._check(lib.hrrt_get_tuning(self._h, ctypes.byref(t)), "get_tuning")
+        return t
+
+    def autotune(self, repeats=3):
+        """Time every projector launch shape on the current inputs and image;
+        keep and return the fastest (Tuning)."""
+        t = Tuning()
+        self._check(lib.hrrt_autotune(self._h, repeats, ctypes.byref(t)), "autotune")
+        return t
+
+    def batch(self, nframes, norm=None, atten=None, storage=STORE_F32):
+        """A dynamic study on this context's geometry (Batch)."""
+        return Batch(self, nframes, norm=norm, atten=atten, storage=storage)
+
     def set_profiling(self, on):
         self._check(lib.hrrt_set_profiling(self._h, 1 if on else 0), "set_profiling")
 
@@ -357,6 +403,75 @@ class Context:
 
 
 LM_SOL = np.dtype([("nsino", np.int32), ("d", np.float32), ("z", np.float32)])
+
+
+class Batch:
+    """hrrt_batch: the frames of a dynamic study, sharing the context's
+    geometry and one normalisation / attenuation, each with its own prompts,
+    randoms, scatter and iteration count; reconstructed together (the frame
+    loop of hrrt_osem3d's main, hrrt_osem3d_span3.cpp:4555-4597)."""
+
+    def __init__(self, ctx, nframes, norm=None, atten=None, storage=STORE_F32):
+        self.ctx = ctx
+        self.nframes = nframes
+        n = _c(norm, np.float32)
+        a = _c(atten, np.float32)
+        need = int(np.prod(ctx.sino_shape))
+        for name, arr in (("norm", n), ("atten", a)):
+            if arr is not None and arr.size != need:
+                raise HrrtError(f"{name}: {arr.size} elements, expected {need}")
+        h = ctypes.c_void_p()
+        ctx._check(lib.hrrt_batch_create(ctx._h, nframes, storage, _ptr(n), _ptr(a), ctypes.byref(h)), "batch_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.hrrt_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_frame(self, frame, prompts, randoms, scatter=None, iterations=1):
+        p = _c(prompts, np.int16)
+        r = _c(randoms, np.float32)
+        s = _c(scatter, np.float32)
+        need = int(np.prod(self.ctx.sino_shape))
+        for name, arr in (("prompts", p), ("randoms", r), ("scatter", s)):
+            if arr is not None and arr.size != need:
+                raise HrrtError(f"{name}: {arr.size} elements, expected {need}")
+        self.ctx._check(lib.hrrt_batch_set_frame(self._h, frame, _ptr(p), _ptr(r), _ptr(s), iterations),
+                        "batch_set_frame")
+
+    def autotune(self, repeats=3):
+        t = Tuning()
+        self.ctx._check(lib.hrrt_batch_autotune(self._h, repeats, ctypes.byref(t)), "batch_autotune")
+        return t
+
+    def run(self):
+        st = BatchStats()
+        self.ctx._check(lib.hrrt_batch_run(self._h, ctypes.byref(st)), "batch_run")
+        return st
+
+    def get_image(self, frame, out=None):
+        """-> (image [z][y][x] float32, FP64 image sum of its last iteration)"""
+        i = self.ctx.info
+        if out is None:
+            out = np.empty((i.nz, i.ny, i.nx), np.float32)
+        elif out.shape != (i.nz, i.ny, i.nx) or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise HrrtError("get_image: out must be C-contiguous float32 [nz][ny][nx]")
+        sm = ctypes.c_double()
+        self.ctx._check(lib.hrrt_batch_get_image(self._h, frame, _ptr(out), ctypes.byref(sm)), "batch_get_image")
+        return out, sm.value
 
 
 def lm_table(name, span=3, maxrd=67):

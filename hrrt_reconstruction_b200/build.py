@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhrrt_gpu.so")
 CLI = os.path.join(HERE, "hrrt_osem3d_gpu")
 
-SOURCES = ["kernels.cu", "hrrt_gpu.cu", "geometry.cpp", "listmode.cu", "lm_tables.cpp"]
+SOURCES = ["kernels.cu", "hrrt_gpu.cu", "batch.cu", "geometry.cpp", "listmode.cu", "lm_tables.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -36,21 +36,37 @@ def _newer(target, deps):
 
 
 def build_library(force=False, verbose=False):
+    """Compile every source to an object under _build/ (in parallel), then
+    link libhrrt_gpu.so."""
+    from concurrent.futures import ThreadPoolExecutor
     deps = [os.path.join(CSRC, s) for s in SOURCES]
-    deps += [os.path.join(CSRC, h) for h in ("kernels.cuh", "geometry.h", "lm_tables.h")]
+    deps += [os.path.join(CSRC, h) for h in ("kernels.cuh", "geometry.h", "lm_tables.h", "context.h")]
     deps += [os.path.join(ROOT, "include", "hrrt_gpu.h"), __file__]
     if not force and _newer(LIB, deps):
         return LIB
-    cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", "-fmad=false", "--shared",
-           "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-I" + os.path.join(ROOT, "include"),
-           "-o", LIB + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES] + ["-lcudart"]
+    obj_dir = os.path.join(HERE, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
+    flags = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2",
+             "-I" + os.path.join(ROOT, "include")]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    r = subprocess.run(cmd, capture_output=True, text=True)
+        flags.insert(0, "-Xptxas=-v")
+
+    def compile_one(src):
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
+        r = subprocess.run([nvcc(), *flags, "-c", os.path.join(CSRC, src), "-o", obj], capture_output=True, text=True)
+        return obj, r
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    for obj, r in results:
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        if verbose:
+            sys.stderr.write(r.stderr)
+    r = subprocess.run([nvcc(), *ARCH, "--shared", "-o", LIB + ".tmp"] + [o for o, _ in results] + ["-lcudart"],
+                       capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
-    if verbose:
-        sys.stderr.write(r.stderr)
+        raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -17,81 +17,10 @@
 #include <string>
 #include <vector>
 
-#include "../../include/hrrt_gpu.h"
-#include "geometry.h"
-#include "kernels.cuh"
+#include "context.h"
 
 using namespace hrrt;
-
-struct KernelTimer {
-  std::string name;
-  cudaEvent_t start, stop;
-};
-
-struct hrrt_ctx {
-  Geometry geo;
-  DevGeom dg{};
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  std::string err;
-  std::vector<void *> allocs;
-
-  int storage = -1;
-  void *q_prompts = nullptr, *q_add = nullptr, *q_mult = nullptr;
-  int16_t *d_nzmask = nullptr;
-  int *d_mask_accum = nullptr;
-  std::vector<int16_t> nzmask;
-
-  float *d_image = nullptr;
-  float *d_nfinv = nullptr;
-  float *d_ratio = nullptr, *d_bc = nullptr, *d_br = nullptr;
-  float *d_tmp_img = nullptr;  // test entry points
-  float *d_rows = nullptr;
-  double *d_partial = nullptr, *d_sum = nullptr;
-  int *d_pair_views = nullptr;  // [subsets][npairs]
-  QuadWork *d_work = nullptr;   // fp lists then bp lists, per subset
-  std::vector<int> fp_off, fp_cnt, bp_off, bp_cnt;
-  int *d_rowstart = nullptr;
-  int npairs = 0;               // view pairs per subset
-  long long vol = 0;            // nx*ny*zp
-  long long quad_pair = 0;      // floats per pair in quad layout
-  int tpt = 1;
-  bool have_inputs = false, have_sens = false, have_image = false;
-
-  // chunked upload: flat-file planes staged through two device buffers, the
-  // copy of one chunk overlapping the prep of the previous one
-  cudaStream_t copy_stream = nullptr;
-  cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
-  char *stage[2] = {nullptr, nullptr};
-  size_t stage_bytes = 0;
-  // pipelined reconstruction: the view pairs of one subset staged pair-major
-  char *pstage[2] = {nullptr, nullptr};
-  size_t pstage_bytes = 0;
-
-  // back projector of the OSEM loop, and the device geometry it runs with
-  // (for the adjoint: segment weights of 1, the forward projector's scaling)
-  int bp_mode = HRRT_BP_REF;
-  DevGeom dg_adj{};
-  int *d_view1 = nullptr;       // one view index, for single-pair entry points
-
-  bool prof = false;
-  std::vector<KernelTimer> pending;
-  std::map<std::string, std::pair<int, double>> kstats;
-
-  ~hrrt_ctx() {
-    for (auto &t : pending) {
-      cudaEventDestroy(t.start);
-      cudaEventDestroy(t.stop);
-    }
-    for (void *p : allocs) cudaFree(p);
-    for (int b = 0; b < 2; b++) {
-      if (ev_copied[b]) cudaEventDestroy(ev_copied[b]);
-      if (ev_free[b]) cudaEventDestroy(ev_free[b]);
-    }
-    if (copy_stream) cudaStreamDestroy(copy_stream);
-    if (stream) cudaStreamDestroy(stream);
-  }
-};
+using namespace hrrt_host;
 
 namespace {
 
@@ -99,78 +28,14 @@ namespace {
 // staging per buffer with all five inputs)
 constexpr int kUploadPlanes = 96;
 
-int fail(hrrt_ctx *ctx, int code, const std::string &msg) {
-  if (ctx) ctx->err = msg;
-  return code;
-}
-int cuda_fail(hrrt_ctx *ctx, cudaError_t e, const char *where) {
-  return fail(ctx, HRRT_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
-}
-#define CK(call, where)                                   \
-  do {                                                    \
-    cudaError_t e_ = (call);                              \
-    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
-  } while (0)
-
-template <typename T>
-T *dalloc(hrrt_ctx *ctx, size_t n, cudaError_t *e) {
-  void *p = nullptr;
-  *e = cudaMalloc(&p, n * sizeof(T) + 16);
-  if (*e != cudaSuccess) return nullptr;
-  *e = cudaMemsetAsync(p, 0, n * sizeof(T) + 16, ctx->stream);
-  ctx->allocs.push_back(p);
-  return (T *)p;
-}
-template <typename T>
-T *dupload(hrrt_ctx *ctx, const std::vector<T> &v, cudaError_t *e) {
-  T *p = dalloc<T>(ctx, std::max<size_t>(v.size(), 1), e);
-  if (!p) return nullptr;
-  if (!v.empty()) *e = cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream);
-  return p;
-}
-
-struct Launch {
-  hrrt_ctx *ctx;
-  KernelTimer t{};
-  Launch(hrrt_ctx *c, const char *name) : ctx(c) {
-    if (ctx->prof) {
-      t.name = name;
-      cudaEventCreate(&t.start);
-      cudaEventCreate(&t.stop);
-      cudaEventRecord(t.start, ctx->stream);
-    }
-  }
-  ~Launch() {
-    if (ctx->prof) {
-      cudaEventRecord(t.stop, ctx->stream);
-      ctx->pending.push_back(t);
-    }
-  }
-};
-
-void drain_timers(hrrt_ctx *ctx) {
-  for (auto &t : ctx->pending) {
-    cudaEventSynchronize(t.stop);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, t.start, t.stop);
-    auto &s = ctx->kstats[t.name];
-    s.first += 1;
-    s.second += ms;
-    cudaEventDestroy(t.start);
-    cudaEventDestroy(t.stop);
-  }
-  ctx->pending.clear();
-}
-
 // Forward-projection tasks shared by every quad: (segment, plane run, kind).
-std::vector<FpTask> build_fp_tasks(const Geometry &g) {
+std::vector<FpTask> build_fp_tasks(const Geometry &g, int PL) {
   std::vector<FpTask> mid, ends;
-  for (int p0 = 0; p0 < g.nz; p0 += kFpPlanes)
-    mid.push_back(FpTask{0, (int16_t)p0, (int16_t)std::min(kFpPlanes, g.nz - p0), 0});
+  for (int p0 = 0; p0 < g.nz; p0 += PL) mid.push_back(FpTask{0, (int16_t)p0, (int16_t)std::min(PL, g.nz - p0), 0});
   for (int s = 1; s < g.nseg; s++) {
     const int ns = g.yr_top[s] - g.yr_bottom[s] + 1;
-    for (int p0 = g.zshift; p0 < ns - g.zshift; p0 += kFpPlanes)
-      mid.push_back(FpTask{(int16_t)s, (int16_t)p0, (int16_t)std::min(kFpPlanes, ns - g.zshift - p0), 1});
+    for (int p0 = g.zshift; p0 < ns - g.zshift; p0 += PL)
+      mid.push_back(FpTask{(int16_t)s, (int16_t)p0, (int16_t)std::min(PL, ns - g.zshift - p0), 1});
     // an end-plane run stays inside one end region, so its lookup entries are consecutive
     for (int p0 = 0; p0 < g.zshift; p0 += kFpEndPlanes)
       ends.push_back(FpTask{(int16_t)s, (int16_t)p0, (int16_t)std::min(kFpEndPlanes, g.zshift - p0), 2});
@@ -193,7 +58,7 @@ std::vector<FpTask> build_fp_tasks(const Geometry &g) {
 // Every shared-memory index the forward projector can form for this geometry
 // must lie inside the staged column; checked once here so the kernel needs no
 // run-time guards.
-std::string validate_fp(const Geometry &g, const std::vector<FpMid> &mid, const std::vector<FpTask> &tasks) {
+std::string validate_fp(const Geometry &g, const std::vector<FpMid> &mid, const std::vector<FpTask> &tasks, int PL) {
   const int ZS = g.zp + kFpZPad, FS = g.flookup_stride();
   int ymin = g.c;
   for (int x = 1; x <= g.c; x++)
@@ -202,7 +67,7 @@ std::string validate_fp(const Geometry &g, const std::vector<FpMid> &mid, const 
     for (const FpTask &t : tasks) {
       if (t.type < 0) continue;
       if (t.type == 0) {
-        if (t.p0 + kFpPlanes >= ZS) return "fp: segment-0 window out of range";
+        if (t.p0 + PL >= ZS) return "fp: segment-0 window out of range";
         continue;
       }
       const int gg = (t.seg + 1) / 2 - 1;
@@ -210,7 +75,7 @@ std::string validate_fp(const Geometry &g, const std::vector<FpMid> &mid, const 
       if (m.z < 0) continue;
       if (t.type == 1) {
         const int za = m.z + t.p0 - g.zshift, zb = m.z2 + t.p0 - g.zshift;
-        if (za < 0 || zb < 0 || za + kFpPlanes >= ZS || zb + kFpPlanes >= ZS) return "fp: middle window out of range";
+        if (za < 0 || zb < 0 || za + PL >= ZS || zb + PL >= ZS) return "fp: middle window out of range";
       } else {
         const int ns = g.yr_top[t.seg] - g.yr_bottom[t.seg] + 1;
         for (int j = 0; j < t.n; j++) {
@@ -225,6 +90,10 @@ std::string validate_fp(const Geometry &g, const std::vector<FpMid> &mid, const 
   }
   return std::string();
 }
+
+}  // namespace
+
+namespace hrrt_host {
 
 // reads (and clears) the device status word after the stream has drained
 int device_status(hrrt_ctx *ctx) {
@@ -280,6 +149,7 @@ int build_work_lists(hrrt_ctx *ctx) {
   }
   ctx->d_work = dupload(ctx, all, &e);
   if (!ctx->d_work) return cuda_fail(ctx, e, "work list");
+  ctx->config_epoch++;
   if (!ctx->d_pair_views) {
     ctx->d_pair_views = dupload(ctx, views, &e);
     if (!ctx->d_pair_views) return cuda_fail(ctx, e, "pair views");
@@ -288,49 +158,41 @@ int build_work_lists(hrrt_ctx *ctx) {
   return HRRT_OK;
 }
 
-int run_subset(hrrt_ctx *ctx, int s) {
-  const DevGeom &g = ctx->dg;
-  const size_t in_stride = (size_t)ctx->quad_pair;
-  if (ctx->bp_mode == HRRT_BP_ADJOINT) {
-    const DevGeom &ga = ctx->dg_adj;
-    {
-      Launch L(ctx, "fp_kernel");
-      CK(launch_fp(ga, ctx->d_image, ctx->d_work + ctx->fp_off[s], ctx->fp_cnt[s], 1, ctx->q_prompts, ctx->q_add,
-                   ctx->storage, ctx->d_ratio, ctx->quad_pair, ctx->tpt, ctx->stream),
-         "fp_kernel");
-    }
+SubsetBufs ctx_bufs(hrrt_ctx *ctx) {
+  return SubsetBufs{ctx->d_image, ctx->q_prompts, ctx->q_add, ctx->d_ratio, ctx->d_bc, ctx->d_br, one_frame()};
+}
+
+int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
+  const bool adj = ctx->bp_mode == HRRT_BP_ADJOINT;
+  const DevGeom &g = adj ? ctx->dg_adj : ctx->dg;
+  const QuadWork *fw = ctx->d_work + ctx->fp_off[s], *bw = ctx->d_work + ctx->bp_off[s];
+  const int *pv = ctx->d_pair_views + (size_t)s * ctx->npairs;
+  float *nf = ctx->d_nfinv + (size_t)s * ctx->vol;
+  {
+    Launch L(ctx, "fp_kernel");
+    CK(launch_fp(g, b.image, fw, ctx->fp_cnt[s], 1, b.prompts, b.add, ctx->storage, b.ratio, ctx->quad_pair,
+                 ctx->tune, b.fr, ctx->stream),
+       "fp_kernel");
+  }
+  if (adj) {
     {
       Launch L(ctx, "adj_kernel");
-      CK(launch_adj(ga, ctx->d_ratio, in_stride, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s], ctx->d_bc, ctx->d_br,
-                    ctx->vol, ctx->stream),
+      CK(launch_adj(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, b.fr, ctx->stream),
          "adj_kernel");
     }
-    {
-      Launch L(ctx, "adj_rotate_kernel");
-      CK(launch_adj_rotate(ga, ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_bc, ctx->d_br,
-                           ctx->vol, ctx->d_image, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 0, ctx->stream),
-         "adj_rotate_kernel");
-    }
+    Launch L(ctx, "adj_rotate_kernel");
+    CK(launch_adj_rotate(g, pv, ctx->npairs, b.bc, b.br, ctx->vol, b.image, nf, nullptr, 0, b.fr, ctx->stream),
+       "adj_rotate_kernel");
     return HRRT_OK;
   }
   {
-    Launch L(ctx, "fp_kernel");
-    CK(launch_fp(g, ctx->d_image, ctx->d_work + ctx->fp_off[s], ctx->fp_cnt[s], 1, ctx->q_prompts, ctx->q_add,
-                 ctx->storage, ctx->d_ratio, ctx->quad_pair, ctx->tpt, ctx->stream),
-       "fp_kernel");
-  }
-  {
     Launch L(ctx, "bp_kernel");
-    CK(launch_bp(g, ctx->d_ratio, in_stride, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s], ctx->d_bc, ctx->d_br,
-                 ctx->vol, ctx->stream),
+    CK(launch_bp(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, ctx->tune, b.fr, ctx->stream),
        "bp_kernel");
   }
-  {
-    Launch L(ctx, "rotback_kernel");
-    CK(launch_rotback(g, ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_bc, ctx->d_br, ctx->vol,
-                      ctx->d_image, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 0, ctx->stream),
-       "rotback_kernel");
-  }
+  Launch L(ctx, "rotback_kernel");
+  CK(launch_rotback(g, pv, ctx->npairs, b.bc, b.br, ctx->vol, b.image, nf, nullptr, 0, b.fr, ctx->stream),
+     "rotback_kernel");
   return HRRT_OK;
 }
 
@@ -375,29 +237,121 @@ int sens_subset(hrrt_ctx *ctx, int s) {
     {
       Launch L(ctx, "adj_kernel");
       CK(launch_adj(ctx->dg_adj, ctx->d_ratio, ctx->quad_pair, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s],
-                    ctx->d_bc, ctx->d_br, ctx->vol, ctx->stream),
+                    ctx->d_bc, ctx->d_br, ctx->vol, one_frame(), ctx->stream),
          "adj_kernel");
     }
     Launch L(ctx, "adj_rotate_kernel");
     CK(launch_adj_rotate(ctx->dg_adj, ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_bc, ctx->d_br,
-                         ctx->vol, nullptr, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 1, ctx->stream),
+                         ctx->vol, nullptr, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 1, one_frame(), ctx->stream),
        "adj_rotate_kernel");
     return HRRT_OK;
   }
   {
     Launch L(ctx, "bp_kernel");
     CK(launch_bp(ctx->dg, ctx->d_ratio, ctx->quad_pair, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s], ctx->d_bc,
-                 ctx->d_br, ctx->vol, ctx->stream),
+                 ctx->d_br, ctx->vol, ctx->tune, one_frame(), ctx->stream),
        "bp_kernel");
   }
   Launch L(ctx, "rotback_kernel");
   CK(launch_rotback(ctx->dg, ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->d_bc, ctx->d_br, ctx->vol,
-                    nullptr, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 1, ctx->stream),
+                    nullptr, ctx->d_nfinv + (size_t)s * ctx->vol, nullptr, 1, one_frame(), ctx->stream),
      "rotback_kernel");
   return HRRT_OK;
 }
 
-}  // namespace
+int upload_flat(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms, const float *norm, const float *atten,
+                const float *scatter, int storage, bool norm_atten_device, void *qp, void *qadd, void *qmult) {
+  const Geometry &g = ctx->geo;
+  cudaError_t e = cudaSuccess;
+  // staging of the raw flat-file arrays, kUploadPlanes planes at a time
+  const float *srcs[4] = {randoms, norm, atten, scatter};
+  const size_t plane_elems = (size_t)g.nviews * g.nbins;
+  const int CP = std::min(g.segmentsize, kUploadPlanes);
+  const size_t chunk = (size_t)CP * plane_elems;
+  const size_t need = chunk * (sizeof(int16_t) + 4 * sizeof(float));
+  if (ctx->stage_bytes < need) {
+    for (int b = 0; b < 2; b++)
+      if (ctx->stage[b]) {
+        cudaFree(ctx->stage[b]);
+        ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)ctx->stage[b]));
+        ctx->stage[b] = nullptr;
+      }
+    ctx->stage_bytes = 0;
+    for (int b = 0; b < 2; b++) {
+      ctx->stage[b] = dalloc<char>(ctx, need, &e);
+      if (!ctx->stage[b]) return fail(ctx, HRRT_ERR_NOMEM, "upload staging");
+    }
+    ctx->stage_bytes = need;
+  }
+  if (!ctx->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream");
+    for (int b = 0; b < 2; b++) {
+      CK(cudaEventCreateWithFlags(&ctx->ev_copied[b], cudaEventDisableTiming), "upload event");
+      CK(cudaEventCreateWithFlags(&ctx->ev_free[b], cudaEventDisableTiming), "upload event");
+    }
+  }
+  CK(cudaMemsetAsync(ctx->d_mask_accum, 0, sizeof(int) * (size_t)(g.nviews / 2) * ctx->dg.nquads, ctx->stream),
+     "upload_inputs");
+  for (int b = 0; b < 2; b++) CK(cudaEventRecord(ctx->ev_free[b], ctx->stream), "upload_inputs");
+  for (int p0 = 0, k = 0; p0 < g.segmentsize && e == cudaSuccess; p0 += CP, k++) {
+    const int b = k & 1, np = std::min(CP, g.segmentsize - p0);
+    const size_t off = (size_t)p0 * plane_elems, cnt = (size_t)np * plane_elems;
+    int16_t *sp = reinterpret_cast<int16_t *>(ctx->stage[b]);
+    float *stg[4] = {nullptr, nullptr, nullptr, nullptr};
+    e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_free[b], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(sp, prompts + off, cnt * sizeof(int16_t), cudaMemcpyHostToDevice, ctx->copy_stream);
+    for (int i = 0; i < 4 && e == cudaSuccess; i++) {
+      if (!srcs[i]) continue;
+      if (norm_atten_device && (i == 1 || i == 2)) {
+        stg[i] = const_cast<float *>(srcs[i]) + off;  // already on the device
+        continue;
+      }
+      stg[i] = reinterpret_cast<float *>(ctx->stage[b] + chunk * sizeof(int16_t) + (size_t)i * chunk * sizeof(float));
+      e = cudaMemcpyAsync(stg[i], srcs[i] + off, cnt * sizeof(float), cudaMemcpyHostToDevice, ctx->copy_stream);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_copied[b], ctx->copy_stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_copied[b], 0);
+    if (e == cudaSuccess) {
+      Launch L(ctx, "prep_kernel");
+      e = launch_prep(ctx->dg, g.nbins, sp, stg[0], stg[1], stg[2], stg[3], g.sp.npskip, g.sp.epsilon2, storage,
+                      qp, qadd, qmult, ctx->d_mask_accum, p0, np, ctx->stream);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_free[b], ctx->stream);
+  }
+  if (e == cudaSuccess) e = launch_finish_mask(ctx->dg, ctx->d_mask_accum, ctx->d_nzmask, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->nzmask.data(), ctx->d_nzmask, ctx->nzmask.size() * sizeof(int16_t),
+                        cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamSynchronize(ctx->stream);
+    return cuda_fail(ctx, e, "upload_inputs");
+  }
+  return HRRT_OK;
+}
+
+
+int apply_tune(hrrt_ctx *ctx, const ProjTune &t) {
+  const int pl = t.fp_planes > 0 ? t.fp_planes : kFpPlanes;
+  int vi = -1;
+  for (int i = 0; i < 3; i++)
+    if (kFpPlaneVariants[i] == pl) vi = i;
+  if (vi < 0 || !ctx->d_fptasks[vi]) return fail(ctx, HRRT_ERR_ARG, "tuning: plane variant unavailable for this geometry");
+  const int cwarps = (ctx->nfptasks[vi] + 31) / 32;
+  if (t.fp_pwarps != 0 && (t.fp_pwarps < 2 || t.fp_pwarps > 6 || cwarps + t.fp_pwarps > kFpVariantWarps[vi]))
+    return fail(ctx, HRRT_ERR_ARG, "tuning: producer warps out of range");
+  if (t.bp_planes != 0 && t.bp_planes != 4 && t.bp_planes != 8)
+    return fail(ctx, HRRT_ERR_ARG, "tuning: back-projection planes must be 4 or 8");
+  ctx->tune = t;
+  ctx->config_epoch++;
+  ctx->dg.fptasks = ctx->dg_adj.fptasks = ctx->d_fptasks[vi];
+  ctx->dg.nfptasks = ctx->dg_adj.nfptasks = ctx->nfptasks[vi];
+  return HRRT_OK;
+}
+
+}  // namespace hrrt_host
 
 extern "C" {
 
@@ -529,14 +483,21 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
       const int z_lo = (zs / kBpZ) * kBpZ, z_hi = (ze / kBpZ) * kBpZ + kBpZ - 1;
       if (z_lo + d < yb - kBpPad || z_hi + d + 1 > yt + kBpPad) return bail(fail(ctx, HRRT_ERR_ARG, "bp: padding"));
     }
-  std::vector<FpTask> tasks = build_fp_tasks(g);
-  m = validate_fp(g, mid, tasks);
-  if (m.empty() && ((int)tasks.size() + 31) / 32 + 2 > kFpMaxWarps) m = "fp: too many projection tasks for one CTA";
+  // forward-projection task lists of every plane variant (one task per
+  // consumer thread, two producer warps at least); the default variant must
+  // fit, the others are offered to the tuner where they do
+  std::vector<FpTask> vtasks[3];
+  for (int i = 0; i < 3; i++) {
+    vtasks[i] = build_fp_tasks(g, kFpPlaneVariants[i]);
+    std::string vm = validate_fp(g, mid, vtasks[i], kFpPlaneVariants[i]);
+    if (vm.empty() && ((int)vtasks[i].size() + 31) / 32 + 2 > kFpVariantWarps[i])
+      vm = "fp: too many projection tasks for one CTA";
+    if (!vm.empty()) {
+      if (kFpPlaneVariants[i] == kFpPlanes) m = vm;
+      vtasks[i].clear();
+    }
+  }
   if (!m.empty()) return bail(fail(ctx, HRRT_ERR_ARG, m));
-  // one task per thread; a quad with more tasks than a CTA's launch bound is
-  // split over several CTAs (each samples the quad's rows itself)
-  ctx->tpt = 1;
-  if (tasks.size() > 30 * 32) return bail(fail(ctx, HRRT_ERR_ARG, "geometry has too many projection tasks"));
   if (g.zp % kBpZ != 0) return bail(fail(ctx, HRRT_ERR_ARG, "padded z must be a multiple of 8"));
   for (int x = 1; x <= g.c; x++)
     if (g.cyl0[x] != g.cyl1[x] && g.cyl0[x] < 1) return bail(fail(ctx, HRRT_ERR_ARG, "FOV reaches the grid edge"));
@@ -581,8 +542,15 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
   d.sin_psi = dupload(ctx, g.sin_psi, &e);
   d.cos_psi = dupload(ctx, g.cos_psi, &e);
   d.fov_xy = dupload(ctx, fovxy, &e);
-  d.fptasks = dupload(ctx, tasks, &e);
-  d.nfptasks = (int)tasks.size();
+  for (int i = 0; i < 3; i++) {
+    if (vtasks[i].empty()) continue;
+    ctx->d_fptasks[i] = dupload(ctx, vtasks[i], &e);
+    ctx->nfptasks[i] = (int)vtasks[i].size();
+    if (kFpPlaneVariants[i] == kFpPlanes) {
+      d.fptasks = ctx->d_fptasks[i];
+      d.nfptasks = ctx->nfptasks[i];
+    }
+  }
   d.plane_seg = dupload(ctx, plane_seg, &e);
   std::vector<int16_t> pplane_seg(g.padded_planes(), -1);
   for (int s = 0; s < g.nseg; s++)
@@ -630,6 +598,7 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
 void hrrt_ctx_destroy(hrrt_ctx *ctx) {
   if (!ctx) return;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->batch) detach_batch(ctx->batch);
   delete ctx;
 }
 
@@ -658,71 +627,11 @@ int hrrt_upload_inputs(hrrt_ctx *ctx, const int16_t *prompts, const float *rando
   if (!ctx) return HRRT_ERR_ARG;
   if (!prompts || !randoms) return fail(ctx, HRRT_ERR_ARG, "prompts and randoms are required");
   if (storage != HRRT_STORE_F32 && storage != HRRT_STORE_16) return fail(ctx, HRRT_ERR_ARG, "unknown storage");
-  const Geometry &g = ctx->geo;
-  cudaError_t e = cudaSuccess;
+  if (ctx->batch) return fail(ctx, HRRT_ERR_STATE, "the context serves a batch (hrrt_batch_destroy first)");
   if (int rc = ensure_input_buffers(ctx, storage)) return rc;
-  // staging of the raw flat-file arrays, kUploadPlanes planes at a time
-  const float *srcs[4] = {randoms, norm, atten, scatter};
-  const size_t plane_elems = (size_t)g.nviews * g.nbins;
-  const int CP = std::min(g.segmentsize, kUploadPlanes);
-  const size_t chunk = (size_t)CP * plane_elems;
-  const size_t need = chunk * (sizeof(int16_t) + 4 * sizeof(float));
-  if (ctx->stage_bytes < need) {
-    for (int b = 0; b < 2; b++)
-      if (ctx->stage[b]) {
-        cudaFree(ctx->stage[b]);
-        ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)ctx->stage[b]));
-        ctx->stage[b] = nullptr;
-      }
-    ctx->stage_bytes = 0;
-    for (int b = 0; b < 2; b++) {
-      ctx->stage[b] = dalloc<char>(ctx, need, &e);
-      if (!ctx->stage[b]) return fail(ctx, HRRT_ERR_NOMEM, "upload staging");
-    }
-    ctx->stage_bytes = need;
-  }
-  if (!ctx->copy_stream) {
-    CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream");
-    for (int b = 0; b < 2; b++) {
-      CK(cudaEventCreateWithFlags(&ctx->ev_copied[b], cudaEventDisableTiming), "upload event");
-      CK(cudaEventCreateWithFlags(&ctx->ev_free[b], cudaEventDisableTiming), "upload event");
-    }
-  }
-  CK(cudaMemsetAsync(ctx->d_mask_accum, 0, sizeof(int) * (size_t)(g.nviews / 2) * ctx->dg.nquads, ctx->stream),
-     "upload_inputs");
-  for (int b = 0; b < 2; b++) CK(cudaEventRecord(ctx->ev_free[b], ctx->stream), "upload_inputs");
-  for (int p0 = 0, k = 0; p0 < g.segmentsize && e == cudaSuccess; p0 += CP, k++) {
-    const int b = k & 1, np = std::min(CP, g.segmentsize - p0);
-    const size_t off = (size_t)p0 * plane_elems, cnt = (size_t)np * plane_elems;
-    int16_t *sp = reinterpret_cast<int16_t *>(ctx->stage[b]);
-    float *stg[4] = {nullptr, nullptr, nullptr, nullptr};
-    e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_free[b], 0);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(sp, prompts + off, cnt * sizeof(int16_t), cudaMemcpyHostToDevice, ctx->copy_stream);
-    for (int i = 0; i < 4 && e == cudaSuccess; i++) {
-      if (!srcs[i]) continue;
-      stg[i] = reinterpret_cast<float *>(ctx->stage[b] + chunk * sizeof(int16_t) + (size_t)i * chunk * sizeof(float));
-      e = cudaMemcpyAsync(stg[i], srcs[i] + off, cnt * sizeof(float), cudaMemcpyHostToDevice, ctx->copy_stream);
-    }
-    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_copied[b], ctx->copy_stream);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_copied[b], 0);
-    if (e == cudaSuccess) {
-      Launch L(ctx, "prep_kernel");
-      e = launch_prep(ctx->dg, g.nbins, sp, stg[0], stg[1], stg[2], stg[3], g.sp.npskip, g.sp.epsilon2, storage,
-                      ctx->q_prompts, ctx->q_add, ctx->q_mult, ctx->d_mask_accum, p0, np, ctx->stream);
-    }
-    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_free[b], ctx->stream);
-  }
-  if (e == cudaSuccess) e = launch_finish_mask(ctx->dg, ctx->d_mask_accum, ctx->d_nzmask, ctx->stream);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(ctx->nzmask.data(), ctx->d_nzmask, ctx->nzmask.size() * sizeof(int16_t),
-                        cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  if (e != cudaSuccess) {
-    cudaStreamSynchronize(ctx->copy_stream);
-    cudaStreamSynchronize(ctx->stream);
-    return cuda_fail(ctx, e, "upload_inputs");
-  }
+  if (int rc = upload_flat(ctx, prompts, randoms, norm, atten, scatter, storage, false, ctx->q_prompts, ctx->q_add,
+                           ctx->q_mult))
+    return rc;
   int rc = build_work_lists(ctx);
   if (rc) return rc;
   ctx->have_inputs = true;
@@ -768,7 +677,7 @@ int hrrt_osem_subsets(hrrt_ctx *ctx, int first, int count) {
   const int S = ctx->geo.sp.subsets;
   for (int i = 0; i < count; i++) {
     const int s = ctx->geo.order[(size_t)(((first + i) % S) + S) % S];
-    int rc = run_subset(ctx, s);
+    int rc = run_subset(ctx, s, ctx_bufs(ctx));
     if (rc) return rc;
   }
   return HRRT_OK;
@@ -786,7 +695,7 @@ int hrrt_osem(hrrt_ctx *ctx, int iterations, hrrt_stats *stats) {
   int done = 0;
   for (int it = 0; it < iterations; it++) {
     for (int i = 0; i < ctx->geo.sp.subsets; i++) {
-      int rc = run_subset(ctx, ctx->geo.order[i]);
+      int rc = run_subset(ctx, ctx->geo.order[i], ctx_bufs(ctx));
       if (rc) {
         cudaEventDestroy(a);
         cudaEventDestroy(b);
@@ -796,7 +705,7 @@ int hrrt_osem(hrrt_ctx *ctx, int iterations, hrrt_stats *stats) {
     }
     {
       Launch L(ctx, "post_iter_kernel");
-      CK(launch_post_iteration(ctx->dg, ctx->d_image, ctx->d_partial, ctx->d_sum, ctx->stream), "post_iteration");
+      CK(launch_post_iteration(ctx->dg, ctx->d_image, ctx->d_partial, ctx->d_sum, one_frame(), ctx->stream), "post_iteration");
     }
   }
   cudaEventRecord(b, ctx->stream);
@@ -822,6 +731,7 @@ int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms
   if (!prompts || !randoms || !image_zyx || iterations < 1)
     return fail(ctx, HRRT_ERR_ARG, "prompts, randoms, an output image and iterations >= 1 are required");
   if (storage != HRRT_STORE_F32 && storage != HRRT_STORE_16) return fail(ctx, HRRT_ERR_ARG, "unknown storage");
+  if (ctx->batch) return fail(ctx, HRRT_ERR_STATE, "the context serves a batch (hrrt_batch_destroy first)");
   const Geometry &g = ctx->geo;
   if (int rc = ensure_input_buffers(ctx, storage)) return rc;
   // pair-major staging of one subset's view pairs, two buffers
@@ -904,11 +814,11 @@ int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms
     if (e == cudaSuccess) e = launch_finish_mask(ctx->dg, ctx->d_mask_accum, ctx->d_nzmask, ctx->stream);
     if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "reconstruct upload"));
     if (int rc = sens_subset(ctx, s)) return bail(rc);
-    if (int rc = run_subset(ctx, s)) return bail(rc);
+    if (int rc = run_subset(ctx, s, ctx_bufs(ctx))) return bail(rc);
   }
   {
     Launch L(ctx, "post_iter_kernel");
-    e = launch_post_iteration(ctx->dg, ctx->d_image, ctx->d_partial, ctx->d_sum, ctx->stream);
+    e = launch_post_iteration(ctx->dg, ctx->d_image, ctx->d_partial, ctx->d_sum, one_frame(), ctx->stream);
     if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "post_iteration"));
   }
   // the mask is complete: the remaining iterations skip masked quads
@@ -921,9 +831,9 @@ int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms
   int done = S;
   for (int it = 1; it < iterations; it++) {
     for (int i = 0; i < S; i++, done++)
-      if (int rc = run_subset(ctx, g.order[i])) return bail(rc);
+      if (int rc = run_subset(ctx, g.order[i], ctx_bufs(ctx))) return bail(rc);
     Launch L(ctx, "post_iter_kernel");
-    e = launch_post_iteration(ctx->dg, ctx->d_image, ctx->d_partial, ctx->d_sum, ctx->stream);
+    e = launch_post_iteration(ctx->dg, ctx->d_image, ctx->d_partial, ctx->d_sum, one_frame(), ctx->stream);
     if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "post_iteration"));
   }
   double sum = 0.0;
@@ -1024,8 +934,7 @@ int hrrt_fp_pair(hrrt_ctx *ctx, const float *image_xyz, int view, float *prj) {
   CK(cudaMemcpyAsync(ctx->d_rows, prj, rows * 4, cudaMemcpyHostToDevice, ctx->stream), "fp_pair");
   {
     Launch L(ctx, "fp_kernel");
-    CK(launch_fp(ctx->dg, ctx->d_tmp_img, dw, (int)work.size(), 0, nullptr, nullptr, 0, ctx->d_ratio, ctx->quad_pair,
-                 ctx->tpt, ctx->stream),
+    CK(launch_fp(ctx->dg, ctx->d_tmp_img, dw, (int)work.size(), 0, nullptr, nullptr, 0, ctx->d_ratio, ctx->quad_pair, ctx->tune, one_frame(), ctx->stream),
        "fp_kernel");
   }
   CK(launch_quad_to_rows(ctx->dg, g.nbins, ctx->d_ratio, dw, (int)work.size(), ctx->d_rows, ctx->stream), "unpack");
@@ -1074,8 +983,7 @@ int hrrt_forward_project(hrrt_ctx *ctx, const float *image_xyz, float *sino) {
     const int cnt = off[b + 1] - off[b];
     {
       Launch L(ctx, "fp_kernel");
-      e = launch_fp(ctx->dg, ctx->d_tmp_img, dw + off[b], cnt, 0, nullptr, nullptr, 0, ctx->d_ratio, ctx->quad_pair,
-                    ctx->tpt, ctx->stream);
+      e = launch_fp(ctx->dg, ctx->d_tmp_img, dw + off[b], cnt, 0, nullptr, nullptr, 0, ctx->d_ratio, ctx->quad_pair, ctx->tune, one_frame(), ctx->stream);
     }
     if (e == cudaSuccess)
       e = launch_quad_to_file(ctx->dg, g.nbins, ctx->d_ratio, ctx->quad_pair, dw + off[b], cnt, dsino, ctx->stream);
@@ -1089,7 +997,10 @@ int hrrt_forward_project(hrrt_ctx *ctx, const float *image_xyz, float *sino) {
 int hrrt_set_backprojector(hrrt_ctx *ctx, int mode) {
   if (!ctx) return HRRT_ERR_ARG;
   if (mode != HRRT_BP_REF && mode != HRRT_BP_ADJOINT) return fail(ctx, HRRT_ERR_ARG, "unknown back projector");
-  if (mode != ctx->bp_mode) ctx->have_sens = false;
+  if (mode != ctx->bp_mode) {
+    ctx->have_sens = false;
+    ctx->config_epoch++;
+  }
   ctx->bp_mode = mode;
   return HRRT_OK;
 }
@@ -1117,7 +1028,7 @@ int hrrt_bp_pair(hrrt_ctx *ctx, const float *prj, int view, float *imagebuf_xyz,
     CK(cudaMemsetAsync(ctx->d_br, 0, ctx->vol * 4, ctx->stream), "bp_pair");
     {
       Launch L(ctx, "adj_kernel");
-      CK(launch_adj(ctx->dg, ctx->d_ratio, ctx->quad_pair, dw, (int)work.size(), ctx->d_bc, ctx->d_br, ctx->vol,
+      CK(launch_adj(ctx->dg, ctx->d_ratio, ctx->quad_pair, dw, (int)work.size(), ctx->d_bc, ctx->d_br, ctx->vol, one_frame(),
                     ctx->stream),
          "adj_kernel");
     }
@@ -1127,7 +1038,7 @@ int hrrt_bp_pair(hrrt_ctx *ctx, const float *prj, int view, float *imagebuf_xyz,
     {
       Launch L(ctx, "adj_rotate_kernel");
       CK(launch_adj_rotate(ctx->dg, ctx->d_view1, 1, ctx->d_bc, ctx->d_br, ctx->vol, nullptr, nullptr,
-                           ctx->d_tmp_img, 2, ctx->stream),
+                           ctx->d_tmp_img, 2, one_frame(), ctx->stream),
          "adj_rotate_kernel");
     }
     CK(cudaMemcpyAsync(imagebuf_xyz, ctx->d_tmp_img, ctx->vol * 4, cudaMemcpyDeviceToHost, ctx->stream), "bp_pair");
@@ -1139,7 +1050,7 @@ int hrrt_bp_pair(hrrt_ctx *ctx, const float *prj, int view, float *imagebuf_xyz,
   CK(launch_rows_to_quad(ctx->dg, g.nbins, ctx->d_rows, ctx->d_ratio, 1, ctx->stream), "pack");
   {
     Launch L(ctx, "bp_kernel");
-    CK(launch_bp(ctx->dg, ctx->d_ratio, ctx->quad_pair, dw, (int)work.size(), ctx->d_bc, ctx->d_br, ctx->vol,
+    CK(launch_bp(ctx->dg, ctx->d_ratio, ctx->quad_pair, dw, (int)work.size(), ctx->d_bc, ctx->d_br, ctx->vol, ctx->tune, one_frame(),
                  ctx->stream),
        "bp_kernel");
   }
@@ -1243,7 +1154,7 @@ int hrrt_rotate_add(hrrt_ctx *ctx, const float *imagebuf_xyz, int view, float *c
   CK(cudaMemcpyAsync(ctx->d_tmp_img, corr_xyz, ctx->vol * 4, cudaMemcpyHostToDevice, ctx->stream), "rotate");
   {
     Launch L(ctx, "rotback_kernel");
-    CK(launch_rotback(ctx->dg, dv, 1, ctx->d_bc, nullptr, ctx->vol, nullptr, nullptr, ctx->d_tmp_img, 2, ctx->stream),
+    CK(launch_rotback(ctx->dg, dv, 1, ctx->d_bc, nullptr, ctx->vol, nullptr, nullptr, ctx->d_tmp_img, 2, one_frame(), ctx->stream),
        "rotback");
   }
   CK(cudaMemcpyAsync(corr_xyz, ctx->d_tmp_img, ctx->vol * 4, cudaMemcpyDeviceToHost, ctx->stream), "rotate");

@@ -221,13 +221,22 @@ template <int ID>
 __device__ __forceinline__ void bar_arrive_id(int count) {
   asm volatile("bar.arrive %0, %1;" ::"n"(ID), "r"(count) : "memory");
 }
+// named barriers with immediate ids (a register id reserves all 16)
 __device__ __forceinline__ void bar_sync(int id, int count) {
   switch (id) {
     case 1: bar_sync_id<1>(count); break;
     case 2: bar_sync_id<2>(count); break;
     case 3: bar_sync_id<3>(count); break;
     case 4: bar_sync_id<4>(count); break;
-    default: bar_sync_id<5>(count); break;
+    case 5: bar_sync_id<5>(count); break;
+    case 6: bar_sync_id<6>(count); break;
+    case 7: bar_sync_id<7>(count); break;
+    case 8: bar_sync_id<8>(count); break;
+    case 9: bar_sync_id<9>(count); break;
+    case 10: bar_sync_id<10>(count); break;
+    case 11: bar_sync_id<11>(count); break;
+    case 12: bar_sync_id<12>(count); break;
+    default: bar_sync_id<13>(count); break;
   }
 }
 __device__ __forceinline__ void bar_arrive(int id, int count) {
@@ -235,36 +244,53 @@ __device__ __forceinline__ void bar_arrive(int id, int count) {
     case 1: bar_arrive_id<1>(count); break;
     case 2: bar_arrive_id<2>(count); break;
     case 3: bar_arrive_id<3>(count); break;
-    default: bar_arrive_id<4>(count); break;
+    case 4: bar_arrive_id<4>(count); break;
+    case 5: bar_arrive_id<5>(count); break;
+    case 6: bar_arrive_id<6>(count); break;
+    case 7: bar_arrive_id<7>(count); break;
+    case 8: bar_arrive_id<8>(count); break;
+    case 9: bar_arrive_id<9>(count); break;
+    case 10: bar_arrive_id<10>(count); break;
+    case 11: bar_arrive_id<11>(count); break;
+    default: bar_arrive_id<12>(count); break;
   }
 }
-constexpr int kBarFull = 1;   // + slot: sampled row ready (producers arrive, consumers wait)
-constexpr int kBarEmpty = 3;  // + slot: sampled row consumed (consumers arrive, producers wait)
-constexpr int kBarProd = 5;   // producers only: corner slot read by every producer
+constexpr int kBarFull = 1;                 // + slot: sampled row ready (producers arrive, consumers wait)
+constexpr int kBarEmpty = 1 + kFpSlots;     // + slot: sampled row consumed (consumers arrive, producers wait)
+constexpr int kBarProd = 1 + 2 * kFpSlots;  // producers only: corner slot read by every producer
+static_assert(kBarProd <= 13, "named barrier ids");
 
-template <int MODE, typename PT, typename AT>
-__global__ void __launch_bounds__(kFpMaxWarps * 32, 1) fp_kernel(DevGeom g, const float *__restrict__ image,
+template <int MODE, int PL, int MW, typename PT, typename AT>
+__global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *__restrict__ image,
                                                      const QuadWork *__restrict__ work,
                                                      const PT *__restrict__ prompts, const AT *__restrict__ add,
                                                      float4 *__restrict__ out, long long out_pair_stride,
-                                                     int nprod_warps) {
-  // shared memory: [2 slots][8 points][2 column pairs][2*zp] staged corner
-  // columns, 2*cpair zeros (the corners of outside points), [2 slots][2 halves]
-  // [ZS] sampled rows, [ZS] centre column
+                                                     int nprod_warps, FrameStrides fr) {
+  // shared memory: [S slots][8 points][2 column pairs][2*zp] staged corner
+  // columns, 2*cpair zeros (the corners of outside points), [S slots][2 halves]
+  // [ZS] sampled rows, [ZS] centre column (S = kFpSlots)
   extern __shared__ float4 smem[];
   const int ZS = g.zp + kFpZPad;
   const int zp = g.zp;
   const int cpair = 2 * zp;  // floats per column pair
   float *corners = reinterpret_cast<float *>(smem);
-  const int zoff = 2 * 8 * 2 * cpair;
+  const int zoff = kFpSlots * 8 * 2 * cpair;
   float *zcol = corners + zoff;
-  float4 *rows = smem + (size_t)(2 * 8 * 2 + 2) * cpair / 4;  // [2][2][ZS]
-  float4 *cen = rows + 4 * ZS;
-  __shared__ ulonglong2 s_w[2][4][2];
-  __shared__ int s_off[2][8];
-  __shared__ __align__(8) uint64_t s_bar[2];
+  float4 *rows = smem + (size_t)(kFpSlots * 8 * 2 + 2) * cpair / 4;  // [S][2][ZS]
+  float4 *cen = rows + 2 * kFpSlots * ZS;
+  __shared__ ulonglong2 s_w[kFpSlots][4][2];
+  __shared__ int s_off[kFpSlots][8];
+  __shared__ __align__(8) uint64_t s_bar[kFpSlots];
 
-  const QuadWork w = work[blockIdx.x];
+  const int nwork = gridDim.x / fr.n, frame = blockIdx.x / nwork, item = blockIdx.x - frame * nwork;
+  const QuadWork w = work[item];
+  const int fs = fr.map ? __ldg(fr.map + frame) : frame;
+  image += (size_t)fs * fr.image;
+  out += (size_t)frame * fr.ratio / 4;
+  if (MODE == 1) {
+    prompts += (size_t)fs * fr.input;
+    add += (size_t)fs * fr.input;
+  }
   const int x = w.x, v = w.view;
   const int N = g.nx, c = g.c;
   const float cosv = g.cos_psi[v], sinv = g.sin_psi[v];
@@ -279,7 +305,7 @@ __global__ void __launch_bounds__(kFpMaxWarps * 32, 1) fp_kernel(DevGeom g, cons
   // TMA issue (producer lanes 0-7, one sample point each): the two contiguous
   // column pairs (ix, iy..iy+1) and (ix+1, iy..iy+1) of each inside point
   auto issue_row = [&](int r) {
-    const int sl = r & 1, y = ystart + r, l = ptid;
+    const int sl = r % kFpSlots, y = ystart + r, l = ptid;
     int a, b;
     switch (l) {
       case 0: a = x; b = y; break;
@@ -316,19 +342,18 @@ __global__ void __launch_bounds__(kFpMaxWarps * 32, 1) fp_kernel(DevGeom g, cons
   };
 
   if (tid == 0) {
-    mbar_init(&s_bar[0], 1);
-    mbar_init(&s_bar[1], 1);
+#pragma unroll
+    for (int s = 0; s < kFpSlots; s++) mbar_init(&s_bar[s], 1);
     fence_mbar_init();
   }
-  for (int i = tid; i < 5 * kFpZPad; i += nthr) {
+  for (int i = tid; i < (2 * kFpSlots + 1) * kFpZPad; i += nthr) {
     const int col = i / kFpZPad, k = i % kFpZPad;
     rows[col * ZS + zp + k] = f4(0.f);
   }
   for (int i = tid; i < 2 * cpair; i += nthr) zcol[i] = 0.f;
   __syncthreads();
   if (producer && ptid < 8) {
-    if (nrows > 0) issue_row(0);
-    if (nrows > 1) issue_row(1);
+    for (int r = 0; r < kFpSlots && r < nrows; r++) issue_row(r);
   }
 
   // centre column y = c (sbrt:1815-1853): lanes (x,c),(N-x,c),(c,x),(c,N-x)
@@ -349,13 +374,13 @@ __global__ void __launch_bounds__(kFpMaxWarps * 32, 1) fp_kernel(DevGeom g, cons
 
   bool timed_out = false;
   if (producer) {
-    // ---------------- producers: bilinear samples, two rows ahead ----------------
+    // ---------------- producers: bilinear samples, kFpSlots rows ahead ----------------
     const int hsplit = nprod / 2;
     const int h_mine = ptid >= hsplit, z_mine = ptid - h_mine * hsplit;
     for (int r = 0; r < nrows; r++) {
-      const int sl = r & 1;
-      if (!mbar_wait(&s_bar[sl], (uint32_t)((r >> 1) & 1), g.err)) timed_out = true;
-      if (r >= 2) bar_sync(kBarEmpty + sl, nthr);  // consumers are done with row r-2
+      const int sl = r % kFpSlots;
+      if (!mbar_wait(&s_bar[sl], (uint32_t)((r / kFpSlots) & 1), g.err)) timed_out = true;
+      if (r >= kFpSlots) bar_sync(kBarEmpty + sl, nthr);  // consumers are done with row r-S
       {
         // lanes (0,1) and (2,3) of this half share nothing but the plane: each
         // lane pair is evaluated with packed pairs, its weights pre-packed
@@ -376,14 +401,15 @@ __global__ void __launch_bounds__(kFpMaxWarps * 32, 1) fp_kernel(DevGeom g, cons
         }
       }
       bar_arrive(kBarFull + sl, nthr);
-      // every producer has finished reading corner slot sl: refill it with row r+2
+      // every producer has finished reading corner slot sl: refill it with row r+S
       bar_sync(kBarProd, nprod);
-      if (ptid < 8 && r + 2 < nrows) issue_row(r + 2);
+      if (ptid < 8 && r + kFpSlots < nrows) issue_row(r + kFpSlots);
     }
     if (timed_out) {
       // results are void (the host reports the status word); give copies
       // still in flight a bounded chance to land before the CTA exits
-      for (int r = max(0, nrows - 2); r < nrows; r++) mbar_wait(&s_bar[r & 1], (uint32_t)((r >> 1) & 1), nullptr);
+      for (int r = max(0, nrows - kFpSlots); r < nrows; r++)
+        mbar_wait(&s_bar[r % kFpSlots], (uint32_t)((r / kFpSlots) & 1), nullptr);
     }
     return;
   }
@@ -391,12 +417,12 @@ __global__ void __launch_bounds__(kFpMaxWarps * 32, 1) fp_kernel(DevGeom g, cons
   // ---------------- consumers: one task (segment, plane run) each ----------------
   // accumulators start at the centre sample of their plane (the reference
   // assigns the centre column before accumulating rows y < c)
-  Q2 acc[kFpPlanes];
+  Q2 acc[PL];
   const FpTask tk = (tid < g.nfptasks) ? g.fptasks[tid] : FpTask{0, 0, 0, -1};
   {
     const int zb = (tk.type < 0) ? 0 : g.ybot[tk.seg] + tk.p0;
 #pragma unroll
-    for (int j = 0; j < kFpPlanes; j++) acc[j] = ldq(cen + min(zb + j, ZS - 1));
+    for (int j = 0; j < PL; j++) acc[j] = ldq(cen + min(zb + j, ZS - 1));
   }
   const int gg = (tk.seg + 1) / 2 - 1;
   const bool odd = tk.seg & 1;  // segment 2k-1: pam2 at z, pam at z2
@@ -406,14 +432,14 @@ __global__ void __launch_bounds__(kFpMaxWarps * 32, 1) fp_kernel(DevGeom g, cons
   const int li0 = gg * 2 * g.zshift + ((tk.p0 < g.zshift) ? tk.p0 : tk.p0 - ns_t + 2 * g.zshift);
   const int G = g.groupmax, FS = g.groupmax * 2 * g.zshift;
   for (int r = 0; r < nrows; r++) {
-    const int sl = r & 1, y = ystart + r;
+    const int sl = r % kFpSlots, y = ystart + r;
     bar_sync(kBarFull + sl, nthr);
     const float4 *pam = rows + (size_t)sl * 2 * ZS;
     const float4 *pam2 = pam + ZS;
     if (tk.type == 0) {
       // theta = 0 (sbrt:1907-1910)
 #pragma unroll
-      for (int j = 0; j < kFpPlanes; j++) acc[j] = qadd(acc[j], qadd(ldq(pam + tk.p0 + j), ldq(pam2 + tk.p0 + j)));
+      for (int j = 0; j < PL; j++) acc[j] = qadd(acc[j], qadd(ldq(pam + tk.p0 + j), ldq(pam2 + tk.p0 + j)));
     } else if (tk.type > 0) {
       const FpMid m = mrow[y * G];
       if (m.z >= 0) {  // else the group is skipped for this row (sbrt:1923-1924)
@@ -426,7 +452,7 @@ __global__ void __launch_bounds__(kFpMaxWarps * 32, 1) fp_kernel(DevGeom g, cons
           const uint64_t f = pk(m.f, m.f), f2 = pk(m.f2, m.f2);
           Q2 a0 = ldq(Aw), b0 = ldq(Bw);
 #pragma unroll
-          for (int j = 0; j < kFpPlanes; j++) {
+          for (int j = 0; j < PL; j++) {
             const Q2 a1 = ldq(Aw + j + 1), b1 = ldq(Bw + j + 1);
             acc[j] = qadd(acc[j], qaddp(qmul(qadd(b1, a0), f2), qmul(qadd(a1, b0), f)));
             a0 = a1;
@@ -449,7 +475,7 @@ __global__ void __launch_bounds__(kFpMaxWarps * 32, 1) fp_kernel(DevGeom g, cons
         }
       }
     }
-    if (r + 2 < nrows) bar_arrive(kBarEmpty + sl, nthr);
+    if (r + kFpSlots < nrows) bar_arrive(kBarEmpty + sl, nthr);
   }
 
   // scale (sbrt:1953-1975), then either store the estimate or the OP ratio
@@ -459,7 +485,7 @@ __global__ void __launch_bounds__(kFpMaxWarps * 32, 1) fp_kernel(DevGeom g, cons
   const size_t qbase = (size_t)x * g.pplanes;
   const int sg = tk.seg;
 #pragma unroll
-  for (int j = 0; j < kFpPlanes; j++) {
+  for (int j = 0; j < PL; j++) {
     if (j >= tk.n) continue;
     const int r = tk.p0 + j, yr = g.ybot[sg] + r;
     const float sc = (sg == 0) ? g.y_size : g.rescale[gg * g.nz + yr];
@@ -534,15 +560,26 @@ __device__ __forceinline__ void store_lane(float *__restrict__ dst, const Q2 (&s
   }
 }
 
-template <int KB, bool ACC = false>
+template <int KB, bool ACC = false, bool MULTI = false>
 __global__ void __launch_bounds__(256, 3) bp_kernel(DevGeom g, const float4 *__restrict__ in, long long in_pair_stride,
                                                  const QuadWork *__restrict__ work, float *__restrict__ bc,
-                                                 float *__restrict__ br, long long vol, int view0 = 0, int x0 = 0) {
+                                                 float *__restrict__ br, long long vol, FrameStrides fr,
+                                                 int view0 = 0, int x0 = 0) {
   extern __shared__ float4 P[];  // [bp_splanes]: segments with kBpPad zero planes each side
   // ACC: one view pair, quads x0 + blockIdx.x, both partial sums added into bc
   // (each voxel receives exactly two terms, so the atomic adds onto a zeroed
   // buffer give a + b whatever their order)
-  const QuadWork w = ACC ? QuadWork{0, (int16_t)(x0 + blockIdx.x), (int16_t)view0, 0} : work[blockIdx.x];
+  // MULTI: several frames per launch (one frame: the frame arithmetic is
+  // compiled out, which keeps the single-frame kernel free of spills)
+  int item = blockIdx.x;
+  if (MULTI) {
+    const int nwork = gridDim.x / fr.n, frame = blockIdx.x / nwork;
+    item = blockIdx.x - frame * nwork;
+    in += (size_t)frame * fr.ratio / 4;
+    bc += (size_t)frame * fr.bc;
+    br += (size_t)frame * fr.bc;
+  }
+  const QuadWork w = ACC ? QuadWork{0, (int16_t)(x0 + blockIdx.x), (int16_t)view0, 0} : work[item];
   const int x = w.x, N = g.nx, c = g.c, zp = g.zp, G = g.groupmax;
   const bool masked = g.nzmask[w.view * g.nquads + x] == 0;
   const float4 *src = in + (size_t)w.slot * in_pair_stride + (size_t)x * g.pplanes;
@@ -650,9 +687,13 @@ __global__ void __launch_bounds__(256, 3) bp_kernel(DevGeom g, const float4 *__r
 template <int KB>
 __global__ void __launch_bounds__(256, 2) adj_kernel(DevGeom g, const float4 *__restrict__ in, long long in_pair_stride,
                                                   const QuadWork *__restrict__ work, float *__restrict__ bc,
-                                                  float *__restrict__ br, long long vol) {
+                                                  float *__restrict__ br, long long vol, FrameStrides fr) {
   extern __shared__ float4 P[];
-  const QuadWork w = work[blockIdx.x];
+  const int nwork = gridDim.x / fr.n, frame = blockIdx.x / nwork, item = blockIdx.x - frame * nwork;
+  const QuadWork w = work[item];
+  in += (size_t)frame * fr.ratio / 4;
+  bc += (size_t)frame * fr.bc;
+  br += (size_t)frame * fr.bc;
   const int x = w.x, N = g.nx, c = g.c, zp = g.zp, G = g.groupmax, ZS = g.zshift, nz = g.nz;
   const int FS = G * 2 * ZS;
   const bool masked = g.nzmask[w.view * g.nquads + x] == 0 || g.cyl0[x] == g.cyl1[x];
@@ -781,8 +822,14 @@ template <int MODE>
 __global__ void __launch_bounds__(256) adj_rotate_kernel(DevGeom g, const int *__restrict__ pair_views, int npairs,
                                                          const float *__restrict__ bc, const float *__restrict__ br,
                                                          long long vol, float *__restrict__ image,
-                                                         float *__restrict__ nf_inv, float *__restrict__ out) {
+                                                         float *__restrict__ nf_inv, float *__restrict__ out,
+                                                         FrameStrides fr) {
   const int nq = g.zp / 4, N = g.nx, c = g.c;
+  if (MODE == 0) {
+    image += (size_t)(fr.map ? __ldg(fr.map + blockIdx.y) : (int)blockIdx.y) * fr.image;
+    bc += (size_t)blockIdx.y * fr.bc;
+    br += (size_t)blockIdx.y * fr.bc;
+  }
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int col = (int)(t / nq), q = (int)(t - (long long)col * nq);
   int i, j;
@@ -860,8 +907,14 @@ template <int MODE>
 __global__ void __launch_bounds__(256) rotback_kernel(DevGeom g, const int *__restrict__ pair_views, int npairs,
                                                       const float *__restrict__ bc, const float *__restrict__ br,
                                                       long long vol, float *__restrict__ image,
-                                                      float *__restrict__ nf_inv, float *__restrict__ corr_out) {
+                                                      float *__restrict__ nf_inv, float *__restrict__ corr_out,
+                                                      FrameStrides fr) {
   const int nq = g.zp / 4;
+  if (MODE == 0) {
+    image += (size_t)(fr.map ? __ldg(fr.map + blockIdx.y) : (int)blockIdx.y) * fr.image;
+    bc += (size_t)blockIdx.y * fr.bc;
+    if (br != nullptr) br += (size_t)blockIdx.y * fr.bc;
+  }
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int col = (int)(t / nq), q = (int)(t - (long long)col * nq);
   if (col >= g.fov_columns) return;
@@ -1023,8 +1076,11 @@ __global__ void init_image_kernel(DevGeom g, float *__restrict__ image) {
 
 // post-iteration pass (drv:4288-4297) with an FP64 sum, deterministic:
 // per-block partial sums, then one block adds them in order.
-__global__ void post_iter_kernel(DevGeom g, float *__restrict__ image, double *__restrict__ partial) {
+__global__ void post_iter_kernel(DevGeom g, float *__restrict__ image, double *__restrict__ partial,
+                                 FrameStrides fr) {
   __shared__ double red[256];
+  image += (size_t)(fr.map ? __ldg(fr.map + blockIdx.y) : (int)blockIdx.y) * fr.image;
+  partial += (size_t)blockIdx.y * fr.partial;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int nz = g.z_max - g.z_min;
   double s = 0.0;
@@ -1046,8 +1102,11 @@ __global__ void post_iter_kernel(DevGeom g, float *__restrict__ image, double *_
 }
 // One block: each thread sums a contiguous run of partials, then a fixed
 // tree adds the runs -- the same order on every call (deterministic).
-__global__ void sum_partials_kernel(const double *__restrict__ partial, int n, double *__restrict__ out) {
+__global__ void sum_partials_kernel(const double *__restrict__ partial, int n, double *__restrict__ out,
+                                    long long frame_stride, const int *__restrict__ map) {
   __shared__ double red[1024];
+  partial += (size_t)blockIdx.x * frame_stride;
+  out += map ? map[blockIdx.x] : (int)blockIdx.x;
   const int t = threadIdx.x, T = blockDim.x;
   const int per = (n + T - 1) / T, b = t * per, e = min(b + per, n);
   double s = 0.0;
@@ -1141,84 +1200,119 @@ __global__ void scale_pairs_kernel(DevGeom g, const T *__restrict__ src, const i
   dst[(size_t)slot * dst_pair_stride + i] = o;
 }
 
-template <int MODE, typename PT, typename AT>
+template <int MODE, int PL, int MW, typename PT, typename AT>
 cudaError_t launch_fp_t(const DevGeom &g, const float *image, const QuadWork *work, int nwork, const void *prompts,
-                        const void *add, float *out, long long out_pair_stride, cudaStream_t st) {
+                        const void *add, float *out, long long out_pair_stride, int pwarps_req,
+                        const FrameStrides &fr, cudaStream_t st) {
   // consumer warps: one task per thread; producer warps: enough to keep the
   // sampled rows ahead of the consumers (a row is ~2*zp bilinear quads)
   const int cwarps = (g.nfptasks + 31) / 32;
-  const int pwarps = min(6, max(2, kFpMaxWarps - cwarps));
-  if (cwarps + pwarps > kFpMaxWarps) return cudaErrorInvalidConfiguration;
+  const int pwarps = pwarps_req > 0 ? pwarps_req : min(6, max(2, MW - cwarps));
+  if (pwarps < 2 || cwarps + pwarps > MW) return cudaErrorInvalidConfiguration;
   const int threads = (cwarps + pwarps) * 32;
   const int ZS = g.zp + kFpZPad;
-  const size_t smem = (size_t)(2 * 8 * 2 + 2) * 2 * g.zp * sizeof(float) + (size_t)5 * ZS * sizeof(float4);
-  auto k = fp_kernel<MODE, PT, AT>;
+  const size_t smem =
+      (size_t)(kFpSlots * 8 * 2 + 2) * 2 * g.zp * sizeof(float) + (size_t)(2 * kFpSlots + 1) * ZS * sizeof(float4);
+  auto k = fp_kernel<MODE, PL, MW, PT, AT>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  k<<<nwork, threads, smem, st>>>(g, image, work, (const PT *)prompts, (const AT *)add,
-                                  reinterpret_cast<float4 *>(out), out_pair_stride / 4, pwarps);
+  k<<<(unsigned)nwork * fr.n, threads, smem, st>>>(g, image, work, (const PT *)prompts, (const AT *)add,
+                                                   reinterpret_cast<float4 *>(out), out_pair_stride / 4, pwarps, fr);
   return cudaGetLastError();
 }
 
-cudaError_t launch_fp_any(const DevGeom &g, const float *image, const QuadWork *work, int nwork, int mode,
-                          const void *prompts, const void *add, int storage, float *out, long long stride,
-                          cudaStream_t st) {
-  if (mode == 0) return launch_fp_t<0, int16_t, float>(g, image, work, nwork, nullptr, nullptr, out, stride, st);
-  if (storage == 0) return launch_fp_t<1, int16_t, float>(g, image, work, nwork, prompts, add, out, stride, st);
-  return launch_fp_t<1, __half, __nv_bfloat16>(g, image, work, nwork, prompts, add, out, stride, st);
+template <int PL, int MW>
+cudaError_t launch_fp_pl(const DevGeom &g, const float *image, const QuadWork *work, int nwork, int mode,
+                         const void *prompts, const void *add, int storage, float *out, long long stride, int pwarps,
+                         const FrameStrides &fr, cudaStream_t st) {
+  if (mode == 0)
+    return launch_fp_t<0, PL, MW, int16_t, float>(g, image, work, nwork, nullptr, nullptr, out, stride, pwarps, fr,
+                                                  st);
+  if (storage == 0)
+    return launch_fp_t<1, PL, MW, int16_t, float>(g, image, work, nwork, prompts, add, out, stride, pwarps, fr, st);
+  return launch_fp_t<1, PL, MW, __half, __nv_bfloat16>(g, image, work, nwork, prompts, add, out, stride, pwarps, fr,
+                                                       st);
 }
 
 }  // namespace
 
 cudaError_t launch_fp(const DevGeom &g, const float *image, const QuadWork *work, int nwork, int mode,
                       const void *prompts, const void *add, int storage, float *out, long long out_pair_stride,
-                      int tasks_per_thread, cudaStream_t st) {
-  if (nwork <= 0) return cudaSuccess;
-  (void)tasks_per_thread;
-  return launch_fp_any(g, image, work, nwork, mode, prompts, add, storage, out, out_pair_stride, st);
+                      const ProjTune &tune, const FrameStrides &fr, cudaStream_t st) {
+  if (nwork <= 0 || fr.n <= 0) return cudaSuccess;
+  static_assert(kFpPlaneVariants[0] == 7 && kFpPlaneVariants[1] == 9 && kFpPlaneVariants[2] == 11, "variants");
+  const int pl = tune.fp_planes > 0 ? tune.fp_planes : kFpPlanes;
+  switch (pl) {
+    case 7:
+      return launch_fp_pl<7, kFpVariantWarps[0]>(g, image, work, nwork, mode, prompts, add, storage, out,
+                                                 out_pair_stride, tune.fp_pwarps, fr, st);
+    case 9:
+      return launch_fp_pl<9, kFpVariantWarps[1]>(g, image, work, nwork, mode, prompts, add, storage, out,
+                                                 out_pair_stride, tune.fp_pwarps, fr, st);
+    case 11:
+      return launch_fp_pl<11, kFpVariantWarps[2]>(g, image, work, nwork, mode, prompts, add, storage, out,
+                                                  out_pair_stride, tune.fp_pwarps, fr, st);
+    default:
+      return cudaErrorInvalidValue;
+  }
 }
 
-cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
-                      float *bc, float *br, long long vol, cudaStream_t st) {
-  if (nwork <= 0) return cudaSuccess;
-  static_assert(kBpPad >= kBpZ, "a straddling window must stay inside the zero planes");
+template <int KB>
+cudaError_t launch_bp_t(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
+                        float *bc, float *br, long long vol, const FrameStrides &fr, cudaStream_t st) {
+  static_assert(kBpPad >= KB, "a straddling window must stay inside the zero planes");
   const size_t smem = (size_t)g.bp_splanes * sizeof(float4);
-  auto k = bp_kernel<kBpZ>;
+  auto k = fr.n > 1 ? bp_kernel<KB, false, true> : bp_kernel<KB, false, false>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  k<<<nwork, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(in), in_pair_stride / 4, work, bc, br, vol, 0, 0);
+  k<<<(unsigned)nwork * fr.n, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(in), in_pair_stride / 4, work, bc,
+                                               br, vol, fr, 0, 0);
   return cudaGetLastError();
 }
 
+cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
+                      float *bc, float *br, long long vol, const ProjTune &tune, const FrameStrides &fr,
+                      cudaStream_t st) {
+  if (nwork <= 0 || fr.n <= 0) return cudaSuccess;
+  const int kb = tune.bp_planes > 0 ? tune.bp_planes : kBpZ;
+  if (kb == 8) return launch_bp_t<8>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, st);
+  if (kb == 4) return launch_bp_t<4>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, st);
+  return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_adj(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
-                       float *bc, float *br, long long vol, cudaStream_t st) {
-  if (nwork <= 0) return cudaSuccess;
+                       float *bc, float *br, long long vol, const FrameStrides &fr, cudaStream_t st) {
+  if (nwork <= 0 || fr.n <= 0) return cudaSuccess;
   const size_t smem = (size_t)g.bp_splanes * sizeof(float4);
   auto k = adj_kernel<kBpZ>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  k<<<nwork, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(in), in_pair_stride / 4, work, bc, br, vol);
+  k<<<(unsigned)nwork * fr.n, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(in), in_pair_stride / 4, work, bc,
+                                               br, vol, fr);
   return cudaGetLastError();
 }
 
 cudaError_t launch_adj_rotate(const DevGeom &g, const int *pair_views, int npairs, const float *bc, const float *br,
-                              long long vol, float *image, float *nf_inv, float *out, int mode, cudaStream_t st) {
+                              long long vol, float *image, float *nf_inv, float *out, int mode,
+                              const FrameStrides &fr, cudaStream_t st) {
+  if (fr.n <= 0) return cudaSuccess;
+  if (mode != 0 && fr.n != 1) return cudaErrorInvalidValue;
   const long long cols = (mode == 2) ? (long long)g.nx * g.nx : (long long)g.fov_columns;
   const long long n = cols * (g.zp / 4);
   const int threads = 256;
-  const unsigned blocks = (unsigned)((n + threads - 1) / threads);
+  const dim3 blocks((unsigned)((n + threads - 1) / threads), fr.n);
   if (mode == 0)
-    adj_rotate_kernel<0><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, out);
+    adj_rotate_kernel<0><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, out, fr);
   else if (mode == 1)
-    adj_rotate_kernel<1><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, out);
+    adj_rotate_kernel<1><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, out, fr);
   else
-    adj_rotate_kernel<2><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, out);
+    adj_rotate_kernel<2><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, out, fr);
   return cudaGetLastError();
 }
 
@@ -1231,21 +1325,25 @@ cudaError_t launch_bp_sum(const DevGeom &g, const float *quad, int view, int x0,
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  k<<<nquads, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(quad), 0, nullptr, out, out, 0, view, x0);
+  k<<<nquads, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(quad), 0, nullptr, out, out, 0, one_frame(), view,
+                               x0);
   return cudaGetLastError();
 }
 
 cudaError_t launch_rotback(const DevGeom &g, const int *pair_views, int npairs, const float *bc, const float *br,
-                           long long vol, float *image, float *nf_inv, float *corr_out, int mode, cudaStream_t st) {
+                           long long vol, float *image, float *nf_inv, float *corr_out, int mode,
+                           const FrameStrides &fr, cudaStream_t st) {
+  if (fr.n <= 0) return cudaSuccess;
+  if (mode != 0 && fr.n != 1) return cudaErrorInvalidValue;
   const long long n = (long long)g.fov_columns * (g.zp / 4);
   const int threads = 256;
-  const unsigned blocks = (unsigned)((n + threads - 1) / threads);
+  const dim3 blocks((unsigned)((n + threads - 1) / threads), fr.n);
   if (mode == 0)
-    rotback_kernel<0><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, corr_out);
+    rotback_kernel<0><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, corr_out, fr);
   else if (mode == 1)
-    rotback_kernel<1><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, corr_out);
+    rotback_kernel<1><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, corr_out, fr);
   else
-    rotback_kernel<2><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, corr_out);
+    rotback_kernel<2><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, corr_out, fr);
   return cudaGetLastError();
 }
 
@@ -1333,11 +1431,14 @@ cudaError_t launch_init_image(const DevGeom &g, float *image, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_post_iteration(const DevGeom &g, float *image, double *partial, double *sum, cudaStream_t st) {
+cudaError_t launch_post_iteration(const DevGeom &g, float *image, double *partial, double *sum,
+                                  const FrameStrides &fr, cudaStream_t st) {
+  if (fr.n <= 0) return cudaSuccess;
   const long long n = (long long)g.fov_columns * (g.z_max - g.z_min);
   const int blocks = (int)((n + 255) / 256);
-  post_iter_kernel<<<blocks, 256, 0, st>>>(g, image, partial);
-  sum_partials_kernel<<<1, 1024, 0, st>>>(partial, blocks, sum);
+  if (fr.n > 1 && fr.partial < blocks) return cudaErrorInvalidValue;
+  post_iter_kernel<<<dim3(blocks, fr.n), 256, 0, st>>>(g, image, partial, fr);
+  sum_partials_kernel<<<fr.n, 1024, 0, st>>>(partial, blocks, sum, fr.partial, fr.map);
   return cudaGetLastError();
 }
 

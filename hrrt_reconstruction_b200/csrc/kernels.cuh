@@ -23,14 +23,11 @@
 
 namespace hrrt {
 
-#ifndef HRRT_FP_PLANES
-#define HRRT_FP_PLANES 9
+#ifndef HRRT_FP_SLOTS
+#define HRRT_FP_SLOTS 3
 #endif
-#ifndef HRRT_FP_MAX_WARPS
-#define HRRT_FP_MAX_WARPS 32
-#endif
-constexpr int kFpPlanes = HRRT_FP_PLANES;     // planes per forward-projection task (odd: bank-conflict free)
-constexpr int kFpMaxWarps = HRRT_FP_MAX_WARPS;  // warps per forward-projection CTA (consumers + producers)
+constexpr int kFpPlanes = 9;                   // default planes per forward-projection task (odd: bank-conflict free)
+constexpr int kFpSlots = HRRT_FP_SLOTS;       // sampled rows in flight between producers and consumers
 constexpr int kFpZPad = 16;     // zeroed entries after each sampled row
 constexpr int kFpEndPlanes = 4; // planes per end-plane task (they cost ~2x a middle plane)
 constexpr int kBpZ = 8;         // z per back-projection task
@@ -39,7 +36,7 @@ constexpr int kBpPad = 8;       // zero planes on each side of a segment in the 
 struct FpTask {
   int16_t seg;   // segment (internal = file order)
   int16_t p0;    // first plane, relative to the segment's yr_bottom
-  int16_t n;     // planes in this task (<= kFpPlanes)
+  int16_t n;     // planes in this task (<= the launch's plane variant)
   int16_t type;  // 0: segment 0, 1: oblique middle planes, 2: oblique end planes
 };
 
@@ -87,23 +84,58 @@ struct QuadWork {  // one (view pair slot, quad) work item
   int16_t pad;
 };
 
+// Frames of a dynamic study batched into one launch.  Frame f of a launch
+// reads and writes its own buffers at f times these strides from frame 0's;
+// the geometry, the work list and the inverse sensitivity are shared.  The
+// projector kernels run the work list once per frame, frame-major (CTA i is
+// item i % nwork of frame i / nwork: one frame's image stays in L2 while its
+// CTAs run, and the next frame's CTAs fill the last wave of the previous);
+// the image-domain kernels take the frame from blockIdx.y.
+// Images, inputs and image sums belong to stored frames, launch frame f being
+// stored frame map[f] (map null: f); the scratch (ratio, partials, partial
+// sums) belongs to the launch frame.
+struct FrameStrides {
+  int n;              // frames in the launch
+  const int *map;     // [n] stored frame of each launch frame (device), or null
+  long long image;    // floats between stored images
+  long long input;    // elements between stored prompts (and additive-term) arrays
+  long long ratio;    // floats between ratio blocks ([pair slot][quad_pair])
+  long long bc;       // floats between back-projection partial blocks (Bc and Br alike)
+  long long partial;  // doubles between post-iteration partial-sum arrays
+};
+inline FrameStrides one_frame() { return FrameStrides{1, nullptr, 0, 0, 0, 0, 0}; }
+
+// launch shape of the projectors (results do not depend on it)
+struct ProjTune {
+  int fp_planes;  // planes per forward-projection task: 7, 9 or 11 (0: kFpPlanes)
+  int fp_pwarps;  // producer warps of the forward projector (0: as many as fit, 2..6)
+  int bp_planes;  // planes per back-projection task: 4 or 8 (0: kBpZ)
+};
+inline ProjTune default_tune() { return ProjTune{0, 0, 0}; }
+constexpr int kFpPlaneVariants[3] = {7, 9, 11};
+// warps per forward-projection CTA for each plane variant (register budget)
+constexpr int kFpVariantWarps[3] = {32, 32, 24};
+
 // ---- launchers (kernels.cu) ----
 // forward projection of the pairs listed in `work` (mode 0: write est*scale into
 // `out`; mode 1: write ratio*bp_scale using prompts/add at their global pair).
+// `g.fptasks` must be the task list built for tune.fp_planes.
 cudaError_t launch_fp(const DevGeom &g, const float *image, const QuadWork *work, int nwork, int mode,
                       const void *prompts, const void *add, int storage, float *out, long long out_pair_stride,
-                      int tasks_per_thread, cudaStream_t st);
+                      const ProjTune &tune, const FrameStrides &fr, cudaStream_t st);
 // back projection of quad-layout input into the column (Bc) / row (Br) partials
 cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
-                      float *bc, float *br, long long vol, cudaStream_t st);
+                      float *bc, float *br, long long vol, const ProjTune &tune, const FrameStrides &fr,
+                      cudaStream_t st);
 // exact adjoint of the forward projector: z-transpose into the column / row
 // partials (rows scaled as the forward projector scales them)
 cudaError_t launch_adj(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
-                       float *bc, float *br, long long vol, cudaStream_t st);
+                       float *bc, float *br, long long vol, const FrameStrides &fr, cudaStream_t st);
 // bilinear-sampling transpose of the partials of every pair; mode 0: OSEM
 // update, 1: inverse sensitivity (FOV columns), 2: out += (every column)
 cudaError_t launch_adj_rotate(const DevGeom &g, const int *pair_views, int npairs, const float *bc, const float *br,
-                              long long vol, float *image, float *nf_inv, float *out, int mode, cudaStream_t st);
+                              long long vol, float *image, float *nf_inv, float *out, int mode,
+                              const FrameStrides &fr, cudaStream_t st);
 // back projection of one view pair's quad-layout input (quads x0..x0+nquads-1)
 // with both partial sums added atomically into `out` (zeroed by the caller)
 cudaError_t launch_bp_sum(const DevGeom &g, const float *quad, int view, int x0, int nquads, float *out,
@@ -111,7 +143,8 @@ cudaError_t launch_bp_sum(const DevGeom &g, const float *quad, int view, int x0,
 // corr = sum over pairs of rotate-back(Bc+Br); mode 0: OSEM update of image with
 // nf_inv; mode 1: write the inverse sensitivity into nf_inv; mode 2: corr_out += corr
 cudaError_t launch_rotback(const DevGeom &g, const int *pair_views, int npairs, const float *bc, const float *br,
-                           long long vol, float *image, float *nf_inv, float *corr_out, int mode, cudaStream_t st);
+                           long long vol, float *image, float *nf_inv, float *corr_out, int mode,
+                           const FrameStrides &fr, cudaStream_t st);
 cudaError_t launch_rotpos(const DevGeom &g, float2 *rotpos, const int *row_start, cudaStream_t st);
 cudaError_t launch_prep(const DevGeom &g, int nbins, const int16_t *prompts, const float *randoms, const float *norm,
                         const float *atten, const float *scatter, int npskip, float eps2, int storage, void *q_prompts,
@@ -127,7 +160,9 @@ cudaError_t launch_finish_mask(const DevGeom &g, const int *accum, int16_t *nzma
 // [z][y][x] image of SaveImage (FOV columns, planes < nz) from [x][y][zp]
 cudaError_t launch_image_zyx(const DevGeom &g, const float *image, float *out, cudaStream_t st);
 cudaError_t launch_init_image(const DevGeom &g, float *image, cudaStream_t st);
-cudaError_t launch_post_iteration(const DevGeom &g, float *image, double *partial, double *sum, cudaStream_t st);
+// per launch frame f: threshold of its image, the FP64 sum into sum[stored frame]
+cudaError_t launch_post_iteration(const DevGeom &g, float *image, double *partial, double *sum,
+                                  const FrameStrides &fr, cudaStream_t st);
 int post_iteration_blocks(const DevGeom &g);
 // copy the quad-layout 1/(NA) of `npairs` view pairs into f32 scratch, times
 // the back projector's segment weight (sbrt:1637-1649 applied in place there)

@@ -223,6 +223,74 @@ int hrrt_kernel_stats(hrrt_ctx *ctx, const char *kernel, int *launches, double *
 int hrrt_reset_kernel_stats(hrrt_ctx *ctx);
 
 /* ------------------------------------------------------------------------ */
+/* Launch shapes of the projectors (no counterpart in the reference)         */
+/* ------------------------------------------------------------------------ */
+
+/* Results are bit-identical for every shape; only the time changes. */
+typedef struct hrrt_tuning {
+  int fp_planes;          /* planes per forward-projection task: 7, 9 or 11 (0: 9) */
+  int fp_producer_warps;  /* sampling warps of the forward projector: 2..6 (0: as many as fit) */
+  int bp_planes;          /* planes per back-projection task: 4 or 8 (0: 8) */
+  double fp_ms, bp_ms;    /* filled by the tuners: the chosen shapes' device time per launch */
+} hrrt_tuning;
+
+int hrrt_set_tuning(hrrt_ctx *ctx, const hrrt_tuning *t);
+int hrrt_get_tuning(hrrt_ctx *ctx, hrrt_tuning *t);
+/* Time every shape this geometry admits on the context's current inputs and
+ * image (the forward projection and back projection of the first subset,
+ * `repeats` launches each; the image is not changed) and keep the fastest. */
+int hrrt_autotune(hrrt_ctx *ctx, int repeats, hrrt_tuning *chosen);
+
+/* ------------------------------------------------------------------------ */
+/* Dynamic studies: frames sharing one normalisation and attenuation         */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * Replaces the frame loop of main (hrrt_osem3d_span3.cpp:4555-4597: the
+ * sensitivity once, then per frame PrepareOsem3dFiles, Init_Image,
+ * CalculateOsem3d(frame), SaveImage; frames found by get_num_frames,
+ * hrrt_osem_utils.cpp:39-64).  Here every frame has its own iteration count,
+ * and the frames are reconstructed together: each projector launch covers a
+ * group of frames (as many as device memory allows, frames with more
+ * iterations first), and one iteration of a group -- every subset's
+ * projection, back projection and update, and the post-iteration pass -- is
+ * one CUDA graph, captured once per (group, active frames) and replayed.  Each
+ * frame's image equals what hrrt_upload_inputs + hrrt_sensitivity +
+ * hrrt_init_image + hrrt_osem(iterations) give for it alone (bit-identical).
+ *
+ * A batch uses its context's geometry, back projector, launch shape and
+ * sensitivity images: creating it replaces the context's inputs (single-frame
+ * calls need hrrt_upload_inputs again).  The context must outlive the batch.
+ */
+typedef struct hrrt_batch hrrt_batch;
+
+typedef struct hrrt_batch_stats {
+  double ms_total;        /* device time of hrrt_batch_run */
+  int subset_iterations;  /* summed over the frames */
+  int groups;             /* frame groups (launches cover one group) */
+  int graphs;             /* CUDA graphs captured */
+  int graph_launches;     /* graph replays (one per iteration of a group) */
+  long long kernel_launches; /* kernels run by those replays */
+} hrrt_batch_stats;
+
+/* norm / atten: flat-file arrays shared by every frame (NULL = 1), copied to
+ * the device; storage: HRRT_STORE_F32 or HRRT_STORE_16. */
+int hrrt_batch_create(hrrt_ctx *ctx, int nframes, int storage, const float *norm, const float *atten,
+                      hrrt_batch **out);
+void hrrt_batch_destroy(hrrt_batch *b);
+/* The inputs of one frame (prepared at once; the host arrays are not kept) and
+ * its iteration count (>= 1). */
+int hrrt_batch_set_frame(hrrt_batch *b, int frame, const int16_t *prompts, const float *randoms,
+                         const float *scatter, int iterations);
+/* hrrt_autotune with the batch's launches (a whole group of frames). */
+int hrrt_batch_autotune(hrrt_batch *b, int repeats, hrrt_tuning *chosen);
+/* Reconstruct every frame (each from the uniform initial image). */
+int hrrt_batch_run(hrrt_batch *b, hrrt_batch_stats *stats);
+/* Frame image in the SaveImage layout [z][y][x]; sum_image (may be NULL): the
+ * FP64 image sum of its last post-iteration pass. */
+int hrrt_batch_get_image(hrrt_batch *b, int frame, float *image_zyx, double *sum_image);
+
+/* ------------------------------------------------------------------------ */
 /* Listmode (64-bit HRRT events) to span-3 / span-9 sinograms               */
 /* ------------------------------------------------------------------------ */
 
@@ -238,9 +306,9 @@ int hrrt_reset_kernel_stats(hrrt_ctx *ctx);
 #define HRRT_LM_IGNORE_BORDER_CRYSTAL 1
 #define HRRT_LM_NO_DOI 2
 #define HRRT_LM_TIME_FROM_COUNT 4
-/* implementation choice (same result): streams of 16 Mi words or more are
- * histogrammed through 64 MB partitions that stay in L2, shorter ones with
- * atomics straight into the sinograms; these flags force one or the other */
+/* implementation choice (same result): by default events are added with
+ * atomics straight into the sinograms; FORCE_PARTITIONED scatters them by
+ * 64 MB partition first and adds each partition in L2 (slower on B200) */
 #define HRRT_LM_FORCE_DIRECT 16
 #define HRRT_LM_FORCE_PARTITIONED 32
 
