@@ -16,12 +16,13 @@ import os
 
 import numpy as np
 
-__all__ = ["Geometry", "HrrtError", "Context", "Batch", "Tuning", "Listmode", "lib", "LIB_PATH", "STORE_F32", "STORE_16", "BP_REF", "BP_ADJOINT",
+__all__ = ["Geometry", "HrrtError", "Context", "Batch", "Tuning", "Listmode", "lib", "LIB_PATH", "STORE_F32", "STORE_16", "STORE_F16", "BP_REF", "BP_ADJOINT",
            "geometry_table", "hrrt_geometry"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libhrrt_gpu.so")
 STORE_F32 = 0
-STORE_16 = 1
+STORE_16 = 1   # bf16 additive and multiplicative terms
+STORE_F16 = 2  # fp16 additive and multiplicative terms
 BP_REF = 0
 BP_ADJOINT = 1
 
@@ -66,7 +67,7 @@ class LmStats(ctypes.Structure):
 class Tuning(ctypes.Structure):
     """hrrt_tuning: launch shape of the projectors (results do not depend on it)."""
     _fields_ = [("fp_planes", ctypes.c_int), ("fp_producer_warps", ctypes.c_int), ("bp_planes", ctypes.c_int),
-                ("fp_ms", ctypes.c_double), ("bp_ms", ctypes.c_double)]
+                ("bp_threads", ctypes.c_int), ("fp_ms", ctypes.c_double), ("bp_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -368,8 +369,8 @@ class Context:
         return co
 
     # ---- timing ----
-    def set_tuning(self, fp_planes=0, fp_producer_warps=0, bp_planes=0):
-        t = Tuning(fp_planes, fp_producer_warps, bp_planes, 0.0, 0.0)
+    def set_tuning(self, fp_planes=0, fp_producer_warps=0, bp_planes=0, bp_threads=0):
+        t = Tuning(fp_planes, fp_producer_warps, bp_planes, bp_threads, 0.0, 0.0)
         self._check(lib.hrrt_set_tuning(self._h, ctypes.byref(t)), "set_tuning")
 
     def get_tuning(self):

@@ -142,9 +142,10 @@ int autotune(hrrt_ctx *ctx, const SubsetBufs &bb, int repeats, hrrt_tuning *chos
   }
   if (int rc = apply_tune(ctx, best)) return rc;
   if (!adj) {
-    for (int kb : {8, 4}) {
+    for (int i = 0; i < 4; i++) {
       ProjTune t = best;
-      t.bp_planes = kb;
+      t.bp_planes = (i & 1) ? 4 : 8;
+      t.bp_threads = (i & 2) ? 384 : 256;
       double ms = 0;
       int rc = time_launch(ctx, repeats, [&] {
         return launch_bp(ctx->dg, bb.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], bb.bc, bb.br, ctx->vol, t, bb.fr,
@@ -153,7 +154,8 @@ int autotune(hrrt_ctx *ctx, const SubsetBufs &bb, int repeats, hrrt_tuning *chos
       if (rc) return rc;
       if (ms < best_bp) {
         best_bp = ms;
-        best.bp_planes = kb;
+        best.bp_planes = t.bp_planes;
+        best.bp_threads = t.bp_threads;
       }
     }
   } else {
@@ -164,6 +166,7 @@ int autotune(hrrt_ctx *ctx, const SubsetBufs &bb, int repeats, hrrt_tuning *chos
     chosen->fp_planes = best.fp_planes;
     chosen->fp_producer_warps = best.fp_pwarps;
     chosen->bp_planes = best.bp_planes;
+    chosen->bp_threads = best.bp_threads;
     chosen->fp_ms = best_fp;
     chosen->bp_ms = best_bp;
   }
@@ -262,7 +265,7 @@ extern "C" {
 
 int hrrt_set_tuning(hrrt_ctx *ctx, const hrrt_tuning *t) {
   if (!ctx || !t) return HRRT_ERR_ARG;
-  return apply_tune(ctx, ProjTune{t->fp_planes, t->fp_producer_warps, t->bp_planes});
+  return apply_tune(ctx, ProjTune{t->fp_planes, t->fp_producer_warps, t->bp_planes, t->bp_threads});
 }
 
 int hrrt_get_tuning(hrrt_ctx *ctx, hrrt_tuning *t) {
@@ -271,6 +274,7 @@ int hrrt_get_tuning(hrrt_ctx *ctx, hrrt_tuning *t) {
   t->fp_planes = ctx->tune.fp_planes > 0 ? ctx->tune.fp_planes : kFpPlanes;
   t->fp_producer_warps = ctx->tune.fp_pwarps;
   t->bp_planes = ctx->tune.bp_planes > 0 ? ctx->tune.bp_planes : kBpZ;
+  t->bp_threads = ctx->tune.bp_threads;
   return HRRT_OK;
 }
 
@@ -287,7 +291,7 @@ int hrrt_batch_create(hrrt_ctx *ctx, int nframes, int storage, const float *norm
   if (!ctx || !out) return HRRT_ERR_ARG;
   *out = nullptr;
   if (nframes < 1) return fail(ctx, HRRT_ERR_ARG, "batch: nframes must be >= 1");
-  if (storage != HRRT_STORE_F32 && storage != HRRT_STORE_16) return fail(ctx, HRRT_ERR_ARG, "unknown storage");
+  if (storage < HRRT_STORE_F32 || storage > HRRT_STORE_F16) return fail(ctx, HRRT_ERR_ARG, "unknown storage");
   if (ctx->batch) return fail(ctx, HRRT_ERR_STATE, "batch: the context already serves a batch");
   if (int rc = ensure_input_buffers(ctx, storage)) return rc;
   const Geometry &g = ctx->geo;

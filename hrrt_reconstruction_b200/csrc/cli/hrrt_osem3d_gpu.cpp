@@ -51,6 +51,7 @@ void usage() {
                "  -p  3D flat integer (int16) prompt scan; -Q: float prompt scan of integer counts\n"
                "  -d  3D flat float delayed (smoothed randoms)\n"
                "  -n  3D flat normalisation, -a attenuation (span 9 accepted for span 3), -s scatter\n"
+               "      (3D, or the unscaled 2D segment followed by 2209 span-9 plane scale factors)\n"
                "  -o  output image (flat float [z][y][x] + .hdr), -O also after each iteration\n"
                "  -h  output the forward projection of the final image (flat float scan)\n");
 }
@@ -243,6 +244,52 @@ std::vector<float> expand_span9_atten(const std::vector<float> &a9, const hrrt_g
   return a3;
 }
 
+// 3D scatter from the unscaled 2D segment (nz planes) followed by the
+// span-9 per-plane scale factors (the s2DFlag file form, drv:4407-4421):
+// convert_s9_s3 (drv:1136-1162) turns the factors into span-3 ones, and
+// apply_scale_factors (drv:1169-1179) scales 2D plane yr_bottom+yr into
+// plane yr of each segment.  Both are restated as the reference runs them,
+// including convert_s9_s3's walk over the span-3 segments three at a time.
+std::vector<float> expand_scatter_2d(const std::vector<float> &file, const hrrt_geom &g, int nz, size_t plane) {
+  const long long tb = hrrt_geometry_table(&g, "segments", nullptr, 0);
+  if (tb <= 0) die("scatter: segment table");
+  std::vector<int> seg((size_t)tb / sizeof(int));
+  hrrt_geometry_table(&g, "segments", seg.data(), (size_t)tb);
+  const int nseg = (int)seg.size() / 3;
+  const int *yb = seg.data(), *yt = seg.data() + nseg, *off = seg.data() + 2 * nseg;
+  const int P = off[nseg - 1] + yt[nseg - 1] - yb[nseg - 1] + 1;
+  const int P9 = 2209;
+  const float *sc2d = file.data(), *sf9 = file.data() + (size_t)nz * plane;
+  std::vector<float> sf(P, 0.f);
+  if (g.span == 9) {
+    std::copy(sf9, sf9 + P9, sf.begin());
+  } else {
+    int i = 0, j = 0;
+    for (int th = 0; th < nseg; th += 3) {
+      int n = yt[th] - yb[th] + 1;
+      if (j + n > P9 || i + n > P) die("scatter: scale factors do not fit this span");
+      for (int p = 0; p < n; p++) sf[i++] = sf9[j++] / 3.0f;
+      for (int k = 1; k <= 2 && th + k < nseg; k++) {
+        const int so = yb[th + k] - yb[th + k - 1];
+        const int m = n - 2 * so;
+        if (m < 0 || i + m > P) die("scatter: scale factors do not fit this span");
+        std::memmove(&sf[i], &sf[i - n + so], (size_t)m * sizeof(float));
+        n = m;
+        i += n;
+      }
+    }
+  }
+  std::vector<float> out((size_t)P * plane);
+  for (int s = 0; s < nseg; s++)
+    for (int yr = 0; yr <= yt[s] - yb[s]; yr++) {
+      const float f = sf[off[s] + yr];
+      const float *src = sc2d + (size_t)(yb[s] + yr) * plane;
+      float *dst = out.data() + (size_t)(off[s] + yr) * plane;
+      for (size_t k = 0; k < plane; k++) dst[k] = src[k] * f;
+    }
+  return out;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -293,7 +340,16 @@ int main(int argc, char **argv) {
     if (file_size(p) != (long long)(nbins * 4)) die("%s: not a float scan of this span", p.c_str());
     return read_flat<float>(p, nbins);
   };
-  const std::vector<float> delayed = read_scan(o.delayed), norm = read_scan(o.norm), scatter = read_scan(o.scatter);
+  const std::vector<float> delayed = read_scan(o.delayed), norm = read_scan(o.norm);
+  std::vector<float> scatter;
+  if (!o.scatter.empty()) {
+    const size_t plane = (size_t)info.nviews * info.nbins;
+    const long long sz = file_size(o.scatter);
+    if (sz == (long long)((plane * info.nz + 2209) * 4))
+      scatter = expand_scatter_2d(read_flat<float>(o.scatter, plane * info.nz + 2209), g, info.nz, plane);
+    else
+      scatter = read_scan(o.scatter);
+  }
   std::vector<float> atten;
   if (!o.atten.empty()) {
     const long long sz = file_size(o.atten);

@@ -180,6 +180,7 @@ SubsetBufs ctx_bufs(hrrt_ctx *ctx);
 // fp -> bp (or the adjoint) -> rotate-back + update of subset s, on ctx->stream
 int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b);
 int device_status(hrrt_ctx *ctx);
+int range_status(hrrt_ctx *ctx);
 int ensure_input_buffers(hrrt_ctx *ctx, int storage);
 int build_work_lists(hrrt_ctx *ctx);
 int sens_subset(hrrt_ctx *ctx, int s);

@@ -108,6 +108,20 @@ int device_status(hrrt_ctx *ctx) {
   return HRRT_OK;
 }
 
+// reads (and clears) the fp16 range flag the input preparation sets
+int range_status(hrrt_ctx *ctx) {
+  int v = 0;
+  cudaError_t e = cudaMemcpyAsync(&v, ctx->dg.range_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "status");
+  if (v != 0) {
+    cudaMemsetAsync(ctx->dg.range_err, 0, sizeof(int), ctx->stream);
+    return fail(ctx, HRRT_ERR_ARG,
+                "an additive or multiplicative term exceeds the fp16 range (65504): use HRRT_STORE_16 or _F32");
+  }
+  return HRRT_OK;
+}
+
 int build_work_lists(hrrt_ctx *ctx) {
   const Geometry &g = ctx->geo;
   const int S = g.sp.subsets;
@@ -329,6 +343,7 @@ int upload_flat(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms, con
     cudaStreamSynchronize(ctx->stream);
     return cuda_fail(ctx, e, "upload_inputs");
   }
+  if (storage == HRRT_STORE_F16) return range_status(ctx);
   return HRRT_OK;
 }
 
@@ -344,6 +359,8 @@ int apply_tune(hrrt_ctx *ctx, const ProjTune &t) {
     return fail(ctx, HRRT_ERR_ARG, "tuning: producer warps out of range");
   if (t.bp_planes != 0 && t.bp_planes != 4 && t.bp_planes != 8)
     return fail(ctx, HRRT_ERR_ARG, "tuning: back-projection planes must be 4 or 8");
+  if (t.bp_threads != 0 && t.bp_threads != 256 && t.bp_threads != 384)
+    return fail(ctx, HRRT_ERR_ARG, "tuning: back-projection threads must be 256 or 384");
   ctx->tune = t;
   ctx->config_epoch++;
   ctx->dg.fptasks = ctx->dg_adj.fptasks = ctx->d_fptasks[vi];
@@ -561,6 +578,7 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
   d.bp_splanes = (int)bp_src.size();
   ctx->d_rowstart = dupload(ctx, rowstart, &e);
   d.err = dalloc<int>(ctx, 1, &e);
+  d.range_err = dalloc<int>(ctx, 1, &e);
   ctx->nzmask = g.norm_zero_mask;
   ctx->d_nzmask = dupload(ctx, ctx->nzmask, &e);
   d.nzmask = ctx->d_nzmask;
@@ -626,7 +644,7 @@ int hrrt_upload_inputs(hrrt_ctx *ctx, const int16_t *prompts, const float *rando
                        const float *atten, const float *scatter, int storage) {
   if (!ctx) return HRRT_ERR_ARG;
   if (!prompts || !randoms) return fail(ctx, HRRT_ERR_ARG, "prompts and randoms are required");
-  if (storage != HRRT_STORE_F32 && storage != HRRT_STORE_16) return fail(ctx, HRRT_ERR_ARG, "unknown storage");
+  if (storage < HRRT_STORE_F32 || storage > HRRT_STORE_F16) return fail(ctx, HRRT_ERR_ARG, "unknown storage");
   if (ctx->batch) return fail(ctx, HRRT_ERR_STATE, "the context serves a batch (hrrt_batch_destroy first)");
   if (int rc = ensure_input_buffers(ctx, storage)) return rc;
   if (int rc = upload_flat(ctx, prompts, randoms, norm, atten, scatter, storage, false, ctx->q_prompts, ctx->q_add,
@@ -730,7 +748,7 @@ int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms
   if (!ctx) return HRRT_ERR_ARG;
   if (!prompts || !randoms || !image_zyx || iterations < 1)
     return fail(ctx, HRRT_ERR_ARG, "prompts, randoms, an output image and iterations >= 1 are required");
-  if (storage != HRRT_STORE_F32 && storage != HRRT_STORE_16) return fail(ctx, HRRT_ERR_ARG, "unknown storage");
+  if (storage < HRRT_STORE_F32 || storage > HRRT_STORE_F16) return fail(ctx, HRRT_ERR_ARG, "unknown storage");
   if (ctx->batch) return fail(ctx, HRRT_ERR_STATE, "the context serves a batch (hrrt_batch_destroy first)");
   const Geometry &g = ctx->geo;
   if (int rc = ensure_input_buffers(ctx, storage)) return rc;
@@ -826,6 +844,8 @@ int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms
                       cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "reconstruct"));
+  if (storage == HRRT_STORE_F16)
+    if (int rc = range_status(ctx)) return bail(rc);
   if (int rc = build_work_lists(ctx)) return bail(rc);
   ctx->have_inputs = ctx->have_sens = ctx->have_image = true;
   int done = S;

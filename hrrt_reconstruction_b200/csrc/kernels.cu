@@ -6,6 +6,8 @@
 // bit-identical to the reference on the same inputs.
 #include "kernels.cuh"
 
+#include <type_traits>
+
 #include <cfloat>
 
 namespace hrrt {
@@ -560,8 +562,8 @@ __device__ __forceinline__ void store_lane(float *__restrict__ dst, const Q2 (&s
   }
 }
 
-template <int KB, bool ACC = false, bool MULTI = false>
-__global__ void __launch_bounds__(256, 3) bp_kernel(DevGeom g, const float4 *__restrict__ in, long long in_pair_stride,
+template <int KB, bool ACC = false, bool MULTI = false, int NT = 256>
+__global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(DevGeom g, const float4 *__restrict__ in, long long in_pair_stride,
                                                  const QuadWork *__restrict__ work, float *__restrict__ bc,
                                                  float *__restrict__ br, long long vol, FrameStrides fr,
                                                  int view0 = 0, int x0 = 0) {
@@ -1049,6 +1051,12 @@ __global__ void prep_kernel(DevGeom g, int nbins, const int16_t *__restrict__ pr
       mv[l] = m;
     }
     const size_t o = ((size_t)vi * g.nquads + x) * g.pplanes + g.poff[s] + r;
+    if (std::is_same<AT, __half>::value) {
+      // fp16 holds magnitudes up to 65504: a larger term is reported, not stored wrapped
+      bool over = false;
+      for (int l = 0; l < 4; l++) over |= fabsf(av[l]) > 65504.f || fabsf(mv[l]) > 65504.f;
+      if (over) atomicOr(g.range_err, 1);
+    }
     store_p4(qp, o, pv);
     store_p4(qadd, o, av);
     store_p4(qmult, o, mv);
@@ -1232,8 +1240,10 @@ cudaError_t launch_fp_pl(const DevGeom &g, const float *image, const QuadWork *w
                                                   st);
   if (storage == 0)
     return launch_fp_t<1, PL, MW, int16_t, float>(g, image, work, nwork, prompts, add, out, stride, pwarps, fr, st);
-  return launch_fp_t<1, PL, MW, __half, __nv_bfloat16>(g, image, work, nwork, prompts, add, out, stride, pwarps, fr,
-                                                       st);
+  if (storage == 1)
+    return launch_fp_t<1, PL, MW, int16_t, __nv_bfloat16>(g, image, work, nwork, prompts, add, out, stride, pwarps,
+                                                          fr, st);
+  return launch_fp_t<1, PL, MW, int16_t, __half>(g, image, work, nwork, prompts, add, out, stride, pwarps, fr, st);
 }
 
 }  // namespace
@@ -1259,18 +1269,18 @@ cudaError_t launch_fp(const DevGeom &g, const float *image, const QuadWork *work
   }
 }
 
-template <int KB>
+template <int KB, int NT>
 cudaError_t launch_bp_t(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
                         float *bc, float *br, long long vol, const FrameStrides &fr, cudaStream_t st) {
   static_assert(kBpPad >= KB, "a straddling window must stay inside the zero planes");
   const size_t smem = (size_t)g.bp_splanes * sizeof(float4);
-  auto k = fr.n > 1 ? bp_kernel<KB, false, true> : bp_kernel<KB, false, false>;
+  auto k = fr.n > 1 ? bp_kernel<KB, false, true, NT> : bp_kernel<KB, false, false, NT>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  k<<<(unsigned)nwork * fr.n, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(in), in_pair_stride / 4, work, bc,
-                                               br, vol, fr, 0, 0);
+  k<<<(unsigned)nwork * fr.n, NT, smem, st>>>(g, reinterpret_cast<const float4 *>(in), in_pair_stride / 4, work, bc,
+                                              br, vol, fr, 0, 0);
   return cudaGetLastError();
 }
 
@@ -1279,8 +1289,14 @@ cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_strid
                       cudaStream_t st) {
   if (nwork <= 0 || fr.n <= 0) return cudaSuccess;
   const int kb = tune.bp_planes > 0 ? tune.bp_planes : kBpZ;
-  if (kb == 8) return launch_bp_t<8>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, st);
-  if (kb == 4) return launch_bp_t<4>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, st);
+  // a CTA stages the quad's whole sinogram column: where that leaves room for
+  // two CTAs per SM or fewer, 384 threads keep more warps resident
+  const size_t smem = (size_t)g.bp_splanes * sizeof(float4);
+  const int nt = tune.bp_threads > 0 ? tune.bp_threads : (smem > (size_t)76 * 1024 ? 384 : 256);
+  if (kb == 8 && nt == 256) return launch_bp_t<8, 256>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, st);
+  if (kb == 8 && nt == 384) return launch_bp_t<8, 384>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, st);
+  if (kb == 4 && nt == 256) return launch_bp_t<4, 256>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, st);
+  if (kb == 4 && nt == 384) return launch_bp_t<4, 384>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, st);
   return cudaErrorInvalidValue;
 }
 
@@ -1364,10 +1380,14 @@ cudaError_t launch_prep(const DevGeom &g, int nbins, const int16_t *prompts, con
     prep_kernel<int16_t, float><<<grid, 128, 0, st>>>(g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2,
                                                       (int16_t *)q_prompts, (float *)q_add, (float *)q_mult,
                                                       quad_mask_accum, ppt, plane0, nplanes, nullptr, sp, sh, 0);
-  else
-    prep_kernel<__half, __nv_bfloat16><<<grid, 128, 0, st>>>(
-        g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (__half *)q_prompts, (__nv_bfloat16 *)q_add,
+  else if (storage == 1)
+    prep_kernel<int16_t, __nv_bfloat16><<<grid, 128, 0, st>>>(
+        g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (int16_t *)q_prompts, (__nv_bfloat16 *)q_add,
         (__nv_bfloat16 *)q_mult, quad_mask_accum, ppt, plane0, nplanes, nullptr, sp, sh, 0);
+  else
+    prep_kernel<int16_t, __half><<<grid, 128, 0, st>>>(
+        g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (int16_t *)q_prompts, (__half *)q_add,
+        (__half *)q_mult, quad_mask_accum, ppt, plane0, nplanes, nullptr, sp, sh, 0);
   return cudaGetLastError();
 }
 
@@ -1399,10 +1419,14 @@ cudaError_t launch_prep_pairs(const DevGeom &g, int nbins, const int16_t *prompt
     prep_kernel<int16_t, float><<<grid, 128, 0, st>>>(g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2,
                                                       (int16_t *)q_prompts, (float *)q_add, (float *)q_mult,
                                                       quad_mask_accum, ppt, 0, g.segmentsize, pair_views, sp, sh, ss);
-  else
-    prep_kernel<__half, __nv_bfloat16><<<grid, 128, 0, st>>>(
-        g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (__half *)q_prompts, (__nv_bfloat16 *)q_add,
+  else if (storage == 1)
+    prep_kernel<int16_t, __nv_bfloat16><<<grid, 128, 0, st>>>(
+        g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (int16_t *)q_prompts, (__nv_bfloat16 *)q_add,
         (__nv_bfloat16 *)q_mult, quad_mask_accum, ppt, 0, g.segmentsize, pair_views, sp, sh, ss);
+  else
+    prep_kernel<int16_t, __half><<<grid, 128, 0, st>>>(
+        g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (int16_t *)q_prompts, (__half *)q_add,
+        (__half *)q_mult, quad_mask_accum, ppt, 0, g.segmentsize, pair_views, sp, sh, ss);
   return cudaGetLastError();
 }
 
@@ -1413,9 +1437,12 @@ cudaError_t launch_scale_pairs(const DevGeom &g, const void *src, int storage, c
   if (storage == 0)
     scale_pairs_kernel<float><<<grid, 256, 0, st>>>(g, (const float *)src, views, reinterpret_cast<float4 *>(dst),
                                                     dst_pair_stride / 4);
-  else
+  else if (storage == 1)
     scale_pairs_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(g, (const __nv_bfloat16 *)src, views,
                                                             reinterpret_cast<float4 *>(dst), dst_pair_stride / 4);
+  else
+    scale_pairs_kernel<__half><<<grid, 256, 0, st>>>(g, (const __half *)src, views, reinterpret_cast<float4 *>(dst),
+                                                     dst_pair_stride / 4);
   return cudaGetLastError();
 }
 

@@ -26,11 +26,15 @@ namespace hrrt {
 #ifndef HRRT_FP_SLOTS
 #define HRRT_FP_SLOTS 3
 #endif
+#ifndef HRRT_BP_MIN_BLOCKS
+#define HRRT_BP_MIN_BLOCKS 3
+#endif
 constexpr int kFpPlanes = 9;                   // default planes per forward-projection task (odd: bank-conflict free)
 constexpr int kFpSlots = HRRT_FP_SLOTS;       // sampled rows in flight between producers and consumers
 constexpr int kFpZPad = 16;     // zeroed entries after each sampled row
 constexpr int kFpEndPlanes = 4; // planes per end-plane task (they cost ~2x a middle plane)
 constexpr int kBpZ = 8;         // z per back-projection task
+constexpr int kBpMinBlocks = HRRT_BP_MIN_BLOCKS;  // resident back-projection CTAs per SM (register budget)
 constexpr int kBpPad = 8;       // zero planes on each side of a segment in the back projector (>= kBpZ)
 
 struct FpTask {
@@ -72,6 +76,7 @@ struct DevGeom {
   const int16_t *plane_seg;         // [segmentsize] segment of each global plane
   const int16_t *pplane_seg;        // [pplanes] segment of each padded plane, -1 on pads
   int *err;                         // device status word: non-zero after a bounded wait gave up
+  int *range_err;                   // non-zero after an input exceeded the fp16 range (HRRT_STORE_F16)
   const int *bp_soff;               // [nseg] back projector: shared-memory plane of yr_bottom
   const int *bp_src;                // [bp_splanes] quad-layout plane of each shared plane, -1 = zero
   int bp_splanes;
@@ -110,8 +115,10 @@ struct ProjTune {
   int fp_planes;  // planes per forward-projection task: 7, 9 or 11 (0: kFpPlanes)
   int fp_pwarps;  // producer warps of the forward projector (0: as many as fit, 2..6)
   int bp_planes;  // planes per back-projection task: 4 or 8 (0: kBpZ)
+  int bp_threads; // threads per back-projection CTA: 256 or 384 (0: 384 where shared memory admits two
+                  // CTAs per SM or fewer, else 256)
 };
-inline ProjTune default_tune() { return ProjTune{0, 0, 0}; }
+inline ProjTune default_tune() { return ProjTune{0, 0, 0, 0}; }
 constexpr int kFpPlaneVariants[3] = {7, 9, 11};
 // warps per forward-projection CTA for each plane variant (register budget)
 constexpr int kFpVariantWarps[3] = {32, 32, 24};

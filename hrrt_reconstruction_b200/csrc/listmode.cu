@@ -244,21 +244,31 @@ __device__ __forceinline__ void bump16(uint32_t *__restrict__ bins, long long ad
   if (!hi && (old & 0xFFFFu) + inc > 0xFFFFu) atomicSub(w, 0x10000u);  // undo the carry into the high bin
 }
 
-// rebin_event (LM_Rebinner_mp.cpp:188-219): address or -1
-__device__ __forceinline__ long long rebin(const LmDev &g, const float *zp, const float *zp2, int mp, int al, int ax,
-                                           int ay, int bl, int bx, int by) {
-  const hrrt::LmSol s = g.sol[((size_t)mp * 144 + ax + 72 * al) * 144 + bx + 72 * bl];
+// Tables every histogram block stages in shared memory.
+constexpr int kMaxSegs = 64;
+struct LmShared {
+  float zp[104], zp2[104];                         // m_c_zpos, m_c_zpos2
+  int z0[kMaxSegs], zmax[kMaxSegs], zoff[kMaxSegs];  // m_segz0, m_segzmax, m_segzoffset
+};
+
+// rebin_event (LM_Rebinner_mp.cpp:188-219) in two halves: the LUT entry of a
+// crystal pair, then the address (or -1) from that entry.
+__device__ __forceinline__ size_t sol_index(int mp, int al, int ax, int bl, int bx) {
+  return ((size_t)mp * 144 + ax + 72 * al) * 144 + bx + 72 * bl;
+}
+__device__ __forceinline__ long long rebin_address(const LmDev &g, const LmShared &t, const hrrt::LmSol &s, int ay,
+                                                   int by) {
   if (s.nsino == -1) return -1;
-  const float cay = zp2[ay];
-  const float dz2 = __fsub_rn(zp[by], zp[ay]);
+  const float cay = t.zp2[ay];
+  const float dz2 = __fsub_rn(t.zp[by], t.zp[ay]);
   const int plane = (int)__fadd_rn(cay, __fmul_rn(s.z, dz2));
   const float seg = (float)(0.5 + (double)__fmul_rn(dz2, s.d));
   int segnum = (int)seg;
   segnum = (seg < 0) ? 1 - 2 * segnum : 2 * segnum;
   if (segnum >= g.nsegs) return -1;
   if (plane < 0 || plane > 206) return -1;
-  if (plane < g.segz0[segnum] || plane > g.segzmax[segnum]) return -1;
-  return (long long)(plane + g.segzoff[segnum]) * kSinoPlane + s.nsino;
+  if (plane < t.z0[segnum] || plane > t.zmax[segnum]) return -1;
+  return (long long)(plane + t.zoff[segnum]) * kSinoPlane + s.nsino;
 }
 
 // Partitions of the histogram for the L2-resident pass: 32 Mi bins (64 MB of
@@ -268,15 +278,22 @@ constexpr int kMaxParts = 64;
 
 // Walk one thread's words from its entry offset: count the statistics (kStats),
 // record time tags in stream order (when tags != null), and hand every
-// histogrammed event to emit(address, sinogram 0/1, subtract).
-template <bool kStats, typename Emit>
-__device__ __forceinline__ void walk_events(const LmDev &g, const float *zp, const float *zp2, const uint32_t *w,
-                                            int s, int e, int pend, long long t0, long long limit, int mode,
-                                            int flags, uint32_t (&c)[kStCount], unsigned long long tagpos,
-                                            long long tag_cap, longlong2 *__restrict__ tags, Emit emit) {
+// histogrammed event to emit(address, sinogram 0/1, subtract) -- the
+// coincidence events together, to emit_events(addresses, live, sinogram-1
+// and subtract bit masks).  The parse
+// runs first and notes where the thread's coincidence events start (at most
+// kSub/2 of them); the events are then decoded and rebinned in an unrolled
+// pass whose LUT loads are independent of one another.  Emission order does
+// not matter: the bins are sums modulo 2^16 and the statistics counts.
+template <bool kStats, typename Emit, typename EmitEvents>
+__device__ __forceinline__ void walk_events(const LmDev &g, const LmShared &t, const uint32_t *w, int s, int e,
+                                            int pend, long long t0, long long limit, int mode, int flags,
+                                            uint32_t (&c)[kStCount], unsigned long long tagpos, long long tag_cap,
+                                            longlong2 *__restrict__ tags, Emit emit, EmitEvents emit_events) {
   const bool doi = (flags & HRRT_LM_NO_DOI) == 0;
   const bool border = (flags & HRRT_LM_IGNORE_BORDER_CRYSTAL) != 0;
   const int xhigh = border ? 71 : 72;
+  uint32_t evmask = 0;  // bit k: an event (below the limit) starts at word s + k
   int pos = s + e;
   while (pos < s + kSub) {
     if (pos + 1 >= pend) break;
@@ -304,7 +321,12 @@ __device__ __forceinline__ void walk_events(const LmDev &g, const float *zp, con
       if (tag & 0x80000000u) continue;
       // a tag value with bit 31 clear reads as an event word
       const bool prompt = (tag & 0x40000000u) != 0;
-      if (kStats) c[prompt ? kStPrompts : kStDelayed]++;
+      if (kStats) {
+        if (prompt)
+          c[kStPrompts]++;
+        else
+          c[kStDelayed]++;
+      }
       const long long addr = tag & 0x3fffffff;
       if (addr < g.sino_size) {
         if (mode == HRRT_LM_PROMPTS_AND_DELAYED)
@@ -315,7 +337,25 @@ __device__ __forceinline__ void walk_events(const LmDev &g, const float *zp, con
       continue;
     }
     if (gp >= limit) continue;
-    // coincidence event (rebin_packet, histogram_mp.cpp:1114-1225)
+    evmask |= 1u << (pos - 2 - s);
+  }
+  if (!evmask) return;
+  // coincidence events (rebin_packet, histogram_mp.cpp:1114-1225): decode,
+  // reject, LUT entry ...
+  constexpr int kEv = kSub / 2;
+  size_t idx[kEv];
+  uint32_t need = 0, delayed = 0;  // bit k: event k is rebinned / is delayed
+  int ays[kEv], bys[kEv];
+  uint32_t m = evmask;
+#pragma unroll
+  for (int k = 0; k < kEv; k++) {
+    idx[k] = 0;
+    ays[k] = bys[k] = 0;
+    if (!m) continue;
+    const int p = __ffs(m) - 1;
+    m &= m - 1;
+    const uint32_t ew1 = w[s + p], ew2 = w[s + p + 1];
+    const int type = ewtype(ew1, ew2);
     const int mpe = ((ew1 >> 16) & 7) | (((ew2 >> 16) & 7) << 3);
     const int ax = ew1 & 0xff, ay = (ew1 >> 8) & 0xff, bx = ew2 & 0xff, by = (ew2 >> 8) & 0xff;
     const int doia = doi ? (int)((ew1 >> 22) & 7) : 1, doib = doi ? (int)((ew2 >> 22) & 7) : 1;
@@ -331,18 +371,71 @@ __device__ __forceinline__ void walk_events(const LmDev &g, const float *zp, con
       if (kStats) c[kStDoiOther]++;
       continue;
     }
-    long long addr = -1;
-    if (!(border && (ax * bx == 0 || ax == xhigh || bx == xhigh)) && !(mode == HRRT_LM_PROMPTS_ONLY && type != 0))
-      addr = rebin(g, zp, zp2, mpe, doia, ax, ay, doib, bx, by);
-    if (addr < 0) {
+    if ((border && (ax * bx == 0 || ax == xhigh || bx == xhigh)) || (mode == HRRT_LM_PROMPTS_ONLY && type != 0)) {
       if (kStats) c[kStUnmapped]++;
       continue;
     }
-    if (kStats) c[type == 0 ? kStPrompts : kStDelayed]++;
-    if (mode == HRRT_LM_PROMPTS_AND_DELAYED)
-      emit(addr, type == 0 ? 0 : 1, false);
-    else
-      emit(addr, 0, type != 0);
+    idx[k] = sol_index(mpe, doia, ax, doib, bx);
+    ays[k] = ay;
+    bys[k] = by;
+    need |= 1u << k;
+    if (type != 0) delayed |= 1u << k;
+  }
+  // ... the LUT entries, all loads in flight together ...
+  hrrt::LmSol sol[kEv];
+#pragma unroll
+  for (int k = 0; k < kEv; k++)
+    if ((need >> k) & 1) sol[k] = g.sol[idx[k]];
+  // ... and the addresses, handed over together
+  long long addr[kEv];
+  uint32_t live = 0, sel = 0, minus = 0;
+#pragma unroll
+  for (int k = 0; k < kEv; k++) {
+    addr[k] = 0;
+    if (!((need >> k) & 1)) continue;
+    const long long a = rebin_address(g, t, sol[k], ays[k], bys[k]);
+    if (a < 0) {
+      if (kStats) c[kStUnmapped]++;
+      continue;
+    }
+    const bool dly = (delayed >> k) & 1;
+    if (kStats) {
+      if (dly)
+        c[kStDelayed]++;
+      else
+        c[kStPrompts]++;
+    }
+    addr[k] = a;
+    live |= 1u << k;
+    if (mode == HRRT_LM_PROMPTS_AND_DELAYED) {
+      if (dly) sel |= 1u << k;
+    } else if (dly) {
+      minus |= 1u << k;
+    }
+  }
+  if (live) emit_events(addr, live, sel, minus);
+}
+
+// The direct histogram of a thread's events: every add issued before any
+// carry is checked, so the read-modify-writes are in flight together.
+template <int kEv>
+__device__ __forceinline__ void bump16_events(uint32_t *__restrict__ sino, uint32_t *__restrict__ dly,
+                                              const long long (&addr)[kEv], uint32_t live, uint32_t sel,
+                                              uint32_t minus) {
+  uint32_t old[kEv];
+#pragma unroll
+  for (int k = 0; k < kEv; k++) {
+    old[k] = 0;
+    if (!((live >> k) & 1)) continue;
+    uint32_t *w = (((sel >> k) & 1) ? dly : sino) + (addr[k] >> 1);
+    const uint32_t inc = ((minus >> k) & 1) ? 0xFFFFu : 1u;
+    old[k] = atomicAdd(w, inc << (16 * (uint32_t)(addr[k] & 1)));
+  }
+#pragma unroll
+  for (int k = 0; k < kEv; k++) {
+    if (!((live >> k) & 1) || (addr[k] & 1)) continue;
+    const uint32_t inc = ((minus >> k) & 1) ? 0xFFFFu : 1u;
+    if ((old[k] & 0xFFFFu) + inc > 0xFFFFu) atomicSub((((sel >> k) & 1) ? dly : sino) + (addr[k] >> 1), 0x10000u);
   }
 }
 
@@ -359,13 +452,18 @@ __global__ void __launch_bounds__(kThreads) lm_hist_kernel(
     unsigned long long *__restrict__ part_cursor, uint32_t *__restrict__ records, int parts_per_sino) {
   __shared__ __align__(16) uint32_t w[kTileWords + 4];
   __shared__ Sub wt[32];
-  __shared__ float zp[104], zp2[104];
+  __shared__ LmShared tb;
   __shared__ unsigned long long st[kStCount];
   __shared__ unsigned int pcount[kMaxParts];
   __shared__ unsigned long long pbase[kMaxParts];
   if (threadIdx.x < 104) {
-    zp[threadIdx.x] = g.zpos[threadIdx.x];
-    zp2[threadIdx.x] = g.zpos2[threadIdx.x];
+    tb.zp[threadIdx.x] = g.zpos[threadIdx.x];
+    tb.zp2[threadIdx.x] = g.zpos2[threadIdx.x];
+  }
+  if (threadIdx.x < g.nsegs) {
+    tb.z0[threadIdx.x] = g.segz0[threadIdx.x];
+    tb.zmax[threadIdx.x] = g.segzmax[threadIdx.x];
+    tb.zoff[threadIdx.x] = g.segzoff[threadIdx.x];
   }
   if (threadIdx.x < kStCount) st[threadIdx.x] = 0;
   if (threadIdx.x < kMaxParts) pcount[threadIdx.x] = 0;
@@ -383,21 +481,32 @@ __global__ void __launch_bounds__(kThreads) lm_hist_kernel(
   longlong2 *tg = tag_cap > 0 ? tags : nullptr;
   uint32_t c[kStCount] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   auto part_of = [&](long long addr, int sel) { return sel * parts_per_sino + (int)(addr >> kPartShift); };
+  // a per-event emitter applied to every event of a thread's batch
+  auto each = [](auto f) {
+    return [f](const auto &a, uint32_t live, uint32_t sel, uint32_t minus) {
+#pragma unroll
+      for (int k = 0; k < kSub / 2; k++)
+        if ((live >> k) & 1) f(a[k], (int)((sel >> k) & 1), ((minus >> k) & 1) != 0);
+    };
+  };
   if (kMode == 0) {
-    walk_events<false>(g, zp, zp2, w, s, e, pend, t0, limit, mode, flags, c, tagpos, tag_cap, tg,
-                       [](long long, int, bool) {});
+    auto none = [](long long, int, bool) {};
+    walk_events<false>(g, tb, w, s, e, pend, t0, limit, mode, flags, c, tagpos, tag_cap, tg, none, each(none));
   } else if (kMode == 1) {
-    walk_events<true>(g, zp, zp2, w, s, e, pend, t0, limit, mode, flags, c, tagpos, tag_cap, tg,
-                      [&](long long addr, int sel, bool minus) { bump16(sel ? dly : sino, addr, minus); });
+    walk_events<true>(g, tb, w, s, e, pend, t0, limit, mode, flags, c, tagpos, tag_cap, tg,
+                      [&](long long addr, int sel, bool minus) { bump16(sel ? dly : sino, addr, minus); },
+                      [&](const long long (&a)[kSub / 2], uint32_t live, uint32_t sel, uint32_t minus) {
+                        bump16_events<kSub / 2>(sino, dly, a, live, sel, minus);
+                      });
   } else if (kMode == 2) {
-    walk_events<true>(g, zp, zp2, w, s, e, pend, t0, limit, mode, flags, c, tagpos, tag_cap, tg,
-                      [&](long long addr, int sel, bool) { atomicAdd(&pcount[part_of(addr, sel)], 1u); });
+    auto count = [&](long long addr, int sel, bool) { atomicAdd(&pcount[part_of(addr, sel)], 1u); };
+    walk_events<true>(g, tb, w, s, e, pend, t0, limit, mode, flags, c, tagpos, tag_cap, tg, count, each(count));
     __syncthreads();
     if (threadIdx.x < 2 * parts_per_sino && pcount[threadIdx.x])
       atomicAdd(&part_cursor[threadIdx.x], (unsigned long long)pcount[threadIdx.x]);
   } else {
-    walk_events<false>(g, zp, zp2, w, s, e, pend, t0, limit, mode, flags, c, tagpos, 0, nullptr,
-                       [&](long long addr, int sel, bool) { atomicAdd(&pcount[part_of(addr, sel)], 1u); });
+    auto count = [&](long long addr, int sel, bool) { atomicAdd(&pcount[part_of(addr, sel)], 1u); };
+    walk_events<false>(g, tb, w, s, e, pend, t0, limit, mode, flags, c, tagpos, 0, nullptr, count, each(count));
     __syncthreads();
     if (threadIdx.x < 2 * parts_per_sino) {
       const unsigned int k = pcount[threadIdx.x];
@@ -405,12 +514,13 @@ __global__ void __launch_bounds__(kThreads) lm_hist_kernel(
       pcount[threadIdx.x] = 0;
     }
     __syncthreads();
-    walk_events<false>(g, zp, zp2, w, s, e, pend, t0, limit, mode, flags, c, tagpos, 0, nullptr,
-                       [&](long long addr, int sel, bool minus) {
-                         const int p = part_of(addr, sel);
-                         const unsigned int k = atomicAdd(&pcount[p], 1u);
-                         records[pbase[p] + k] = (uint32_t)addr | ((uint32_t)sel << 29) | ((uint32_t)minus << 30);
-                       });
+    auto scatter = [&](long long addr, int sel, bool minus) {
+      const int p = part_of(addr, sel);
+      const unsigned int k = atomicAdd(&pcount[p], 1u);
+      records[pbase[p] + k] = (uint32_t)addr | ((uint32_t)sel << 29) | ((uint32_t)minus << 30);
+    };
+    walk_events<false>(g, tb, w, s, e, pend, t0, limit, mode, flags, c, tagpos, 0, nullptr, scatter,
+                       each(scatter));
   }
   if (kMode == 1 || kMode == 2) {
     // block reduction of the counters
@@ -568,6 +678,12 @@ int hrrt_lm_create(int span, int maxrd, int device, hrrt_lm **out) {
   if (e == cudaSuccess) d.segzmax = lm_upload(h.get(), h->tab.segzmax, &e);
   if (e == cudaSuccess) d.segzoff = lm_upload(h.get(), h->tab.segzoffset, &e);
   d.nsegs = h->tab.nsegs;
+  if (d.nsegs > kMaxSegs) {
+    hrrt_lm *raw = h.release();
+    raw->err = "hrrt_lm_create: too many segments";
+    *out = raw;
+    return HRRT_ERR_ARG;
+  }
   d.sino_size = h->tab.sino_size();
   if (e != cudaSuccess) {
     hrrt_lm *raw = h.release();

@@ -3,7 +3,8 @@
 Seeded Poisson prompts, flat randoms and a lognormal normalisation at the
 HRRT geometry of the chosen span; uploads, computes the sensitivity images,
 runs `--subsets` subsets and prints the per-kernel device times.  It holds
-the span-3 inputs (about 2 GB in the quad layout) and nothing else large, so
+the span-3 inputs (about 5 GB in the quad layout, 3 GB with --storage 16) and
+nothing else large, so
 it suits a profiler capture of a single kernel launch.
 
     python hrrt_reconstruction_b200/profile_case.py --span 3 --subsets 2

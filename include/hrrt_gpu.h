@@ -42,10 +42,13 @@ typedef enum {
   HRRT_ERR_DEVICE = -5    /* a device-side check reported an error */
 } hrrt_status;
 
-/* storage types of the sinogram-shaped inputs on the device */
+/* storage types of the sinogram-shaped inputs on the device (prompts are
+ * always int16, the reference's own type, exact over its whole range) */
 enum {
-  HRRT_STORE_F32 = 0,     /* prompts int16, 1/(NA) and additive term float32 (the reference) */
-  HRRT_STORE_16 = 1       /* prompts fp16 (exact integers), 1/(NA) and additive term bf16 */
+  HRRT_STORE_F32 = 0,     /* 1/(NA) and additive term float32 (the reference) */
+  HRRT_STORE_16 = 1,      /* 1/(NA) and additive term bf16 (8-bit significand, float32 range) */
+  HRRT_STORE_F16 = 2      /* 1/(NA) and additive term fp16 (11-bit significand; a term above 65504 is
+                             reported by the upload as HRRT_ERR_ARG) */
 };
 
 /* back projector variants */
@@ -231,6 +234,7 @@ typedef struct hrrt_tuning {
   int fp_planes;          /* planes per forward-projection task: 7, 9 or 11 (0: 9) */
   int fp_producer_warps;  /* sampling warps of the forward projector: 2..6 (0: as many as fit) */
   int bp_planes;          /* planes per back-projection task: 4 or 8 (0: 8) */
+  int bp_threads;         /* threads per back-projection CTA: 256 or 384 (0: by the CTA's shared memory) */
   double fp_ms, bp_ms;    /* filled by the tuners: the chosen shapes' device time per launch */
 } hrrt_tuning;
 

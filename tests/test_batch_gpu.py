@@ -124,11 +124,12 @@ def _shapes(ctx):
     for pl in (7, 9, 11):
         for pw in (0, 2, 3, 4, 6):
             for kb in (4, 8):
-                try:
-                    ctx.set_tuning(pl, pw, kb)
-                except H.HrrtError:
-                    continue
-                out.append((pl, pw, kb))
+                for nt in (0, 256, 384):
+                    try:
+                        ctx.set_tuning(pl, pw, kb, nt)
+                    except H.HrrtError:
+                        continue
+                    out.append((pl, pw, kb, nt))
     ctx.set_tuning()
     return out
 
@@ -147,7 +148,7 @@ def test_launch_shapes_bit_identical(name):
         ctx.osem_subsets(0, 1)
         img0 = ctx.get_image_xyz()
         shapes = _shapes(ctx)
-        assert (9, 0, 8) in shapes and len(shapes) >= 8, shapes
+        assert (9, 0, 8, 0) in shapes and len(shapes) >= 24, shapes
         want = None
         for t in shapes:
             ctx.set_tuning(*t)
@@ -172,7 +173,7 @@ def test_launch_shapes_bit_identical(name):
     with H.Context(product_geom(d)) as ctx:
         from geoms import random_image
         x = random_image(ctx.image_shape, O.cylwiny(), seed=5, zvalid=O.nz)
-        ctx.set_tuning(7, 2, 4)
+        ctx.set_tuning(7, 2, 4, 384)
         assert np.array_equal(ctx.fp_pair(x, 3).view(np.uint32), O.fp_pair(x, 3).view(np.uint32))
 
 

@@ -5,7 +5,8 @@ which exit before a GPU is touched.  GPU: a span-9 OP-OSEM reconstruction
 from flat files gives the same image, bit for bit, as the library called
 directly on the same arrays; a span-9 attenuation file drives a span-3
 reconstruction exactly like the expanded span-3 attenuation
-(Atten3D_Span9, hrrt_osem3d_span3.cpp:1762-1796)."""
+(Atten3D_Span9, hrrt_osem3d_span3.cpp:1762-1796); a 2D scatter segment with
+span-9 scale factors exactly like its 3D expansion (drv:1136-1179, 4407-4421)."""
 import os
 import subprocess
 
@@ -125,6 +126,69 @@ def test_span9_attenuation_for_span3(cli, tmp_path):
     out = tmp_path / "img3.i"
     r = run(cli, "-p", str(tmp_path / "p.s"), "-d", str(tmp_path / "d.s"), "-a", str(tmp_path / "a9.s"), "-o",
             str(out), "-W", "3", "-I", "1", "-m", "3,67")
+    assert r.returncode == 0, r.stderr
+    got = np.fromfile(out, np.float32).reshape(want.shape)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def scatter_2d_to_3d(sc2d, sf9, span):
+    """The reference's 2D-scatter input (drv:4407-4421): convert_s9_s3
+    (drv:1136-1162) makes span-3 plane factors from the span-9 ones -- a walk
+    over the span-3 segments three at a time, each next segment a trimmed
+    copy of the previous -- and apply_scale_factors (drv:1169-1179) scales 2D
+    plane yr_bottom+yr into plane yr of every segment."""
+    yb, npl, off = span_segments(span)
+    P = sum(npl)
+    if span == 9:
+        sf = sf9.astype(np.float32)
+    else:
+        sf = np.zeros(P, np.float32)
+        i = j = 0
+        for th in range(0, len(yb), 3):
+            n = npl[th]
+            sf[i:i + n] = sf9[j:j + n] / np.float32(3.0)
+            i += n
+            j += n
+            for k in (1, 2):
+                so = yb[th + k] - yb[th + k - 1]
+                m = n - 2 * so
+                sf[i:i + m] = sf[i - n + so:i - n + so + m]
+                n = m
+                i += m
+    out = np.empty((P,) + sc2d.shape[1:], np.float32)
+    for s in range(len(yb)):
+        for yr in range(npl[s]):
+            out[off[s] + yr] = sc2d[yb[s] + yr] * sf[off[s] + yr]
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("span", [9, 3])
+def test_scatter_2d_with_scale_factors(cli, tmp_path, span):
+    """-s with an unscaled 2D scatter segment + 2209 span-9 scale factors
+    reconstructs exactly like the expanded 3D scatter."""
+    import hrrt_reconstruction_b200 as H
+    rng = np.random.default_rng(13 + span)
+    with H.Context(H.hrrt_geometry(span=span)) as ctx:
+        shape = ctx.sino_shape
+        nz = ctx.info.nz
+        sc2d = (0.05 * rng.random((nz,) + shape[1:], dtype=np.float32)).astype(np.float32)
+        sf9 = (0.5 + rng.random(2209, dtype=np.float32)).astype(np.float32)
+        s3 = scatter_2d_to_3d(sc2d, sf9, span)
+        assert s3.shape == shape
+        prompts = rng.poisson(0.8, size=shape).astype(np.int16)
+        delayed = np.full(shape, 0.1, np.float32)
+        prompts.tofile(tmp_path / "p.s")
+        delayed.tofile(tmp_path / "d.s")
+        np.concatenate([sc2d.reshape(-1), sf9]).tofile(tmp_path / "s2d.s")
+        ctx.upload_inputs(prompts, delayed, None, None, s3)
+        ctx.sensitivity()
+        ctx.init_image()
+        ctx.osem(1)
+        want = ctx.get_image()
+    out = tmp_path / "img.i"
+    r = run(cli, "-p", str(tmp_path / "p.s"), "-d", str(tmp_path / "d.s"), "-s", str(tmp_path / "s2d.s"), "-o",
+            str(out), "-W", "3", "-I", "1", "-m", f"{span},67")
     assert r.returncode == 0, r.stderr
     got = np.fromfile(out, np.float32).reshape(want.shape)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
