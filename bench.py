@@ -323,6 +323,8 @@ def run_ours(args, ws, rank, local):
     }
     if args.storage == "f32" and args.compare_16:
         out["storage16"] = run_storage16(args, torch, H, ctx, st, host, names, img, cs, dist, local, ws, ms)
+        out["storage_f16"] = run_storage16(args, torch, H, ctx, st, host, names, img, cs, dist, local, ws, ms,
+                                           storage=H.STORE_F16)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     ctx.close()
@@ -339,13 +341,14 @@ def run_ours(args, ws, rank, local):
         dist.destroy_process_group()
 
 
-def run_storage16(args, torch, H, ctx, st, host, names, img_f32, cs, dist, local, ws, ms_f32):
-    """The same study with the sinogram-shaped inputs stored in 16 bits (prompts
-    fp16, 1/(NA) and the additive term bf16; FP32 arithmetic): device-resident
-    subset-iterations/s over the same steps, and the rel-L2 of its image after
-    the e2e reconstruction against the f32-stored image."""
+def run_storage16(args, torch, H, ctx, st, host, names, img_f32, cs, dist, local, ws, ms_f32, storage=None):
+    """The same study with 1/(NA) and the additive term stored in 16 bits (bf16
+    by default, fp16 with storage=STORE_F16; prompts int16; FP32 arithmetic):
+    device-resident subset-iterations/s over the same steps, and the rel-L2
+    of its image after the e2e reconstruction against the f32-stored image."""
+    storage = H.STORE_16 if storage is None else storage
     img16 = pinned_copy(torch, np.zeros_like(img_f32))
-    ctx.reconstruct(*(host.get(k) for k in names), storage=H.STORE_16, iterations=ITERATIONS, out=img16)
+    ctx.reconstruct(*(host.get(k) for k in names), storage=storage, iterations=ITERATIONS, out=img16)
     a = img16.astype(np.float64)
     b = img_f32.astype(np.float64)
     rel = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
@@ -364,7 +367,8 @@ def run_storage16(args, torch, H, ctx, st, host, names, img_f32, cs, dist, local
             "speedup_vs_f32": ms_f32 / ms, "rel_l2_vs_f32_image": rel,
             "rel_l2_note": f"image after {ITERATIONS} iterations x {SUBSETS} subsets (hrrt_reconstruct), "
                            "16-bit-stored vs f32-stored inputs, same prompts",
-            "storage": "prompts fp16, 1/(NA) and additive term bf16; FP32 accumulation, FP64 image sum"}
+            "storage": ("prompts int16, 1/(NA) and additive term " + ("fp16" if storage == H.STORE_F16 else "bf16")
+                        + "; FP32 accumulation, FP64 image sum")}
 
 
 # Dynamic study: 24 span-9 frames of the config-0 phantom, sphere activity
@@ -464,16 +468,25 @@ def run_dynamic(args, torch, H, local, dist, ws):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(dist, ev[0].elapsed_time(ev[1]), local)
     sums = [b.get_image(f, out=imgs[f])[1] for f in range(nf)]
-    # precision: two frames reconstructed alone with f32-stored inputs
-    rel = {}
+    # precision: two frames reconstructed alone with f32-stored inputs (and,
+    # for comparison, with fp16-stored terms)
+    rel, rel16 = {}, {}
+
+    def rl2(a, b):
+        a = a.astype(np.float64)
+        b = b.astype(np.float64)
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
     for f in (int(np.argmin(counts)), int(np.argmax(counts))):
         ctx2 = H.Context(geom, device=local)
         want, _ = ctx2.reconstruct(host_p[f], host_r[f], atten=atten, storage=H.STORE_F32,
                                    iterations=int(iters[f]))
+        f16, _ = ctx2.reconstruct(host_p[f], host_r[f], atten=atten, storage=H.STORE_F16,
+                                  iterations=int(iters[f]))
         ctx2.close()
-        a = imgs[f].astype(np.float64)
-        rel[f"frame{f} ({counts[f]:.3g} counts, {int(iters[f])} it)"] = float(
-            np.linalg.norm(a - want) / max(np.linalg.norm(want.astype(np.float64)), 1e-30))
+        key = f"frame{f} ({counts[f]:.3g} counts, {int(iters[f])} it)"
+        rel[key] = rl2(imgs[f], want)
+        rel16[key] = rl2(f16, want)
     h2d = sum(int(a.nbytes) for a in host_p) + sum(int(a.nbytes) for a in host_r)
     d2h = sum(int(a.nbytes) for a in imgs)
     b.close()
@@ -492,6 +505,7 @@ def run_dynamic(args, torch, H, local, dist, ws):
                 "h2d_bytes_per_step": h2d // max(est.subset_iterations, 1),
                 "d2h_bytes_per_step": d2h // max(est.subset_iterations, 1)},
         "rel_l2_vs_f32_stored": rel,
+        "rel_l2_vs_f32_stored_fp16_terms": rel16,
         "clocks": clk, "data_gen_s": gen_s,
     }
 

@@ -138,6 +138,8 @@ def _load():
         "hrrt_lm_table": (ctypes.c_longlong, [i, i, ctypes.c_char_p, vp, ctypes.c_size_t]),
         "hrrt_lm_histogram": (i, [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, ctypes.POINTER(LmStats)]),
         "hrrt_lm_histogram_device": (i, [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, ctypes.POINTER(LmStats), vp]),
+        "hrrt_lm_smooth_randoms": (i, [vp, vp, f, f, vp, ctypes.POINTER(i)]),
+        "hrrt_lm_crystal_singles": (i, [vp, f, f, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -475,6 +477,17 @@ class Batch:
         return out, sm.value
 
 
+def crystal_singles(delayed_counts, scan_duration=1.0, tau=6.0e-9):
+    """Host-only: gen_delays' crystal singles estimate from the 119808 delayed
+    crystal counts of a coincidence histogram -> (singles float32, iterations)."""
+    d = np.ascontiguousarray(delayed_counts, np.int32).reshape(-1)
+    if d.size != 2 * 104 * 8 * 72:
+        raise HrrtError("delayed counts: 119808 crystals expected")
+    out = np.zeros(d.size, np.float32)
+    it = lib.hrrt_lm_crystal_singles(_ptr(d), scan_duration, tau, _ptr(out))
+    return out, it
+
+
 def lm_table(name, span=3, maxrd=67):
     """One listmode rebinning table (host-only): "sol" [21][144][144] LM_SOL,
     "zpos"/"zpos2" float [104], "segz0"/"segzmax"/"segzoffset" int32."""
@@ -550,6 +563,18 @@ class Listmode:
         self._check(lib.hrrt_lm_histogram(self._h, _ptr(w), w.size, mode, duration, flags, _ptr(sino), _ptr(dly),
                                           ctypes.byref(st)), "lm_histogram")
         return sino, dly, st.as_dict()
+
+    def smooth_randoms(self, coinc_hist, scan_duration=1.0, tau=6.0e-9):
+        """gen_delays: the randoms sinogram (float32, this context's span) from
+        a coincidence histogram [2][119808] int32 -> (sino, iterations)."""
+        h = np.ascontiguousarray(coinc_hist, np.int32).reshape(-1)
+        if h.size != 2 * 2 * 104 * 8 * 72:
+            raise HrrtError("coincidence histogram: 2 x 119808 counts expected")
+        out = np.empty(self.sino_size, np.float32)
+        it = ctypes.c_int()
+        self._check(lib.hrrt_lm_smooth_randoms(self._h, _ptr(h), scan_duration, tau, _ptr(out), ctypes.byref(it)),
+                    "lm_smooth_randoms")
+        return out, it.value
 
     def histogram_device(self, d_words, nwords, d_sino, d_delayed=None, mode=LM_PROMPTS_AND_DELAYED, duration=0,
                          flags=0, stream=None):

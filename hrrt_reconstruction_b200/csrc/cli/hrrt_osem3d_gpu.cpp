@@ -49,7 +49,8 @@ void usage() {
                "       [-f rel_fov,trim,zmin,zmax] [-k npskip] [-e eps1,eps2,eps3] [-u image_max] [-Q]\n"
                "       [-F in_flip,out_flip] [-T threads] [-N] [-D dir] [-L log] [-v level] [-X 256]\n"
                "  -p  3D flat integer (int16) prompt scan; -Q: float prompt scan of integer counts\n"
-               "  -d  3D flat float delayed (smoothed randoms)\n"
+               "  -d  3D flat float delayed (smoothed randoms), or a coincidence histogram (.ch) from which the\n"
+               "      smoothed randoms are computed over the scan duration in the prompt sinogram's .hdr\n"
                "  -n  3D flat normalisation, -a attenuation (span 9 accepted for span 3), -s scatter\n"
                "      (3D, or the unscaled 2D segment followed by 2209 span-9 plane scale factors)\n"
                "  -o  output image (flat float [z][y][x] + .hdr), -O also after each iteration\n"
@@ -290,6 +291,21 @@ std::vector<float> expand_scatter_2d(const std::vector<float> &file, const hrrt_
   return out;
 }
 
+// get_scan_duration (hrrt_osem_utils.cpp:8-25): "image duration := <s>" in
+// the prompt sinogram's .hdr
+bool scan_duration_of(const std::string &sino, float *out) {
+  FILE *f = std::fopen((sino + ".hdr").c_str(), "rt");
+  if (!f) return false;
+  char line[256];
+  bool found = false;
+  while (!found && std::fgets(line, sizeof line, f)) {
+    const char *p = std::strstr(line, "image duration");
+    if (p && (p = std::strstr(p, ":=")) && std::sscanf(p + 2, "%g", out) == 1) found = true;
+  }
+  std::fclose(f);
+  return found;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
@@ -340,7 +356,30 @@ int main(int argc, char **argv) {
     if (file_size(p) != (long long)(nbins * 4)) die("%s: not a float scan of this span", p.c_str());
     return read_flat<float>(p, nbins);
   };
-  const std::vector<float> delayed = read_scan(o.delayed), norm = read_scan(o.norm);
+  const std::vector<float> norm = read_scan(o.norm);
+  std::vector<float> delayed;
+  // a coincidence histogram (.ch: int32 counts per crystal and DOI
+  // combination, drv:4424-4471) stands for the smoothed randoms gen_delays
+  // computes from it, over the prompt sinogram's scan duration
+  const long long ch_bytes = (long long)2 * 2 * 104 * 8 * 72 * 4;
+  if (file_size(o.delayed) == ch_bytes) {
+    float duration = 0.f;
+    if (!scan_duration_of(o.prompt, &duration))
+      die("Error: scan duration not found in sinogram %s header", o.prompt.c_str());
+    const std::vector<int32_t> ch = read_flat<int32_t>(o.delayed, (size_t)ch_bytes / 4);
+    hrrt_lm *lm = nullptr;
+    if (hrrt_lm_create(o.span, o.maxdel, o.device, &lm) != HRRT_OK) die("%s", hrrt_lm_last_error(lm));
+    if ((size_t)hrrt_lm_sino_size(lm) != nbins) die("smoothed randoms: sinogram size mismatch");
+    delayed.resize(nbins);
+    int iters = 0;
+    if (hrrt_lm_smooth_randoms(lm, ch.data(), duration, 0.f, delayed.data(), &iters) != HRRT_OK)
+      die("%s", hrrt_lm_last_error(lm));
+    hrrt_lm_destroy(lm);
+    if (o.verbose) std::printf("smoothed randoms from %s (%g s, %d singles iterations)\n", o.delayed.c_str(),
+                               duration, iters);
+  } else {
+    delayed = read_scan(o.delayed);
+  }
   std::vector<float> scatter;
   if (!o.scatter.empty()) {
     const size_t plane = (size_t)info.nviews * info.nbins;

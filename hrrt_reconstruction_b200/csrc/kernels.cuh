@@ -115,8 +115,7 @@ struct ProjTune {
   int fp_planes;  // planes per forward-projection task: 7, 9 or 11 (0: kFpPlanes)
   int fp_pwarps;  // producer warps of the forward projector (0: as many as fit, 2..6)
   int bp_planes;  // planes per back-projection task: 4 or 8 (0: kBpZ)
-  int bp_threads; // threads per back-projection CTA: 256 or 384 (0: 384 where shared memory admits two
-                  // CTAs per SM or fewer, else 256)
+  int bp_threads; // threads per back-projection CTA: 256 or 384 (0: 384)
 };
 inline ProjTune default_tune() { return ProjTune{0, 0, 0, 0}; }
 constexpr int kFpPlaneVariants[3] = {7, 9, 11};

@@ -51,13 +51,18 @@ constexpr int kTileWords = kThreads * kSub;    // 4096
 constexpr long long kPacketWords = 2LL << 20;  // 1 Mi 64-bit events
 static_assert(kPacketWords % kTileWords == 0, "tiles must not straddle packets");
 constexpr int kSinoPlane = 256 * 288;
-// The partitioned histogram path (events scattered by 64 MB partition, then
-// added partition by partition in L2) gives the same sinograms; on B200 it
-// measured slower than the direct atomics (18.3 vs 13.8 ms for 2.5e8 events:
-// its two extra parses cost more than the DRAM read-modify-writes it saves),
-// so it runs only when asked for (HRRT_LM_FORCE_PARTITIONED).
+// Three ways to the same sinograms.  Direct (the default): 16-bit bins updated
+// with atomics whose old value is checked for a carry.  Wide: 32-bit counters
+// updated with reductions that return nothing, folded into the 16-bit bins at
+// the end.  Partitioned: events scattered by 64 MB partition and added
+// partition by partition in L2.  On B200, for 2.5e8 events: direct 14.3 ms,
+// wide 17.0 ms (the random read-modify-write of a DRAM sector per event bounds
+// both; the wide path adds a clear and a fold of 4-byte counters), partitioned
+// 21.0 ms (two extra parses), so the other two run only when asked for.
 constexpr bool kPartitionedByDefault = false;
 constexpr long long kPartitionMinWords = 1LL << 24;
+constexpr bool kWideByDefault = false;
+constexpr long long kWideMinWords = 1LL << 26;
 // EWTYPES (geometry_info.h:76) packed two bits per entry: index =
 // (ew1 >> 30) << 2 | (ew2 >> 30); 0 prompt, 1 delayed, 2 tag, 3 out of sync
 constexpr uint32_t kEwTypes = (3u << 0) | (3u << 2) | (1u << 4) | (0u << 6) | (3u << 8) | (3u << 10) | (2u << 12) |
@@ -441,8 +446,10 @@ __device__ __forceinline__ void bump16_events(uint32_t *__restrict__ sino, uint3
 
 // kMode 0: time tags only; 1: histogram directly (atomics into the 16-bit
 // bins); 2: count events per histogram partition; 3: scatter packed event
-// records (address | sinogram << 29 | subtract << 30) partition-major.
-// Statistics are counted by modes 1 and 2.
+// records (address | sinogram << 29 | subtract << 30) partition-major; 4:
+// histogram into 32-bit counters with reductions that return nothing (no
+// carry to check, so no read-modify-write round trip per event), folded into
+// the 16-bit bins afterwards.  Statistics are counted by modes 1, 2 and 4.
 template <int kMode>
 __global__ void __launch_bounds__(kThreads) lm_hist_kernel(
     LmDev g, const uint32_t *__restrict__ words, long long n, const uint8_t *__restrict__ tile_entry,
@@ -498,6 +505,10 @@ __global__ void __launch_bounds__(kThreads) lm_hist_kernel(
                       [&](const long long (&a)[kSub / 2], uint32_t live, uint32_t sel, uint32_t minus) {
                         bump16_events<kSub / 2>(sino, dly, a, live, sel, minus);
                       });
+  } else if (kMode == 4) {
+    int *cs = reinterpret_cast<int *>(records), *cd = cs + g.sino_size;
+    auto wide = [&](long long addr, int sel, bool minus) { atomicAdd((sel ? cd : cs) + addr, minus ? -1 : 1); };
+    walk_events<true>(g, tb, w, s, e, pend, t0, limit, mode, flags, c, tagpos, tag_cap, tg, wide, each(wide));
   } else if (kMode == 2) {
     auto count = [&](long long addr, int sel, bool) { atomicAdd(&pcount[part_of(addr, sel)], 1u); };
     walk_events<true>(g, tb, w, s, e, pend, t0, limit, mode, flags, c, tagpos, tag_cap, tg, count, each(count));
@@ -522,7 +533,7 @@ __global__ void __launch_bounds__(kThreads) lm_hist_kernel(
     walk_events<false>(g, tb, w, s, e, pend, t0, limit, mode, flags, c, tagpos, 0, nullptr, scatter,
                        each(scatter));
   }
-  if (kMode == 1 || kMode == 2) {
+  if (kMode == 1 || kMode == 2 || kMode == 4) {
     // block reduction of the counters
 #pragma unroll
     for (int k = 0; k < kStCount; k++) {
@@ -565,6 +576,71 @@ __global__ void __launch_bounds__(kThreads) lm_part_hist_kernel(const uint32_t *
     const uint32_t r = __ldg(records + i);
     bump16(((r >> 29) & 1) ? dly : sino, r & 0x1FFFFFFFu, ((r >> 30) & 1) != 0);
   }
+}
+
+// Smoothed randoms: compute_delays (gen_delays_lib/gen_delays_lib.cpp:89-153)
+// for every head pair at once.  Thread = (head pair, crystal A (layer, y, x),
+// layer of crystal B, run of 8 crystal-B x positions); for each B crystal and
+// every B ring within maxrd + 6 rings of A the crystal pair is rebinned
+// exactly as an event is (rebin_address) and singles(A) * singles(B) * 2 tau
+// * T is added to its bin.  Crystal A's singles use the index of
+// gen_delays_fromarchive.cpp:191 (layer, y, head, x): the library copy at
+// gen_delays_lib.cpp:117 multiplies y by a whole layer and reads past the
+// singles array.
+__constant__ int c_pair_heads[21][2];
+constexpr int kDelayBxRun = 8;
+__global__ void __launch_bounds__(128) lm_delays_kernel(LmDev g, const float *__restrict__ csings, float tauftime,
+                                                        int maxrd, float *__restrict__ out) {
+  __shared__ LmShared tb;
+  if (threadIdx.x < 104) {
+    tb.zp[threadIdx.x] = g.zpos[threadIdx.x];
+    tb.zp2[threadIdx.x] = g.zpos2[threadIdx.x];
+  }
+  if (threadIdx.x < g.nsegs) {
+    tb.z0[threadIdx.x] = g.segz0[threadIdx.x];
+    tb.zmax[threadIdx.x] = g.segzmax[threadIdx.x];
+    tb.zoff[threadIdx.x] = g.segzoff[threadIdx.x];
+  }
+  __syncthreads();
+  constexpr int kRuns = 72 / kDelayBxRun;
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int run = (int)(t % kRuns);
+  t /= kRuns;
+  const int bl = (int)(t % 2);
+  t /= 2;
+  const int ax = (int)(t % 72);
+  t /= 72;
+  const int ay = (int)(t % 104);
+  t /= 104;
+  const int al = (int)(t % 2);
+  const int mp = (int)(t / 2) + 1;
+  if (mp > 20) return;
+  const int ahead = c_pair_heads[mp][0], bhead = c_pair_heads[mp][1];
+  const float awt = csings[al * 59904 + ay * 576 + ahead * 72 + ax] * tauftime;
+  if (awt == 0) return;
+  // B rings with |ay - by| < maxrd + 6
+  const int bs = max(0, ay - (maxrd + 5)), be = min(103, ay + maxrd + 5);
+  for (int bx = run * kDelayBxRun; bx < (run + 1) * kDelayBxRun; bx++) {
+    const hrrt::LmSol sol = g.sol[sol_index(mp, al, ax, bl, bx)];
+    if (sol.nsino == -1) continue;
+    const float *sb = csings + bl * 59904 + bhead * 72 + bx;
+    for (int by = bs; by <= be; by++) {
+      const long long a = rebin_address(g, tb, sol, ay, by);
+      if (a >= 0) atomicAdd(out + a, sb[576 * by] * awt);
+    }
+  }
+}
+
+// The 32-bit counts of mode 4 added into the 16-bit bins modulo 2^16 (the
+// reference's short bins wrap the same way), two bins (one 32-bit word) per
+// thread.
+__global__ void lm_fold_kernel(const int2 *__restrict__ counts, uint32_t *__restrict__ bins, long long npairs) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npairs) return;
+  const int2 c = counts[i];
+  const uint32_t b = bins[i];
+  const uint32_t lo = (b + (uint32_t)c.x) & 0xFFFFu, hi = ((b >> 16) + (uint32_t)c.y) & 0xFFFFu;
+  bins[i] = lo | (hi << 16);
 }
 
 }  // namespace
@@ -792,13 +868,23 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
   // histogrammed partition by partition in L2) for long ones.
   const int pps = (int)((h->dev.sino_size + (1LL << kPartShift) - 1) >> kPartShift);
   bool partitioned = kPartitionedByDefault && nwords >= kPartitionMinWords;
-  if (flags & HRRT_LM_FORCE_DIRECT) partitioned = false;
-  if (flags & HRRT_LM_FORCE_PARTITIONED) partitioned = true;
+  bool wide = kWideByDefault && nwords >= kWideMinWords;
+  if (flags & HRRT_LM_FORCE_DIRECT) partitioned = wide = false;
+  if (flags & HRRT_LM_FORCE_PARTITIONED) {
+    partitioned = true;
+    wide = false;
+  }
+  if (flags & HRRT_LM_FORCE_WIDE) {
+    wide = true;
+    partitioned = false;
+  }
   if (2 * pps > kMaxParts) partitioned = false;
   unsigned long long *cursor = stats + kStCount + 1;          // [kMaxParts]
   unsigned long long *starts = cursor + kMaxParts;            // [kMaxParts + 1]
-  if (partitioned && e == cudaSuccess) {
-    const long long cap = nwords / 2 + 1;
+  if ((partitioned || wide) && e == cudaSuccess) {
+    // partitioned: one packed record per event; wide: 32-bit counters for
+    // both sinograms
+    const long long cap = partitioned ? nwords / 2 + 1 : 2 * h->dev.sino_size;
     if (cap > h->rec_cap) {
       if (h->records) cudaFree(h->records);
       h->records = nullptr;
@@ -806,7 +892,7 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
       e = cudaMalloc(&h->records, sizeof(uint32_t) * (size_t)cap);
       if (e != cudaSuccess) {
         h->records = nullptr;
-        partitioned = false;  // not enough memory: fall back to the direct path
+        partitioned = wide = false;  // not enough memory: fall back to the direct path
         e = cudaSuccess;
         cudaGetLastError();
       } else {
@@ -815,6 +901,7 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
     }
   }
   if (partitioned && e == cudaSuccess) e = cudaMemsetAsync(cursor, 0, 8 * kMaxParts, st);
+  if (wide && e == cudaSuccess) e = cudaMemsetAsync(h->records, 0, sizeof(uint32_t) * 2 * h->dev.sino_size, st);
   auto launch = [&](int kmode, long long lim, long long tcap) {
     const unsigned nb = (unsigned)ntiles;
     uint32_t *sn = (uint32_t *)d_sino, *dl = (uint32_t *)d_delayed;
@@ -831,6 +918,10 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
         lm_hist_kernel<2><<<nb, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
                                                    mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
         break;
+      case 4:
+        lm_hist_kernel<4><<<nb, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
+                                                   mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
+        break;
       default:
         lm_hist_kernel<3><<<nb, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
                                                    mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
@@ -840,7 +931,8 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
   // pass 1: the ordered time tags (and, without a frame length, the counts
   // or the histogram itself)
   const bool one_pass = duration <= 0;
-  if (e == cudaSuccess) e = launch(one_pass ? (partitioned ? 2 : 1) : 0, one_pass ? nwords : -1, tag_cap);
+  const int hist_mode = partitioned ? 2 : (wide ? 4 : 1);
+  if (e == cudaSuccess) e = launch(one_pass ? hist_mode : 0, one_pass ? nwords : -1, tag_cap);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   std::vector<longlong2> htags;
   if (e == cudaSuccess && ntags > 0) {
@@ -856,7 +948,15 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
   const long long end_tag = replay_clock(h, htags.data(), (long long)ntags, duration, flags, &frame_start);
   long long limit = nwords;
   if (end_tag >= 0) limit = htags[end_tag].x;
-  if (!one_pass) e = launch(partitioned ? 2 : 1, limit, 0);
+  if (!one_pass) e = launch(hist_mode, limit, 0);
+  if (wide && e == cudaSuccess) {
+    const long long np = h->dev.sino_size / 2;  // bin pairs (sinogram sizes are multiples of 4)
+    const unsigned nb = (unsigned)((np + 255) / 256);
+    const int2 *cs = reinterpret_cast<const int2 *>(h->records);
+    lm_fold_kernel<<<nb, 256, 0, st>>>(cs, (uint32_t *)d_sino, np);
+    if (mode == HRRT_LM_PROMPTS_AND_DELAYED) lm_fold_kernel<<<nb, 256, 0, st>>>(cs + np, (uint32_t *)d_delayed, np);
+    e = cudaGetLastError();
+  }
   if (partitioned && e == cudaSuccess) {
     lm_part_scan_kernel<<<1, 32, 0, st>>>(cursor, 2 * pps, starts);
     e = launch(3, limit, 0);
@@ -965,6 +1065,49 @@ int hrrt_lm_histogram(hrrt_lm *h, const uint32_t *words, long long nwords, int m
     e = cudaMemcpyAsync(delayed, h->h_sino_dev + S, sizeof(uint16_t) * S, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_histogram");
+  return HRRT_OK;
+}
+
+int hrrt_lm_crystal_singles(const int32_t *delayed_counts, float scan_duration, float tau, float *singles) {
+  if (!delayed_counts || !singles) return HRRT_ERR_ARG;
+  return hrrt::singles_from_delayed(delayed_counts, tau > 0 ? tau : 6.0e-9f, scan_duration > 0 ? scan_duration : 1.0f,
+                                    singles);
+}
+
+int hrrt_lm_smooth_randoms(hrrt_lm *h, const int32_t *coinc_hist, float scan_duration, float tau, float *sino,
+                           int *iterations) {
+  if (!h) return HRRT_ERR_ARG;
+  if (!coinc_hist || !sino) return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_smooth_randoms: null buffer");
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_smooth_randoms");
+  // gen_delays: the delayed half of the histogram gives the crystal singles
+  // (g_tau 6 ns and g_ftime 1 s unless given, gen_delays_lib.cpp:322-323)
+  const float t = tau > 0 ? tau : 6.0e-9f, ft = scan_duration > 0 ? scan_duration : 1.0f;
+  std::vector<float> cs(hrrt::kCrystals);
+  const int it = hrrt::singles_from_delayed(coinc_hist + hrrt::kCrystals, t, ft, cs.data());
+  if (iterations) *iterations = it;
+  int heads[21][2];
+  for (int mp = 0; mp < 21; mp++) hrrt::pair_heads(mp, &heads[mp][0], &heads[mp][1]);
+  const long long S = h->dev.sino_size;
+  cudaStream_t st = h->stream;
+  float *d_cs = nullptr, *d_out = nullptr;
+  e = cudaMemcpyToSymbolAsync(c_pair_heads, heads, sizeof(heads), 0, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_cs, sizeof(float) * hrrt::kCrystals, st);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_out, sizeof(float) * S, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_cs, cs.data(), sizeof(float) * hrrt::kCrystals, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_out, 0, sizeof(float) * S, st);
+  if (e == cudaSuccess) {
+    const long long threads = 20LL * 2 * 104 * 72 * 2 * (72 / kDelayBxRun);
+    lm_delays_kernel<<<(unsigned)((threads + 127) / 128), 128, 0, st>>>(h->dev, d_cs, t * ft, h->tab.maxrd, d_out);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sino, d_out, sizeof(float) * S, cudaMemcpyDeviceToHost, st);
+  if (d_cs) cudaFreeAsync(d_cs, st);
+  if (d_out) cudaFreeAsync(d_out, st);
+  const cudaError_t e2 = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = e2;
+  if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_smooth_randoms");
   return HRRT_OK;
 }
 

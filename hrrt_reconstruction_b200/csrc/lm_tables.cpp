@@ -140,4 +140,92 @@ std::string LmTables::build(int span_, int maxrd_) {
   return std::string();
 }
 
+// ---- crystal singles from delayed coincidences (gen_delays_lib.cpp:163-255) ----
+// Crystal index i = x + 72*head + 576*y + 59904*layer (compute_drate, :175).
+
+void pair_heads(int mp, int *ahead, int *bhead) {
+  *ahead = kPairHeads[mp][0];
+  *bhead = kPairHeads[mp][1];
+}
+
+namespace {
+
+constexpr int kNH = LmTables::kHeads, kNX = LmTables::kXCrys, kNY = LmTables::kYCrys, kND = LmTables::kLayers;
+constexpr int kPerLayer = kNH * kNX * kNY;
+
+int crystal(int head, int layer, int cx, int cy) { return kNX * head + cx + kNX * kNH * cy + kPerLayer * layer; }
+
+// per-head singles totals in the reference's summation order (layer, x, y)
+void head_sums(const float *srate, float *hsum) {
+  for (int head = 0; head < kNH; head++) {
+    hsum[head] = 0.0f;
+    for (int layer = 0; layer < kND; layer++)
+      for (int cx = 0; cx < kNX; cx++)
+        for (int cy = 0; cy < kNY; cy++) hsum[head] += srate[crystal(head, layer, cx, cy)];
+  }
+}
+
+// the five heads facing `head` (heads head+2 .. head+6)
+float facing_sum(const float *hsum, int head) {
+  float s = 0.0f;
+  for (int j = 0; j < 5; j++) s += hsum[(head + j + 2) % kNH];
+  return s;
+}
+
+// compute_drate (:163-193): expected delayed rate of every crystal
+void drate_of(const float *srate, float tau, float *drate) {
+  float hsum[kNH];
+  head_sums(srate, hsum);
+  for (int head = 0; head < kNH; head++) {
+    const float oh = facing_sum(hsum, head);
+    for (int layer = 0; layer < kND; layer++)
+      for (int cx = 0; cx < kNX; cx++)
+        for (int cy = 0; cy < kNY; cy++) {
+          const int i = crystal(head, layer, cx, cy);
+          drate[i] = srate[i] * tau * oh;
+        }
+  }
+}
+
+// estimate_srate (:195-222): halfway towards the rates that explain drate
+void update_srate(const float *drate, float tau, float *srate) {
+  float hsum[kNH];
+  head_sums(srate, hsum);
+  for (int head = 0; head < kNH; head++) {
+    const float oh = facing_sum(hsum, head);
+    for (int layer = 0; layer < kND; layer++)
+      for (int cx = 0; cx < kNX; cx++)
+        for (int cy = 0; cy < kNY; cy++) {
+          const int i = crystal(head, layer, cx, cy);
+          srate[i] = (srate[i] + drate[i] / (tau * oh)) / 2.0f;
+        }
+  }
+}
+
+}  // namespace
+
+int singles_from_delayed(const int32_t *dcoins, float tau, float dt, float *srates) {
+  std::vector<float> drates(kCrystals), xrates(kCrystals);
+  for (int i = 0; i < kCrystals; i++) drates[i] = dcoins[i] / dt;
+  // compute_initial_srate (:224-232)
+  float dtotal = 0.0f;
+  for (int i = 0; i < kCrystals; i++) dtotal += drates[i];
+  const float stotal = (float)(8.0 * std::sqrt(dtotal / (40. * tau)));
+  for (int i = 0; i < kCrystals; i++) srates[i] = drates[i] * stotal / dtotal;
+  int iter;
+  for (iter = 0; iter < 100; iter++) {
+    drate_of(srates, tau, xrates.data());
+    // errtotal (:234-243): squared rounding error of the predicted counts, in
+    // the reference's int arithmetic (wrapping, as its build does)
+    uint32_t err = 0;
+    for (int i = 0; i < kCrystals; i++) {
+      const uint32_t d = (uint32_t)(int)(dcoins[i] - (0.5 + xrates[i] * dt));
+      err += d * d;
+    }
+    if (iter && err == 0) break;
+    update_srate(drates.data(), tau, srates);
+  }
+  return iter;
+}
+
 }  // namespace hrrt

@@ -35,4 +35,14 @@ struct LmTables {
   std::string build(int span, int maxrd);
 };
 
+// Crystal singles rates from the delayed coincidence counts of a
+// coincidence histogram (compute_csings_from_drates and its helpers,
+// gen_delays_lib/gen_delays_lib.cpp:163-255): `dcoins` and `srates` are
+// [layer 2][y 104][head 8][x 72]; `dt` the scan duration (s), `tau` the
+// coincidence window (s).  Returns the iterations run (at most 100).
+int singles_from_delayed(const int32_t *dcoins, float tau, float dt, float *srates);
+constexpr int kCrystals = LmTables::kLayers * LmTables::kYCrys * LmTables::kHeads * LmTables::kXCrys;  // 119808
+// head pair mp (1..20) -> (head a, head b)
+void pair_heads(int mp, int *ahead, int *bhead);
+
 }  // namespace hrrt

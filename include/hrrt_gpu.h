@@ -234,7 +234,7 @@ typedef struct hrrt_tuning {
   int fp_planes;          /* planes per forward-projection task: 7, 9 or 11 (0: 9) */
   int fp_producer_warps;  /* sampling warps of the forward projector: 2..6 (0: as many as fit) */
   int bp_planes;          /* planes per back-projection task: 4 or 8 (0: 8) */
-  int bp_threads;         /* threads per back-projection CTA: 256 or 384 (0: by the CTA's shared memory) */
+  int bp_threads;         /* threads per back-projection CTA: 256 or 384 (0: 384) */
   double fp_ms, bp_ms;    /* filled by the tuners: the chosen shapes' device time per launch */
 } hrrt_tuning;
 
@@ -310,11 +310,14 @@ int hrrt_batch_get_image(hrrt_batch *b, int frame, float *image_zyx, double *sum
 #define HRRT_LM_IGNORE_BORDER_CRYSTAL 1
 #define HRRT_LM_NO_DOI 2
 #define HRRT_LM_TIME_FROM_COUNT 4
-/* implementation choice (same result): by default events are added with
- * atomics straight into the sinograms; FORCE_PARTITIONED scatters them by
- * 64 MB partition first and adds each partition in L2 (slower on B200) */
+/* implementation choice (same result): by default events are added straight
+ * into the 16-bit bins; FORCE_WIDE counts into 32-bit scratch counters
+ * (reductions without a round trip) folded into the 16-bit bins at the end,
+ * FORCE_PARTITIONED scatters events by 64 MB partition first and adds each
+ * partition in L2.  Both measured slower than the default on B200. */
 #define HRRT_LM_FORCE_DIRECT 16
 #define HRRT_LM_FORCE_PARTITIONED 32
+#define HRRT_LM_FORCE_WIDE 64
 
 typedef struct hrrt_lm_stats {
   long long words_used;  /* words consumed: through the tag that ended the frame, or all */
@@ -369,6 +372,25 @@ int hrrt_lm_histogram(hrrt_lm *lm, const uint32_t *words, long long nwords, int 
  * aligned), ADDING into sino / delayed, on `stream` (NULL: the library's). */
 int hrrt_lm_histogram_device(hrrt_lm *lm, const uint32_t *d_words, long long nwords, int mode, int duration,
                              int flags, uint16_t *d_sino, uint16_t *d_delayed, hrrt_lm_stats *stats, void *stream);
+
+/* Smoothed randoms from a coincidence histogram (.ch: int32 [2][119808],
+ * prompt then delayed counts per crystal [layer 2][ring 104][head 8][x 72]).
+ * Replaces gen_delays (gen_delays_lib/gen_delays_lib.cpp:285-548), which
+ * hrrt_osem3d runs when -d names a .ch file (hrrt_osem3d_span3.cpp:4424-4471):
+ * crystal singles from the delayed counts (compute_csings_from_drates,
+ * :163-255, on the host), then for every crystal pair within maxrd + 6 rings
+ * singles(A) * singles(B) * 2 tau * T added to the pair's bin of the
+ * context's span (compute_delays, :89-153, on the device).  Crystal A's
+ * singles are indexed as gen_delays_fromarchive.cpp:191 does (the library
+ * copy's index reads past the array).  sino: the flat float sinogram
+ * (hrrt_lm_sino_size floats); scan_duration <= 0 means 1 s, tau <= 0 means
+ * 6 ns; *iterations (may be NULL): the singles estimate's iterations.  Sums are
+ * accumulated in float with device atomics (order varies at rounding level). */
+int hrrt_lm_smooth_randoms(hrrt_lm *lm, const int32_t *coinc_hist, float scan_duration, float tau, float *sino,
+                           int *iterations);
+/* Host-only (no GPU needed): the crystal singles estimate alone, from the
+ * 119808 delayed crystal counts; returns the iterations run. */
+int hrrt_lm_crystal_singles(const int32_t *delayed_counts, float scan_duration, float tau, float *singles);
 
 #ifdef __cplusplus
 }

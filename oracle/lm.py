@@ -60,6 +60,9 @@ def lib():
             getattr(L, n).restype = None
         L.lm_rebin_event.argtypes = [vp, i, i, i, i, i, i, i]
         L.lm_histogram.argtypes = [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, vp, vp]
+        f = ctypes.c_float
+        L.lm_crystal_singles.argtypes = [vp, f, f, vp]
+        L.lm_smooth_randoms.argtypes = [vp, vp, f, f, i, vp]
         _L = L
     return _L
 
@@ -127,6 +130,40 @@ class LMOracle:
         self.L.lm_histogram(self.t, _p(w), w.size, mode, duration, flags, ctypes.byref(self.clock), _p(sino),
                             _p(delayed), ctypes.byref(st))
         return sino, delayed, st.as_dict()
+
+
+NCRYSTALS = 2 * 104 * 8 * 72  # [layer][ring][head][x]
+
+
+def crystal_singles(delayed_counts, scan_duration=1.0, tau=6.0e-9):
+    """gen_delays' crystal singles estimate (gen_delays_lib.cpp:163-255):
+    -> (singles float32 [119808], iterations)."""
+    d = np.ascontiguousarray(delayed_counts, np.int32).reshape(-1)
+    assert d.size == NCRYSTALS
+    out = np.zeros(NCRYSTALS, np.float32)
+    it = lib().lm_crystal_singles(_p(d), tau, scan_duration, _p(out))
+    return out, it
+
+
+def smooth_randoms(oracle, coinc_hist, scan_duration=1.0, tau=6.0e-9, maxrd=67):
+    """gen_delays' randoms sinogram (float32, the oracle's span) from a
+    coincidence histogram [2][119808] int32 -> (sino, iterations)."""
+    h = np.ascontiguousarray(coinc_hist, np.int32).reshape(-1)
+    assert h.size == 2 * NCRYSTALS
+    out = np.zeros(oracle.sino_size, np.float32)
+    it = lib().lm_smooth_randoms(oracle.t, _p(h), scan_duration, tau, maxrd, _p(out))
+    return out, it
+
+
+def delayed_counts_from_singles(singles, scan_duration=1.0, tau=6.0e-9):
+    """The forward model the estimator inverts (compute_drate,
+    gen_delays_lib.cpp:163-193), rounded to counts: a coincidence histogram's
+    delayed half for known crystal singles rates."""
+    s = np.asarray(singles, np.float64).reshape(2, 104, 8, 72)
+    hsum = s.sum(axis=(0, 1, 3))
+    facing = np.array([sum(hsum[(h + j + 2) % 8] for j in range(5)) for h in range(8)])
+    rate = s * tau * facing[None, None, :, None]
+    return np.floor(rate * scan_duration + 0.5).astype(np.int32).reshape(-1)
 
 
 # ---- word builders (the l64 event layout, histogram_mp.cpp:1026-1233) ----

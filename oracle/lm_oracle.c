@@ -394,3 +394,109 @@ int lm_histogram(const lm_tables *t, const uint32_t *w, long long n, int mode, i
   st->duration = clk->current_time - frame_start;
   return 0;
 }
+
+/* ---- smoothed randoms (gen_delays_lib/gen_delays_lib.cpp) ---------------- */
+/* crystal index of the coincidence histogram and of the singles:
+ * x + 72 head + 576 y + 59904 layer (compute_drate, gdl:175) */
+#define NCRYS (NDOIS * NYCRYS * NHEADS * NXCRYS)
+static int crys(int head, int layer, int cx, int cy) {
+  return NXCRYS * head + cx + NXCRYS * NHEADS * cy + NXCRYS * NYCRYS * NHEADS * layer;
+}
+static void head_sums(const float *srate, float *hsum) {
+  for (int head = 0; head < NHEADS; head++) {
+    hsum[head] = 0.0f;
+    for (int layer = 0; layer < NDOIS; layer++)
+      for (int cx = 0; cx < NXCRYS; cx++)
+        for (int cy = 0; cy < NYCRYS; cy++) hsum[head] += srate[crys(head, layer, cx, cy)];
+  }
+}
+static float facing(const float *hsum, int head) {
+  float s = 0.0f;
+  for (int j = 0; j < 5; j++) s += hsum[(head + j + 2) % NHEADS];
+  return s;
+}
+
+/* compute_csings_from_drates with compute_initial_srate, compute_drate,
+ * errtotal and estimate_srate (gdl:163-255) */
+int lm_crystal_singles(const int32_t *dcoins, float tau, float dt, float *srates) {
+  float *drates = (float *)malloc(sizeof(float) * NCRYS), *xrates = (float *)malloc(sizeof(float) * NCRYS);
+  float hsum[NHEADS];
+  for (int i = 0; i < NCRYS; i++) drates[i] = dcoins[i] / dt;
+  float dtotal = 0.0f;
+  for (int i = 0; i < NCRYS; i++) dtotal += drates[i];
+  const float stotal = (float)(8.0 * sqrt(dtotal / (40. * tau)));
+  for (int i = 0; i < NCRYS; i++) srates[i] = drates[i] * stotal / dtotal;
+  int iter;
+  for (iter = 0; iter < 100; iter++) {
+    head_sums(srates, hsum);
+    for (int head = 0; head < NHEADS; head++) {
+      const float oh = facing(hsum, head);
+      for (int layer = 0; layer < NDOIS; layer++)
+        for (int cx = 0; cx < NXCRYS; cx++)
+          for (int cy = 0; cy < NYCRYS; cy++) {
+            const int i = crys(head, layer, cx, cy);
+            xrates[i] = srates[i] * tau * oh;
+          }
+    }
+    uint32_t err = 0; /* int arithmetic of errtotal, wrapping */
+    for (int i = 0; i < NCRYS; i++) {
+      const uint32_t d = (uint32_t)(int)(dcoins[i] - (0.5 + xrates[i] * dt));
+      err += d * d;
+    }
+    if (iter && err == 0) break;
+    head_sums(srates, hsum);
+    for (int head = 0; head < NHEADS; head++) {
+      const float oh = facing(hsum, head);
+      for (int layer = 0; layer < NDOIS; layer++)
+        for (int cx = 0; cx < NXCRYS; cx++)
+          for (int cy = 0; cy < NYCRYS; cy++) {
+            const int i = crys(head, layer, cx, cy);
+            srates[i] = (srates[i] + drates[i] / (tau * oh)) / 2.0f;
+          }
+    }
+  }
+  free(drates);
+  free(xrates);
+  return iter;
+}
+
+/* gen_delays (gdl:285-548) on one thread: singles from the delayed half of
+ * the histogram, then compute_delays (gdl:89-153) for head pairs 1..20 in
+ * turn, crystal A's singles indexed as gen_delays_fromarchive.cpp:191 does.
+ * sino: lm_sino_size() floats, overwritten. */
+int lm_smooth_randoms(const lm_tables *t, const int32_t *coinc_hist, float scan_duration, float tau, int maxrd,
+                      float *sino) {
+  const float tt = tau > 0 ? tau : 6.0e-9f, ft = scan_duration > 0 ? scan_duration : 1.0f;
+  float *cs = (float *)malloc(sizeof(float) * NCRYS);
+  const int it = lm_crystal_singles(coinc_hist + NCRYS, tt, ft, cs);
+  memset(sino, 0, sizeof(float) * (size_t)lm_sino_size(t));
+  const float tauftime = tt * ft;
+  for (int mp = 1; mp <= NMPAIRS; mp++) {
+    const int ahead = HRRT_MPAIRS[mp][0], bhead = HRRT_MPAIRS[mp][1];
+    for (int al = 0; al < NDOIS; al++)
+      for (int ay = 0; ay < NYCRYS; ay++) {
+        int bs = 1000, be = -1000;
+        for (int by = 0; by < NYCRYS; by++) {
+          const int rd = ay > by ? ay - by : by - ay;
+          if (rd < maxrd + 6) {
+            if (bs > by) bs = by;
+            if (be < by) be = by;
+          }
+        }
+        for (int ax = 0; ax < NXCRYS; ax++) {
+          const float aw = cs[al * NHEADS * NXCRYS * NYCRYS + ay * NHEADS * NXCRYS + ahead * NXCRYS + ax];
+          const float awt = aw * tauftime;
+          if (awt == 0) continue;
+          for (int bl = 0; bl < NDOIS; bl++)
+            for (int bx = 0; bx < NXCRYS; bx++)
+              for (int by = bs; by <= be; by++) {
+                const int a = lm_rebin_event(t, mp, al, ax, ay, bl, bx, by);
+                if (a < 0) continue;
+                sino[a] += cs[bl * NHEADS * NXCRYS * NYCRYS + bhead * NXCRYS + bx + NHEADS * NXCRYS * by] * awt;
+              }
+        }
+      }
+  }
+  free(cs);
+  return it;
+}

@@ -81,6 +81,14 @@ void lm_clock_init(lm_clock *c);
 int lm_histogram(const lm_tables *t, const uint32_t *words, long long nwords, int mode, int duration, int flags,
                  lm_clock *clock, uint16_t *sino, uint16_t *delayed, lm_stats *st);
 
+/* smoothed randoms (gen_delays): crystal singles from the 119808 delayed
+ * crystal counts (returns the iterations), and the randoms sinogram from a
+ * coincidence histogram [2][119808] (prompt then delayed counts), both as
+ * gen_delays_lib.cpp computes them */
+int lm_crystal_singles(const int32_t *dcoins, float tau, float dt, float *srates);
+int lm_smooth_randoms(const lm_tables *t, const int32_t *coinc_hist, float scan_duration, float tau, int maxrd,
+                      float *sino);
+
 #ifdef __cplusplus
 }
 #endif

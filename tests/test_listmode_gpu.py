@@ -52,7 +52,8 @@ def random_stream(seed, nevents, tag_every=1000, p_resync=1e-4, p_bad=0.01, p_de
     return np.concatenate(chunks).astype(np.uint32)
 
 
-FORCE_DIRECT, FORCE_PARTITIONED = 16, 32  # device path selection (same result)
+FORCE_DIRECT, FORCE_PARTITIONED, FORCE_WIDE = 16, 32, 64  # device path selection (same result)
+PATHS = (FORCE_DIRECT, FORCE_PARTITIONED, FORCE_WIDE)
 
 
 def compare(O, D, words, mode, duration=0, flags=0, path=0):
@@ -86,7 +87,7 @@ def test_known_answer_streams(pair):
         event_words(3, 35, 50, 35, 50, doia=3), event_words(3, 35, 50, 35, 50, doib=7), tag_words(0xA0000005),
         tag_words(0x40000000 | 12345), tag_words(777), good)]).astype(np.uint32)
     for mode in (lm.TRUES, lm.PROMPTS_AND_DELAYED, lm.PROMPTS_ONLY):
-        for path in (FORCE_DIRECT, FORCE_PARTITIONED):
+        for path in PATHS:
             compare(O, D, w, mode, path=path)
 
 
@@ -97,7 +98,7 @@ def test_wrap_and_trues(pair):
                            prompt=np.arange(n) % 3 != 0)
     w = interleave(ew1, ew2)
     for mode in (lm.TRUES, lm.PROMPTS_AND_DELAYED):
-        for path in (FORCE_DIRECT, FORCE_PARTITIONED):
+        for path in PATHS:
             compare(O, D, w, mode, path=path)
 
 
@@ -110,8 +111,11 @@ def test_random_stream_packets(pair, seed):
     st = compare(O, D, w, lm.PROMPTS_AND_DELAYED, path=FORCE_DIRECT)
     assert st["prompts"] > 0 and st["resyncs"] > 0 and st["invalid"] > 0 and st["doi7"] > 0
     compare(O, D, w, lm.PROMPTS_AND_DELAYED, path=FORCE_PARTITIONED)
+    compare(O, D, w, lm.PROMPTS_AND_DELAYED, path=FORCE_WIDE)
     compare(O, D, w, lm.TRUES, flags=lm.IGNORE_BORDER_CRYSTAL, path=FORCE_PARTITIONED)
+    compare(O, D, w, lm.TRUES, flags=lm.IGNORE_BORDER_CRYSTAL, path=FORCE_WIDE)
     compare(O, D, w, lm.PROMPTS_ONLY, flags=lm.NO_DOI, path=FORCE_PARTITIONED)
+    compare(O, D, w, lm.PROMPTS_ONLY, flags=lm.NO_DOI, path=FORCE_WIDE)
 
 
 def test_frames_follow_the_clock(pair):
@@ -124,7 +128,7 @@ def test_frames_follow_the_clock(pair):
     pos_o = pos_d = 0
     for k in range(3):
         so, do, sto = O.histogram(w[pos_o:], duration=1)
-        sd, dd, std = D.histogram(w[pos_d:], duration=1, flags=FORCE_PARTITIONED if k % 2 else FORCE_DIRECT)
+        sd, dd, std = D.histogram(w[pos_d:], duration=1, flags=PATHS[k % 3])
         assert np.array_equal(so, sd) and np.array_equal(do, dd)
         for key in STAT_KEYS:
             assert sto[key] == std[key], (key, sto[key], std[key])
@@ -142,9 +146,9 @@ def test_device_entry_adds_into_buffers(pair):
     dw = torch.from_numpy(w.view(np.int32)).cuda()
     ds = torch.zeros(D.sino_size, dtype=torch.int16, device="cuda")
     dd = torch.zeros(D.sino_size, dtype=torch.int16, device="cuda")
-    for _ in range(2):
+    for path in (FORCE_DIRECT, FORCE_WIDE):
         D.reset_clock()
-        D.histogram_device(dw.data_ptr(), w.size, ds.data_ptr(), dd.data_ptr())
+        D.histogram_device(dw.data_ptr(), w.size, ds.data_ptr(), dd.data_ptr(), flags=path)
     torch.cuda.synchronize()
     got_s = ds.cpu().numpy().view(np.uint16)
     got_d = dd.cpu().numpy().view(np.uint16)
