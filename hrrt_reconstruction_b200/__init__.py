@@ -120,6 +120,9 @@ def _load():
         "hrrt_set_profiling": (i, [vp, i]),
         "hrrt_kernel_stats": (i, [vp, ctypes.c_char_p, ctypes.POINTER(i), ctypes.POINTER(d)]),
         "hrrt_reset_kernel_stats": (i, [vp]),
+        "hrrt_set_psf": (i, [vp, i, f, f, f]),
+        "hrrt_psf_convolve": (i, [vp, vp, vp]),
+        "hrrt_psf_kernel": (ctypes.c_longlong, [f, f, f, f, vp, i]),
         "hrrt_set_tuning": (i, [vp, ctypes.POINTER(Tuning)]),
         "hrrt_get_tuning": (i, [vp, ctypes.POINTER(Tuning)]),
         "hrrt_autotune": (i, [vp, i, ctypes.POINTER(Tuning)]),
@@ -371,6 +374,19 @@ class Context:
         return co
 
     # ---- timing ----
+    def set_psf(self, enable=True, fwhm1=0.0, fwhm2=0.0, ratio=0.0):
+        """-B fwhm1,fwhm2,ratio: PSF modelling in the sensitivity and the
+        subsets from now on (fwhm1 0: the HRRT defaults)."""
+        self._check(lib.hrrt_set_psf(self._h, 1 if enable else 0, fwhm1, fwhm2, ratio), "set_psf")
+
+    def psf(self, image_xyz):
+        """convolve3d of an [x][y][zp] image on FOV columns (set_psf first)."""
+        img = _c(image_xyz, np.float32)
+        assert img.shape == self.image_shape
+        out = np.empty(self.image_shape, np.float32)
+        self._check(lib.hrrt_psf_convolve(self._h, _ptr(img), _ptr(out)), "psf")
+        return out
+
     def set_tuning(self, fp_planes=0, fp_producer_warps=0, bp_planes=0, bp_threads=0):
         t = Tuning(fp_planes, fp_producer_warps, bp_planes, bp_threads, 0.0, 0.0)
         self._check(lib.hrrt_set_tuning(self._h, ctypes.byref(t)), "set_tuning")
@@ -475,6 +491,15 @@ class Batch:
         sm = ctypes.c_double()
         self.ctx._check(lib.hrrt_batch_get_image(self._h, frame, _ptr(out), ctypes.byref(sm)), "batch_get_image")
         return out, sm.value
+
+
+def psf_kernel(fwhm1=0.0, fwhm2=0.0, ratio=0.0, pixel_size=1.21875):
+    """Host-only: make1d_psf_filter's taps (fwhm1 0: the HRRT defaults)."""
+    k = np.zeros(256, np.float32)
+    n = lib.hrrt_psf_kernel(fwhm1, fwhm2, ratio, pixel_size, _ptr(k), 256)
+    if n < 1:
+        raise HrrtError("no PSF kernel for these parameters")
+    return k[:n].copy()
 
 
 def crystal_singles(delayed_counts, scan_duration=1.0, tau=6.0e-9):

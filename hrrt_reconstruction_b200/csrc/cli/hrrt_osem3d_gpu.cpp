@@ -7,10 +7,12 @@
 // projection of the final image as a flat float sinogram.
 //
 // Supported: -p -d -n -a -s -o -O -i -h -I -S -W 3 -m -f -k -e -u -Q -F -T -N
-// -D -L -v -X 256 -M 999 -g, -z 1, -Z 1.  The attenuation may be the span-9
-// file of a span-3 reconstruction (Atten3D_Span9, :1762-1796).  Options for
-// paths outside OP-OSEM (-t trues, -P/-R pre-corrected / 4-byte scans, -B PSF,
-// -A MAP, -U mu-map, -C compression, -w) are refused with a message.
+// -D -L -v -X 256 -M 999 -g -B, -z 1, -Z 1.  The attenuation may be the
+// span-9 file of a span-3 reconstruction (Atten3D_Span9, :1762-1796), the
+// scatter a 2D segment with span-9 scale factors, the randoms a coincidence
+// histogram (.ch).  Options for paths outside OP-OSEM (-t trues, -P/-R
+// pre-corrected / 4-byte scans, -A MAP, -U mu-map, -C compression, -w) are
+// refused with a message.
 #include <cerrno>
 #include <chrono>
 #include <cmath>
@@ -29,6 +31,8 @@ struct Options {
   std::string prompt, delayed, norm, atten, scatter, out, init, out3d;
   bool save_each = false, float_prompts = false;
   int iterations = 1, subsets = 16, weighting = 2, span = 9, maxdel = 67, npskip = 0, verbose = 0, device = 0;
+  bool psf = false;
+  float psf_fwhm1 = 0.f, psf_fwhm2 = 0.f, psf_ratio = 0.f;
   int in_flip = 0, out_flip = 0, trim = 0;
   float rel_fov = 0.95f, image_max = 1.e4f, eps1 = 5.e-2f, eps2 = 1.e-2f, eps3 = 1.e-10f;
   int z_min = 6, z_max = 200;
@@ -54,7 +58,8 @@ void usage() {
                "  -n  3D flat normalisation, -a attenuation (span 9 accepted for span 3), -s scatter\n"
                "      (3D, or the unscaled 2D segment followed by 2209 span-9 plane scale factors)\n"
                "  -o  output image (flat float [z][y][x] + .hdr), -O also after each iteration\n"
-               "  -h  output the forward projection of the final image (flat float scan)\n");
+               "  -h  output the forward projection of the final image (flat float scan)\n"
+               "  -B  fwhm1,fwhm2,ratio: PSF resolution modelling (0,0,0: the HRRT defaults)\n");
 }
 
 bool parse(int argc, char **argv, Options &o) {
@@ -117,7 +122,10 @@ bool parse(int argc, char **argv, Options &o) {
       }
       case 't': die("-t (trues input) is outside the OP-OSEM path; use -p and -d");
       case 'P': case 'R': die("-%s: pre-corrected / 4-byte scans are outside the OP-OSEM path", a + 1);
-      case 'B': die("-B (PSF resolution modelling) is not supported");
+      case 'B':
+        if (std::sscanf(val(), "%f,%f,%f", &o.psf_fwhm1, &o.psf_fwhm2, &o.psf_ratio) != 3) die("error decoding -B");
+        o.psf = true;
+        break;
       case 'A': die("-A (MAP) is not supported");
       case 'U': die("-U (mu-map reconstruction) is not supported");
       case 'C': die("-C (sinogram compression) is not supported");
@@ -181,7 +189,8 @@ void write_header(const Options &o, const hrrt_info &info, float voxel_mm, float
   std::fprintf(f, "scaling factor (mm/pixel) [1] := %f\n", voxel_mm);
   std::fprintf(f, "scaling factor (mm/pixel) [2] := %f\n", voxel_mm);
   std::fprintf(f, "scaling factor (mm/pixel) [3] := %f\n", plane_mm);
-  std::fprintf(f, "reconstruction method := inki-2006-may-OSEM3D-OP\n");
+  std::fprintf(f, o.psf ? "reconstruction method := inki-2006-may-OSEM3D-OP-PSF\n"
+                        : "reconstruction method := inki-2006-may-OSEM3D-OP\n");
   std::fprintf(f, "reconstruction version := hrrt_osem3d_gpu\n");
   std::fprintf(f, "prompt file used := %s\n", base(o.prompt));
   std::fprintf(f, "delayed file used := %s\n", base(o.delayed));
@@ -403,6 +412,8 @@ int main(int argc, char **argv) {
   if (hrrt_upload_inputs(ctx, prompts.data(), delayed.data(), norm.empty() ? nullptr : norm.data(),
                          atten.empty() ? nullptr : atten.data(), scatter.empty() ? nullptr : scatter.data(),
                          HRRT_STORE_F32) != HRRT_OK)
+    die("%s", hrrt_last_error(ctx));
+  if (o.psf && hrrt_set_psf(ctx, 1, o.psf_fwhm1, o.psf_fwhm2, o.psf_ratio) != HRRT_OK)
     die("%s", hrrt_last_error(ctx));
   if (hrrt_sensitivity(ctx) != HRRT_OK) die("%s", hrrt_last_error(ctx));
   const size_t vox = (size_t)info.nx * info.ny * info.nz;

@@ -73,8 +73,16 @@ struct hrrt_ctx {
   // a dynamic study using this context's geometry, mult and sensitivity
   struct hrrt_batch *batch = nullptr;
   // bumped whenever what a captured launch sequence depends on changes (back
-  // projector, launch shape, work lists)
+  // projector, launch shape, work lists, PSF)
   int config_epoch = 0;
+
+  // PSF resolution modelling (-B): the x / y filters (2h+1 taps), the
+  // inverted z tap sums, and three volumes: the blurred image, the
+  // correction image and the x pass
+  bool psf_on = false;
+  int psf_h = 0;
+  float *d_psf_fx = nullptr, *d_psf_fy = nullptr, *d_psf_normz = nullptr;
+  float *d_image_psf = nullptr, *d_corr = nullptr, *d_psf_tmp = nullptr;
 
   bool prof = false;
   std::vector<KernelTimer> pending;
@@ -192,6 +200,8 @@ int upload_flat(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms, con
                 const float *scatter, int storage, bool norm_atten_device, void *qp, void *qadd, void *qmult);
 // the forward-projection task list of tune.fp_planes into ctx->dg / dg_adj
 int apply_tune(hrrt_ctx *ctx, const ProjTune &t);
+// convolve3d of the PSF: out = psf(in) on FOV columns (in may equal out)
+int run_psf(hrrt_ctx *ctx, const float *in, float *out);
 // defined in batch.cu: a context being destroyed leaves its batch unusable
 void detach_batch(hrrt_batch *b);
 

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -27,6 +28,36 @@ namespace {
 // flat-file planes per upload chunk (96 planes of 288 x 256 bins: 127 MB of
 // staging per buffer with all five inputs)
 constexpr int kUploadPlanes = 96;
+
+// make1d_psf_filter (psf.cpp:21-70): two Gaussians of FWHM fwhm1, fwhm2 (mm)
+// -- the second scaled by ratio -- sampled at the pixel size over 2h+1 taps
+// (h from 1.5 FWHM at the 10 % level) and normalised by their float sum;
+// fwhm1 == 0 selects the HRRT's defaults (0.9 and 2.5 sigma in mm, ratio
+// 0.05).  Empty when fwhm1 < 0.
+std::vector<float> psf_taps(float fwhm1, float fwhm2, float ratio, float pixel_size) {
+  if (fwhm1 == 0.0) {
+    fwhm1 = (float)(0.9 * std::sqrt(8.0 * std::log(2.0)));
+    fwhm2 = (float)(2.5 * std::sqrt(8.0 * std::log(2.0)));
+    ratio = 0.05f;
+  }
+  if (!(fwhm1 > 0.0)) return {};
+  const double w = (fwhm2 > 0.0 && ratio > 0.0) ? fwhm2 : fwhm1;
+  const int size = 2 * ((int)(1.5 * w * std::sqrt(std::log(10.0) / std::log(2.)) / pixel_size / 2.0)) + 1;
+  if (size < 1 || size > 255) return {};
+  const float sigma1 = (float)(fwhm1 / (std::sqrt(8.0 * std::log(2.0)) * pixel_size));
+  const float sigma2 = (float)(fwhm2 / (std::sqrt(8.0 * std::log(2.0)) * pixel_size));
+  const int bin0 = (size - 1) / 2;
+  std::vector<float> k(size);
+  float norm = 0.0f;
+  for (int b = 0; b < size; b++) {
+    k[b] = (float)std::exp(-0.5 * (std::pow((double)(b - bin0) / sigma1, 2.0)));
+    if (fwhm2 > 0.0 && ratio > 0.0)
+      k[b] = (float)(k[b] + ratio * std::exp(-0.5 * (std::pow((double)(b - bin0) / sigma2, 2.0))));
+    norm += k[b];
+  }
+  for (int b = 0; b < size; b++) k[b] /= norm;
+  return k;
+}
 
 // Forward-projection tasks shared by every quad: (segment, plane run, kind).
 std::vector<FpTask> build_fp_tasks(const Geometry &g, int PL) {
@@ -182,6 +213,36 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
   const QuadWork *fw = ctx->d_work + ctx->fp_off[s], *bw = ctx->d_work + ctx->bp_off[s];
   const int *pv = ctx->d_pair_views + (size_t)s * ctx->npairs;
   float *nf = ctx->d_nfinv + (size_t)s * ctx->vol;
+  if (ctx->psf_on) {
+    // -B (drv:4172, :4201-4202, :4229): project the blurred image, blur the
+    // correction image, then update
+    if (b.fr.n != 1 || b.fr.map) return fail(ctx, HRRT_ERR_STATE, "PSF runs one frame at a time");
+    if (int rc = run_psf(ctx, b.image, ctx->d_image_psf)) return rc;
+    {
+      Launch L(ctx, "fp_kernel");
+      CK(launch_fp(g, ctx->d_image_psf, fw, ctx->fp_cnt[s], 1, b.prompts, b.add, ctx->storage, b.ratio,
+                   ctx->quad_pair, ctx->tune, b.fr, ctx->stream),
+         "fp_kernel");
+    }
+    if (adj) {
+      CK(launch_adj(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, b.fr, ctx->stream),
+         "adj_kernel");
+      CK(cudaMemsetAsync(ctx->d_corr, 0, sizeof(float) * ctx->vol, ctx->stream), "psf");
+      CK(launch_adj_rotate(g, pv, ctx->npairs, b.bc, b.br, ctx->vol, nullptr, nullptr, ctx->d_corr, 2, b.fr,
+                           ctx->stream),
+         "adj_rotate_kernel");
+    } else {
+      CK(launch_bp(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, ctx->tune, b.fr,
+                   ctx->stream),
+         "bp_kernel");
+      CK(launch_rotback(g, pv, ctx->npairs, b.bc, b.br, ctx->vol, nullptr, nullptr, ctx->d_corr, 3, b.fr,
+                        ctx->stream),
+         "rotback_kernel");
+    }
+    if (int rc = run_psf(ctx, ctx->d_corr, ctx->d_corr)) return rc;
+    CK(launch_apply_corr(g, ctx->d_corr, b.image, nf, 0, ctx->stream), "update");
+    return HRRT_OK;
+  }
   {
     Launch L(ctx, "fp_kernel");
     CK(launch_fp(g, b.image, fw, ctx->fp_cnt[s], 1, b.prompts, b.add, ctx->storage, b.ratio, ctx->quad_pair,
@@ -240,6 +301,32 @@ int ensure_input_buffers(hrrt_ctx *ctx, int storage) {
 // inverse sensitivity of subset s (CalculateNormfac's subset body)
 int sens_subset(hrrt_ctx *ctx, int s) {
   const bool adj = ctx->bp_mode == HRRT_BP_ADJOINT;
+  if (ctx->psf_on) {
+    // the back projection blurred before its inversion (drv:3835-3841)
+    const DevGeom &g = adj ? ctx->dg_adj : ctx->dg;
+    const int *pv = ctx->d_pair_views + (size_t)s * ctx->npairs;
+    CK(launch_scale_pairs(g, ctx->q_mult, ctx->storage, pv, ctx->npairs, ctx->d_ratio, ctx->quad_pair, ctx->stream),
+       "scale_pairs");
+    if (adj) {
+      CK(launch_adj(g, ctx->d_ratio, ctx->quad_pair, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s], ctx->d_bc,
+                    ctx->d_br, ctx->vol, one_frame(), ctx->stream),
+         "adj_kernel");
+      CK(cudaMemsetAsync(ctx->d_corr, 0, sizeof(float) * ctx->vol, ctx->stream), "psf");
+      CK(launch_adj_rotate(g, pv, ctx->npairs, ctx->d_bc, ctx->d_br, ctx->vol, nullptr, nullptr, ctx->d_corr, 2,
+                           one_frame(), ctx->stream),
+         "adj_rotate_kernel");
+    } else {
+      CK(launch_bp(g, ctx->d_ratio, ctx->quad_pair, ctx->d_work + ctx->bp_off[s], ctx->bp_cnt[s], ctx->d_bc,
+                   ctx->d_br, ctx->vol, ctx->tune, one_frame(), ctx->stream),
+         "bp_kernel");
+      CK(launch_rotback(g, pv, ctx->npairs, ctx->d_bc, ctx->d_br, ctx->vol, nullptr, nullptr, ctx->d_corr, 3,
+                        one_frame(), ctx->stream),
+         "rotback_kernel");
+    }
+    if (int rc = run_psf(ctx, ctx->d_corr, ctx->d_corr)) return rc;
+    CK(launch_apply_corr(g, ctx->d_corr, nullptr, ctx->d_nfinv + (size_t)s * ctx->vol, 1, ctx->stream), "inverse");
+    return HRRT_OK;
+  }
   {
     Launch L(ctx, "scale_pairs_kernel");
     CK(launch_scale_pairs(adj ? ctx->dg_adj : ctx->dg, ctx->q_mult, ctx->storage,
@@ -347,6 +434,14 @@ int upload_flat(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms, con
   return HRRT_OK;
 }
 
+
+int run_psf(hrrt_ctx *ctx, const float *in, float *out) {
+  Launch L(ctx, "psf_kernel");
+  CK(launch_psf(ctx->dg, in, ctx->d_psf_tmp, out, ctx->d_psf_fx, ctx->psf_h, ctx->d_psf_fy, ctx->psf_h,
+                ctx->d_psf_normz, ctx->stream),
+     "psf");
+  return HRRT_OK;
+}
 
 int apply_tune(hrrt_ctx *ctx, const ProjTune &t) {
   const int pl = t.fp_planes > 0 ? t.fp_planes : kFpPlanes;
@@ -1012,6 +1107,81 @@ int hrrt_forward_project(hrrt_ctx *ctx, const float *image_xyz, float *sino) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return done(cuda_fail(ctx, e, "forward_project"));
   return done(device_status(ctx));
+}
+
+long long hrrt_psf_kernel(float fwhm1, float fwhm2, float ratio, float pixel_size, float *taps, int capacity) {
+  const std::vector<float> k = psf_taps(fwhm1, fwhm2, ratio, pixel_size);
+  if (k.empty()) return HRRT_ERR_ARG;
+  if (taps && capacity >= (int)k.size()) std::memcpy(taps, k.data(), k.size() * sizeof(float));
+  return (long long)k.size();
+}
+
+int hrrt_set_psf(hrrt_ctx *ctx, int enable, float fwhm1, float fwhm2, float ratio) {
+  if (!ctx) return HRRT_ERR_ARG;
+  if (ctx->batch && enable) return fail(ctx, HRRT_ERR_STATE, "PSF: not available while the context serves a batch");
+  const Geometry &g = ctx->geo;
+  if (!enable) {
+    if (ctx->psf_on) {
+      ctx->psf_on = false;
+      ctx->have_sens = false;
+      ctx->config_epoch++;
+    }
+    return HRRT_OK;
+  }
+  const std::vector<float> kx = psf_taps(fwhm1, fwhm2, ratio, g.x_size), ky = psf_taps(fwhm1, fwhm2, ratio, g.y_size),
+                           kz = psf_taps(fwhm1, fwhm2, ratio, g.z_size);
+  if (kx.empty() || ky.empty() || kz.empty()) return fail(ctx, HRRT_ERR_ARG, "PSF: fwhm1 must be >= 0");
+  if (kx.size() != ky.size()) return fail(ctx, HRRT_ERR_ARG, "PSF: x and y kernels differ in size");
+  // convolveyz's z tap sums (psf.cpp:397-416): loop bound and index both use
+  // the y kernel's half width; the sums cover planes [z_min, z_max)
+  const int h = (int)(ky.size() - 1) / 2;
+  std::vector<float> kzp(std::max(kz.size(), ky.size()), 0.f);
+  std::copy(kz.begin(), kz.end(), kzp.begin());
+  std::vector<float> normz(g.zp, 0.f);
+  for (int mask = -h; mask < h; mask++)
+    for (int z = 0; z < g.zp; z++) {
+      const int m2 = z + mask;
+      if (m2 < g.sp.z_min || m2 >= g.sp.z_max) continue;
+      normz[z] += kzp[mask + h];
+    }
+  for (int z = 0; z < g.zp; z++)
+    if (normz[z] > 0) normz[z] = 1 / normz[z];
+  cudaError_t e = cudaSuccess;
+  for (float **p : {&ctx->d_psf_fx, &ctx->d_psf_fy, &ctx->d_psf_normz})
+    if (*p) {
+      cudaFree(*p);
+      ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)*p));
+      *p = nullptr;
+    }
+  ctx->d_psf_fx = dupload(ctx, kx, &e);
+  ctx->d_psf_fy = dupload(ctx, ky, &e);
+  ctx->d_psf_normz = dupload(ctx, normz, &e);
+  if (!ctx->d_image_psf) ctx->d_image_psf = dalloc<float>(ctx, ctx->vol, &e);
+  if (!ctx->d_corr) ctx->d_corr = dalloc<float>(ctx, ctx->vol, &e);
+  if (!ctx->d_psf_tmp) ctx->d_psf_tmp = dalloc<float>(ctx, ctx->vol, &e);
+  if (!ctx->d_psf_fx || !ctx->d_psf_fy || !ctx->d_psf_normz || !ctx->d_image_psf || !ctx->d_corr || !ctx->d_psf_tmp)
+    return fail(ctx, HRRT_ERR_NOMEM, "PSF buffers");
+  CK(cudaStreamSynchronize(ctx->stream), "psf");
+  ctx->psf_h = h;
+  ctx->psf_on = true;
+  ctx->have_sens = false;
+  ctx->config_epoch++;
+  return HRRT_OK;
+}
+
+int hrrt_psf_convolve(hrrt_ctx *ctx, const float *image_xyz, float *out_xyz) {
+  if (!ctx || !image_xyz || !out_xyz) return HRRT_ERR_ARG;
+  if (!ctx->psf_on) return fail(ctx, HRRT_ERR_STATE, "hrrt_set_psf must come first");
+  cudaError_t e = cudaSuccess;
+  if (!ctx->d_tmp_img) ctx->d_tmp_img = dalloc<float>(ctx, ctx->vol, &e);
+  if (!ctx->d_tmp_img) return fail(ctx, HRRT_ERR_NOMEM, "scratch");
+  CK(cudaMemcpyAsync(ctx->d_tmp_img, image_xyz, sizeof(float) * ctx->vol, cudaMemcpyHostToDevice, ctx->stream),
+     "psf");
+  CK(cudaMemsetAsync(ctx->d_corr, 0, sizeof(float) * ctx->vol, ctx->stream), "psf");
+  if (int rc = run_psf(ctx, ctx->d_tmp_img, ctx->d_corr)) return rc;
+  CK(cudaMemcpyAsync(out_xyz, ctx->d_corr, sizeof(float) * ctx->vol, cudaMemcpyDeviceToHost, ctx->stream), "psf");
+  CK(cudaStreamSynchronize(ctx->stream), "psf");
+  return HRRT_OK;
 }
 
 int hrrt_set_backprojector(hrrt_ctx *ctx, int mode) {

@@ -965,9 +965,11 @@ __global__ void __launch_bounds__(256) rotback_kernel(DevGeom g, const int *__re
       r[l] = (z < g.nz && fabsf(a[l]) > g.eps1) ? (1.0f / a[l]) : 0.f;
     }
     reinterpret_cast<float4 *>(nf_inv)[o] = make_float4(r[0], r[1], r[2], r[3]);
-  } else {
+  } else if (MODE == 2) {
     float4 *co = reinterpret_cast<float4 *>(corr_out);
     co[o] = co[o] + acc;
+  } else {
+    reinterpret_cast<float4 *>(corr_out)[o] = acc;
   }
 }
 
@@ -1357,8 +1359,10 @@ cudaError_t launch_rotback(const DevGeom &g, const int *pair_views, int npairs, 
     rotback_kernel<0><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, corr_out, fr);
   else if (mode == 1)
     rotback_kernel<1><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, corr_out, fr);
-  else
+  else if (mode == 2)
     rotback_kernel<2><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, corr_out, fr);
+  else
+    rotback_kernel<3><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, corr_out, fr);
   return cudaGetLastError();
 }
 
@@ -1502,6 +1506,123 @@ cudaError_t launch_add_partials(const DevGeom &g, const float *bc, const float *
   add_partials_kernel<<<(unsigned)((n4 + 255) / 256), 256, 0, st>>>(n4, reinterpret_cast<const float4 *>(bc),
                                                                      reinterpret_cast<const float4 *>(br),
                                                                      reinterpret_cast<float4 *>(out));
+  return cudaGetLastError();
+}
+
+// ============================================================================
+// PSF resolution modelling (psf.cpp), on the FOV columns of [x][y][zp] images.
+// psf_x_kernel is convolvex (psf.cpp:163-206): taps mask in [-h, h) of the
+// x kernel over the x positions inside the FOV of row y, the result divided
+// by the sum of the taps used unless that sum is 0 or 1.  psf_yz_kernel is
+// convolveyz (psf.cpp:350-460): the same along y (its tap sum kept, not
+// applied), then along z over the planes [z_min, z_max) -- with the y
+// kernel's taps, as the reference's loop reads them -- scaled by
+// norm_z[z] / (y tap sum), norm_z the inverse of the z kernel taps that fall
+// inside [z_min, z_max) (host-computed).  One CTA per FOV column, one thread
+// per plane; sums in tap order, unfused.
+// ============================================================================
+__global__ void psf_x_kernel(DevGeom g, const float *__restrict__ in, float *__restrict__ out,
+                             const float *__restrict__ filt, int h) {
+  const int col = blockIdx.x, z = threadIdx.x;
+  if (z >= g.zp) return;
+  const short2 xy = g.fov_xy[col];
+  const int x = xy.x, y = xy.y, N = g.nx;
+  const int lo = g.cyl0[y], hi = g.cyl1[y];
+  float acc = 0.f, norm = 0.f;
+  for (int mask = -h; mask < h; mask++) {
+    const int x2 = x + mask;
+    if (x2 < lo || x2 >= hi) continue;
+    const float c = __ldg(filt + mask + h);
+    norm = norm + c;
+    acc = acc + __ldg(in + ((size_t)x2 * N + y) * g.zp + z) * c;
+  }
+  if (norm != 1.0f && norm != 0.0f) acc = acc * (1.0f / norm);
+  out[((size_t)x * N + y) * g.zp + z] = acc;
+}
+
+__global__ void psf_yz_kernel(DevGeom g, const float *__restrict__ in, float *__restrict__ out,
+                              const float *__restrict__ filty, int h, const float *__restrict__ normz) {
+  extern __shared__ float col[];  // [zp] the y-convolved column
+  const int c = blockIdx.x, z = threadIdx.x;
+  const short2 xy = g.fov_xy[c];
+  const int x = xy.x, y = xy.y, N = g.nx, zp = g.zp;
+  const int lo = g.cyl0[x], hi = g.cyl1[x];
+  float acc = 0.f, norm = 0.f;
+  for (int mask = -h; mask < h; mask++) {
+    const int y2 = y + mask;
+    if (y2 < lo || y2 >= hi) continue;
+    const float f = __ldg(filty + mask + h);
+    norm = norm + f;
+    if (z < zp) acc = acc + __ldg(in + ((size_t)x * N + y2) * zp + z) * f;
+  }
+  if (z < zp) col[z] = acc;
+  __syncthreads();
+  if (z >= zp) return;
+  float o = 0.f;
+  if (norm != 0.0f) {
+    for (int mask = -h; mask < h; mask++) {
+      const int z2 = z + mask;
+      if (z2 < g.z_min || z2 >= g.z_max || z >= g.nz) continue;
+      o = o + col[z2] * __ldg(filty + mask + h);
+    }
+    o = o * (__ldg(normz + z) * (1.0f / norm));
+  }
+  out[((size_t)x * N + y) * zp + z] = o;
+}
+
+// The consumers of the correction image once it is a separate volume (the
+// PSF path): MODE 0 the OSEM update, MODE 1 the inverse sensitivity; the
+// arithmetic of rotback_kernel's modes 0 and 1.
+template <int MODE>
+__global__ void __launch_bounds__(256) apply_corr_kernel(DevGeom g, const float *__restrict__ corr,
+                                                         float *__restrict__ image, float *__restrict__ nf_inv) {
+  const int nq = g.zp / 4;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int col = (int)(t / nq), q = (int)(t - (long long)col * nq);
+  if (col >= g.fov_columns) return;
+  const short2 xy = g.fov_xy[col];
+  const size_t o = ((size_t)xy.x * g.nx + xy.y) * nq + q;
+  const float4 acc = reinterpret_cast<const float4 *>(corr)[o];
+  if (MODE == 0) {
+    float4 *im = reinterpret_cast<float4 *>(image);
+    const float4 nf = reinterpret_cast<const float4 *>(nf_inv)[o];
+    float4 iv = im[o];
+    float a[4] = {acc.x, acc.y, acc.z, acc.w}, b[4] = {iv.x, iv.y, iv.z, iv.w}, n[4] = {nf.x, nf.y, nf.z, nf.w};
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      const float lo = (0.01f > a[l]) ? 0.01f : a[l];
+      const float cl = (100.0f < lo) ? 100.0f : lo;
+      const float u = b[l] * (cl * n[l]);
+      b[l] = (g.image_max < u) ? g.image_max : u;
+    }
+    im[o] = make_float4(b[0], b[1], b[2], b[3]);
+  } else {
+    float a[4] = {acc.x, acc.y, acc.z, acc.w}, r[4];
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      const int z = q * 4 + l;
+      r[l] = (z < g.nz && fabsf(a[l]) > g.eps1) ? (1.0f / a[l]) : 0.f;
+    }
+    reinterpret_cast<float4 *>(nf_inv)[o] = make_float4(r[0], r[1], r[2], r[3]);
+  }
+}
+
+cudaError_t launch_psf(const DevGeom &g, const float *in, float *tmp, float *out, const float *filt_x, int hx,
+                       const float *filt_y, int hy, const float *normz, cudaStream_t st) {
+  const int threads = ((g.zp + 31) / 32) * 32;
+  psf_x_kernel<<<g.fov_columns, threads, 0, st>>>(g, in, tmp, filt_x, hx);
+  psf_yz_kernel<<<g.fov_columns, threads, g.zp * sizeof(float), st>>>(g, tmp, out, filt_y, hy, normz);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_apply_corr(const DevGeom &g, const float *corr, float *image, float *nf_inv, int mode,
+                              cudaStream_t st) {
+  const long long n = (long long)g.fov_columns * (g.zp / 4);
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  if (mode == 0)
+    apply_corr_kernel<0><<<blocks, 256, 0, st>>>(g, corr, image, nf_inv);
+  else
+    apply_corr_kernel<1><<<blocks, 256, 0, st>>>(g, corr, image, nf_inv);
   return cudaGetLastError();
 }
 

@@ -147,11 +147,20 @@ cudaError_t launch_adj_rotate(const DevGeom &g, const int *pair_views, int npair
 cudaError_t launch_bp_sum(const DevGeom &g, const float *quad, int view, int x0, int nquads, float *out,
                           cudaStream_t st);
 // corr = sum over pairs of rotate-back(Bc+Br); mode 0: OSEM update of image with
-// nf_inv; mode 1: write the inverse sensitivity into nf_inv; mode 2: corr_out += corr
+// nf_inv; mode 1: write the inverse sensitivity into nf_inv; mode 2: corr_out += corr;
+// mode 3: corr_out = corr (FOV columns)
 cudaError_t launch_rotback(const DevGeom &g, const int *pair_views, int npairs, const float *bc, const float *br,
                            long long vol, float *image, float *nf_inv, float *corr_out, int mode,
                            const FrameStrides &fr, cudaStream_t st);
 cudaError_t launch_rotpos(const DevGeom &g, float2 *rotpos, const int *row_start, cudaStream_t st);
+// PSF (convolve3d, psf.cpp:463-540): out = yz(x(in)) on the FOV columns, tmp
+// holds the x pass; filters of 2h+1 taps (taps -h..h-1 used); normz [zp] the
+// inverted z tap sums
+cudaError_t launch_psf(const DevGeom &g, const float *in, float *tmp, float *out, const float *filt_x, int hx,
+                       const float *filt_y, int hy, const float *normz, cudaStream_t st);
+// mode 0: OSEM update of image from the correction volume; 1: inverse sensitivity into nf_inv
+cudaError_t launch_apply_corr(const DevGeom &g, const float *corr, float *image, float *nf_inv, int mode,
+                              cudaStream_t st);
 cudaError_t launch_prep(const DevGeom &g, int nbins, const int16_t *prompts, const float *randoms, const float *norm,
                         const float *atten, const float *scatter, int npskip, float eps2, int storage, void *q_prompts,
                         void *q_add, void *q_mult, int *quad_mask_accum, int plane0, int nplanes,

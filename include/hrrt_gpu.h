@@ -204,6 +204,22 @@ int hrrt_set_backprojector(hrrt_ctx *ctx, int mode);
  */
 int hrrt_bp_pair_noalloc(hrrt_ctx *ctx, const float *d_prj, int view, float *d_imagebuf, void *stream);
 
+/* PSF resolution modelling, the -B fwhm1,fwhm2,ratio option of hrrt_osem3d
+ * (psf.cpp; drv:3328-3330, :4521-4540).  enable = 1 builds the x, y and z
+ * kernels of make1d_psf_filter (fwhm1 = 0: the HRRT defaults) for the voxel
+ * sizes; hrrt_sensitivity then blurs each subset's back projection before
+ * inverting it (drv:3835-3841), and every OSEM subset projects the blurred
+ * image and blurs the correction image before the update (drv:4172, :4229).
+ * enable = 0 turns it off.  Either clears the sensitivity images.  Not
+ * available together with a batch. */
+int hrrt_set_psf(hrrt_ctx *ctx, int enable, float fwhm1, float fwhm2, float ratio);
+/* convolve3d (psf.cpp:463-540) of image_xyz on FOV columns into out_xyz
+ * (other columns zero) with the kernels hrrt_set_psf built. */
+int hrrt_psf_convolve(hrrt_ctx *ctx, const float *image_xyz, float *out_xyz);
+/* Host-only (no GPU needed): make1d_psf_filter's taps for one pixel size into
+ * `taps` (capacity); returns the tap count or a negative status. */
+long long hrrt_psf_kernel(float fwhm1, float fwhm2, float ratio, float pixel_size, float *taps, int capacity);
+
 /* Replaces rotate_image_buf (sbrt:1701-1725) for one view: corr_xyz +=
  * rotate-back(imagebuf_xyz). */
 int hrrt_rotate_add(hrrt_ctx *ctx, const float *imagebuf_xyz, int view, float *corr_xyz);

@@ -54,6 +54,11 @@ struct orc_geom {
   int16_t *nzmask;                   /* [nviews/2][nbins/2+1] */
   int *vieworder;                    /* [subsets][sviews] */
   int16_t *order;                    /* [subsets] */
+  /* PSF resolution modelling (psf.cpp), off unless orc_set_psf */
+  int psf_on, psf_h;                 /* half width h of the x / y kernels (taps -h..h-1 used) */
+  int psf_zmin, psf_zmax;            /* planes of the z convolution */
+  float *psf_fx, *psf_fy, *psf_fz;   /* [2h+1] */
+  float *psf_normz;                  /* [zp] inverted z tap sums */
 };
 
 int orc_real_bytes(void) { return (int)sizeof(R); }
@@ -88,7 +93,8 @@ void orc_destroy(orc_geom *g) {
   if (!g) return;
   void *p[] = {g->yb, g->yt, g->soff, g->sin_theta, g->cos_theta, g->sin_psi, g->cos_psi, g->vcos, g->vsin,
                g->cyl, g->tantheta, g->rescale, g->fl_zzi, g->fl_zzz0, g->bl_zsa, g->bl_zea, g->bl_yra,
-               g->bl_yr2a, g->bp_scale, g->nzmask, g->vieworder, g->order};
+               g->bl_yr2a, g->bp_scale, g->nzmask, g->vieworder, g->order,
+               g->psf_fx, g->psf_fy, g->psf_fz, g->psf_normz};
   for (size_t i = 0; i < sizeof(p) / sizeof(p[0]); i++) free(p[i]);
   free(g);
 }
@@ -1024,6 +1030,136 @@ static void run_subset_pairs(const orc_geom *g, int isubset, int T, const R *ima
   free(views);
 }
 
+/* ---- PSF resolution modelling (psf.cpp) ---------------------------------- */
+
+/* make1d_psf_filter (psf.cpp:21-70): two Gaussians (fwhm1, fwhm2 in mm, the
+ * second scaled by ratio) sampled at the pixel size over 2h+1 taps and
+ * normalised; fwhm1 == 0 selects the HRRT defaults.  Returns the tap count
+ * written to k (capacity cap), or -1. */
+int orc_psf_kernel(float fwhm1, float fwhm2, float ratio, float pixel_size, float *k, int cap) {
+  if (fwhm1 == 0.0) {
+    fwhm1 = (float)(0.9 * sqrt(8.0 * log(2.0)));
+    fwhm2 = (float)(2.5 * sqrt(8.0 * log(2.0)));
+    ratio = 0.05f;
+  }
+  if (!(fwhm1 > 0.0)) return -1;
+  int size;
+  if (fwhm2 > 0.0 && ratio > 0.0)
+    size = 2 * ((int)(1.5 * fwhm2 * sqrt(log(10.0) / log(2.)) / pixel_size / 2.0)) + 1;
+  else
+    size = 2 * ((int)(1.5 * fwhm1 * sqrt(log(10.0) / log(2.)) / pixel_size / 2.0)) + 1;
+  if (size > cap) return -1;
+  const float sigma1 = (float)(fwhm1 / (sqrt(8.0 * log(2.0)) * pixel_size));
+  const float sigma2 = (float)(fwhm2 / (sqrt(8.0 * log(2.0)) * pixel_size));
+  const int bin0 = (size - 1) / 2;
+  float norm = 0.0f;
+  for (int b = 0; b < size; b++) {
+    k[b] = (float)exp(-0.5 * (pow((double)(b - bin0) / sigma1, 2.0)));
+    if (fwhm2 > 0.0 && ratio > 0.0) k[b] = (float)(k[b] + ratio * exp(-0.5 * (pow((double)(b - bin0) / sigma2, 2.0))));
+    norm += k[b];
+  }
+  for (int b = 0; b < size; b++) k[b] /= norm;
+  return size;
+}
+
+int orc_set_psf(orc_geom *g, int on, float fwhm1, float fwhm2, float ratio, int z_min, int z_max) {
+  free(g->psf_fx);
+  free(g->psf_fy);
+  free(g->psf_fz);
+  free(g->psf_normz);
+  g->psf_fx = g->psf_fy = g->psf_fz = g->psf_normz = NULL;
+  g->psf_on = 0;
+  if (!on) return 0;
+  float kx[256], ky[256], kz[256];
+  const int nx = orc_psf_kernel(fwhm1, fwhm2, ratio, g->x_size, kx, 256);
+  const int ny = orc_psf_kernel(fwhm1, fwhm2, ratio, g->y_size, ky, 256);
+  const int nz = orc_psf_kernel(fwhm1, fwhm2, ratio, g->plane_sep, kz, 256);
+  if (nx < 1 || ny < 1 || nz < 1 || nx != ny) return -1;
+  g->psf_h = (nx - 1) / 2;
+  g->psf_fx = NEW(float, nx);
+  g->psf_fy = NEW(float, ny);
+  g->psf_fz = NEW(float, nz > ny ? nz : ny);
+  memcpy(g->psf_fx, kx, sizeof(float) * nx);
+  memcpy(g->psf_fy, ky, sizeof(float) * ny);
+  memcpy(g->psf_fz, kz, sizeof(float) * nz);
+  /* convolveyz's z tap sums (psf.cpp:397-416): the loop bound and the index
+   * both use the y kernel's half width */
+  const int h = (ny - 1) / 2;
+  g->psf_normz = NEW(float, g->zp);
+  for (int z = 0; z < g->zp; z++) g->psf_normz[z] = 0.0f;
+  for (int mask = -h; mask < h; mask++)
+    for (int z = 0; z < g->zp; z++) {
+      const int m2 = z + mask;
+      if (m2 < z_min || m2 >= z_max) continue;
+      g->psf_normz[z] += g->psf_fz[mask + h];
+    }
+  for (int z = 0; z < g->zp; z++)
+    if (g->psf_normz[z] > 0) g->psf_normz[z] = 1 / g->psf_normz[z];
+  g->psf_zmin = z_min;
+  g->psf_zmax = z_max;
+  g->psf_on = 1;
+  return 0;
+}
+
+/* convolve3d (psf.cpp:463-540): convolvex (:163-206) into a buffer, then
+ * convolveyz (:350-460), on FOV columns; out may be in */
+void orc_psf(const orc_geom *g, const R *in, R *out) {
+  const int N = g->nx, zp = g->zp, h = g->psf_h;
+  const size_t vol = (size_t)N * g->ny * zp;
+  R *buf = NEW(R, vol), *col = NEW(R, zp), *acc = NEW(R, zp);
+  for (int x = 0; x < N; x++) {
+    if (g->cyl[2 * x + 1] == 0) continue;
+    for (int y = g->cyl[2 * x]; y < g->cyl[2 * x + 1]; y++) {
+      for (int z = 0; z < zp; z++) acc[z] = 0;
+      float norm = 0;
+      for (int mask = -h; mask < h; mask++) {
+        const int m2 = x + mask;
+        if (m2 < g->cyl[2 * y] || m2 >= g->cyl[2 * y + 1]) continue;
+        const R c = (R)g->psf_fx[mask + h];
+        norm += g->psf_fx[mask + h];
+        for (int z = 0; z < zp; z++) acc[z] = acc[z] + in[((size_t)m2 * N + y) * zp + z] * c;
+      }
+      R *o = buf + ((size_t)x * N + y) * zp;
+      if (norm != 1 && norm != 0) {
+        const R c = (R)(1 / norm);
+        for (int z = 0; z < zp; z++) o[z] = acc[z] * c;
+      } else {
+        for (int z = 0; z < zp; z++) o[z] = acc[z];
+      }
+    }
+  }
+  for (int x = 0; x < N; x++) {
+    if (g->cyl[2 * x + 1] == 0) continue;
+    for (int y = g->cyl[2 * x]; y < g->cyl[2 * x + 1]; y++) {
+      for (int z = 0; z < zp; z++) col[z] = 0;
+      float norm = 0;
+      for (int mask = -h; mask < h; mask++) {
+        const int m2 = y + mask;
+        if (m2 < g->cyl[2 * x] || m2 >= g->cyl[2 * x + 1]) continue;
+        const R c = (R)g->psf_fy[mask + h];
+        norm += g->psf_fy[mask + h];
+        for (int z = 0; z < zp; z++) col[z] = col[z] + buf[((size_t)x * N + m2) * zp + z] * c;
+      }
+      R *o = out + ((size_t)x * N + y) * zp;
+      for (int z = 0; z < zp; z++) o[z] = 0;
+      if (norm != 0) {
+        for (int mask = -h; mask < h; mask++) {
+          int zs = g->psf_zmin - mask, ze = g->psf_zmax - mask;
+          if (zs < 0) zs = 0;
+          if (ze > g->nz) ze = g->nz;
+          const R f = (R)g->psf_fy[mask + h];
+          for (int z = zs; z < ze; z++) o[z] = o[z] + col[z + mask] * f;
+        }
+        const R c = (R)(1 / norm);
+        for (int z = 0; z < zp; z++) o[z] = o[z] * ((R)g->psf_normz[z] * c);
+      }
+    }
+  }
+  free(buf);
+  free(col);
+  free(acc);
+}
+
 /* CalculateNormfac (drv:3760-3865): per subset the back projection of
  * 1/(N*A), inverted where |.| > epsilon1 on FOV columns, planes < nz
  * (pt_normfac_calculate, drv:1852-1894) */
@@ -1033,6 +1169,7 @@ void orc_sensitivity(const orc_geom *g, const float *mult, R *nf_inv, int nthrea
   for (int s = 0; s < g->subsets; s++) {
     memset(nf, 0, sizeof(R) * vol);
     run_subset_pairs(g, s, nthreads, NULL, NULL, mult, 1, nf);
+    if (g->psf_on) orc_psf(g, nf, nf); /* drv:3835-3841 */
     R *out = nf_inv + (size_t)s * vol;
     memset(out, 0, sizeof(R) * vol);
     for (int x = 0; x < g->nx; x++)
@@ -1068,7 +1205,15 @@ void orc_osem_subset(const orc_geom *g, R *image, const R *nf, const int16_t *pr
                      int isubset, int nthreads) {
   const size_t vol = (size_t)g->nx * g->ny * g->zp;
   R *corr = NEW(R, vol);
-  run_subset_pairs(g, isubset, nthreads, image, prompts, add, 0, corr);
+  if (g->psf_on) { /* the projection of the blurred image, the blurred correction (drv:4172, :4229) */
+    R *ipsf = NEW(R, vol);
+    orc_psf(g, image, ipsf);
+    run_subset_pairs(g, isubset, nthreads, ipsf, prompts, add, 0, corr);
+    free(ipsf);
+    orc_psf(g, corr, corr);
+  } else {
+    run_subset_pairs(g, isubset, nthreads, image, prompts, add, 0, corr);
+  }
   const R amax = (R)100.00f, amin = (R)0.01f, imax = (R)g->image_max;
   for (int x = 0; x < g->nx; x++)
     for (int y = g->cyl[2 * x]; y < g->cyl[2 * x + 1]; y++) {

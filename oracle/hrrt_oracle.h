@@ -90,6 +90,15 @@ void orc_osem_subset(const orc_geom *g, orc_real *image, const orc_real *nf_inv_
 /* post-iteration threshold (< 1e-16 -> 0) and sum over FOV x [z_min, z_max) */
 double orc_post_iteration(const orc_geom *g, orc_real *image, int z_min, int z_max);
 
+/* PSF resolution modelling (psf.cpp): the 1D kernel of make1d_psf_filter
+ * (returns its size or -1), and convolve3d on FOV columns once orc_set_psf
+ * has enabled it (it then also applies in orc_sensitivity and
+ * orc_osem_subset, as -B does in the reference; z_min / z_max: the planes of
+ * the z convolution) */
+int orc_psf_kernel(float fwhm1, float fwhm2, float ratio, float pixel_size, float *k, int cap);
+int orc_set_psf(orc_geom *g, int on, float fwhm1, float fwhm2, float ratio, int z_min, int z_max);
+void orc_psf(const orc_geom *g, const orc_real *in, orc_real *out);
+
 #ifdef __cplusplus
 }
 #endif

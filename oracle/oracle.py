@@ -62,6 +62,12 @@ def lib(precision="f64"):
                 getattr(L, n).restype = None
             L.orc_post_iteration.argtypes = [vp, vp, i, i]
             L.orc_post_iteration.restype = ctypes.c_double
+            L.orc_psf_kernel.argtypes = [f, f, f, f, vp, i]
+            L.orc_psf_kernel.restype = i
+            L.orc_set_psf.argtypes = [vp, i, f, f, f, i, i]
+            L.orc_set_psf.restype = i
+            L.orc_psf.argtypes = [vp, vp, vp]
+            L.orc_psf.restype = None
             assert L.orc_real_bytes() == np.dtype(DTYPES[precision]).itemsize
             _libs[precision] = L
         return _libs[precision]
@@ -192,6 +198,26 @@ class Oracle:
         a = np.ascontiguousarray(add, np.float32)
         self.L.orc_osem_subset(self.g, _p(image), _p(nf), _p(p), _p(a), isubset, nthreads or self.nthreads)
         return image
+
+    def psf_kernel(self, fwhm1=0.0, fwhm2=0.0, ratio=0.0, pixel_size=1.21875):
+        """make1d_psf_filter's taps (psf.cpp:21-70); fwhm1 0: the HRRT defaults."""
+        k = np.zeros(256, np.float32)
+        n = self.L.orc_psf_kernel(fwhm1, fwhm2, ratio, pixel_size, _p(k), 256)
+        if n < 1:
+            raise ValueError("no PSF kernel for these parameters")
+        return k[:n].copy()
+
+    def set_psf(self, on=True, fwhm1=0.0, fwhm2=0.0, ratio=0.0):
+        """-B fwhm1,fwhm2,ratio: the PSF in sensitivity and subsets from now on."""
+        if self.L.orc_set_psf(self.g, 1 if on else 0, fwhm1, fwhm2, ratio, self.z_min, self.z_max) != 0:
+            raise ValueError("no PSF kernel for these parameters")
+
+    def psf(self, image):
+        """convolve3d (psf.cpp:463-540) of an [x][y][zp] image on FOV columns."""
+        img = self._r(image)
+        out = np.zeros(self.image_shape, self.dtype)
+        self.L.orc_psf(self.g, _p(img), _p(out))
+        return out
 
     def post_iteration(self, image, zmin=None, zmax=None):
         zmin = self.z_min if zmin is None else zmin

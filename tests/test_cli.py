@@ -37,9 +37,11 @@ def test_usage_and_argument_errors(cli):
     assert r.returncode == 1 and "-p prompts and -d delayed are required" in r.stderr
     r = run(cli, "-p", "a", "-d", "b", "-o", "x.i", "-W", "2")
     assert r.returncode == 1 and "-W 3" in r.stderr
-    for opt, word in (("-B", "PSF"), ("-A", "MAP"), ("-t", "trues")):
-        r = run(cli, opt, "1,1,1" if opt == "-B" else "x", "-p", "a", "-d", "b", "-o", "x.i", "-W", "3")
+    for opt, word in (("-A", "MAP"), ("-t", "trues")):
+        r = run(cli, opt, "x", "-p", "a", "-d", "b", "-o", "x.i", "-W", "3")
         assert r.returncode == 1 and word in r.stderr
+    r = run(cli, "-B", "x", "-p", "a", "-d", "b", "-o", "x.i", "-W", "3")
+    assert r.returncode == 1 and "-B" in r.stderr
     r = run(cli, "-X", "128", "-p", "a", "-d", "b", "-o", "x.i", "-W", "3")
     assert r.returncode == 1 and "256" in r.stderr
 
