@@ -197,7 +197,7 @@ def algorithmic_model(info, add_bytes=4):
     samples = pairs * 2 * info.fov_columns * info.segmentsize
     return {
         "bins_per_subset": bins,
-        "fp_kernel": {"bytes": vol + bins * (6 + add_bytes), "flops": samples * 3},
+        "fp_kernel": {"bytes": vol + bins * (6 + add_bytes), "flops": samples * 3, "smem_bytes": samples * 8},
         "bp_kernel": {"bytes": bins * 4 + vol, "flops": samples * 4},
         "rotback_kernel": {"bytes": 4 * vol, "flops": info.fov_columns * info.zp * pairs * 16},
         # prompts + additive term read, ratio written and read back, image
@@ -313,6 +313,17 @@ def run_ours(args, ws, rank, local):
                          "peak_at_clock": FP32_TFLOPS_NOMINAL * sm_mhz / 1965.0,
                          "frac_nominal": model[dom]["flops"] / avg_s / 1e12 / FP32_TFLOPS_NOMINAL,
                          "frac_at_clock": model[dom]["flops"] / avg_s / 1e12 / (FP32_TFLOPS_NOMINAL * sm_mhz / 1965.0)},
+        # the bound the forward projector actually meets: every interpolation
+        # sample reads its two row entries (4 B each) from shared memory;
+        # peak = 148 SMs x 128 B per clock at the sampled SM clock
+        "roofline_smem": {"bound": "shared memory", "kernel": "fp_kernel", "unit": "GB/s",
+                          "bytes_per_launch": model["fp_kernel"]["smem_bytes"],
+                          "achieved": model["fp_kernel"]["smem_bytes"] / (kstats["fp_kernel"][1] /
+                                                                           max(kstats["fp_kernel"][0], 1) / 1e3) / 1e9,
+                          "peak_nominal": 148 * 128 * sm_mhz * 1e6 / 1e9,
+                          "frac": model["fp_kernel"]["smem_bytes"] / (kstats["fp_kernel"][1] /
+                                                                       max(kstats["fp_kernel"][0], 1) / 1e3)
+                          / (148 * 128 * sm_mhz * 1e6)},
         # the whole subset-iteration against HBM: algorithmic bytes per subset
         # (bins x (input bytes + 8) + 3 image volumes) over the step time
         "roofline_subset": {"bound": "hbm", "unit": "GB/s", "bytes_per_step": model["subset_bytes"],
