@@ -83,6 +83,7 @@ class BatchStats(ctypes.Structure):
 
 LM_TRUES, LM_PROMPTS_AND_DELAYED, LM_PROMPTS_ONLY = 0, 1, 2
 LM_IGNORE_BORDER_CRYSTAL, LM_NO_DOI, LM_TIME_FROM_COUNT = 1, 2, 4
+LM_FORCE_DIRECT, LM_FORCE_PARTITIONED, LM_FORCE_WIDE, LM_HEAD_CURVE, LM_CRYSTAL_COUNTS = 16, 32, 64, 128, 256
 
 
 def _load():
@@ -142,6 +143,9 @@ def _load():
         "hrrt_lm_histogram": (i, [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, ctypes.POINTER(LmStats)]),
         "hrrt_lm_histogram_device": (i, [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, ctypes.POINTER(LmStats), vp]),
         "hrrt_lm_smooth_randoms": (i, [vp, vp, f, f, vp, ctypes.POINTER(i)]),
+        "hrrt_lm_head_curve": (i, [vp, vp, i]),
+        "hrrt_lm_crystal_counts": (i, [vp, vp]),
+        "hrrt_lm_block_singles": (i, [vp, vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
         "hrrt_lm_crystal_singles": (i, [vp, f, f, vp]),
     }
     for name, (res, args) in sig.items():
@@ -588,6 +592,30 @@ class Listmode:
         self._check(lib.hrrt_lm_histogram(self._h, _ptr(w), w.size, mode, duration, flags, _ptr(sino), _ptr(dly),
                                           ctypes.byref(st)), "lm_histogram")
         return sino, dly, st.as_dict()
+
+    def head_curve(self):
+        """The head curve of the last histogram call made with LM_HEAD_CURVE:
+        int64 [n][4] (time ms, prompts, randoms, total singles)."""
+        n = lib.hrrt_lm_head_curve(self._h, None, 0)
+        out = np.zeros((max(n, 0), 4), np.int64)
+        if n > 0:
+            lib.hrrt_lm_head_curve(self._h, _ptr(out), n)
+        return out
+
+    def crystal_counts(self):
+        """The coincidence histogram of the last LM_CRYSTAL_COUNTS call:
+        uint32 [2][119808] (prompt, delayed)."""
+        out = np.zeros(2 * 2 * 104 * 8 * 72, np.uint32)
+        self._check(lib.hrrt_lm_crystal_counts(self._h, _ptr(out)), "lm_crystal_counts")
+        return out
+
+    def block_singles(self):
+        """-> (average singles rate of each of the 936 blocks, (total prompts,
+        total randoms) of the head-curve lines) of the last LM_HEAD_CURVE call."""
+        rates = np.zeros(936, np.int32)
+        tp, tr = ctypes.c_longlong(), ctypes.c_longlong()
+        lib.hrrt_lm_block_singles(self._h, _ptr(rates), ctypes.byref(tp), ctypes.byref(tr))
+        return rates, (tp.value, tr.value)
 
     def smooth_randoms(self, coinc_hist, scan_duration=1.0, tau=6.0e-9):
         """gen_delays: the randoms sinogram (float32, this context's span) from

@@ -74,7 +74,22 @@ struct LmDev {
   const int *segz0, *segzmax, *segzoff;  // [nsegs]
   int nsegs;
   long long sino_size;
+  // head curve (HRRT_LM_HEAD_CURVE; null otherwise): prompts / delayed of the
+  // events before time tag i (after tag i-1) in ivl[2i], ivl[2i+1]; block
+  // singles tags (position, value) appended to sing
+  unsigned long long *ivl;
+  longlong2 *sing;
+  unsigned int *sing_n;
+  long long sing_cap;
+  // coincidence histogram (HRRT_LM_CRYSTAL_COUNTS; null otherwise): prompt
+  // then delayed counts per crystal [layer 2][ring 104][head 8][x 72]
+  unsigned int *ccounts;
 };
+
+// head pairs of the 20 coincidence combinations (geometry_info.h:68-75)
+__constant__ int c_pair_heads[21][2] = {{-1, -1}, {0, 2}, {0, 3}, {0, 4}, {0, 5}, {0, 6}, {1, 3}, {1, 4},
+                                        {1, 5},   {1, 6}, {1, 7}, {2, 4}, {2, 5}, {2, 6}, {2, 7}, {3, 5},
+                                        {3, 6},   {3, 7}, {4, 6}, {4, 7}, {5, 7}};
 
 enum : int { kStPrompts, kStDelayed, kStTimetags, kStTags, kStInvalid, kStUnmapped, kStDoiOther, kStDoi7, kStResync,
              kStCount };
@@ -299,6 +314,8 @@ __device__ __forceinline__ void walk_events(const LmDev &g, const LmShared &t, c
   const bool border = (flags & HRRT_LM_IGNORE_BORDER_CRYSTAL) != 0;
   const int xhigh = border ? 71 : 72;
   uint32_t evmask = 0;  // bit k: an event (below the limit) starts at word s + k
+  uint32_t ttmask = 0;  // bit k: a time tag starts at word s + k (head curve)
+  const unsigned long long tagpos0 = tagpos;
   int pos = s + e;
   while (pos < s + kSub) {
     if (pos + 1 >= pend) break;
@@ -317,6 +334,11 @@ __device__ __forceinline__ void walk_events(const LmDev &g, const LmShared &t, c
       if (timetag) {
         if (tags && (long long)tagpos < tag_cap) tags[tagpos] = make_longlong2(gp, (long long)tag);
         tagpos++;
+        ttmask |= 1u << (pos - 2 - s);
+      } else if (tags && g.sing && (tag & 0xE0000000u) == 0xA0000000u) {
+        // block singles (process_tagword, histogram_mp.cpp:260-270), in stream order later
+        const unsigned int k = atomicAdd(g.sing_n, 1u);
+        if ((long long)k < g.sing_cap) g.sing[k] = make_longlong2(gp, (long long)tag);
       }
       if (gp >= limit) continue;
       if (kStats) {
@@ -331,6 +353,7 @@ __device__ __forceinline__ void walk_events(const LmDev &g, const LmShared &t, c
           c[kStPrompts]++;
         else
           c[kStDelayed]++;
+        if (g.ivl) atomicAdd(g.ivl + 2 * tagpos + (prompt ? 0 : 1), 1ull);
       }
       const long long addr = tag & 0x3fffffff;
       if (addr < g.sino_size) {
@@ -376,6 +399,14 @@ __device__ __forceinline__ void walk_events(const LmDev &g, const LmShared &t, c
       if (kStats) c[kStDoiOther]++;
       continue;
     }
+    if (kStats && g.ccounts) {
+      // the coincidence histogram counts both crystals of every emission
+      // event with DOI 0/1, mapped or not (rebin_packet, histogram_mp.cpp:1212-1223)
+      const int ah = c_pair_heads[mpe][0], bh = c_pair_heads[mpe][1];
+      unsigned int *cc = g.ccounts + (type ? 119808 : 0);
+      atomicAdd(cc + doia * 59904 + ah * 72 + ax + ay * 576, 1u);
+      atomicAdd(cc + doib * 59904 + bh * 72 + bx + by * 576, 1u);
+    }
     if ((border && (ax * bx == 0 || ax == xhigh || bx == xhigh)) || (mode == HRRT_LM_PROMPTS_ONLY && type != 0)) {
       if (kStats) c[kStUnmapped]++;
       continue;
@@ -394,9 +425,15 @@ __device__ __forceinline__ void walk_events(const LmDev &g, const LmShared &t, c
   // ... and the addresses, handed over together
   long long addr[kEv];
   uint32_t live = 0, sel = 0, minus = 0;
+  // head curve: each event counts towards the interval of the time tags
+  // before it, accumulated while the interval stays the same
+  unsigned long long hc_iv = ~0ull, hc_p = 0, hc_d = 0;
+  uint32_t m2 = evmask;
 #pragma unroll
   for (int k = 0; k < kEv; k++) {
     addr[k] = 0;
+    const int p = m2 ? __ffs(m2) - 1 : 0;
+    if (m2) m2 &= m2 - 1;
     if (!((need >> k) & 1)) continue;
     const long long a = rebin_address(g, t, sol[k], ays[k], bys[k]);
     if (a < 0) {
@@ -409,6 +446,21 @@ __device__ __forceinline__ void walk_events(const LmDev &g, const LmShared &t, c
         c[kStDelayed]++;
       else
         c[kStPrompts]++;
+      if (g.ivl) {
+        const unsigned long long iv = tagpos0 + __popc(ttmask & ((1u << p) - 1u));
+        if (iv != hc_iv) {
+          if (hc_iv != ~0ull) {
+            if (hc_p) atomicAdd(g.ivl + 2 * hc_iv, hc_p);
+            if (hc_d) atomicAdd(g.ivl + 2 * hc_iv + 1, hc_d);
+          }
+          hc_iv = iv;
+          hc_p = hc_d = 0;
+        }
+        if (dly)
+          hc_d++;
+        else
+          hc_p++;
+      }
     }
     addr[k] = a;
     live |= 1u << k;
@@ -417,6 +469,10 @@ __device__ __forceinline__ void walk_events(const LmDev &g, const LmShared &t, c
     } else if (dly) {
       minus |= 1u << k;
     }
+  }
+  if (kStats && g.ivl && hc_iv != ~0ull) {
+    if (hc_p) atomicAdd(g.ivl + 2 * hc_iv, hc_p);
+    if (hc_d) atomicAdd(g.ivl + 2 * hc_iv + 1, hc_d);
   }
   if (live) emit_events(addr, live, sel, minus);
 }
@@ -587,7 +643,6 @@ __global__ void __launch_bounds__(kThreads) lm_part_hist_kernel(const uint32_t *
 // gen_delays_fromarchive.cpp:191 (layer, y, head, x): the library copy at
 // gen_delays_lib.cpp:117 multiplies y by a whole layer and reads past the
 // singles array.
-__constant__ int c_pair_heads[21][2];
 constexpr int kDelayBxRun = 8;
 __global__ void __launch_bounds__(128) lm_delays_kernel(LmDev g, const float *__restrict__ csings, float tauftime,
                                                         int maxrd, float *__restrict__ out) {
@@ -665,6 +720,16 @@ struct hrrt_lm {
   long long tag_cap = 0;
   uint32_t *records = nullptr;      // partitioned path: packed event records
   long long rec_cap = 0;
+  // head curve of the last call (HRRT_LM_HEAD_CURVE)
+  unsigned long long *ivl = nullptr;
+  long long ivl_cap = 0;
+  longlong2 *sing = nullptr;
+  unsigned int *sing_n = nullptr;
+  long long sing_cap = 0;
+  unsigned int *ccounts = nullptr;  // coincidence histogram of the last call
+  std::vector<hrrt_lm_second> hc;
+  std::vector<int> block_rates;
+  long long hc_prompts = 0, hc_randoms = 0;
   // clock carried across frames (process_tagword's statics)
   long long current_time = -1, current_time_msec = -1, prev_time = 0;
   int clock_reset = 0;
@@ -676,6 +741,10 @@ struct hrrt_lm {
     if (scratch) cudaFree(scratch);
     if (tagbuf) cudaFree(tagbuf);
     if (records) cudaFree(records);
+    if (ivl) cudaFree(ivl);
+    if (sing) cudaFree(sing);
+    if (sing_n) cudaFree(sing_n);
+    if (ccounts) cudaFree(ccounts);
     if (h_words_dev) cudaFree(h_words_dev);
     if (h_sino_dev) cudaFree(h_sino_dev);
     if (stream) cudaStreamDestroy(stream);
@@ -705,6 +774,74 @@ T *lm_upload(hrrt_lm *h, const std::vector<T> &v, cudaError_t *e) {
 
 // process_tagword's time-tag branch (histogram_mp.cpp:225-260) over the
 // ordered time tags; returns the index of the tag that ends the frame or -1.
+struct ClockState {
+  long long time, msec, prev;
+  int reset;
+};
+
+// The head curve and block singles of one frame (process_tagword,
+// histogram_mp.cpp:225-303, replayed in stream order from the clock as the
+// frame found it): at every change of second a record (time in ms, prompts
+// and delayed events since the previous record, the sum over blocks of their
+// latest singles sample), the singles tags updating each block's latest
+// sample, total and sample count.  ivl[2i], ivl[2i+1]: the events before time
+// tag i; sing: (position, tag) of the block singles tags.
+void build_head_curve(hrrt_lm *h, ClockState c, long long frame_start, const std::vector<longlong2> &tags,
+                      long long end_tag, const std::vector<unsigned long long> &ivl, std::vector<longlong2> sing,
+                      int duration, int flags, long long limit) {
+  constexpr int kBlocks = 936;  // GeometryInfo::NBLOCKS
+  std::sort(sing.begin(), sing.end(), [](const longlong2 &a, const longlong2 &b) { return a.x < b.x; });
+  struct Blk {
+    long long last = 0, total = 0, n = 0;
+  };
+  std::vector<Blk> blk(kBlocks);
+  auto take = [&](uint32_t tag) {
+    const int b = (int)((tag & 0x1ff80000u) >> 19);
+    if (b >= 0 && b < kBlocks) {
+      blk[b].last = tag & 0x0007ffff;
+      blk[b].total += tag & 0x0007ffff;
+      blk[b].n++;
+    }
+  };
+  h->hc.clear();
+  long long pacc = 0, racc = 0, tp = 0, tr = 0;
+  size_t si = 0;
+  const long long n = (long long)tags.size(), last = end_tag >= 0 ? end_tag : n - 1;
+  for (long long i = 0; i <= last; i++) {
+    pacc += (long long)ivl[2 * i];
+    racc += (long long)ivl[2 * i + 1];
+    while (si < sing.size() && sing[si].x < tags[i].x) take((uint32_t)sing[si++].y);
+    const uint32_t tag = (uint32_t)tags[i].y;
+    if (flags & HRRT_LM_TIME_FROM_COUNT)
+      c.msec++;
+    else
+      c.msec = tag & 0x3fffffff;
+    if (c.prev > c.msec && !c.reset) {
+      c.time = c.msec / 1000;
+      c.reset = 1;
+      continue;
+    }
+    c.prev = c.msec;
+    if (c.time != c.msec / 1000) {
+      long long singles = 0;
+      for (const Blk &b : blk) singles += b.last;
+      h->hc.push_back(hrrt_lm_second{c.msec, pacc, racc, singles});
+      tp += pacc;
+      tr += racc;
+      pacc = racc = 0;
+      c.time = c.msec / 1000;
+      if (frame_start < 0) frame_start = c.time;
+      if (duration > 0 && c.time - frame_start >= duration) break;
+    }
+  }
+  if (end_tag < 0)  // the frame ran to the end of the stream
+    while (si < sing.size() && sing[si].x < limit) take((uint32_t)sing[si++].y);
+  h->block_rates.assign(kBlocks, 0);
+  for (int b = 0; b < kBlocks; b++) h->block_rates[b] = blk[b].n ? (int)(blk[b].total / blk[b].n) : 0;
+  h->hc_prompts = tp;
+  h->hc_randoms = tr;
+}
+
 long long replay_clock(hrrt_lm *h, const longlong2 *tags, long long ntags, int duration, int flags,
                        long long *frame_start) {
   for (long long i = 0; i < ntags; i++) {
@@ -902,38 +1039,90 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
   }
   if (partitioned && e == cudaSuccess) e = cudaMemsetAsync(cursor, 0, 8 * kMaxParts, st);
   if (wide && e == cudaSuccess) e = cudaMemsetAsync(h->records, 0, sizeof(uint32_t) * 2 * h->dev.sino_size, st);
+  LmDev dv = h->dev;  // this call's copy: the head-curve buffers when asked for
   auto launch = [&](int kmode, long long lim, long long tcap) {
     const unsigned nb = (unsigned)ntiles;
     uint32_t *sn = (uint32_t *)d_sino, *dl = (uint32_t *)d_delayed;
     switch (kmode) {
       case 0:
-        lm_hist_kernel<0><<<nb, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
+        lm_hist_kernel<0><<<nb, kThreads, 0, st>>>(dv, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
                                                    mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
         break;
       case 1:
-        lm_hist_kernel<1><<<nb, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
+        lm_hist_kernel<1><<<nb, kThreads, 0, st>>>(dv, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
                                                    mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
         break;
       case 2:
-        lm_hist_kernel<2><<<nb, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
+        lm_hist_kernel<2><<<nb, kThreads, 0, st>>>(dv, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
                                                    mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
         break;
       case 4:
-        lm_hist_kernel<4><<<nb, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
+        lm_hist_kernel<4><<<nb, kThreads, 0, st>>>(dv, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
                                                    mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
         break;
       default:
-        lm_hist_kernel<3><<<nb, kThreads, 0, st>>>(h->dev, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
+        lm_hist_kernel<3><<<nb, kThreads, 0, st>>>(dv, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
                                                    mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
     }
     return cudaGetLastError();
   };
   // pass 1: the ordered time tags (and, without a frame length, the counts
   // or the histogram itself)
-  const bool one_pass = duration <= 0;
+  // head curve: the tags pass also collects the block singles tags, and the
+  // histogram pass counts events per time-tag interval
+  const bool hc = (flags & HRRT_LM_HEAD_CURVE) != 0;
+  if (hc && e == cudaSuccess) {
+    auto grow = [&](void **p, long long *cap, long long want, size_t elem) {
+      if (want <= *cap) return cudaSuccess;
+      if (*p) cudaFree(*p);
+      *p = nullptr;
+      *cap = 0;
+      cudaError_t r = cudaMalloc(p, elem * (size_t)want);
+      if (r == cudaSuccess) *cap = want;
+      return r;
+    };
+    e = grow((void **)&h->ivl, &h->ivl_cap, 2 * ((long long)ntags + 1), sizeof(unsigned long long));
+    if (e == cudaSuccess) e = grow((void **)&h->sing, &h->sing_cap, std::max<long long>(4096, 2 * (long long)ntags), 16);
+    if (e == cudaSuccess && !h->sing_n) e = cudaMalloc(&h->sing_n, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->ivl, 0, sizeof(unsigned long long) * 2 * (ntags + 1), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->sing_n, 0, sizeof(unsigned int), st);
+    dv.sing = h->sing;
+    dv.sing_n = h->sing_n;
+    dv.sing_cap = h->sing_cap;
+  }
+  if ((flags & HRRT_LM_CRYSTAL_COUNTS) && e == cudaSuccess) {
+    if (!h->ccounts) e = cudaMalloc(&h->ccounts, sizeof(unsigned int) * 2 * hrrt::kCrystals);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->ccounts, 0, sizeof(unsigned int) * 2 * hrrt::kCrystals, st);
+  }
+  const bool one_pass = duration <= 0 && !hc;
   const int hist_mode = partitioned ? 2 : (wide ? 4 : 1);
+  if (one_pass && (flags & HRRT_LM_CRYSTAL_COUNTS)) dv.ccounts = h->ccounts;
   if (e == cudaSuccess) e = launch(one_pass ? hist_mode : 0, one_pass ? nwords : -1, tag_cap);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  unsigned int nsing = 0;
+  if (hc && e == cudaSuccess) {
+    e = cudaMemcpy(&nsing, h->sing_n, sizeof(unsigned int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && (long long)nsing > h->sing_cap) {  // more singles tags than room: again, sized
+      cudaFree(h->sing);
+      h->sing = nullptr;
+      h->sing_cap = 0;
+      e = cudaMalloc(&h->sing, 16 * (size_t)nsing);
+      if (e == cudaSuccess) {
+        h->sing_cap = nsing;
+        dv.sing = h->sing;
+        dv.sing_cap = h->sing_cap;
+        e = cudaMemsetAsync(h->sing_n, 0, sizeof(unsigned int), st);
+        if (e == cudaSuccess) e = launch(0, -1, tag_cap);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      }
+    }
+    dv.sing = nullptr;
+    dv.ivl = h->ivl;
+  }
+  // the crystal counts are taken in the histogram pass only
+  auto hist_dev = [&]() {
+    if (flags & HRRT_LM_CRYSTAL_COUNTS) dv.ccounts = h->ccounts;
+  };
   std::vector<longlong2> htags;
   if (e == cudaSuccess && ntags > 0) {
     htags.resize(ntags);
@@ -945,10 +1134,15 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
     cudaEventDestroy(ev1);
     return lm_cuda(h, e, "hrrt_lm_histogram");
   }
+  const ClockState clock0{h->current_time, h->current_time_msec, h->prev_time, h->clock_reset};
+  const long long frame_start0 = frame_start;
   const long long end_tag = replay_clock(h, htags.data(), (long long)ntags, duration, flags, &frame_start);
   long long limit = nwords;
   if (end_tag >= 0) limit = htags[end_tag].x;
-  if (!one_pass) e = launch(hist_mode, limit, 0);
+  if (!one_pass) {
+    hist_dev();
+    e = launch(hist_mode, limit, 0);
+  }
   if (wide && e == cudaSuccess) {
     const long long np = h->dev.sino_size / 2;  // bin pairs (sinogram sizes are multiples of 4)
     const unsigned nb = (unsigned)((np + 255) / 256);
@@ -966,6 +1160,15 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
                                                                  (uint32_t *)d_delayed);
       e = cudaGetLastError();
     }
+  }
+  std::vector<unsigned long long> hivl;
+  std::vector<longlong2> hsing;
+  if (hc && e == cudaSuccess) {
+    hivl.resize(2 * (ntags + 1));
+    hsing.resize(nsing);
+    e = cudaMemcpyAsync(hivl.data(), h->ivl, 8 * hivl.size(), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && nsing)
+      e = cudaMemcpyAsync(hsing.data(), h->sing, 16 * (size_t)nsing, cudaMemcpyDeviceToHost, st);
   }
   unsigned long long hs[kStCount] = {};
   cudaEventRecord(ev1, st);
@@ -992,7 +1195,35 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
   out->frame_start = frame_start;
   out->duration = h->current_time - frame_start;
   out->ms = ms;
+  if (hc) build_head_curve(h, clock0, frame_start0, htags, end_tag, hivl, std::move(hsing), duration, flags, limit);
   return HRRT_OK;
+}
+
+int hrrt_lm_head_curve(hrrt_lm *h, hrrt_lm_second *out, int capacity) {
+  if (!h) return HRRT_ERR_ARG;
+  const int n = (int)h->hc.size();
+  if (out)
+    for (int i = 0; i < n && i < capacity; i++) out[i] = h->hc[i];
+  return n;
+}
+
+int hrrt_lm_crystal_counts(hrrt_lm *h, uint32_t *counts) {
+  if (!h || !counts) return HRRT_ERR_ARG;
+  if (!h->ccounts) return lm_fail(h, HRRT_ERR_STATE, "no call with HRRT_LM_CRYSTAL_COUNTS yet");
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(counts, h->ccounts, sizeof(uint32_t) * 2 * hrrt::kCrystals, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_crystal_counts");
+  return HRRT_OK;
+}
+
+int hrrt_lm_block_singles(hrrt_lm *h, int *rates, long long *total_prompts, long long *total_randoms) {
+  if (!h) return HRRT_ERR_ARG;
+  if (rates)
+    for (size_t b = 0; b < h->block_rates.size(); b++) rates[b] = h->block_rates[b];
+  if (total_prompts) *total_prompts = h->hc_prompts;
+  if (total_randoms) *total_randoms = h->hc_randoms;
+  return (int)h->block_rates.size();
 }
 
 long long hrrt_lm_table(int span, int maxrd, const char *name, void *out, size_t bytes) {
@@ -1091,8 +1322,8 @@ int hrrt_lm_smooth_randoms(hrrt_lm *h, const int32_t *coinc_hist, float scan_dur
   const long long S = h->dev.sino_size;
   cudaStream_t st = h->stream;
   float *d_cs = nullptr, *d_out = nullptr;
-  e = cudaMemcpyToSymbolAsync(c_pair_heads, heads, sizeof(heads), 0, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMallocAsync(&d_cs, sizeof(float) * hrrt::kCrystals, st);
+  (void)heads;
+  e = cudaMallocAsync(&d_cs, sizeof(float) * hrrt::kCrystals, st);
   if (e == cudaSuccess) e = cudaMallocAsync(&d_out, sizeof(float) * S, st);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(d_cs, cs.data(), sizeof(float) * hrrt::kCrystals, cudaMemcpyHostToDevice, st);

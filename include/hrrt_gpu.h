@@ -334,6 +334,21 @@ int hrrt_batch_get_image(hrrt_batch *b, int frame, float *image_zyx, double *sum
 #define HRRT_LM_FORCE_DIRECT 16
 #define HRRT_LM_FORCE_PARTITIONED 32
 #define HRRT_LM_FORCE_WIDE 64
+/* also collect the frame's head curve and block singles (hrrt_lm_head_curve,
+ * hrrt_lm_block_singles); costs one more parse of the words */
+#define HRRT_LM_HEAD_CURVE 128
+/* also count the coincidence histogram (hrrt_lm_crystal_counts) */
+#define HRRT_LM_CRYSTAL_COUNTS 256
+
+/* one line of the head curve (.hc, process_tagword histogram_mp.cpp:241-258):
+ * at each change of second, the time, the prompt and delayed events since the
+ * previous line and the sum over blocks of their latest singles sample */
+typedef struct hrrt_lm_second {
+  long long time_ms;
+  long long prompts;
+  long long randoms;
+  long long total_singles;
+} hrrt_lm_second;
 
 typedef struct hrrt_lm_stats {
   long long words_used;  /* words consumed: through the tag that ended the frame, or all */
@@ -388,6 +403,22 @@ int hrrt_lm_histogram(hrrt_lm *lm, const uint32_t *words, long long nwords, int 
  * aligned), ADDING into sino / delayed, on `stream` (NULL: the library's). */
 int hrrt_lm_histogram_device(hrrt_lm *lm, const uint32_t *d_words, long long nwords, int mode, int duration,
                              int flags, uint16_t *d_sino, uint16_t *d_delayed, hrrt_lm_stats *stats, void *stream);
+
+/* After a hrrt_lm_histogram[_device] call with HRRT_LM_HEAD_CURVE: its head
+ * curve lines (copies min(n, capacity), returns n), and its block singles
+ * (rates: [936] average of each block's samples over the frame, the
+ * header's "block singles i"; the totals of the lines' prompts and randoms,
+ * the header's total prompts / randoms, histogram_mp.cpp:181-190). */
+int hrrt_lm_head_curve(hrrt_lm *lm, hrrt_lm_second *out, int capacity);
+int hrrt_lm_block_singles(hrrt_lm *lm, int *rates, long long *total_prompts, long long *total_randoms);
+/* After a call with HRRT_LM_CRYSTAL_COUNTS: the frame's coincidence histogram
+ * (the .ch file write_coin_map writes, histogram_mp.cpp:646-680): uint32
+ * [2][119808], prompt then delayed counts of both crystals of every emission
+ * event with DOI 0/1 (rebin_packet :1212-1223), crystal index
+ * layer*59904 + head*72 + x + ring*576.  The reference counts whole packets,
+ * so its map also holds the events after a frame's end in the same packet;
+ * here it holds the frame's events. */
+int hrrt_lm_crystal_counts(hrrt_lm *lm, uint32_t *counts);
 
 /* Smoothed randoms from a coincidence histogram (.ch: int32 [2][119808],
  * prompt then delayed counts per crystal [layer 2][ring 104][head 8][x 72]).

@@ -61,6 +61,7 @@ def lib():
         L.lm_rebin_event.argtypes = [vp, i, i, i, i, i, i, i]
         L.lm_histogram.argtypes = [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, vp, vp]
         f = ctypes.c_float
+        L.lm_histogram_hc.argtypes = [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, vp, vp, vp, i, vp, vp, vp]
         L.lm_crystal_singles.argtypes = [vp, f, f, vp]
         L.lm_smooth_randoms.argtypes = [vp, vp, f, f, i, vp]
         _L = L
@@ -130,6 +131,24 @@ class LMOracle:
         self.L.lm_histogram(self.t, _p(w), w.size, mode, duration, flags, ctypes.byref(self.clock), _p(sino),
                             _p(delayed), ctypes.byref(st))
         return sino, delayed, st.as_dict()
+
+    def histogram_hc(self, words, mode=PROMPTS_AND_DELAYED, duration=0, flags=0, max_lines=1 << 20):
+        """histogram() that also returns the frame's head curve (int64 [n][4]:
+        time ms, prompts, randoms, total singles), the blocks' average singles
+        rates [936] and the totals of the lines' prompts and randoms; the
+        coincidence histogram is left in self.last_crystal_counts."""
+        w = np.ascontiguousarray(words, np.uint32)
+        sino = np.zeros(self.sino_size, np.uint16)
+        delayed = np.zeros(self.sino_size, np.uint16) if mode == PROMPTS_AND_DELAYED else None
+        st = Stats()
+        hc = np.zeros((max_lines, 4), np.int64)
+        rates = np.zeros(936, np.int32)
+        tot = np.zeros(2, np.int64)
+        cc = np.zeros(2 * NCRYSTALS, np.uint32)
+        n = self.L.lm_histogram_hc(self.t, _p(w), w.size, mode, duration, flags, ctypes.byref(self.clock), _p(sino),
+                                   _p(delayed), ctypes.byref(st), _p(hc), max_lines, _p(rates), _p(tot), _p(cc))
+        self.last_crystal_counts = cc
+        return sino, delayed, st.as_dict(), hc[:min(n, max_lines)].copy(), rates, (int(tot[0]), int(tot[1]))
 
 
 NCRYSTALS = 2 * 104 * 8 * 72  # [layer][ring][head][x]

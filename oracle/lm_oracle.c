@@ -260,7 +260,26 @@ void lm_clock_init(lm_clock *c) {
 
 /* process_tagword time-tag branch (hist:225-260); returns 1 when the frame
  * ends at this tag */
-static int time_tag(lm_clock *c, unsigned tag, int duration, int flags, long long *frame_start) {
+/* head curve and block singles of a frame (process_tagword, hist:225-303) */
+#define NBLOCKS 936
+typedef struct {
+  lm_second *out;
+  int cap, n;
+  long long prompts, randoms, t_prompts, t_randoms;
+  long long last[NBLOCKS], total[NBLOCKS], nsamples[NBLOCKS];
+} hc_state;
+
+static int time_tag(lm_clock *c, unsigned tag, int duration, int flags, long long *frame_start, hc_state *hc) {
+  if (hc && (tag & 0xE0000000u) == 0xA0000000u) { /* block singles (hist:260-270) */
+    const int block = (int)((tag & 0x1ff80000u) >> 19);
+    const long long v = tag & 0x0007ffff;
+    if (block >= 0 && block < NBLOCKS) {
+      hc->last[block] = v;
+      hc->total[block] += v;
+      hc->nsamples[block]++;
+    }
+    return 0;
+  }
   if ((tag & 0xE0000000u) != 0x80000000u) return 0;
   if (flags & LM_TIME_FROM_COUNT)
     c->current_time_msec++;
@@ -275,6 +294,15 @@ static int time_tag(lm_clock *c, unsigned tag, int duration, int flags, long lon
   }
   c->prev_time = c->current_time_msec;
   if (c->current_time != c->current_time_msec / 1000) {
+    if (hc) { /* the head-curve line (hist:241-258) */
+      long long singles = 0;
+      for (int b = 0; b < NBLOCKS; b++) singles += hc->last[b];
+      if (hc->n < hc->cap) hc->out[hc->n] = (lm_second){c->current_time_msec, hc->prompts, hc->randoms, singles};
+      hc->n++;
+      hc->t_prompts += hc->prompts;
+      hc->t_randoms += hc->randoms;
+      hc->prompts = hc->randoms = 0;
+    }
     c->current_time = c->current_time_msec / 1000;
     if (*frame_start < 0) *frame_start = c->current_time;
     if (duration > 0 && (c->current_time - *frame_start) >= duration) return 1;
@@ -289,8 +317,9 @@ static void bump(uint16_t *h, long long a, int delta) { h[a] = (uint16_t)(h[a] +
  * their own first word: a word left over at a packet end is dropped
  * (`(src_pos + 1) < count`).  The reference's reader exits on a short last
  * packet; here the last packet is parsed like the others. */
-int lm_histogram(const lm_tables *t, const uint32_t *w, long long n, int mode, int duration, int flags, lm_clock *clk,
-                 uint16_t *sino, uint16_t *delayed, lm_stats *st) {
+static int histogram_impl(const lm_tables *t, const uint32_t *w, long long n, int mode, int duration, int flags,
+                          lm_clock *clk, uint16_t *sino, uint16_t *delayed, lm_stats *st, hc_state *hc,
+                          uint32_t *ccounts) {
   memset(st, 0, sizeof(*st));
   const long long sino_size = lm_sino_size(t);
   const int ignore_border = flags & LM_IGNORE_BORDER_CRYSTAL;
@@ -342,6 +371,12 @@ int lm_histogram(const lm_tables *t, const uint32_t *w, long long n, int mode, i
           st->doi7++;
           continue;
         }
+        if ((doia == 1 || doia == 0) && (doib == 1 || doib == 0) && ccounts) {
+          /* the coincidence histogram (hist:1212-1223) */
+          uint32_t *cc = ccounts + (type ? NXCRYS * NYCRYS * NHEADS * NDOIS : 0);
+          cc[doia * NXCRYS * NYCRYS * NHEADS + HRRT_MPAIRS[mpe][0] * NXCRYS + ax + ay * NXCRYS * NHEADS]++;
+          cc[doib * NXCRYS * NYCRYS * NHEADS + HRRT_MPAIRS[mpe][1] * NXCRYS + bx + by * NXCRYS * NHEADS]++;
+        }
         if ((doia == 1 || doia == 0) && (doib == 1 || doib == 0)) {
           if (ignore_border && (ax * bx == 0 || ax == xhigh || bx == xhigh)) {
             address = -1;
@@ -365,7 +400,7 @@ int lm_histogram(const lm_tables *t, const uint32_t *w, long long n, int mode, i
       /* next_event_32 (hist:334-382) and histogram (hist:1316-1362) */
       if (word32 & 0x80000000u) {
         st->timetags += ((word32 & 0xE0000000u) == 0x80000000u);
-        if (time_tag(clk, word32, duration, flags, &frame_start)) terminated = 1;
+        if (time_tag(clk, word32, duration, flags, &frame_start, hc)) terminated = 1;
         continue;
       }
       const int prompt = (word32 & 0x40000000u) != 0;
@@ -374,6 +409,12 @@ int lm_histogram(const lm_tables *t, const uint32_t *w, long long n, int mode, i
         st->prompts++;
       else
         st->delayed++;
+      if (hc) {
+        if (prompt)
+          hc->prompts++;
+        else
+          hc->randoms++;
+      }
       if (value >= 0 && value < sino_size) {
         if (mode == LM_PROMPTS_AND_DELAYED) {
           if (prompt)
@@ -393,6 +434,27 @@ int lm_histogram(const lm_tables *t, const uint32_t *w, long long n, int mode, i
   st->frame_start = frame_start;
   st->duration = clk->current_time - frame_start;
   return 0;
+}
+
+int lm_histogram(const lm_tables *t, const uint32_t *w, long long n, int mode, int duration, int flags, lm_clock *clk,
+                 uint16_t *sino, uint16_t *delayed, lm_stats *st) {
+  return histogram_impl(t, w, n, mode, duration, flags, clk, sino, delayed, st, NULL, NULL);
+}
+
+int lm_histogram_hc(const lm_tables *t, const uint32_t *w, long long n, int mode, int duration, int flags,
+                    lm_clock *clk, uint16_t *sino, uint16_t *delayed, lm_stats *st, lm_second *hc_out, int hc_cap,
+                    int *block_rates, long long *totals, uint32_t *ccounts) {
+  hc_state *hc = (hc_state *)calloc(1, sizeof(hc_state));
+  hc->out = hc_out;
+  hc->cap = hc_cap;
+  if (ccounts) memset(ccounts, 0, sizeof(uint32_t) * 2 * NXCRYS * NYCRYS * NHEADS * NDOIS);
+  const int r = histogram_impl(t, w, n, mode, duration, flags, clk, sino, delayed, st, hc, ccounts);
+  for (int b = 0; b < NBLOCKS; b++) block_rates[b] = hc->nsamples[b] ? (int)(hc->total[b] / hc->nsamples[b]) : 0;
+  totals[0] = hc->t_prompts;
+  totals[1] = hc->t_randoms;
+  const int lines = hc->n;
+  free(hc);
+  return r < 0 ? r : lines;
 }
 
 /* ---- smoothed randoms (gen_delays_lib/gen_delays_lib.cpp) ---------------- */

@@ -81,6 +81,19 @@ void lm_clock_init(lm_clock *c);
 int lm_histogram(const lm_tables *t, const uint32_t *words, long long nwords, int mode, int duration, int flags,
                  lm_clock *clock, uint16_t *sino, uint16_t *delayed, lm_stats *st);
 
+/* one head-curve line: time (ms), prompts and delayed since the previous
+ * line, sum of the blocks' latest singles samples */
+typedef struct {
+  long long time_ms, prompts, randoms, total_singles;
+} lm_second;
+/* lm_histogram that also writes the frame's head curve (returns the number of
+ * lines, up to hc_cap stored), the blocks' average singles rates [936], the
+ * totals of the lines' prompts and randoms [2] and, when ccounts is not
+ * NULL, the coincidence histogram [2][119808] */
+int lm_histogram_hc(const lm_tables *t, const uint32_t *words, long long nwords, int mode, int duration, int flags,
+                    lm_clock *clock, uint16_t *sino, uint16_t *delayed, lm_stats *st, lm_second *hc_out, int hc_cap,
+                    int *block_rates, long long *totals, uint32_t *ccounts);
+
 /* smoothed randoms (gen_delays): crystal singles from the 119808 delayed
  * crystal counts (returns the iterations), and the randoms sinogram from a
  * coincidence histogram [2][119808] (prompt then delayed counts), both as

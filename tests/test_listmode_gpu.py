@@ -154,3 +154,58 @@ def test_device_entry_adds_into_buffers(pair):
     got_d = dd.cpu().numpy().view(np.uint16)
     assert np.array_equal(got_s, (2 * so.astype(np.uint32)).astype(np.uint16))
     assert np.array_equal(got_d, (2 * do.astype(np.uint32)).astype(np.uint16))
+
+
+def singles_stream(seed, nevents, tag_every=700):
+    """random_stream's events with block singles tags (random blocks and
+    rates) after every time tag, and a clock that skips a millisecond now and
+    then."""
+    rng = np.random.default_rng(seed)
+    base = random_stream(seed, nevents, tag_every=tag_every, p_resync=0.0)
+    out = []
+    i = 0
+    while i < base.size:
+        if i + 1 < base.size and (base[i] >> 30) == 1 and (base[i + 1] >> 30) == 3:
+            out.append(base[i:i + 2])
+            tag = (int(base[i]) & 0xffff) | ((int(base[i + 1]) & 0xffff) << 16)
+            if (tag & 0xE0000000) == 0x80000000:
+                for _ in range(int(rng.integers(0, 4))):
+                    blk = int(rng.integers(0, 936))
+                    val = int(rng.integers(0, 1 << 19))
+                    s1, s2 = tag_words(np.uint32(0xA0000000 | (blk << 19) | val))
+                    out.append(np.array([s1, s2], np.uint32))
+            i += 2
+        else:
+            out.append(base[i:i + 1])
+            i += 1
+    return np.concatenate(out).astype(np.uint32)
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_head_curve_and_block_singles(pair, path):
+    """LM_HEAD_CURVE | LM_CRYSTAL_COUNTS: the per-second lines, the block
+    singles averages, the line totals and the coincidence histogram equal the
+    oracle's (whole stream, then 1-s frames)."""
+    import hrrt_reconstruction_b200 as H
+    O, D = pair
+    w = singles_stream(11, 2_200_000)
+    for duration in (0, 1):
+        O.reset_clock()
+        D.reset_clock()
+        pos = 0
+        for k in range(2 if duration else 1):
+            so, do, sto, hco, rates_o, tot_o = O.histogram_hc(w[pos:], duration=duration)
+            sd, dd, std = D.histogram(w[pos:], duration=duration,
+                                      flags=path | H.LM_HEAD_CURVE | H.LM_CRYSTAL_COUNTS)
+            assert np.array_equal(so, sd) and np.array_equal(do, dd)
+            for key in STAT_KEYS:
+                assert sto[key] == std[key], (key, sto[key], std[key])
+            hcd = D.head_curve()
+            rates_d, tot_d = D.block_singles()
+            assert hco.shape[0] > 0
+            assert np.array_equal(hcd, hco), (hcd[:3], hco[:3])
+            assert np.array_equal(rates_d, rates_o)
+            assert tot_d == tot_o
+            cc = D.crystal_counts()
+            assert cc.sum() > 0 and np.array_equal(cc, O.last_crystal_counts)
+            pos += sto["words_used"]
