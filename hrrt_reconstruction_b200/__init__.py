@@ -145,6 +145,8 @@ def _load():
         "hrrt_lm_smooth_randoms": (i, [vp, vp, f, f, vp, ctypes.POINTER(i)]),
         "hrrt_lm_head_curve": (i, [vp, vp, i]),
         "hrrt_lm_crystal_counts": (i, [vp, vp]),
+        "hrrt_lm_convert_span9": (ctypes.c_longlong, [vp, vp, vp, i]),
+        "hrrt_lm_trues_span9_device": (i, [vp, vp, vp, vp, vp]),
         "hrrt_lm_block_singles": (i, [vp, vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
         "hrrt_lm_crystal_singles": (i, [vp, f, f, vp]),
     }
@@ -517,6 +519,20 @@ def crystal_singles(delayed_counts, scan_duration=1.0, tau=6.0e-9):
     return out, it
 
 
+def convert_span9(span3, delayed=None, maxrd=67):
+    """Host-only: convert_span9 of a span-3 int16 sinogram (minus `delayed`
+    when given: the -PR trues) -> the 2209-plane span-9 int16 sinogram."""
+    a = np.ascontiguousarray(span3).view(np.int16).reshape(-1)
+    d = None if delayed is None else np.ascontiguousarray(delayed).view(np.int16).reshape(-1)
+    if d is not None and d.size != a.size:
+        raise HrrtError("convert_span9: prompts and delayed differ in size")
+    out = np.empty(2209 * 288 * 256, np.int16)
+    n = lib.hrrt_lm_convert_span9(_ptr(a), _ptr(d) if d is not None else None, _ptr(out), maxrd)
+    if n < 0:
+        raise HrrtError(f"convert_span9: {n}")
+    return out[:n * 288 * 256]
+
+
 def lm_table(name, span=3, maxrd=67):
     """One listmode rebinning table (host-only): "sol" [21][144][144] LM_SOL,
     "zpos"/"zpos2" float [104], "segz0"/"segzmax"/"segzoffset" int32."""
@@ -628,6 +644,14 @@ class Listmode:
         self._check(lib.hrrt_lm_smooth_randoms(self._h, _ptr(h), scan_duration, tau, _ptr(out), ctypes.byref(it)),
                     "lm_smooth_randoms")
         return out, it.value
+
+    def trues_span9_device(self, d_prompts, d_delayed, d_out, stream=None):
+        """Device pointers (ints; d_delayed may be 0): the span-3 prompts minus
+        delayed folded into span 9 (2209 planes of int16) on `stream`."""
+        self._check(lib.hrrt_lm_trues_span9_device(self._h, ctypes.c_void_p(d_prompts),
+                                                   ctypes.c_void_p(d_delayed) if d_delayed else None,
+                                                   ctypes.c_void_p(d_out),
+                                                   ctypes.c_void_p(stream) if stream else None), "lm_trues_span9")
 
     def histogram_device(self, d_words, nwords, d_sino, d_delayed=None, mode=LM_PROMPTS_AND_DELAYED, duration=0,
                          flags=0, stream=None):

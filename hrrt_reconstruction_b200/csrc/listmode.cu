@@ -38,6 +38,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/hrrt_gpu.h"
@@ -698,6 +699,42 @@ __global__ void lm_fold_kernel(const int2 *__restrict__ counts, uint32_t *__rest
   bins[i] = lo | (hi << 16);
 }
 
+// The span-3 -> span-9 fold of the trues sinogram (convert_span9 after the
+// prompts - delayed subtraction of write_sino, lmhistogram_mp.cpp:650-676):
+// one thread per 8 bins (16 bytes) of a span-9 plane adds, in 16-bit lanes
+// that wrap like the reference's shorts, prompts - delayed of the plane's
+// (up to three) span-3 source planes.  Grid: x over the 9216 16-byte words
+// of a plane, y over the span-9 planes.  HBM-bound: 16 B read per source
+// plane and input, 16 B written.
+__global__ void __launch_bounds__(256) lm_span9_kernel(const uint4 *__restrict__ prompts,
+                                                       const uint4 *__restrict__ delayed,
+                                                       const int4 *__restrict__ src, uint4 *__restrict__ out) {
+  constexpr int kWords = 256 * 288 / 8;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kWords) return;
+  const int4 s = src[blockIdx.y];
+  const int sp[3] = {s.x, s.y, s.z};
+  uint4 acc = make_uint4(0, 0, 0, 0);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    if (sp[k] < 0) continue;
+    const size_t at = (size_t)sp[k] * kWords + i;
+    uint4 v = __ldcs(prompts + at);
+    if (delayed) {
+      const uint4 d = __ldcs(delayed + at);
+      v.x = __vsub2(v.x, d.x);
+      v.y = __vsub2(v.y, d.y);
+      v.z = __vsub2(v.z, d.z);
+      v.w = __vsub2(v.w, d.w);
+    }
+    acc.x = __vadd2(acc.x, v.x);
+    acc.y = __vadd2(acc.y, v.y);
+    acc.z = __vadd2(acc.z, v.z);
+    acc.w = __vadd2(acc.w, v.w);
+  }
+  __stcs(out + (size_t)blockIdx.y * kWords + i, acc);
+}
+
 }  // namespace
 
 // ============================================================================
@@ -727,6 +764,8 @@ struct hrrt_lm {
   unsigned int *sing_n = nullptr;
   long long sing_cap = 0;
   unsigned int *ccounts = nullptr;  // coincidence histogram of the last call
+  int4 *span9_src = nullptr;        // span-9 plane -> span-3 source planes
+  int span9_planes = 0;
   std::vector<hrrt_lm_second> hc;
   std::vector<int> block_rates;
   long long hc_prompts = 0, hc_randoms = 0;
@@ -745,6 +784,7 @@ struct hrrt_lm {
     if (sing) cudaFree(sing);
     if (sing_n) cudaFree(sing_n);
     if (ccounts) cudaFree(ccounts);
+    if (span9_src) cudaFree(span9_src);
     if (h_words_dev) cudaFree(h_words_dev);
     if (h_sino_dev) cudaFree(h_sino_dev);
     if (stream) cudaStreamDestroy(stream);
@@ -1317,12 +1357,9 @@ int hrrt_lm_smooth_randoms(hrrt_lm *h, const int32_t *coinc_hist, float scan_dur
   std::vector<float> cs(hrrt::kCrystals);
   const int it = hrrt::singles_from_delayed(coinc_hist + hrrt::kCrystals, t, ft, cs.data());
   if (iterations) *iterations = it;
-  int heads[21][2];
-  for (int mp = 0; mp < 21; mp++) hrrt::pair_heads(mp, &heads[mp][0], &heads[mp][1]);
   const long long S = h->dev.sino_size;
   cudaStream_t st = h->stream;
   float *d_cs = nullptr, *d_out = nullptr;
-  (void)heads;
   e = cudaMallocAsync(&d_cs, sizeof(float) * hrrt::kCrystals, st);
   if (e == cudaSuccess) e = cudaMallocAsync(&d_out, sizeof(float) * S, st);
   if (e == cudaSuccess)
@@ -1339,6 +1376,61 @@ int hrrt_lm_smooth_randoms(hrrt_lm *h, const int32_t *coinc_hist, float scan_dur
   const cudaError_t e2 = cudaStreamSynchronize(st);
   if (e == cudaSuccess) e = e2;
   if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_smooth_randoms");
+  return HRRT_OK;
+}
+
+long long hrrt_lm_convert_span9(const int16_t *span3, const int16_t *delayed, int16_t *span9, int maxrd) {
+  std::vector<int32_t> src;
+  const int planes9 = hrrt::span9_plane_sources(maxrd, hrrt::LmTables::kYCrys, &src);
+  if (planes9 < 0 || !span3 || !span9) return HRRT_ERR_ARG;
+  constexpr long long kPix = 256LL * 288;
+  auto fold = [&](int p0, int p1) {
+    for (int p = p0; p < p1; p++) {
+      uint16_t *o = (uint16_t *)span9 + p * kPix;
+      std::memset(o, 0, sizeof(uint16_t) * kPix);
+      for (int k = 0; k < 3; k++) {
+        const int32_t sp = src[(size_t)p * 3 + k];
+        if (sp < 0) continue;
+        const uint16_t *a = (const uint16_t *)span3 + sp * kPix;
+        const uint16_t *d = delayed ? (const uint16_t *)delayed + sp * kPix : nullptr;
+        for (long long j = 0; j < kPix; j++) o[j] = (uint16_t)(o[j] + a[j] - (d ? d[j] : 0));
+      }
+    }
+  };
+  const int nt = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; t++) pool.emplace_back(fold, planes9 * t / nt, planes9 * (t + 1) / nt);
+  for (auto &th : pool) th.join();
+  return planes9;
+}
+
+int hrrt_lm_trues_span9_device(hrrt_lm *h, const uint16_t *d_prompts, const uint16_t *d_delayed, int16_t *d_span9,
+                               void *stream) {
+  if (!h) return HRRT_ERR_ARG;
+  if (h->tab.span != 3) return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_trues_span9_device: the handle is not span 3");
+  if (!d_prompts || !d_span9) return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_trues_span9_device: null buffer");
+  if (((uintptr_t)d_prompts | (uintptr_t)d_delayed | (uintptr_t)d_span9) & 15)
+    return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_trues_span9_device: buffers must be 16-byte aligned");
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_trues_span9_device");
+  if (!h->span9_src) {
+    std::vector<int32_t> src;
+    const int planes9 = hrrt::span9_plane_sources(h->tab.maxrd, hrrt::LmTables::kYCrys, &src);
+    if (planes9 < 0) return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_trues_span9_device: maxrd has no span-9 fold");
+    std::vector<int4> packed(planes9);
+    for (int p = 0; p < planes9; p++) packed[p] = make_int4(src[3 * p], src[3 * p + 1], src[3 * p + 2], -1);
+    e = cudaMalloc(&h->span9_src, sizeof(int4) * planes9);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(h->span9_src, packed.data(), sizeof(int4) * planes9, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_trues_span9_device: tables");
+    h->span9_planes = planes9;
+  }
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  const dim3 grid((256 * 288 / 8 + 255) / 256, (unsigned)h->span9_planes);
+  lm_span9_kernel<<<grid, 256, 0, st>>>((const uint4 *)d_prompts, (const uint4 *)d_delayed, h->span9_src,
+                                         (uint4 *)d_span9);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_trues_span9_device");
   return HRRT_OK;
 }
 

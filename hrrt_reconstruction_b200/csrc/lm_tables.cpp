@@ -228,4 +228,43 @@ int singles_from_delayed(const int32_t *dcoins, float tau, float dt, float *srat
   return iter;
 }
 
+// convert_span9 folds in place: span-9 segment 0 is span-3 segment 0 plus
+// segments -1 / +1 at their plane offset; span-9 segment -k / +k starts as
+// a copy of span-3 segment -(3k-1) / +(3k-1) and adds -(3k) / +(3k) and
+// -(3k+1) / +(3k+1) at theirs.  Every read is ahead of every write, so the
+// fold equals this gather of the input planes.
+int span9_plane_sources(int maxrd, int nrings, std::vector<int32_t> *src) {
+  const int nseg = (2 * maxrd + 1) / 3, nseg9 = (2 * maxrd + 1) / 9;
+  if (nseg9 < 1 || nseg != 3 * nseg9 || nseg % 2 == 0) return -1;
+  std::vector<int> nplns(nseg), move(nseg, 0);
+  for (int i = 0; i < nseg; i++) {
+    const int seg = (i + 1) / 2, seg9 = (i + 3) / 6;
+    nplns[i] = seg > 0 ? 2 * nrings - 3 * (2 * seg - 1) - 2 : 2 * nrings - 1;
+    const int n9 = seg > 1 ? 2 * nrings - 9 * (2 * seg9 - 1) - 2 : 2 * nrings - 1;
+    if (seg > 0) move[i] = (n9 - nplns[i]) / 2;
+  }
+  std::vector<int> start(nseg + 1, 0);
+  for (int i = 0; i < nseg; i++) start[i + 1] = start[i] + nplns[i];
+  int planes9 = nplns[0];
+  for (int k = 1; 2 * k - 1 < nseg9; k++) planes9 += 2 * nplns[6 * k - 3];
+  src->assign((size_t)planes9 * 3, -1);
+  auto add = [&](int dst_plane, int slot, int seg) {
+    for (int q = 0; q < nplns[seg]; q++) (*src)[(size_t)(dst_plane + q) * 3 + slot] = start[seg] + q;
+  };
+  add(0, 0, 0);
+  add(move[1], 1, 1);
+  add(move[2], 2, 2);
+  int pos9 = nplns[0];
+  for (int first = 3; first < nseg; first += 6) {
+    const int nout = nplns[first];
+    for (int k = 0; k < 6; k++) {
+      const int seg = first + k;
+      const int base = pos9 + (k % 2 ? nout : 0);
+      add(base + (k < 2 ? 0 : move[seg]), k / 2, seg);
+    }
+    pos9 += 2 * nout;
+  }
+  return planes9;
+}
+
 }  // namespace hrrt

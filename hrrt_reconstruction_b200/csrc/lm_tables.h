@@ -45,4 +45,11 @@ constexpr int kCrystals = LmTables::kLayers * LmTables::kYCrys * LmTables::kHead
 // head pair mp (1..20) -> (head a, head b)
 void pair_heads(int mp, int *ahead, int *bhead);
 
+// The span-3 -> span-9 plane fold of convert_span9
+// (lmhistogram_mp/convert_span9.cpp:13-150) as a gather: for every span-9
+// plane the (up to three) span-3 planes that sum into it, -1 for none.
+// Returns the span-9 plane count (2209 at maxrd 67, 104 rings), or -1 when
+// maxrd does not give whole span-9 segments.
+int span9_plane_sources(int maxrd, int nrings, std::vector<int32_t> *src /* [planes9][3] */);
+
 }  // namespace hrrt

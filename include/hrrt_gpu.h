@@ -439,6 +439,20 @@ int hrrt_lm_smooth_randoms(hrrt_lm *lm, const int32_t *coinc_hist, float scan_du
  * 119808 delayed crystal counts; returns the iterations run. */
 int hrrt_lm_crystal_singles(const int32_t *delayed_counts, float scan_duration, float tau, float *singles);
 
+/* convert_span9 (lmhistogram_mp/convert_span9.cpp:13, called from
+ * write_sino, lmhistogram_mp.cpp:668-677): the span-3 sinogram (minus the
+ * delayed sinogram when `delayed` is not NULL: the trues of -PR mode) folded
+ * into the 2209-plane span-9 sinogram, 16-bit sums that wrap like the
+ * reference's shorts.  Host code, out of place (span9 holds 2209 planes and
+ * may not alias the inputs); returns the span-9 plane count or a negative
+ * error code. */
+long long hrrt_lm_convert_span9(const int16_t *span3, const int16_t *delayed, int16_t *span9, int maxrd);
+/* The same fold on the device from a span-3 handle's histograms (d_delayed
+ * may be NULL), enqueued on `stream` (NULL: the handle's stream); 16-byte
+ * aligned device buffers, output not aliasing the inputs. */
+int hrrt_lm_trues_span9_device(hrrt_lm *lm, const uint16_t *d_prompts, const uint16_t *d_delayed, int16_t *d_span9,
+                               void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -64,6 +64,8 @@ def lib():
         L.lm_histogram_hc.argtypes = [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, vp, vp, vp, i, vp, vp, vp]
         L.lm_crystal_singles.argtypes = [vp, f, f, vp]
         L.lm_smooth_randoms.argtypes = [vp, vp, f, f, i, vp]
+        L.lm_convert_span9.argtypes = [vp, i, i]
+        L.lm_convert_span9.restype = None
         _L = L
     return _L
 
@@ -172,6 +174,14 @@ def smooth_randoms(oracle, coinc_hist, scan_duration=1.0, tau=6.0e-9, maxrd=67):
     out = np.zeros(oracle.sino_size, np.float32)
     it = lib().lm_smooth_randoms(oracle.t, _p(h), scan_duration, tau, maxrd, _p(out))
     return out, it
+
+
+def convert_span9(span3, maxrd=67, nrings=104):
+    """convert_span9: the span-3 int16 sinogram folded into span 9 (returns the
+    2209 span-9 planes; 16-bit sums wrap)."""
+    w = np.array(span3, np.int16).reshape(-1)
+    lib().lm_convert_span9(_p(w), maxrd, nrings)
+    return w[:2209 * 288 * 256].copy()
 
 
 def delayed_counts_from_singles(singles, scan_duration=1.0, tau=6.0e-9):

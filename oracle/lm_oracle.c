@@ -562,3 +562,57 @@ int lm_smooth_randoms(const lm_tables *t, const int32_t *coinc_hist, float scan_
   free(cs);
   return it;
 }
+
+/* convert_span9 (lmhistogram_mp/convert_span9.cpp:13-150): the span-3 trues
+ * sinogram folded in place into span 9.  Span-9 segment 0 is span-3 segment
+ * 0 plus segments -1 and +1 shifted by their plane offset; every further
+ * span-9 segment -k / +k is the copy of span-3 segment -(3k-1) / +(3k-1)
+ * plus segments -(3k) / +(3k) and -(3k+1) / +(3k+1) shifted by theirs.  The
+ * sums are 16-bit (they wrap); the first 2209 planes hold the result. */
+void lm_convert_span9(int16_t *sino, int maxrd, int nrings) {
+  const int nseg = (2 * maxrd + 1) / 3, nseg9 = (2 * maxrd + 1) / 9;
+  const long long npix = 256LL * 288;
+  int nplns[64], nplns9[64], move[64];
+  if (nseg > 64) return;
+  for (int i = 0; i < nseg; i++) {
+    const int seg = (i + 1) / 2, seg9 = (i + 3) / 6;
+    nplns[i] = nplns9[i] = 207;
+    move[i] = 0;
+    if (seg > 0) nplns[i] = 2 * nrings - 3 * (2 * seg - 1) - 2;
+    if (seg > 1) nplns9[i] = 2 * nrings - 9 * (2 * seg9 - 1) - 2;
+    if (seg > 0) move[i] = (nplns9[i] - nplns[i]) / 2;
+  }
+  int iseg = 0, iseg9 = 0;
+  long long pos3 = 0, pos9 = 0;
+  while (iseg9 < nseg9) {
+    const int nout = nplns[iseg];
+    if (iseg9 == 0) {
+      /* segment 0 stays; add -1 and +1 */
+      int16_t *out = sino + move[1] * npix;
+      for (int k = 1; k <= 2; k++) {
+        pos3 += nplns[k - 1];
+        const int16_t *in = sino + pos3 * npix;
+        const long long n = npix * nplns[1];
+        for (long long j = 0; j < n; j++) out[j] = (int16_t)(out[j] + in[j]);
+      }
+      pos9 = nout;
+      iseg = 3;
+      iseg9 = 1;
+    } else {
+      int16_t *neg = sino + pos9 * npix;
+      int16_t *pos = neg + (long long)nout * npix;
+      for (int k = 0; k < 6; k++, iseg++) {
+        pos3 += nplns[iseg - 1];
+        const int16_t *in = sino + pos3 * npix;
+        const long long n = npix * nplns[iseg];
+        int16_t *out = (k % 2 == 0 ? neg : pos) + (k < 2 ? 0 : (long long)move[iseg] * npix);
+        if (k < 2)
+          memcpy(out, in, sizeof(int16_t) * n);
+        else
+          for (long long j = 0; j < n; j++) out[j] = (int16_t)(out[j] + in[j]);
+      }
+      pos9 += 2LL * nout;
+      iseg9 += 2;
+    }
+  }
+}

@@ -102,6 +102,10 @@ int lm_crystal_singles(const int32_t *dcoins, float tau, float dt, float *srates
 int lm_smooth_randoms(const lm_tables *t, const int32_t *coinc_hist, float scan_duration, float tau, int maxrd,
                       float *sino);
 
+/* convert_span9: a span-3 trues sinogram (45 segments, maxrd 67) folded in
+ * place into span 9; the first 2209 planes hold the result */
+void lm_convert_span9(int16_t *sino, int maxrd, int nrings);
+
 #ifdef __cplusplus
 }
 #endif

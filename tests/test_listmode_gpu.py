@@ -209,3 +209,38 @@ def test_head_curve_and_block_singles(pair, path):
             cc = D.crystal_counts()
             assert cc.sum() > 0 and np.array_equal(cc, O.last_crystal_counts)
             pos += sto["words_used"]
+
+
+def test_trues_span9_device(pair):
+    """hrrt_lm_trues_span9_device: the device histograms' prompts - delayed
+    folded into span 9 equal the oracle's convert_span9 of the same trues and
+    the library's host fold; full-range random planes wrap like shorts."""
+    import torch
+    import hrrt_reconstruction_b200 as H
+    O, D = pair
+    S = D.sino_size
+    if O.span != 3:
+        buf = torch.zeros(8, dtype=torch.int16, device="cuda")
+        with pytest.raises(H.HrrtError):
+            D.trues_span9_device(buf.data_ptr(), 0, buf.data_ptr())
+        return
+    w = random_stream(21, 400_000)
+    D.reset_clock()
+    dw = torch.from_numpy(w.view(np.int32)).cuda()
+    ds = torch.zeros(S, dtype=torch.int16, device="cuda")
+    dd = torch.zeros(S, dtype=torch.int16, device="cuda")
+    D.histogram_device(dw.data_ptr(), w.size, ds.data_ptr(), dd.data_ptr())
+    out = torch.empty(2209 * 288 * 256, dtype=torch.int16, device="cuda")
+    D.trues_span9_device(ds.data_ptr(), dd.data_ptr(), out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    p, d = ds.cpu().numpy(), dd.cpu().numpy()
+    want = lm.convert_span9((p - d).astype(np.int16))
+    assert np.count_nonzero(want) > 10_000 and np.array_equal(got, want)
+    assert np.array_equal(got, H.convert_span9(p, d))
+    rng = np.random.default_rng(4)
+    a = rng.integers(-32768, 32768, S, dtype=np.int16)
+    ds.copy_(torch.from_numpy(a))
+    D.trues_span9_device(ds.data_ptr(), 0, out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), lm.convert_span9(a))

@@ -206,3 +206,51 @@ def test_device_lut_matches_oracle():
         assert np.array_equal(H.lm_table("segz0", span), z0)
         assert np.array_equal(H.lm_table("segzmax", span), zm)
         assert np.array_equal(H.lm_table("segzoffset", span), off)
+
+
+def test_convert_span9_folds_the_span3_histogram_into_span9():
+    """convert_span9 (convert_span9.cpp:13) of the span-3 trues equals the
+    span-9 rebinning of the same events, bin for bin: the fold's segment
+    grouping and plane offsets agree with the span-9 LUT."""
+    from test_listmode_gpu import random_stream
+    w = random_stream(5, 200_000)
+    s3, d3, _ = LMOracle(3).histogram(w)
+    s9, d9, _ = LMOracle(9).histogram(w)
+    t3 = (s3.view(np.int16) - d3.view(np.int16)).astype(np.int16)
+    t9 = (s9.view(np.int16) - d9.view(np.int16)).astype(np.int16)
+    got = lm.convert_span9(t3)
+    assert got.size == LMOracle(9).sino_size
+    assert np.count_nonzero(t9) > 10_000 and np.array_equal(got, t9)
+
+
+def test_convert_span9_known_planes():
+    """Span-9 segment 0 plane q = span-3 segment 0 plane q + segments -1 and
+    +1 (203 planes each, after 207) at plane q - 2; segment -1 of span 9
+    (197 planes, after 207) starts with span-3 segment -2 (after 207+2*203)."""
+    t3 = np.zeros(6367 * SINO_PLANE, np.int16)
+    planes = t3.reshape(6367, SINO_PLANE)
+    planes[10, 0] = 1
+    planes[207 + 8, 0] = 10
+    planes[207 + 203 + 8, 0] = 100
+    planes[207 + 2 * 203 + 4, 5] = 7
+    planes[0, 1] = 32767
+    planes[207 + 0, 1] = 1   # segment -1 plane 0 -> span-9 plane 2
+    planes[2, 1] = 32767
+    got = lm.convert_span9(t3).reshape(2209, SINO_PLANE)
+    assert got[10, 0] == 111
+    assert got[207 + 4, 5] == 7
+    assert got[0, 1] == 32767 and got[2, 1] == -32768  # 16-bit wrap
+
+
+def test_library_convert_span9_matches_oracle():
+    """The library's host fold (hrrt_lm_convert_span9) against the oracle's
+    in-place restatement over the full int16 range, with and without the
+    delayed subtraction."""
+    import hrrt_reconstruction_b200 as H
+    rng = np.random.default_rng(3)
+    a = rng.integers(-32768, 32768, 6367 * SINO_PLANE, dtype=np.int16)
+    d = rng.integers(-32768, 32768, a.size, dtype=np.int16)
+    assert np.array_equal(H.convert_span9(a, d), lm.convert_span9((a - d).astype(np.int16)))
+    assert np.array_equal(H.convert_span9(a), lm.convert_span9(a))
+    with pytest.raises(H.HrrtError):
+        H.convert_span9(a, maxrd=66)
