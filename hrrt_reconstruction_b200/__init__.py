@@ -145,6 +145,8 @@ def _load():
         "hrrt_lm_smooth_randoms": (i, [vp, vp, f, f, vp, ctypes.POINTER(i)]),
         "hrrt_lm_head_curve": (i, [vp, vp, i]),
         "hrrt_lm_crystal_counts": (i, [vp, vp]),
+        "hrrt_lm_histogram_at": (i, [vp, vp, ctypes.c_longlong, ctypes.c_longlong, i, i, i, vp, vp, vp]),
+        "hrrt_lm_seek": (i, [vp, vp, ctypes.c_longlong, ctypes.c_longlong, i, i, vp]),
         "hrrt_lm_convert_span9": (ctypes.c_longlong, [vp, vp, vp, i]),
         "hrrt_lm_trues_span9_device": (i, [vp, vp, vp, vp, vp]),
         "hrrt_lm_block_singles": (i, [vp, vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
@@ -595,9 +597,11 @@ class Listmode:
         """cudaStream_t (int) of the host-buffer entry point."""
         return lib.hrrt_lm_get_stream(self._h)
 
-    def histogram(self, words, mode=LM_PROMPTS_AND_DELAYED, duration=0, flags=0, out=None):
+    def histogram(self, words, mode=LM_PROMPTS_AND_DELAYED, duration=0, flags=0, out=None, offset=0):
         """One frame from host words -> (sino, delayed or None, stats dict);
-        `out` = (sino, delayed) uint16 host arrays to fill."""
+        `out` = (sino, delayed) uint16 host arrays to fill; `offset` = the
+        position of words[0] in the listmode file (packets count from its
+        start)."""
         w = _c(words, np.uint32)
         if out is None:
             sino = np.empty(self.sino_size, np.uint16)
@@ -605,9 +609,17 @@ class Listmode:
         else:
             sino, dly = out
         st = LmStats()
-        self._check(lib.hrrt_lm_histogram(self._h, _ptr(w), w.size, mode, duration, flags, _ptr(sino), _ptr(dly),
-                                          ctypes.byref(st)), "lm_histogram")
+        self._check(lib.hrrt_lm_histogram_at(self._h, _ptr(w), w.size, offset, mode, duration, flags, _ptr(sino),
+                                             _ptr(dly), ctypes.byref(st)), "lm_histogram")
         return sino, dly, st.as_dict()
+
+    def seek(self, words, target, offset=0, flags=0):
+        """goto_event: words consumed up to the time tag reaching `target` s
+        (the 0-ms tag for 0); raises HrrtError when the stream ends first."""
+        w = _c(words, np.uint32)
+        n = ctypes.c_longlong()
+        self._check(lib.hrrt_lm_seek(self._h, _ptr(w), w.size, offset, target, flags, ctypes.byref(n)), "lm_seek")
+        return n.value
 
     def head_curve(self):
         """The head curve of the last histogram call made with LM_HEAD_CURVE:

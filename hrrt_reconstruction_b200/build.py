@@ -16,6 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhrrt_gpu.so")
 CLI = os.path.join(HERE, "hrrt_osem3d_gpu")
+LMCLI = os.path.join(HERE, "lmhistogram_gpu")
 
 SOURCES = ["kernels.cu", "hrrt_gpu.cu", "batch.cu", "geometry.cpp", "listmode.cu", "lm_tables.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -71,20 +72,31 @@ def build_library(force=False, verbose=False):
     return LIB
 
 
-def build_cli(force=False):
-    src = os.path.join(CSRC, "cli", "hrrt_osem3d_gpu.cpp")
+def _build_tool(name, force):
+    src = os.path.join(CSRC, "cli", name + ".cpp")
+    exe = os.path.join(HERE, name)
     if not os.path.exists(src):
         return None
-    deps = [src, LIB]
-    if not force and _newer(CLI, deps):
-        return CLI
+    deps = [src, LIB, os.path.join(ROOT, "include", "hrrt_gpu.h")]
+    if not force and _newer(exe, deps):
+        return exe
     cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I" + os.path.join(ROOT, "include"), src,
-           "-o", CLI + ".tmp", "-L" + HERE, "-lhrrt_gpu", "-Wl,-rpath,$ORIGIN", "-lpthread"]
+           "-o", exe + ".tmp", "-L" + HERE, "-lhrrt_gpu", "-Wl,-rpath,$ORIGIN", "-lpthread"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("g++ failed:\n" + r.stdout + r.stderr)
-    os.replace(CLI + ".tmp", CLI)
-    return CLI
+    os.replace(exe + ".tmp", exe)
+    return exe
+
+
+def build_cli(force=False):
+    """The command lines: hrrt_osem3d_gpu (returned) and lmhistogram_gpu."""
+    _build_tool("lmhistogram_gpu", force)
+    return _build_tool("hrrt_osem3d_gpu", force)
+
+
+def build_lmhistogram(force=False):
+    return _build_tool("lmhistogram_gpu", force)
 
 
 def build_all(force=False, verbose=False):

@@ -1300,8 +1300,19 @@ long long hrrt_lm_table(int span, int maxrd, const char *name, void *out, size_t
 
 int hrrt_lm_histogram(hrrt_lm *h, const uint32_t *words, long long nwords, int mode, int duration, int flags,
                       uint16_t *sino, uint16_t *delayed, hrrt_lm_stats *out) {
+  return hrrt_lm_histogram_at(h, words, nwords, 0, mode, duration, flags, sino, delayed, out);
+}
+
+// Packets count from the file start: the staging buffer holds `phase`
+// filler words before the caller's words, each a word whose top bits (10)
+// make it out of sync whatever follows (EWTYPES, histogram_mp.cpp:1056-1062),
+// so the parse steps over them one by one and meets words[0] in sync, where
+// the reference's parse stands after the previous frame.  The filler shows
+// in no output but the resync count and the words used, which are corrected.
+int hrrt_lm_histogram_at(hrrt_lm *h, const uint32_t *words, long long nwords, long long file_offset, int mode,
+                         int duration, int flags, uint16_t *sino, uint16_t *delayed, hrrt_lm_stats *out) {
   if (!h) return HRRT_ERR_ARG;
-  if (nwords < 0 || (nwords > 0 && !words) || !sino || !out)
+  if (nwords < 0 || file_offset < 0 || (nwords > 0 && !words) || !sino || !out)
     return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_histogram: null buffer or negative length");
   if (mode == HRRT_LM_PROMPTS_AND_DELAYED && !delayed)
     return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_histogram: the delayed sinogram is required in this mode");
@@ -1315,22 +1326,26 @@ int hrrt_lm_histogram(hrrt_lm *h, const uint32_t *words, long long nwords, int m
       return lm_fail(h, HRRT_ERR_NOMEM, "hrrt_lm_histogram: sinograms");
     }
   }
-  if ((size_t)nwords > h->h_words_cap) {
+  const long long phase = file_offset % kPacketWords, staged = nwords + phase;
+  if ((size_t)staged > h->h_words_cap) {
     if (h->h_words_dev) cudaFree(h->h_words_dev);
     h->h_words_dev = nullptr;
     h->h_words_cap = 0;
-    e = cudaMalloc(&h->h_words_dev, sizeof(uint32_t) * std::max<long long>(nwords, 4));
+    e = cudaMalloc(&h->h_words_dev, sizeof(uint32_t) * std::max<long long>(staged, 4));
     if (e != cudaSuccess) return lm_fail(h, HRRT_ERR_NOMEM, "hrrt_lm_histogram: event staging");
-    h->h_words_cap = (size_t)nwords;
+    h->h_words_cap = (size_t)staged;
   }
   cudaStream_t st = h->stream;
   e = cudaMemsetAsync(h->h_sino_dev, 0, sizeof(uint16_t) * 2 * (size_t)S, st);
+  if (e == cudaSuccess && phase > 0) e = cudaMemsetAsync(h->h_words_dev, 0x80, sizeof(uint32_t) * phase, st);
   if (e == cudaSuccess && nwords > 0)
-    e = cudaMemcpyAsync(h->h_words_dev, words, sizeof(uint32_t) * nwords, cudaMemcpyHostToDevice, st);
+    e = cudaMemcpyAsync(h->h_words_dev + phase, words, sizeof(uint32_t) * nwords, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_histogram");
-  int rc = hrrt_lm_histogram_device(h, h->h_words_dev, nwords, mode, duration, flags, h->h_sino_dev,
+  int rc = hrrt_lm_histogram_device(h, h->h_words_dev, staged, mode, duration, flags, h->h_sino_dev,
                                     h->h_sino_dev + S, out, st);
   if (rc != HRRT_OK) return rc;
+  out->words_used -= phase;
+  out->resyncs -= phase;
   e = cudaMemcpyAsync(sino, h->h_sino_dev, sizeof(uint16_t) * S, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess && delayed && mode == HRRT_LM_PROMPTS_AND_DELAYED)
     e = cudaMemcpyAsync(delayed, h->h_sino_dev + S, sizeof(uint16_t) * S, cudaMemcpyDeviceToHost, st);
@@ -1377,6 +1392,45 @@ int hrrt_lm_smooth_randoms(hrrt_lm *h, const int32_t *coinc_hist, float scan_dur
   if (e == cudaSuccess) e = e2;
   if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_smooth_randoms");
   return HRRT_OK;
+}
+
+int hrrt_lm_seek(hrrt_lm *h, const uint32_t *words, long long nwords, long long file_offset, int target_s, int flags,
+                 long long *consumed) {
+  if (!h) return HRRT_ERR_ARG;
+  if (nwords < 0 || file_offset < 0 || (nwords > 0 && !words) || !consumed)
+    return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_seek: null buffer or negative length");
+  *consumed = 0;
+  if ((flags & HRRT_LM_TIME_FROM_COUNT) && target_s == 0) return HRRT_OK;
+  for (long long p0 = -(file_offset % kPacketWords); p0 < nwords; p0 += kPacketWords) {
+    const long long end = std::min(p0 + kPacketWords, nwords);
+    long long i = std::max(p0, 0LL);
+    while (i + 1 < end) {
+      const uint32_t ew1 = words[i], ew2 = words[i + 1];
+      const int t = (int)((kEwTypes >> (2 * (((ew1 >> 30) << 2) | (ew2 >> 30)))) & 3);
+      if (t == 3) {
+        i++;
+        continue;
+      }
+      i += 2;
+      if (t != 2) continue;
+      const uint32_t tag = (ew1 & 0xffff) | ((ew2 & 0xffff) << 16);
+      if ((tag & 0xE0000000u) != 0x80000000u) continue;
+      const long long ms = tag & 0x3fffffff;
+      if (ms == 0 && target_s == 0) {
+        h->current_time = 0;
+        *consumed = i;
+        return HRRT_OK;
+      }
+      if (h->current_time != ms / 1000) {
+        h->current_time = ms / 1000;
+        if (h->current_time == target_s) {
+          *consumed = i;
+          return HRRT_OK;
+        }
+      }
+    }
+  }
+  return lm_fail(h, HRRT_ERR_NOT_FOUND, "hrrt_lm_seek: the stream ends before the requested time");
 }
 
 long long hrrt_lm_convert_span9(const int16_t *span3, const int16_t *delayed, int16_t *span9, int maxrd) {

@@ -39,7 +39,8 @@ typedef enum {
   HRRT_ERR_CUDA = -2,     /* CUDA runtime error */
   HRRT_ERR_STATE = -3,    /* call made in the wrong order */
   HRRT_ERR_NOMEM = -4,    /* device allocation failed */
-  HRRT_ERR_DEVICE = -5    /* a device-side check reported an error */
+  HRRT_ERR_DEVICE = -5,   /* a device-side check reported an error */
+  HRRT_ERR_NOT_FOUND = -6 /* hrrt_lm_seek: the stream ends before the requested time */
 } hrrt_status;
 
 /* storage types of the sinogram-shaped inputs on the device (prompts are
@@ -399,6 +400,21 @@ int hrrt_lm_reset_clock(hrrt_lm *lm);
  * (from stats.words_used) for the next frame. */
 int hrrt_lm_histogram(hrrt_lm *lm, const uint32_t *words, long long nwords, int mode, int duration, int flags,
                       uint16_t *sino, uint16_t *delayed, hrrt_lm_stats *stats);
+/* hrrt_lm_histogram of words that sit `file_offset` words into the listmode
+ * file: the reader's packets of 1 Mi 64-bit events count from the file start
+ * (LM_Reader_mp.cpp:124), so the frames of one file, histogrammed call by
+ * call at their offsets, parse as one pass over the file does. */
+int hrrt_lm_histogram_at(hrrt_lm *lm, const uint32_t *words, long long nwords, long long file_offset, int mode,
+                         int duration, int flags, uint16_t *sino, uint16_t *delayed, hrrt_lm_stats *stats);
+/* goto_event (histogram_mp.cpp:384-425, 619-623): advance over the words
+ * (at `file_offset` in the file) to just past the time tag that reaches
+ * `target_s` seconds -- for 0, the tag that reads 0 ms, the coincidence
+ * processor's clock reset -- setting the handle's clock second on the way;
+ * nothing is histogrammed.  With HRRT_LM_TIME_FROM_COUNT a seek to 0 does
+ * nothing.  *consumed: the words advanced; HRRT_ERR_NOT_FOUND when the
+ * stream ends first. */
+int hrrt_lm_seek(hrrt_lm *lm, const uint32_t *words, long long nwords, long long file_offset, int target_s, int flags,
+                 long long *consumed);
 /* The same on device buffers (words 16-byte aligned, sinograms 4-byte
  * aligned), ADDING into sino / delayed, on `stream` (NULL: the library's). */
 int hrrt_lm_histogram_device(hrrt_lm *lm, const uint32_t *d_words, long long nwords, int mode, int duration,
@@ -408,7 +424,8 @@ int hrrt_lm_histogram_device(hrrt_lm *lm, const uint32_t *d_words, long long nwo
  * curve lines (copies min(n, capacity), returns n), and its block singles
  * (rates: [936] average of each block's samples over the frame, the
  * header's "block singles i"; the totals of the lines' prompts and randoms,
- * the header's total prompts / randoms, histogram_mp.cpp:181-190). */
+ * histogram_mp.cpp:181-190 -- the header's totals add the events after the
+ * last line, :1387-1388, which are the stats' prompts / delayed). */
 int hrrt_lm_head_curve(hrrt_lm *lm, hrrt_lm_second *out, int capacity);
 int hrrt_lm_block_singles(hrrt_lm *lm, int *rates, long long *total_prompts, long long *total_randoms);
 /* After a call with HRRT_LM_CRYSTAL_COUNTS: the frame's coincidence histogram

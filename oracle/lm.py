@@ -61,7 +61,11 @@ def lib():
         L.lm_rebin_event.argtypes = [vp, i, i, i, i, i, i, i]
         L.lm_histogram.argtypes = [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, vp, vp]
         f = ctypes.c_float
-        L.lm_histogram_hc.argtypes = [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, vp, vp, vp, i, vp, vp, vp]
+        L.lm_histogram_hc.argtypes = [vp, vp, ctypes.c_longlong, ctypes.c_longlong, i, i, i, vp, vp, vp, vp, vp, i,
+                                      vp, vp, vp]
+        L.lm_seek.argtypes = [vp, ctypes.c_longlong, ctypes.c_longlong, i, i, vp]
+        L.lm_histogram_at.argtypes = [vp, vp, ctypes.c_longlong, ctypes.c_longlong, i, i, i, vp, vp, vp, vp]
+        L.lm_seek.restype = ctypes.c_longlong
         L.lm_crystal_singles.argtypes = [vp, f, f, vp]
         L.lm_smooth_randoms.argtypes = [vp, vp, f, f, i, vp]
         L.lm_convert_span9.argtypes = [vp, i, i]
@@ -122,23 +126,26 @@ class LMOracle:
     def rebin_event(self, mp, al, ax, ay, bl, bx, by):
         return self.L.lm_rebin_event(self.t, mp, al, ax, ay, bl, bx, by)
 
-    def histogram(self, words, mode=PROMPTS_AND_DELAYED, duration=0, flags=0, sino=None, delayed=None):
-        """-> (sino, delayed, stats dict); adds into sino/delayed when given."""
+    def histogram(self, words, mode=PROMPTS_AND_DELAYED, duration=0, flags=0, sino=None, delayed=None, offset=0):
+        """-> (sino, delayed, stats dict); adds into sino/delayed when given;
+        `offset`: the position of words[0] in the file (packets count from
+        its start)."""
         w = np.ascontiguousarray(words, np.uint32)
         if sino is None:
             sino = np.zeros(self.sino_size, np.uint16)
         if delayed is None and mode == PROMPTS_AND_DELAYED:
             delayed = np.zeros(self.sino_size, np.uint16)
         st = Stats()
-        self.L.lm_histogram(self.t, _p(w), w.size, mode, duration, flags, ctypes.byref(self.clock), _p(sino),
-                            _p(delayed), ctypes.byref(st))
+        self.L.lm_histogram_at(self.t, _p(w), w.size, offset, mode, duration, flags, ctypes.byref(self.clock),
+                               _p(sino), _p(delayed), ctypes.byref(st))
         return sino, delayed, st.as_dict()
 
-    def histogram_hc(self, words, mode=PROMPTS_AND_DELAYED, duration=0, flags=0, max_lines=1 << 20):
+    def histogram_hc(self, words, mode=PROMPTS_AND_DELAYED, duration=0, flags=0, max_lines=1 << 20, offset=0):
         """histogram() that also returns the frame's head curve (int64 [n][4]:
         time ms, prompts, randoms, total singles), the blocks' average singles
         rates [936] and the totals of the lines' prompts and randoms; the
-        coincidence histogram is left in self.last_crystal_counts."""
+        coincidence histogram is left in self.last_crystal_counts.  `offset`:
+        the position of words[0] in the file (packets count from its start)."""
         w = np.ascontiguousarray(words, np.uint32)
         sino = np.zeros(self.sino_size, np.uint16)
         delayed = np.zeros(self.sino_size, np.uint16) if mode == PROMPTS_AND_DELAYED else None
@@ -147,10 +154,17 @@ class LMOracle:
         rates = np.zeros(936, np.int32)
         tot = np.zeros(2, np.int64)
         cc = np.zeros(2 * NCRYSTALS, np.uint32)
-        n = self.L.lm_histogram_hc(self.t, _p(w), w.size, mode, duration, flags, ctypes.byref(self.clock), _p(sino),
-                                   _p(delayed), ctypes.byref(st), _p(hc), max_lines, _p(rates), _p(tot), _p(cc))
+        n = self.L.lm_histogram_hc(self.t, _p(w), w.size, offset, mode, duration, flags, ctypes.byref(self.clock),
+                                   _p(sino), _p(delayed), ctypes.byref(st), _p(hc), max_lines, _p(rates), _p(tot),
+                                   _p(cc))
         self.last_crystal_counts = cc
         return sino, delayed, st.as_dict(), hc[:min(n, max_lines)].copy(), rates, (int(tot[0]), int(tot[1]))
+
+    def seek(self, words, target, offset=0, flags=0):
+        """goto_event: words consumed up to the time tag reaching `target` s
+        (the 0-ms tag for 0), -1 when the stream ends first."""
+        w = np.ascontiguousarray(words, np.uint32)
+        return self.L.lm_seek(_p(w), w.size, offset, target, flags, ctypes.byref(self.clock))
 
 
 NCRYSTALS = 2 * 104 * 8 * 72  # [layer][ring][head][x]

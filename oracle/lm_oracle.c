@@ -317,9 +317,9 @@ static void bump(uint16_t *h, long long a, int delta) { h[a] = (uint16_t)(h[a] +
  * their own first word: a word left over at a packet end is dropped
  * (`(src_pos + 1) < count`).  The reference's reader exits on a short last
  * packet; here the last packet is parsed like the others. */
-static int histogram_impl(const lm_tables *t, const uint32_t *w, long long n, int mode, int duration, int flags,
-                          lm_clock *clk, uint16_t *sino, uint16_t *delayed, lm_stats *st, hc_state *hc,
-                          uint32_t *ccounts) {
+static int histogram_impl(const lm_tables *t, const uint32_t *w, long long n, long long offset, int mode,
+                          int duration, int flags, lm_clock *clk, uint16_t *sino, uint16_t *delayed, lm_stats *st,
+                          hc_state *hc, uint32_t *ccounts) {
   memset(st, 0, sizeof(*st));
   const long long sino_size = lm_sino_size(t);
   const int ignore_border = flags & LM_IGNORE_BORDER_CRYSTAL;
@@ -329,9 +329,11 @@ static int histogram_impl(const lm_tables *t, const uint32_t *w, long long n, in
   long long frame_start = (clk->current_time >= 0) ? clk->current_time : -1;
   int terminated = 0;
   long long pos = 0;
-  for (long long p0 = 0; p0 < n && !terminated; p0 += PACKET_WORDS) {
+  /* packets are counted from the start of the file: words[0] sits at
+   * `offset` words into it */
+  for (long long p0 = -(offset % PACKET_WORDS); p0 < n && !terminated; p0 += PACKET_WORDS) {
     const long long count = (n - p0 < PACKET_WORDS) ? n - p0 : PACKET_WORDS;
-    long long sp = 0;
+    long long sp = p0 < 0 ? -p0 : 0;
     while (sp + 1 < count && !terminated) {
       const unsigned ew1 = w[p0 + sp], ew2 = w[p0 + sp + 1];
       const int type = EWTYPES[((ew2 & 0xc0000000u) >> 30) | ((ew1 & 0xc0000000u) >> 28)];
@@ -438,17 +440,22 @@ static int histogram_impl(const lm_tables *t, const uint32_t *w, long long n, in
 
 int lm_histogram(const lm_tables *t, const uint32_t *w, long long n, int mode, int duration, int flags, lm_clock *clk,
                  uint16_t *sino, uint16_t *delayed, lm_stats *st) {
-  return histogram_impl(t, w, n, mode, duration, flags, clk, sino, delayed, st, NULL, NULL);
+  return histogram_impl(t, w, n, 0, mode, duration, flags, clk, sino, delayed, st, NULL, NULL);
 }
 
-int lm_histogram_hc(const lm_tables *t, const uint32_t *w, long long n, int mode, int duration, int flags,
-                    lm_clock *clk, uint16_t *sino, uint16_t *delayed, lm_stats *st, lm_second *hc_out, int hc_cap,
-                    int *block_rates, long long *totals, uint32_t *ccounts) {
+int lm_histogram_at(const lm_tables *t, const uint32_t *w, long long n, long long offset, int mode, int duration,
+                    int flags, lm_clock *clk, uint16_t *sino, uint16_t *delayed, lm_stats *st) {
+  return histogram_impl(t, w, n, offset, mode, duration, flags, clk, sino, delayed, st, NULL, NULL);
+}
+
+int lm_histogram_hc(const lm_tables *t, const uint32_t *w, long long n, long long offset, int mode, int duration,
+                    int flags, lm_clock *clk, uint16_t *sino, uint16_t *delayed, lm_stats *st, lm_second *hc_out,
+                    int hc_cap, int *block_rates, long long *totals, uint32_t *ccounts) {
   hc_state *hc = (hc_state *)calloc(1, sizeof(hc_state));
   hc->out = hc_out;
   hc->cap = hc_cap;
   if (ccounts) memset(ccounts, 0, sizeof(uint32_t) * 2 * NXCRYS * NYCRYS * NHEADS * NDOIS);
-  const int r = histogram_impl(t, w, n, mode, duration, flags, clk, sino, delayed, st, hc, ccounts);
+  const int r = histogram_impl(t, w, n, offset, mode, duration, flags, clk, sino, delayed, st, hc, ccounts);
   for (int b = 0; b < NBLOCKS; b++) block_rates[b] = hc->nsamples[b] ? (int)(hc->total[b] / hc->nsamples[b]) : 0;
   totals[0] = hc->t_prompts;
   totals[1] = hc->t_randoms;
@@ -615,4 +622,39 @@ void lm_convert_span9(int16_t *sino, int maxrd, int nrings) {
       iseg9 += 2;
     }
   }
+}
+
+/* goto_event (histogram_mp.cpp:384-425, 619-623) over the l64 words: the
+ * parse of histogram_impl, every time tag setting the clock's second, up to
+ * and including the tag that reaches `target` s (for target 0: the tag that
+ * reads 0 ms).  Returns the words consumed, or -1 when the stream ends
+ * first.  Without time-tag processing a seek to 0 is a no-op. */
+long long lm_seek(const uint32_t *w, long long n, long long offset, int target, int flags, lm_clock *clk) {
+  if ((flags & LM_TIME_FROM_COUNT) && target == 0) return 0;
+  for (long long p0 = -(offset % PACKET_WORDS); p0 < n; p0 += PACKET_WORDS) {
+    const long long count = (n - p0 < PACKET_WORDS) ? n - p0 : PACKET_WORDS;
+    long long sp = p0 < 0 ? -p0 : 0;
+    while (sp + 1 < count) {
+      const unsigned ew1 = w[p0 + sp], ew2 = w[p0 + sp + 1];
+      const int type = EWTYPES[((ew2 & 0xc0000000u) >> 30) | ((ew1 & 0xc0000000u) >> 28)];
+      if (type == 3) {
+        sp++;
+        continue;
+      }
+      sp += 2;
+      if (type != 2) continue;
+      const unsigned tag = (ew1 & 0xffff) | ((ew2 & 0xffff) << 16);
+      if ((tag & 0xE0000000u) != 0x80000000u) continue;
+      const long long ms = tag & 0x3fffffff;
+      if (ms == 0 && target == 0) {
+        clk->current_time = 0;
+        return p0 + sp;
+      }
+      if (clk->current_time != ms / 1000) {
+        clk->current_time = ms / 1000;
+        if (clk->current_time == target) return p0 + sp;
+      }
+    }
+  }
+  return -1;
 }

@@ -80,19 +80,30 @@ void lm_clock_init(lm_clock *c);
  * bins that the call adds to.  duration <= 0: the whole stream. */
 int lm_histogram(const lm_tables *t, const uint32_t *words, long long nwords, int mode, int duration, int flags,
                  lm_clock *clock, uint16_t *sino, uint16_t *delayed, lm_stats *st);
+/* lm_histogram of words that sit `offset` words into the file: its packets
+ * of 2 Mi words count from the file start */
+int lm_histogram_at(const lm_tables *t, const uint32_t *words, long long nwords, long long offset, int mode,
+                    int duration, int flags, lm_clock *clock, uint16_t *sino, uint16_t *delayed, lm_stats *st);
 
 /* one head-curve line: time (ms), prompts and delayed since the previous
  * line, sum of the blocks' latest singles samples */
 typedef struct {
   long long time_ms, prompts, randoms, total_singles;
 } lm_second;
-/* lm_histogram that also writes the frame's head curve (returns the number of
- * lines, up to hc_cap stored), the blocks' average singles rates [936], the
+/* lm_histogram of words that sit `offset` words into the file (packets
+ * count from the file start) that also writes the frame's head curve
+ * (returns the number of lines, up to hc_cap stored), the blocks' average
+ * singles rates [936], the
  * totals of the lines' prompts and randoms [2] and, when ccounts is not
  * NULL, the coincidence histogram [2][119808] */
-int lm_histogram_hc(const lm_tables *t, const uint32_t *words, long long nwords, int mode, int duration, int flags,
-                    lm_clock *clock, uint16_t *sino, uint16_t *delayed, lm_stats *st, lm_second *hc_out, int hc_cap,
-                    int *block_rates, long long *totals, uint32_t *ccounts);
+int lm_histogram_hc(const lm_tables *t, const uint32_t *words, long long nwords, long long offset, int mode,
+                    int duration, int flags, lm_clock *clock, uint16_t *sino, uint16_t *delayed, lm_stats *st,
+                    lm_second *hc_out, int hc_cap, int *block_rates, long long *totals, uint32_t *ccounts);
+/* goto_event: the words consumed up to and including the time tag that
+ * reaches `target` s (the 0-ms tag for target 0), the clock's second set on
+ * the way; -1 when the stream ends first.  `offset`: position of words[0]
+ * in the file (packets of 2 Mi words count from the file start). */
+long long lm_seek(const uint32_t *words, long long nwords, long long offset, int target, int flags, lm_clock *clock);
 
 /* smoothed randoms (gen_delays): crystal singles from the 119808 delayed
  * crystal counts (returns the iterations), and the randoms sinogram from a

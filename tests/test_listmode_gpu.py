@@ -14,11 +14,11 @@ STAT_KEYS = ("words_used", "prompts", "delayed", "timetags", "tags", "invalid", 
              "resyncs", "frame_start", "duration", "terminated")
 
 
-def random_stream(seed, nevents, tag_every=1000, p_resync=1e-4, p_bad=0.01, p_delayed=0.1):
+def random_stream(seed, nevents, tag_every=1000, p_resync=1e-4, p_bad=0.01, p_delayed=0.1, ms0=5000):
     """Seeded l64 words: coincidences (10 % delayed) with random head pairs,
     crystals and DOI (mostly valid), a time tag every `tag_every` events
-    counting milliseconds from 5 s, block-singles tags, lone out-of-sync
-    words."""
+    counting milliseconds from `ms0` (5 s), block-singles tags, lone
+    out-of-sync words."""
     rng = np.random.default_rng(seed)
     mp = rng.integers(1, 21, nevents)
     ax, bx = rng.integers(0, 72, nevents), rng.integers(0, 72, nevents)
@@ -37,7 +37,7 @@ def random_stream(seed, nevents, tag_every=1000, p_resync=1e-4, p_bad=0.01, p_de
     ev = interleave(ew1, ew2).reshape(-1, 2)
     # insert tags and lone words
     chunks = []
-    ms = 5000
+    ms = ms0
     for i in range(0, nevents, tag_every):
         t1, t2 = tag_words(np.uint32(0x80000000 | ms))
         chunks.append(np.array([[t1, t2]], np.uint32).reshape(-1))
@@ -156,12 +156,12 @@ def test_device_entry_adds_into_buffers(pair):
     assert np.array_equal(got_d, (2 * do.astype(np.uint32)).astype(np.uint16))
 
 
-def singles_stream(seed, nevents, tag_every=700):
+def singles_stream(seed, nevents, tag_every=700, ms0=5000):
     """random_stream's events with block singles tags (random blocks and
     rates) after every time tag, and a clock that skips a millisecond now and
     then."""
     rng = np.random.default_rng(seed)
-    base = random_stream(seed, nevents, tag_every=tag_every, p_resync=0.0)
+    base = random_stream(seed, nevents, tag_every=tag_every, p_resync=0.0, ms0=ms0)
     out = []
     i = 0
     while i < base.size:
@@ -244,3 +244,39 @@ def test_trues_span9_device(pair):
     D.trues_span9_device(ds.data_ptr(), 0, out.data_ptr(), torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     assert np.array_equal(out.cpu().numpy(), lm.convert_span9(a))
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_frames_at_file_offsets(pair, path):
+    """hrrt_lm_histogram_at: 2-s frames of a stream with lone out-of-sync
+    words, each histogrammed at its file offset (packets counted from the
+    file start), equal the oracle's frame for frame; so does a seek
+    (goto_event) to 6 s followed by a frame."""
+    O, D = pair
+    w = random_stream(9, 1_100_000, tag_every=100, p_resync=2e-3)
+    O.reset_clock()
+    D.reset_clock()
+    pos, nframes = 0, 0
+    while pos < w.size:
+        so, do, sto = O.histogram(w[pos:], duration=2, offset=pos)
+        sd, dd, std = D.histogram(w[pos:], duration=2, flags=path, offset=pos)
+        assert np.array_equal(so, sd) and np.array_equal(do, dd), (nframes, pos)
+        for k in STAT_KEYS:
+            assert sto[k] == std[k], (nframes, k, sto[k], std[k])
+        pos += sto["words_used"]
+        nframes += 1
+        if not sto["terminated"]:
+            break
+    assert nframes > 3
+    O.reset_clock()
+    D.reset_clock()
+    n_o = O.seek(w, 6)
+    n_d = D.seek(w, 6)
+    assert n_o == n_d > 0
+    so, do, sto = O.histogram(w[n_o:], duration=1, offset=n_o)
+    sd, dd, std = D.histogram(w[n_d:], duration=1, flags=path, offset=n_d)
+    assert np.array_equal(so, sd) and np.array_equal(do, dd)
+    assert sto["frame_start"] == std["frame_start"] == 6
+    import hrrt_reconstruction_b200 as H
+    with pytest.raises(H.HrrtError):
+        D.seek(w, 10_000)

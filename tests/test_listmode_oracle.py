@@ -254,3 +254,54 @@ def test_library_convert_span9_matches_oracle():
     assert np.array_equal(H.convert_span9(a), lm.convert_span9(a))
     with pytest.raises(H.HrrtError):
         H.convert_span9(a, maxrd=66)
+
+
+def test_frames_at_file_offsets_sum_to_one_pass():
+    """Packets count from the file start (LM_Reader_mp.cpp:124): frames
+    histogrammed at their file offsets add up, bin for bin and count for
+    count, to one pass over the file -- with lone out-of-sync words that put
+    the stream at odd word positions across packet boundaries."""
+    from test_listmode_gpu import random_stream
+    O = LMOracle(9)
+    w = random_stream(9, 1_100_000, tag_every=100, p_resync=2e-3)
+    assert w.size > lm.PACKET_WORDS
+    O.reset_clock()
+    s1, d1, st1 = O.histogram(w)
+    O.reset_clock()
+    s = np.zeros_like(s1)
+    d = np.zeros_like(d1)
+    pos, frames = 0, []
+    while pos < w.size:
+        _, _, st = O.histogram(w[pos:], duration=2, sino=s, delayed=d, offset=pos)
+        frames.append(st)
+        pos += st["words_used"]
+        if not st["terminated"]:
+            break
+    assert len(frames) > 3
+    assert np.array_equal(s, s1) and np.array_equal(d, d1)
+    for k in ("prompts", "delayed", "resyncs", "invalid", "tags"):
+        assert sum(f[k] for f in frames) == st1[k], k
+
+
+def test_seek_known_answer(O3):
+    """goto_event: time tags at 5000, 5001, ... ms with 3 events between;
+    a seek to 7 s stops just past the 7000-ms tag and sets the clock's second;
+    a seek to 0 needs the 0-ms tag; without one the stream ends first."""
+    ev = interleave(*event_words(np.array([1, 1, 1]), np.array([3, 4, 5]), np.array([10, 10, 10]),
+                                 np.array([3, 4, 5]), np.array([10, 10, 10])))
+    parts = []
+    for ms in range(5000, 8000):
+        parts.append(interleave(*tag_words(np.uint32(0x80000000 | ms))))
+        parts.append(ev)
+    w = np.concatenate(parts).astype(np.uint32)
+    per = 2 + ev.size
+    O3.reset_clock()
+    n = O3.seek(w, 7)
+    assert n == (7000 - 5000) * per + 2
+    assert O3.clock.current_time == 7
+    O3.reset_clock()
+    assert O3.seek(w, 0) == -1
+    w0 = np.concatenate([ev, interleave(*tag_words(np.uint32(0x80000000))), ev]).astype(np.uint32)
+    O3.reset_clock()
+    assert O3.seek(w0, 0) == ev.size + 2 and O3.clock.current_time == 0
+    assert O3.seek(w0, 0, flags=lm.TIME_FROM_COUNT) == 0
