@@ -123,6 +123,8 @@ def _load():
         "hrrt_reset_kernel_stats": (i, [vp]),
         "hrrt_set_psf": (i, [vp, i, f, f, f]),
         "hrrt_psf_convolve": (i, [vp, vp, vp]),
+        "hrrt_set_map": (i, [vp, i, f, i]),
+        "hrrt_map_prior": (i, [vp, vp, vp]),
         "hrrt_psf_kernel": (ctypes.c_longlong, [f, f, f, f, vp, i]),
         "hrrt_set_tuning": (i, [vp, ctypes.POINTER(Tuning)]),
         "hrrt_get_tuning": (i, [vp, ctypes.POINTER(Tuning)]),
@@ -393,6 +395,20 @@ class Context:
         assert img.shape == self.image_shape
         out = np.empty(self.image_shape, np.float32)
         self._check(lib.hrrt_psf_convolve(self._h, _ptr(img), _ptr(out)), "psf")
+        return out
+
+    def set_map(self, technique=1, beta=0.0, first_subset=5):
+        """-b technique,beta of je_hrrt_osem3d: MAP (technique 1, Green's
+        one-step-late prior) from subset `first_subset` after the image was
+        set; technique 0 or beta 0 turns it off."""
+        self._check(lib.hrrt_set_map(self._h, technique, beta, first_subset), "set_map")
+
+    def map_prior(self, image_xyz):
+        """calculate_DPF_image (technique 1) of an [x][y][zp] image (set_map first)."""
+        img = _c(image_xyz, np.float32)
+        assert img.shape == self.image_shape
+        out = np.empty(self.image_shape, np.float32)
+        self._check(lib.hrrt_map_prior(self._h, _ptr(img), _ptr(out)), "map_prior")
         return out
 
     def set_tuning(self, fp_planes=0, fp_producer_warps=0, bp_planes=0, bp_threads=0):

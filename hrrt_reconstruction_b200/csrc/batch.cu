@@ -294,6 +294,7 @@ int hrrt_batch_create(hrrt_ctx *ctx, int nframes, int storage, const float *norm
   if (storage < HRRT_STORE_F32 || storage > HRRT_STORE_F16) return fail(ctx, HRRT_ERR_ARG, "unknown storage");
   if (ctx->batch) return fail(ctx, HRRT_ERR_STATE, "batch: the context already serves a batch");
   if (ctx->psf_on) return fail(ctx, HRRT_ERR_STATE, "batch: PSF modelling runs one frame at a time");
+  if (ctx->map_on) return fail(ctx, HRRT_ERR_STATE, "batch: MAP runs one frame at a time");
   if (int rc = ensure_input_buffers(ctx, storage)) return rc;
   const Geometry &g = ctx->geo;
   auto *b = new hrrt_batch();

@@ -7,12 +7,13 @@
 // projection of the final image as a flat float sinogram.
 //
 // Supported: -p -d -n -a -s -o -O -i -h -I -S -W 3 -m -f -k -e -u -Q -F -T -N
-// -D -L -v -X 256 -M 999 -g -B, -z 1, -Z 1.  The attenuation may be the
-// span-9 file of a span-3 reconstruction (Atten3D_Span9, :1762-1796), the
-// scatter a 2D segment with span-9 scale factors, the randoms a coincidence
-// histogram (.ch).  Options for paths outside OP-OSEM (-t trues, -P/-R
-// pre-corrected / 4-byte scans, -A MAP, -U mu-map, -C compression, -w) are
-// refused with a message.
+// -D -L -v -X 256 -M 999 -g -B, -z 1, -Z 1, and je_hrrt_osem3d's -b 1,beta
+// (MAP, hrrt_osem3d.cpp:3360-3369).  The attenuation may be the span-9 file
+// of a span-3 reconstruction (Atten3D_Span9, :1762-1796), the scatter a 2D
+// segment with span-9 scale factors, the randoms a coincidence histogram
+// (.ch).  Options for paths outside OP-OSEM (-t trues, -P/-R pre-corrected /
+// 4-byte scans, -A MAP-EM gradient variant, -U mu-map, -C compression, -w)
+// are refused with a message.
 #include <cerrno>
 #include <chrono>
 #include <cmath>
@@ -33,6 +34,8 @@ struct Options {
   int iterations = 1, subsets = 16, weighting = 2, span = 9, maxdel = 67, npskip = 0, verbose = 0, device = 0;
   bool psf = false;
   float psf_fwhm1 = 0.f, psf_fwhm2 = 0.f, psf_ratio = 0.f;
+  int map_technique = 0;
+  float map_beta = 0.f;
   int in_flip = 0, out_flip = 0, trim = 0;
   float rel_fov = 0.95f, image_max = 1.e4f, eps1 = 5.e-2f, eps2 = 1.e-2f, eps3 = 1.e-10f;
   int z_min = 6, z_max = 200;
@@ -59,7 +62,8 @@ void usage() {
                "      (3D, or the unscaled 2D segment followed by 2209 span-9 plane scale factors)\n"
                "  -o  output image (flat float [z][y][x] + .hdr), -O also after each iteration\n"
                "  -h  output the forward projection of the final image (flat float scan)\n"
-               "  -B  fwhm1,fwhm2,ratio: PSF resolution modelling (0,0,0: the HRRT defaults)\n");
+               "  -B  fwhm1,fwhm2,ratio: PSF resolution modelling (0,0,0: the HRRT defaults)\n"
+               "  -b  technique,beta: MAP with the one-step-late prior of je_hrrt_osem3d (technique 1)\n");
 }
 
 bool parse(int argc, char **argv, Options &o) {
@@ -126,7 +130,14 @@ bool parse(int argc, char **argv, Options &o) {
         if (std::sscanf(val(), "%f,%f,%f", &o.psf_fwhm1, &o.psf_fwhm2, &o.psf_ratio) != 3) die("error decoding -B");
         o.psf = true;
         break;
-      case 'A': die("-A (MAP) is not supported");
+      case 'A': die("-A (the MAP-EM gradient variant) is not supported; -b 1,beta gives je_hrrt_osem3d's MAP");
+      case 'b':
+        // -b technique,beta (je_hrrt_osem3d/hrrt_osem3d.cpp:3360-3369)
+        if (std::sscanf(val(), "%d,%f", &o.map_technique, &o.map_beta) != 2) die("error decoding -b");
+        if (o.map_technique == 0) o.map_beta = 0.f;
+        if (o.map_beta == 0.f) o.map_technique = 0;
+        if (o.map_technique != 0 && o.map_technique != 1) die("-b: MAP technique 1 only");
+        break;
       case 'U': die("-U (mu-map reconstruction) is not supported");
       case 'C': die("-C (sinogram compression) is not supported");
       case 'w': die("-w is not supported");
@@ -415,6 +426,10 @@ int main(int argc, char **argv) {
     die("%s", hrrt_last_error(ctx));
   if (o.psf && hrrt_set_psf(ctx, 1, o.psf_fwhm1, o.psf_fwhm2, o.psf_ratio) != HRRT_OK)
     die("%s", hrrt_last_error(ctx));
+  // MAP from the sixth subset of the first iteration on (i_min_MAP,
+  // je_hrrt_osem3d/hrrt_osem3d.cpp:4332-4341)
+  if (o.map_technique && hrrt_set_map(ctx, o.map_technique, o.map_beta, 5) != HRRT_OK)
+    die("MAP: %s", hrrt_last_error(ctx));
   if (hrrt_sensitivity(ctx) != HRRT_OK) die("%s", hrrt_last_error(ctx));
   const size_t vox = (size_t)info.nx * info.ny * info.nz;
   std::vector<float> img(vox);

@@ -83,6 +83,14 @@ struct hrrt_ctx {
   int psf_h = 0;
   float *d_psf_fx = nullptr, *d_psf_fy = nullptr, *d_psf_normz = nullptr;
   float *d_image_psf = nullptr, *d_corr = nullptr, *d_psf_tmp = nullptr;
+  // MAP technique 1 (je_hrrt_osem3d -b 1,beta): the prior replaces the update
+  // from subset map_first on (counted from the last image initialisation)
+  bool map_on = false;
+  float map_beta = 0.f;
+  int map_first = 5;
+  long long subsets_done = 0;
+  float *d_dpf = nullptr;
+  unsigned int *d_mapmax = nullptr;
 
   bool prof = false;
   std::vector<KernelTimer> pending;

@@ -213,6 +213,53 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
   const QuadWork *fw = ctx->d_work + ctx->fp_off[s], *bw = ctx->d_work + ctx->bp_off[s];
   const int *pv = ctx->d_pair_views + (size_t)s * ctx->npairs;
   float *nf = ctx->d_nfinv + (size_t)s * ctx->vol;
+  const bool single = b.fr.n == 1 && !b.fr.map;
+  const bool map = single && ctx->map_on && ctx->subsets_done >= ctx->map_first;
+  if (single) ctx->subsets_done++;
+  if (map) {
+    // je_hrrt_osem3d's subset with MAP (hrrt_osem3d.cpp:4439-4463): the
+    // correction image (blurred with -B), the prior of the image before the
+    // update, then pt_cal_updateimage_mapem
+    const float *proj = b.image;
+    if (ctx->psf_on) {
+      if (int rc = run_psf(ctx, b.image, ctx->d_image_psf)) return rc;
+      proj = ctx->d_image_psf;
+    }
+    {
+      Launch L(ctx, "fp_kernel");
+      CK(launch_fp(g, proj, fw, ctx->fp_cnt[s], 1, b.prompts, b.add, ctx->storage, b.ratio, ctx->quad_pair,
+                   ctx->tune, b.fr, ctx->stream),
+         "fp_kernel");
+    }
+    if (adj) {
+      CK(launch_adj(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, b.fr, ctx->stream),
+         "adj_kernel");
+      CK(cudaMemsetAsync(ctx->d_corr, 0, sizeof(float) * ctx->vol, ctx->stream), "map");
+      CK(launch_adj_rotate(g, pv, ctx->npairs, b.bc, b.br, ctx->vol, nullptr, nullptr, ctx->d_corr, 2, b.fr,
+                           ctx->stream),
+         "adj_rotate_kernel");
+    } else {
+      {
+        Launch L(ctx, "bp_kernel");
+        CK(launch_bp(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, ctx->tune, b.fr,
+                     ctx->stream),
+           "bp_kernel");
+      }
+      Launch L(ctx, "rotback_kernel");
+      CK(launch_rotback(g, pv, ctx->npairs, b.bc, b.br, ctx->vol, nullptr, nullptr, ctx->d_corr, 3, b.fr,
+                        ctx->stream),
+         "rotback_kernel");
+    }
+    if (ctx->psf_on)
+      if (int rc = run_psf(ctx, ctx->d_corr, ctx->d_corr)) return rc;
+    {
+      Launch L(ctx, "map_dpf_kernel");
+      CK(launch_map_prior(ctx->dg, b.image, ctx->d_mapmax, ctx->d_dpf, ctx->stream), "map prior");
+    }
+    Launch L(ctx, "apply_corr_kernel");
+    CK(launch_apply_corr(ctx->dg, ctx->d_corr, b.image, nf, 2, ctx->stream, ctx->d_dpf, ctx->map_beta), "map update");
+    return HRRT_OK;
+  }
   if (ctx->psf_on) {
     // -B (drv:4172, :4201-4202, :4229): project the blurred image, blur the
     // correction image, then update
@@ -780,6 +827,7 @@ int hrrt_init_image(hrrt_ctx *ctx, const float *image_zyx) {
   }
   CK(cudaStreamSynchronize(ctx->stream), "init_image");
   ctx->have_image = true;
+  ctx->subsets_done = 0;
   return HRRT_OK;
 }
 
@@ -1001,6 +1049,7 @@ int hrrt_set_image_xyz(hrrt_ctx *ctx, const float *image_xyz) {
   CK(cudaMemcpyAsync(ctx->d_image, image_xyz, ctx->vol * 4, cudaMemcpyHostToDevice, ctx->stream), "set_image");
   CK(cudaStreamSynchronize(ctx->stream), "set_image");
   ctx->have_image = true;
+  ctx->subsets_done = 0;
   return HRRT_OK;
 }
 
@@ -1181,6 +1230,53 @@ int hrrt_psf_convolve(hrrt_ctx *ctx, const float *image_xyz, float *out_xyz) {
   if (int rc = run_psf(ctx, ctx->d_tmp_img, ctx->d_corr)) return rc;
   CK(cudaMemcpyAsync(out_xyz, ctx->d_corr, sizeof(float) * ctx->vol, cudaMemcpyDeviceToHost, ctx->stream), "psf");
   CK(cudaStreamSynchronize(ctx->stream), "psf");
+  return HRRT_OK;
+}
+
+int hrrt_set_map(hrrt_ctx *ctx, int technique, float beta, int first_subset) {
+  if (!ctx) return HRRT_ERR_ARG;
+  // -b technique,beta (hrrt_osem3d.cpp:3360-3369): either 0 turns MAP off
+  if (technique == 0 || beta == 0.f) {
+    ctx->map_on = false;
+    return HRRT_OK;
+  }
+  if (technique != 1)
+    return fail(ctx, HRRT_ERR_ARG,
+                "MAP: technique 1 only (technique 2 needs an MR image, and its voxel loop in dpfcalc.c:245 "
+                "tests the wrong counter)");
+  if (first_subset < 0) return fail(ctx, HRRT_ERR_ARG, "MAP: first subset must be >= 0");
+  if (ctx->batch) return fail(ctx, HRRT_ERR_STATE, "MAP: not available while the context serves a batch");
+  cudaError_t e = cudaSuccess;
+  if (!ctx->d_corr) ctx->d_corr = dalloc<float>(ctx, ctx->vol, &e);
+  if (!ctx->d_dpf) {
+    ctx->d_dpf = dalloc<float>(ctx, ctx->vol, &e);
+    // the prior is written on FOV columns only; the rest stays 0
+    if (ctx->d_dpf) CK(cudaMemsetAsync(ctx->d_dpf, 0, sizeof(float) * ctx->vol, ctx->stream), "map");
+  }
+  if (!ctx->d_mapmax) ctx->d_mapmax = dalloc<unsigned int>(ctx, 1, &e);
+  if (!ctx->d_corr || !ctx->d_dpf || !ctx->d_mapmax) return fail(ctx, HRRT_ERR_NOMEM, "MAP buffers");
+  CK(cudaStreamSynchronize(ctx->stream), "map");
+  ctx->map_on = true;
+  ctx->map_beta = beta;
+  ctx->map_first = first_subset;
+  return HRRT_OK;
+}
+
+int hrrt_map_prior(hrrt_ctx *ctx, const float *image_xyz, float *prior_xyz) {
+  if (!ctx || !image_xyz || !prior_xyz) return HRRT_ERR_ARG;
+  if (!ctx->map_on) return fail(ctx, HRRT_ERR_STATE, "hrrt_set_map must come first");
+  cudaError_t e = cudaSuccess;
+  if (!ctx->d_tmp_img) ctx->d_tmp_img = dalloc<float>(ctx, ctx->vol, &e);
+  if (!ctx->d_tmp_img) return fail(ctx, HRRT_ERR_NOMEM, "scratch");
+  CK(cudaMemcpyAsync(ctx->d_tmp_img, image_xyz, sizeof(float) * ctx->vol, cudaMemcpyHostToDevice, ctx->stream),
+     "map prior");
+  {
+    Launch L(ctx, "map_dpf_kernel");
+    CK(launch_map_prior(ctx->dg, ctx->d_tmp_img, ctx->d_mapmax, ctx->d_dpf, ctx->stream), "map prior");
+  }
+  CK(cudaMemcpyAsync(prior_xyz, ctx->d_dpf, sizeof(float) * ctx->vol, cudaMemcpyDeviceToHost, ctx->stream),
+     "map prior");
+  CK(cudaStreamSynchronize(ctx->stream), "map prior");
   return HRRT_OK;
 }
 

@@ -1572,10 +1572,15 @@ __global__ void psf_yz_kernel(DevGeom g, const float *__restrict__ in, float *__
 
 // The consumers of the correction image once it is a separate volume (the
 // PSF path): MODE 0 the OSEM update, MODE 1 the inverse sensitivity; the
-// arithmetic of rotback_kernel's modes 0 and 1.
+// arithmetic of rotback_kernel's modes 0 and 1.  MODE 2: the MAP update of
+// pt_cal_updateimage_mapem (je_hrrt_osem3d/hrrt_osem3d.cpp:2031-2073),
+// image = min(image_max, image * min(100, max(0.1, corr / (beta * dpf + 1 / nf_inv))))
+// with SSE's min/max rule; the reference's _mm_rcp_ps approximation of
+// 1 / nf_inv (relative error up to 1.5 * 2^-12) is the exact reciprocal here.
 template <int MODE>
 __global__ void __launch_bounds__(256) apply_corr_kernel(DevGeom g, const float *__restrict__ corr,
-                                                         float *__restrict__ image, float *__restrict__ nf_inv) {
+                                                         float *__restrict__ image, float *__restrict__ nf_inv,
+                                                         const float *__restrict__ dpf, float beta) {
   const int nq = g.zp / 4;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int col = (int)(t / nq), q = (int)(t - (long long)col * nq);
@@ -1593,6 +1598,23 @@ __global__ void __launch_bounds__(256) apply_corr_kernel(DevGeom g, const float 
       const float lo = (0.01f > a[l]) ? 0.01f : a[l];
       const float cl = (100.0f < lo) ? 100.0f : lo;
       const float u = b[l] * (cl * n[l]);
+      b[l] = (g.image_max < u) ? g.image_max : u;
+    }
+    im[o] = make_float4(b[0], b[1], b[2], b[3]);
+  } else if (MODE == 2) {
+    float4 *im = reinterpret_cast<float4 *>(image);
+    const float4 nf = reinterpret_cast<const float4 *>(nf_inv)[o];
+    const float4 dp = reinterpret_cast<const float4 *>(dpf)[o];
+    float4 iv = im[o];
+    float a[4] = {acc.x, acc.y, acc.z, acc.w}, b[4] = {iv.x, iv.y, iv.z, iv.w}, n[4] = {nf.x, nf.y, nf.z, nf.w},
+          d[4] = {dp.x, dp.y, dp.z, dp.w};
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      const float den = __fadd_rn(__fmul_rn(beta, d[l]), __frcp_rn(n[l]));
+      const float q = __fdiv_rn(a[l], den);
+      const float lo = (0.1f > q) ? 0.1f : q;
+      const float cl = (100.0f < lo) ? 100.0f : lo;
+      const float u = __fmul_rn(b[l], cl);
       b[l] = (g.image_max < u) ? g.image_max : u;
     }
     im[o] = make_float4(b[0], b[1], b[2], b[3]);
@@ -1615,14 +1637,97 @@ cudaError_t launch_psf(const DevGeom &g, const float *in, float *tmp, float *out
   return cudaGetLastError();
 }
 
+// ============================================================================
+// MAP, technique 1 of je_hrrt_osem3d (-b 1,beta): Green's one-step-late
+// prior.  calculate_DPF_image (je_hrrt_osem3d/dpfcalc.c:23-31, :66-85,
+// :266-300) and the update pt_cal_updateimage_mapem (hrrt_osem3d.cpp:
+// 2031-2073).
+//   map_max_kernel : the image maximum over the FOV columns and planes
+//                    [0, nz), never below 0 (the float's bits, an unsigned
+//                    maximum, order like the values for non-negative floats);
+//   map_dpf_kernel : one thread per FOV voxel: delta = (1.2 max) / 20 and,
+//                    for 1 <= x < nx-1 and 1 <= z < nz-1, the 6 face and
+//                    (times sqrt(0.5)) 12 edge terms tanh((c - n) / delta) =
+//                    (e - 1) / (e + 1), e = exp(2 (c - n) / delta), summed in
+//                    the source's order in float, combined in double; 0
+//                    elsewhere.  e is exp() in double rounded to float, the
+//                    correctly rounded value.
+//   MAP update     : apply_corr_kernel<2>.
+// ============================================================================
+__global__ void __launch_bounds__(256) map_max_kernel(DevGeom g, const float *__restrict__ img,
+                                                      unsigned int *__restrict__ mx) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned int v = 0;
+  if (t < (long long)g.fov_columns * g.nz) {
+    const int col = (int)(t / g.nz), z = (int)(t - (long long)col * g.nz);
+    const short2 xy = g.fov_xy[col];
+    const float f = img[((size_t)xy.x * g.nx + xy.y) * g.zp + z];
+    if (f > 0.f) v = __float_as_uint(f);
+  }
+  v = __reduce_max_sync(0xffffffffu, v);
+  if ((threadIdx.x & 31) == 0 && v) atomicMax(mx, v);
+}
+
+__device__ __forceinline__ float map_tanh(float r, float delta) {
+  const float e = __double2float_rn(exp((double)__fdiv_rn(__fmul_rn(2.0f, r), delta)));
+  return __fdiv_rn(__fsub_rn(e, 1.0f), __fadd_rn(e, 1.0f));
+}
+
+__global__ void __launch_bounds__(256) map_dpf_kernel(DevGeom g, const float *__restrict__ img,
+                                                      const unsigned int *__restrict__ mx, float *__restrict__ dpf) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)g.fov_columns * g.zp) return;
+  const int col = (int)(t / g.zp), z = (int)(t - (long long)col * g.zp);
+  const short2 xy = g.fov_xy[col];
+  const int x = xy.x, y = xy.y, N = g.nx, zp = g.zp;
+  float out = 0.f;
+  if (x >= 1 && x < N - 1 && z >= 1 && z < g.nz - 1) {
+    const float maxpet = __double2float_rn(1.2 * (double)__uint_as_float(*mx));
+    const float delta = __double2float_rn((double)maxpet / 20.0);
+    auto I = [&](int a, int b, int c) { return __ldg(img + ((size_t)a * N + b) * zp + c); };
+    const float c = I(x, y, z);
+    float a = map_tanh(__fsub_rn(c, I(x, y, z - 1)), delta);
+    a = __fadd_rn(a, map_tanh(__fsub_rn(c, I(x, y, z + 1)), delta));
+    a = __fadd_rn(a, map_tanh(__fsub_rn(c, I(x - 1, y, z)), delta));
+    a = __fadd_rn(a, map_tanh(__fsub_rn(c, I(x + 1, y, z)), delta));
+    a = __fadd_rn(a, map_tanh(__fsub_rn(c, I(x, y - 1, z)), delta));
+    a = __fadd_rn(a, map_tanh(__fsub_rn(c, I(x, y + 1, z)), delta));
+    float b = map_tanh(__fsub_rn(c, I(x - 1, y, z - 1)), delta);
+    b = __fadd_rn(b, map_tanh(__fsub_rn(c, I(x, y - 1, z - 1)), delta));
+    b = __fadd_rn(b, map_tanh(__fsub_rn(c, I(x + 1, y, z - 1)), delta));
+    b = __fadd_rn(b, map_tanh(__fsub_rn(c, I(x, y + 1, z - 1)), delta));
+    b = __fadd_rn(b, map_tanh(__fsub_rn(c, I(x - 1, y - 1, z)), delta));
+    b = __fadd_rn(b, map_tanh(__fsub_rn(c, I(x - 1, y + 1, z)), delta));
+    b = __fadd_rn(b, map_tanh(__fsub_rn(c, I(x + 1, y - 1, z)), delta));
+    b = __fadd_rn(b, map_tanh(__fsub_rn(c, I(x + 1, y + 1, z)), delta));
+    b = __fadd_rn(b, map_tanh(__fsub_rn(c, I(x - 1, y, z + 1)), delta));
+    b = __fadd_rn(b, map_tanh(__fsub_rn(c, I(x, y - 1, z + 1)), delta));
+    b = __fadd_rn(b, map_tanh(__fsub_rn(c, I(x + 1, y, z + 1)), delta));
+    b = __fadd_rn(b, map_tanh(__fsub_rn(c, I(x, y + 1, z + 1)), delta));
+    out = __double2float_rn(__dadd_rn((double)a, __dmul_rn(0.70710678118654752440, (double)b)));
+  }
+  dpf[((size_t)x * N + y) * zp + z] = out;
+}
+
+cudaError_t launch_map_prior(const DevGeom &g, const float *image, unsigned int *mx, float *dpf, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(mx, 0, sizeof(unsigned int), st);
+  if (e != cudaSuccess) return e;
+  const long long n1 = (long long)g.fov_columns * g.nz, n2 = (long long)g.fov_columns * g.zp;
+  map_max_kernel<<<(unsigned)((n1 + 255) / 256), 256, 0, st>>>(g, image, mx);
+  map_dpf_kernel<<<(unsigned)((n2 + 255) / 256), 256, 0, st>>>(g, image, mx, dpf);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_apply_corr(const DevGeom &g, const float *corr, float *image, float *nf_inv, int mode,
-                              cudaStream_t st) {
+                              cudaStream_t st, const float *dpf, float beta) {
   const long long n = (long long)g.fov_columns * (g.zp / 4);
   const unsigned blocks = (unsigned)((n + 255) / 256);
   if (mode == 0)
-    apply_corr_kernel<0><<<blocks, 256, 0, st>>>(g, corr, image, nf_inv);
+    apply_corr_kernel<0><<<blocks, 256, 0, st>>>(g, corr, image, nf_inv, nullptr, 0.f);
+  else if (mode == 1)
+    apply_corr_kernel<1><<<blocks, 256, 0, st>>>(g, corr, image, nf_inv, nullptr, 0.f);
   else
-    apply_corr_kernel<1><<<blocks, 256, 0, st>>>(g, corr, image, nf_inv);
+    apply_corr_kernel<2><<<blocks, 256, 0, st>>>(g, corr, image, nf_inv, dpf, beta);
   return cudaGetLastError();
 }
 

@@ -158,9 +158,13 @@ cudaError_t launch_rotpos(const DevGeom &g, float2 *rotpos, const int *row_start
 // inverted z tap sums
 cudaError_t launch_psf(const DevGeom &g, const float *in, float *tmp, float *out, const float *filt_x, int hx,
                        const float *filt_y, int hy, const float *normz, cudaStream_t st);
-// mode 0: OSEM update of image from the correction volume; 1: inverse sensitivity into nf_inv
+// mode 0: OSEM update of image from the correction volume; 1: inverse
+// sensitivity into nf_inv; 2: the MAP update with the prior volume dpf
 cudaError_t launch_apply_corr(const DevGeom &g, const float *corr, float *image, float *nf_inv, int mode,
-                              cudaStream_t st);
+                              cudaStream_t st, const float *dpf = nullptr, float beta = 0.f);
+// MAP technique 1 prior (calculate_DPF_image, je_hrrt_osem3d/dpfcalc.c) of
+// image into dpf on the FOV columns; mx: one device word of scratch
+cudaError_t launch_map_prior(const DevGeom &g, const float *image, unsigned int *mx, float *dpf, cudaStream_t st);
 cudaError_t launch_prep(const DevGeom &g, int nbins, const int16_t *prompts, const float *randoms, const float *norm,
                         const float *atten, const float *scatter, int npskip, float eps2, int storage, void *q_prompts,
                         void *q_add, void *q_mult, int *quad_mask_accum, int plane0, int nplanes,

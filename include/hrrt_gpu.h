@@ -217,6 +217,23 @@ int hrrt_set_psf(hrrt_ctx *ctx, int enable, float fwhm1, float fwhm2, float rati
 /* convolve3d (psf.cpp:463-540) of image_xyz on FOV columns into out_xyz
  * (other columns zero) with the kernels hrrt_set_psf built. */
 int hrrt_psf_convolve(hrrt_ctx *ctx, const float *image_xyz, float *out_xyz);
+/* MAP reconstruction, technique 1 of je_hrrt_osem3d's -b technique,beta
+ * (je_hrrt_osem3d/hrrt_osem3d.cpp:3360-3369, :4330-4463): Green's
+ * one-step-late prior.  From subset `first_subset` on (counted from the last
+ * hrrt_init_image / hrrt_set_image_xyz; the reference's i_min_MAP is 5) each
+ * OSEM subset replaces the update with pt_cal_updateimage_mapem (:2031-2073),
+ * image = min(image_max, image * min(100, max(0.1, corr / (beta * prior + 1 / nf_inv)))),
+ * the prior being calculate_DPF_image (dpfcalc.c) of the image before the
+ * update.  The reference forms 1 / nf_inv with _mm_rcp_ps (relative error up
+ * to 1.5 * 2^-12); here it is exact.  technique 0 or beta 0 turns MAP off;
+ * technique 2 (the MR joint-entropy prior) is refused.  Not available
+ * together with a batch.  The je_hrrt_osem3d defaults eps1 = eps2 = 1e-4 and
+ * image_max = 1e10 go in the hrrt_geom given to hrrt_ctx_create. */
+int hrrt_set_map(hrrt_ctx *ctx, int technique, float beta, int first_subset);
+/* calculate_DPF_image (technique 1) of image_xyz into prior_xyz on the
+ * device, after hrrt_set_map. */
+int hrrt_map_prior(hrrt_ctx *ctx, const float *image_xyz, float *prior_xyz);
+
 /* Host-only (no GPU needed): make1d_psf_filter's taps for one pixel size into
  * `taps` (capacity); returns the tap count or a negative status. */
 long long hrrt_psf_kernel(float fwhm1, float fwhm2, float ratio, float pixel_size, float *taps, int capacity);

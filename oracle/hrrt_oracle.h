@@ -89,6 +89,12 @@ void orc_osem_subset(const orc_geom *g, orc_real *image, const orc_real *nf_inv_
                      const float *add, int isubset, int nthreads);
 /* post-iteration threshold (< 1e-16 -> 0) and sum over FOV x [z_min, z_max) */
 double orc_post_iteration(const orc_geom *g, orc_real *image, int z_min, int z_max);
+/* MAP technique 1 (je_hrrt_osem3d): the prior image calculate_DPF_image
+ * makes from `image` ([x][y][zp]), and one OP-OSEM subset with the MAP update
+ * (exact reciprocal of nf_inv where the reference uses _mm_rcp_ps) */
+void orc_map_dpf(const orc_geom *g, const orc_real *image, orc_real *dpf);
+void orc_osem_subset_map(const orc_geom *g, orc_real *image, const orc_real *nf_inv_subset, const int16_t *prompts,
+                         const float *add, int isubset, int nthreads, float beta);
 
 /* PSF resolution modelling (psf.cpp): the 1D kernel of make1d_psf_filter
  * (returns its size or -1), and convolve3d on FOV columns once orc_set_psf

@@ -56,6 +56,7 @@ def lib(precision="f64"):
                 "orc_rotate_add": [vp, vp, i, vp], "orc_prep": [vp, vp, vp, vp, vp, vp, vp, vp, vp],
                 "orc_sensitivity": [vp, vp, vp, i], "orc_init_image": [vp, vp, i, i],
                 "orc_osem_subset": [vp, vp, vp, vp, vp, i, i],
+                "orc_map_dpf": [vp, vp, vp], "orc_osem_subset_map": [vp, vp, vp, vp, vp, i, i, f],
             }
             for n, a in sigs.items():
                 getattr(L, n).argtypes = a
@@ -197,6 +198,23 @@ class Oracle:
         p = np.ascontiguousarray(prompts, np.int16)
         a = np.ascontiguousarray(add, np.float32)
         self.L.orc_osem_subset(self.g, _p(image), _p(nf), _p(p), _p(a), isubset, nthreads or self.nthreads)
+        return image
+
+    def map_dpf(self, image):
+        """calculate_DPF_image technique 1 (dpfcalc.c) of an [x][y][zp] image."""
+        im = self._r(image)
+        out = np.zeros_like(im)
+        self.L.orc_map_dpf(self.g, _p(im), _p(out))
+        return out
+
+    def osem_subset_map(self, image, nf_inv_subset, prompts, add, isubset, beta, nthreads=None):
+        """One OP-OSEM subset with the MAP (technique 1) update, in place."""
+        assert image.dtype == self.dtype and image.flags.c_contiguous
+        nf = self._r(nf_inv_subset)
+        p = np.ascontiguousarray(prompts, np.int16)
+        a = np.ascontiguousarray(add, np.float32)
+        self.L.orc_osem_subset_map(self.g, _p(image), _p(nf), _p(p), _p(a), isubset, nthreads or self.nthreads,
+                                   beta)
         return image
 
     def psf_kernel(self, fwhm1=0.0, fwhm2=0.0, ratio=0.0, pixel_size=1.21875):

@@ -197,3 +197,47 @@ class RefProjector:
         m = np.zeros((self.views // 2, self.nx // 2 + 1), np.int16)
         self.L.ref_get_norm_zero_mask(_p(m))
         return m
+
+
+# ---- the MAP prior of je_hrrt_osem3d (oracle/_ref/libmap_ref.so) ----
+MAP_LIB = os.path.join(HERE, "_ref", "libmap_ref.so")
+_M = None
+
+
+def map_lib():
+    global _M
+    if _M is None:
+        if not os.path.exists(MAP_LIB):
+            raise FileNotFoundError(MAP_LIB)
+        M = ctypes.CDLL(MAP_LIB)
+        vp, i, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+        M.ref_map_dpf.argtypes = [vp, i, i, i, vp, vp]
+        M.ref_map_dpf.restype = i
+        M.ref_map_update.argtypes = [vp, vp, vp, vp, i, i, vp, f, f]
+        M.ref_map_update.restype = None
+        _M = M
+    return _M
+
+
+def map_dpf(image, nz, cylwiny):
+    """calculate_DPF_image(image, NULL, dpf, 1) of the reference (dpfcalc.c)
+    on a float32 [nx][nx][zp] image with nz planes."""
+    im = np.ascontiguousarray(image, np.float32)
+    nx, _, zp = im.shape
+    cyl = np.ascontiguousarray(cylwiny, np.int32).reshape(-1)
+    out = np.zeros_like(im)
+    assert map_lib().ref_map_dpf(_p(im), nx, nz, zp, _p(cyl), _p(out)) == 1
+    return out
+
+
+def map_update(image, corr, nf_inv, dpf, cylwiny, beta, image_max):
+    """pt_cal_updateimage_mapem's SSE update (with _mm_rcp_ps of nf_inv) on
+    float32 [nx][nx][zp] arrays; returns the new image."""
+    im = np.array(image, np.float32, order="C")
+    c = np.array(corr, np.float32, order="C")
+    nf = np.ascontiguousarray(nf_inv, np.float32)
+    d = np.ascontiguousarray(dpf, np.float32)
+    nx, _, zp = im.shape
+    cyl = np.ascontiguousarray(cylwiny, np.int32).reshape(-1)
+    map_lib().ref_map_update(_p(im), _p(c), _p(nf), _p(d), nx, zp, _p(cyl), beta, image_max)
+    return im
