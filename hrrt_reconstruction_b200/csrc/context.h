@@ -63,6 +63,8 @@ struct hrrt_ctx {
   // pipelined reconstruction: the view pairs of one subset staged pair-major
   char *pstage[2] = {nullptr, nullptr};
   size_t pstage_bytes = 0;
+  int16_t *pflat = nullptr;  // hrrt_reconstruct: the whole prompt sinogram
+  size_t pflat_elems = 0;
 
   // back projector of the OSEM loop, and the device geometry it runs with
   // (for the adjoint: segment weights of 1, the forward projector's scaling)

@@ -915,6 +915,21 @@ int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms
     }
     ctx->pstage_bytes = need;
   }
+  // The prompts go up whole, in one contiguous copy at the full link rate,
+  // and the prep reads each subset's rows from there: a view's row of int16
+  // prompts is only 512 bytes, short enough to slow a strided host copy.
+  const size_t pelems = P * V * N;
+  if (ctx->pflat_elems < pelems) {
+    if (ctx->pflat) {
+      cudaFree(ctx->pflat);
+      ctx->allocs.erase(std::find(ctx->allocs.begin(), ctx->allocs.end(), (void *)ctx->pflat));
+      ctx->pflat = nullptr;
+    }
+    ctx->pflat_elems = 0;
+    ctx->pflat = dalloc<int16_t>(ctx, pelems, &e);
+    if (!ctx->pflat) return fail(ctx, HRRT_ERR_NOMEM, "reconstruct prompts");
+    ctx->pflat_elems = pelems;
+  }
   if (!ctx->copy_stream) {
     CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking), "copy stream");
     for (int b = 0; b < 2; b++) {
@@ -942,18 +957,19 @@ int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms
   };
   cudaEventRecord(ta, ctx->stream);
   for (int b = 0; b < 2; b++) CK(cudaEventRecord(ctx->ev_free[b], ctx->stream), "reconstruct");
+  // ahead of every subset's copies on the copy stream, so each subset's
+  // ev_copied also covers it
+  CK(cudaMemcpyAsync(ctx->pflat, prompts, sizeof(int16_t) * pelems, cudaMemcpyHostToDevice, ctx->copy_stream),
+     "reconstruct prompts");
   const int S = g.sp.subsets;
   for (int k = 0; k < S; k++) {
     const int s = g.order[k], b = k & 1;
-    int16_t *sp = reinterpret_cast<int16_t *>(ctx->pstage[b]);
     float *stg[4] = {nullptr, nullptr, nullptr, nullptr};
     e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_free[b], 0);
     for (int j = 0; j < ctx->npairs && e == cudaSuccess; j++) {
       const int v = g.vieworder[(size_t)s * g.sviews + j];
       for (int h = 0; h < 2 && e == cudaSuccess; h++) {
         const size_t view = v + h * (V / 2), doff = j * pair_elems + h * P * N;
-        e = cudaMemcpy2DAsync(sp + doff, N * sizeof(int16_t), prompts + view * N, V * N * sizeof(int16_t),
-                              N * sizeof(int16_t), P, cudaMemcpyHostToDevice, ctx->copy_stream);
         for (int i = 0; i < 4 && e == cudaSuccess; i++) {
           if (!srcs[i]) continue;
           stg[i] = reinterpret_cast<float *>(ctx->pstage[b] + set_elems * sizeof(int16_t) +
@@ -967,9 +983,9 @@ int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms
     if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_copied[b], 0);
     if (e == cudaSuccess) {
       Launch L(ctx, "prep_kernel");
-      e = launch_prep_pairs(ctx->dg, g.nbins, sp, stg[0], stg[1], stg[2], stg[3], g.sp.npskip, g.sp.epsilon2,
-                            storage, ctx->q_prompts, ctx->q_add, ctx->q_mult, ctx->d_mask_accum,
-                            ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->stream);
+      e = launch_prep_pairs(ctx->dg, g.nbins, ctx->pflat, stg[0], stg[1], stg[2], stg[3], g.sp.npskip,
+                            g.sp.epsilon2, storage, ctx->q_prompts, ctx->q_add, ctx->q_mult, ctx->d_mask_accum,
+                            ctx->d_pair_views + (size_t)s * ctx->npairs, ctx->npairs, ctx->stream, true);
     }
     if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_free[b], ctx->stream);
     if (e == cudaSuccess) e = launch_finish_mask(ctx->dg, ctx->d_mask_accum, ctx->d_nzmask, ctx->stream);

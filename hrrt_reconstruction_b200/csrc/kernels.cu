@@ -1007,11 +1007,13 @@ __global__ void prep_kernel(DevGeom g, int nbins, const int16_t *__restrict__ pr
                             float eps2, PT *__restrict__ qp, AT *__restrict__ qadd, AT *__restrict__ qmult,
                             int *__restrict__ mask_accum, int planes_per_thread, int plane0, int nplanes,
                             const int *__restrict__ pair_views, long long s_plane, long long s_half,
-                            long long s_slot) {
+                            long long s_slot, long long pf_plane, long long pf_half) {
   // Input element of plane gp, lane l: base + (gp - plane0)*s_plane + h*s_half
   // + bin.  Flat-file chunk (pair_views null): pair = blockIdx.z, base =
   // pair*nbins, planes [plane0, plane0 + nplanes).  Pair-major staging: pair =
-  // pair_views[blockIdx.z], base = blockIdx.z*s_slot, all planes.
+  // pair_views[blockIdx.z], base = blockIdx.z*s_slot, all planes.  With
+  // pf_plane > 0 the prompts are the whole sinogram instead: element
+  // gp*pf_plane + pair*nbins + h*pf_half + bin.
   const int x = blockIdx.x * blockDim.x + threadIdx.x;  // quad
   const int vi = pair_views ? pair_views[blockIdx.z] : (int)blockIdx.z;
   const long long base = pair_views ? (long long)blockIdx.z * s_slot : (long long)vi * nbins;
@@ -1046,7 +1048,10 @@ __global__ void prep_kernel(DevGeom g, int nbins, const int16_t *__restrict__ pr
       float a = __ldg(randoms + i) * nz;
       if (scatter) a = a + __ldg(scatter + i);
       a = a * araw;
-      const float p = (nz == 0.0f) ? 0.f : (float)__ldg(prompts + i);
+      const size_t pi = pf_plane > 0 ? (size_t)((long long)gp * pf_plane + (long long)vi * nbins +
+                                                hl[l] * pf_half + bins[l])
+                                     : i;
+      const float p = (nz == 0.0f) ? 0.f : (float)__ldg(prompts + pi);
       if (nz != 0.0f) any = 1;
       pv[l] = p;
       av[l] = a;
@@ -1382,15 +1387,15 @@ cudaError_t launch_prep(const DevGeom &g, int nbins, const int16_t *prompts, con
   if (storage == 0)
     prep_kernel<int16_t, float><<<grid, 128, 0, st>>>(g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2,
                                                       (int16_t *)q_prompts, (float *)q_add, (float *)q_mult,
-                                                      quad_mask_accum, ppt, plane0, nplanes, nullptr, sp, sh, 0);
+                                                      quad_mask_accum, ppt, plane0, nplanes, nullptr, sp, sh, 0, 0, 0);
   else if (storage == 1)
     prep_kernel<int16_t, __nv_bfloat16><<<grid, 128, 0, st>>>(
         g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (int16_t *)q_prompts, (__nv_bfloat16 *)q_add,
-        (__nv_bfloat16 *)q_mult, quad_mask_accum, ppt, plane0, nplanes, nullptr, sp, sh, 0);
+        (__nv_bfloat16 *)q_mult, quad_mask_accum, ppt, plane0, nplanes, nullptr, sp, sh, 0, 0, 0);
   else
     prep_kernel<int16_t, __half><<<grid, 128, 0, st>>>(
         g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (int16_t *)q_prompts, (__half *)q_add,
-        (__half *)q_mult, quad_mask_accum, ppt, plane0, nplanes, nullptr, sp, sh, 0);
+        (__half *)q_mult, quad_mask_accum, ppt, plane0, nplanes, nullptr, sp, sh, 0, 0, 0);
   return cudaGetLastError();
 }
 
@@ -1414,22 +1419,23 @@ cudaError_t launch_image_zyx(const DevGeom &g, const float *image, float *out, c
 cudaError_t launch_prep_pairs(const DevGeom &g, int nbins, const int16_t *prompts, const float *randoms,
                               const float *norm, const float *atten, const float *scatter, int npskip, float eps2,
                               int storage, void *q_prompts, void *q_add, void *q_mult, int *quad_mask_accum,
-                              const int *pair_views, int npairs, cudaStream_t st) {
+                              const int *pair_views, int npairs, cudaStream_t st, bool flat_prompts) {
   const int ppt = 16;
   dim3 grid((g.nquads + 127) / 128, (g.segmentsize + ppt - 1) / ppt, npairs);
   const long long P = g.segmentsize, sp = nbins, sh = P * nbins, ss = 2 * P * nbins;
+  const long long fp = flat_prompts ? (long long)g.nviews * nbins : 0, fh = (long long)(g.nviews / 2) * nbins;
   if (storage == 0)
     prep_kernel<int16_t, float><<<grid, 128, 0, st>>>(g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2,
                                                       (int16_t *)q_prompts, (float *)q_add, (float *)q_mult,
-                                                      quad_mask_accum, ppt, 0, g.segmentsize, pair_views, sp, sh, ss);
+                                                      quad_mask_accum, ppt, 0, g.segmentsize, pair_views, sp, sh, ss, fp, fh);
   else if (storage == 1)
     prep_kernel<int16_t, __nv_bfloat16><<<grid, 128, 0, st>>>(
         g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (int16_t *)q_prompts, (__nv_bfloat16 *)q_add,
-        (__nv_bfloat16 *)q_mult, quad_mask_accum, ppt, 0, g.segmentsize, pair_views, sp, sh, ss);
+        (__nv_bfloat16 *)q_mult, quad_mask_accum, ppt, 0, g.segmentsize, pair_views, sp, sh, ss, fp, fh);
   else
     prep_kernel<int16_t, __half><<<grid, 128, 0, st>>>(
         g, nbins, prompts, randoms, norm, atten, scatter, npskip, eps2, (int16_t *)q_prompts, (__half *)q_add,
-        (__half *)q_mult, quad_mask_accum, ppt, 0, g.segmentsize, pair_views, sp, sh, ss);
+        (__half *)q_mult, quad_mask_accum, ppt, 0, g.segmentsize, pair_views, sp, sh, ss, fp, fh);
   return cudaGetLastError();
 }
 

@@ -171,10 +171,13 @@ cudaError_t launch_prep(const DevGeom &g, int nbins, const int16_t *prompts, con
                         cudaStream_t st);
 // the same from pair-major staging: for each of `npairs` slots, the rows of
 // view pair_views[slot] and its partner, [2 views][segmentsize][nbins]
+// (flat_prompts: the prompts are instead the whole [plane][view][bin]
+// sinogram on the device)
 cudaError_t launch_prep_pairs(const DevGeom &g, int nbins, const int16_t *prompts, const float *randoms,
                               const float *norm, const float *atten, const float *scatter, int npskip, float eps2,
                               int storage, void *q_prompts, void *q_add, void *q_mult, int *quad_mask_accum,
-                              const int *pair_views, int npairs, cudaStream_t st);
+                              const int *pair_views, int npairs, cudaStream_t st,
+                              bool flat_prompts = false);
 cudaError_t launch_finish_mask(const DevGeom &g, const int *accum, int16_t *nzmask, cudaStream_t st);
 // [z][y][x] image of SaveImage (FOV columns, planes < nz) from [x][y][zp]
 cudaError_t launch_image_zyx(const DevGeom &g, const float *image, float *out, cudaStream_t st);
