@@ -67,7 +67,8 @@ class LmStats(ctypes.Structure):
 class Tuning(ctypes.Structure):
     """hrrt_tuning: launch shape of the projectors (results do not depend on it)."""
     _fields_ = [("fp_planes", ctypes.c_int), ("fp_producer_warps", ctypes.c_int), ("bp_planes", ctypes.c_int),
-                ("bp_threads", ctypes.c_int), ("fp_ms", ctypes.c_double), ("bp_ms", ctypes.c_double)]
+                ("bp_threads", ctypes.c_int), ("bp_tile", ctypes.c_int), ("fp_ms", ctypes.c_double),
+                ("bp_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -411,8 +412,8 @@ class Context:
         self._check(lib.hrrt_map_prior(self._h, _ptr(img), _ptr(out)), "map_prior")
         return out
 
-    def set_tuning(self, fp_planes=0, fp_producer_warps=0, bp_planes=0, bp_threads=0):
-        t = Tuning(fp_planes, fp_producer_warps, bp_planes, bp_threads, 0.0, 0.0)
+    def set_tuning(self, fp_planes=0, fp_producer_warps=0, bp_planes=0, bp_threads=0, bp_tile=0):
+        t = Tuning(fp_planes, fp_producer_warps, bp_planes, bp_threads, bp_tile, 0.0, 0.0)
         self._check(lib.hrrt_set_tuning(self._h, ctypes.byref(t)), "set_tuning")
 
     def get_tuning(self):

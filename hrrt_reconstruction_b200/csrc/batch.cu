@@ -142,10 +142,11 @@ int autotune(hrrt_ctx *ctx, const SubsetBufs &bb, int repeats, hrrt_tuning *chos
   }
   if (int rc = apply_tune(ctx, best)) return rc;
   if (!adj) {
-    for (int i = 0; i < 4; i++) {
+    for (int i = 0; i < 12; i++) {
       ProjTune t = best;
       t.bp_planes = (i & 1) ? 4 : 8;
       t.bp_threads = (i & 2) ? 384 : 256;
+      t.bp_tile = (i < 4) ? 2 : (i < 8) ? 4 : 8;
       double ms = 0;
       int rc = time_launch(ctx, repeats, [&] {
         return launch_bp(ctx->dg, bb.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], bb.bc, bb.br, ctx->vol, t, bb.fr,
@@ -156,6 +157,7 @@ int autotune(hrrt_ctx *ctx, const SubsetBufs &bb, int repeats, hrrt_tuning *chos
         best_bp = ms;
         best.bp_planes = t.bp_planes;
         best.bp_threads = t.bp_threads;
+        best.bp_tile = t.bp_tile;
       }
     }
   } else {
@@ -167,6 +169,7 @@ int autotune(hrrt_ctx *ctx, const SubsetBufs &bb, int repeats, hrrt_tuning *chos
     chosen->fp_producer_warps = best.fp_pwarps;
     chosen->bp_planes = best.bp_planes;
     chosen->bp_threads = best.bp_threads;
+    chosen->bp_tile = best.bp_tile;
     chosen->fp_ms = best_fp;
     chosen->bp_ms = best_bp;
   }
@@ -265,7 +268,7 @@ extern "C" {
 
 int hrrt_set_tuning(hrrt_ctx *ctx, const hrrt_tuning *t) {
   if (!ctx || !t) return HRRT_ERR_ARG;
-  return apply_tune(ctx, ProjTune{t->fp_planes, t->fp_producer_warps, t->bp_planes, t->bp_threads});
+  return apply_tune(ctx, ProjTune{t->fp_planes, t->fp_producer_warps, t->bp_planes, t->bp_threads, t->bp_tile});
 }
 
 int hrrt_get_tuning(hrrt_ctx *ctx, hrrt_tuning *t) {
@@ -275,6 +278,7 @@ int hrrt_get_tuning(hrrt_ctx *ctx, hrrt_tuning *t) {
   t->fp_producer_warps = ctx->tune.fp_pwarps;
   t->bp_planes = ctx->tune.bp_planes > 0 ? ctx->tune.bp_planes : kBpZ;
   t->bp_threads = ctx->tune.bp_threads;
+  t->bp_tile = ctx->tune.bp_tile;
   return HRRT_OK;
 }
 

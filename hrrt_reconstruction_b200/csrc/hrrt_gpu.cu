@@ -503,6 +503,8 @@ int apply_tune(hrrt_ctx *ctx, const ProjTune &t) {
     return fail(ctx, HRRT_ERR_ARG, "tuning: back-projection planes must be 4 or 8");
   if (t.bp_threads != 0 && t.bp_threads != 256 && t.bp_threads != 384)
     return fail(ctx, HRRT_ERR_ARG, "tuning: back-projection threads must be 256 or 384");
+  if (t.bp_tile < 0 || t.bp_tile > 32 || (t.bp_tile & (t.bp_tile - 1)) != 0)
+    return fail(ctx, HRRT_ERR_ARG, "tuning: back-projection tile must be a power of 2 up to 32");
   ctx->tune = t;
   ctx->config_epoch++;
   ctx->dg.fptasks = ctx->dg_adj.fptasks = ctx->d_fptasks[vi];
@@ -632,6 +634,8 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
     for (int r = 0; r < ns; r++) bp_src.push_back(g.padded_offset(s) + r);
     for (int k = 0; k < kBpPad; k++) bp_src.push_back(-1);
   }
+  // whole groups of 8 planes: the back projector swizzles within them
+  while (bp_src.size() % 8) bp_src.push_back(-1);
   // no back-projection window may run past its segment's zero planes
   for (int y = 1; y < g.ny; y++)
     for (int gg = 0; gg < g.groupmax; gg++) {

@@ -527,17 +527,26 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
 // p+nviews/2 (its row quad); they go to Bc and Br and are added in the
 // rotate-back, which is the reference's assign-then-accumulate order.
 // ============================================================================
+// The shared planes are stored swizzled: plane i at bsw(i), its position
+// within its aligned group of 8 XORed with the group's index.  Threads of a
+// warp take consecutive 8-plane runs of one row, so their loads of the same
+// window offset are 8 planes (128 bytes) apart; the swizzle puts them in
+// different 16-byte bank groups without the shared memory a padding would
+// cost.
+__device__ __forceinline__ int bsw(int i) { return i ^ ((i >> 3) & 7); }
+
 template <int KB>
-__device__ __forceinline__ void bp_lerp(Q2 (&s)[KB], const float4 *__restrict__ p, const BpLut &bl, int z0) {
+__device__ __forceinline__ void bp_lerp(Q2 (&s)[KB], const float4 *__restrict__ P, int pbase, const BpLut &bl,
+                                        int z0) {
   // windows wholly outside [zs, ze] contribute nothing; a window that
   // straddles an end reads the segment's zero planes for its outside planes
   if (z0 + KB - 1 < bl.zs || z0 > bl.ze) return;
-  const float4 *pw = p + z0 + bl.d;
+  const int i0 = pbase + z0 + bl.d;
   const uint64_t f = pk(bl.f, bl.f);
-  Q2 a = ldq(pw);
+  Q2 a = ldq(P + bsw(i0));
 #pragma unroll
   for (int j = 0; j < KB; j++) {
-    const Q2 b = ldq(pw + j + 1);
+    const Q2 b = ldq(P + bsw(i0 + j + 1));
     // the reference's p[yr] + f*(p[yr+1]-p[yr]) (sbrt:4312-4315)
     s[j] = qadd(s[j], qaddp(a, qmul(qsub(b, a), f)));
     a = b;
@@ -566,7 +575,7 @@ template <int KB, bool ACC = false, bool MULTI = false, int NT = 256>
 __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(DevGeom g, const float4 *__restrict__ in, long long in_pair_stride,
                                                  const QuadWork *__restrict__ work, float *__restrict__ bc,
                                                  float *__restrict__ br, long long vol, FrameStrides fr,
-                                                 int view0 = 0, int x0 = 0) {
+                                                 int view0, int x0, int rlog) {
   extern __shared__ float4 P[];  // [bp_splanes]: segments with kBpPad zero planes each side
   // ACC: one view pair, quads x0 + blockIdx.x, both partial sums added into bc
   // (each voxel receives exactly two terms, so the atomic adds onto a zeroed
@@ -588,7 +597,7 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(De
   if (!masked)
     for (int i = threadIdx.x; i < g.bp_splanes; i += blockDim.x) {
       const int q = __ldg(g.bp_src + i);
-      P[i] = (q >= 0) ? src[q] : f4(0.f);
+      P[bsw(i)] = (q >= 0) ? src[q] : f4(0.f);
     }
   __syncthreads();
 
@@ -596,17 +605,24 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(De
   float *brp = br + (size_t)w.slot * vol;
   const int ystart = g.cyl0[x];
   const int nyq = c - ystart + 1, nzc = zp / KB;
-  const float4 *P0 = P + g.bp_soff[0];
-  // task = (half, plane run, row); half 0 builds sumt1 (voxels (x,y),(N-x,y),
+  const int o0 = g.bp_soff[0];
+  // task = (half, row, plane run); half 0 builds sumt1 (voxels (x,y),(N-x,y),
   // (N-y,x),(N-y,N-x)), half 1 sumt2 (voxels (x,N-y),(N-x,N-y),(y,x),(y,N-x)).
-  // Consecutive threads take consecutive rows at the same planes: their window
-  // starts z0 + d(y) differ by the slowly varying d(y), so the 16-byte shared
-  // loads of a warp fall in distinct banks or broadcast.
-  const int per_half = nyq * nzc;
+  // A warp's 32 tasks are a tile of R = 2^rlog consecutive plane runs of
+  // 32/R consecutive rows.  Along the runs a warp's stores of a voxel column
+  // are contiguous, and the swizzle spreads its shared loads over the banks;
+  // along the rows the row entries differ, but windows at the same planes
+  // and a slowly varying offset d(y) often coincide (broadcast).  Many
+  // segment groups favour few runs, few groups (store-heavy) many.
+  const int R = 1 << rlog, RW = 32 >> rlog;
+  const int CT = (nzc + R - 1) >> rlog, RT = (nyq + RW - 1) / RW;
+  const int per_half = RT * CT * 32;
   for (int task = threadIdx.x; task < 2 * per_half; task += blockDim.x) {
     const int half = task >= per_half;
     const int t2 = task - half * per_half;
-    const int zc = t2 / nyq, yi = t2 - zc * nyq, z0 = zc * KB;
+    const int tile = t2 >> 5, l = t2 & 31, ty = tile / CT, tc = tile - ty * CT;
+    const int yi = ty * RW + (l >> rlog), zc = (tc << rlog) + (l & (R - 1)), z0 = zc * KB;
+    if (yi >= nyq || zc >= nzc) continue;
     const int y = ystart + yi;
     if (half && y == c) continue;  // the centre row has a single voxel set
     Q2 s[KB];
@@ -617,32 +633,32 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(De
     } else if (y == c) {
       // centre row (sbrt:4260-4284): rays pass plane yr = z exactly
 #pragma unroll
-      for (int j = 0; j < KB; j++) s[j] = ldq(P0 + z0 + j);
+      for (int j = 0; j < KB; j++) s[j] = ldq(P + bsw(o0 + z0 + j));
       for (int gg = 0; gg < G; gg++) {
         const int se = 2 * gg + 2, so = 2 * gg + 1;
         const int yb = g.ybot[se], yt = g.ytop[se];
-        const float4 *pe = P + g.bp_soff[se] - yb, *po = P + g.bp_soff[so] - yb;
+        const int pe = g.bp_soff[se] - yb, po = g.bp_soff[so] - yb;
 #pragma unroll
         for (int j = 0; j < KB; j++) {
           const int z = z0 + j;
-          if (z >= yb && z <= yt) s[j] = qadd(s[j], qadd(ldq(pe + z), ldq(po + z)));
+          if (z >= yb && z <= yt) s[j] = qadd(s[j], qadd(ldq(P + bsw(pe + z)), ldq(P + bsw(po + z))));
         }
       }
     } else {
 #pragma unroll
-      for (int j = 0; j < KB; j++) s[j] = ldq(P0 + z0 + j);
-      // bplut is [group][row]: the rows of a warp read consecutive entries
+      for (int j = 0; j < KB; j++) s[j] = ldq(P + bsw(o0 + z0 + j));
+      // bplut is [group][row]: the threads of a row read the same entries
       const BpLut *l1 = g.bplut + y, *l2 = g.bplut + (N - y);
       BpLut b1 = l1[0], b2 = l2[0];
       for (int gg = 0; gg < G; gg++) {
         const int se = 2 * gg + 2, so = 2 * gg + 1;
         const int yb = g.ybot[se];
-        const float4 *pe = P + g.bp_soff[se] - yb, *po = P + g.bp_soff[so] - yb;
+        const int pe = g.bp_soff[se] - yb, po = g.bp_soff[so] - yb;
         const int gn = (gg + 1 < G) ? gg + 1 : gg;
         const BpLut n1 = l1[(size_t)gn * N], n2 = l2[(size_t)gn * N];  // next group, in flight
         // sumt1: segment 2k at +u and 2k-1 at -u; sumt2: the converse
-        bp_lerp<KB>(s, half ? po : pe, b1, z0);
-        bp_lerp<KB>(s, half ? pe : po, b2, z0);
+        bp_lerp<KB>(s, P, half ? po : pe, b1, z0);
+        bp_lerp<KB>(s, P, half ? pe : po, b2, z0);
         b1 = n1;
         b2 = n2;
       }
@@ -1276,9 +1292,20 @@ cudaError_t launch_fp(const DevGeom &g, const float *image, const QuadWork *work
   }
 }
 
+// log2 of the back projector's tile width (bp_kernel): the tuned one, else
+// 2 runs where there are many segment groups and 4 where there are few
+// (measured on B200 over 1..32: span 3 1.56 ms at 2, span 9 0.57 ms at 4);
+// -1 if invalid
+int bp_tile_log2(const DevGeom &g, const ProjTune &t) {
+  const int r = t.bp_tile > 0 ? t.bp_tile : (g.groupmax > 12 ? 2 : 4);
+  for (int l = 0; l <= 5; l++)
+    if (r == 1 << l) return l;
+  return -1;
+}
+
 template <int KB, int NT>
 cudaError_t launch_bp_t(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
-                        float *bc, float *br, long long vol, const FrameStrides &fr, cudaStream_t st) {
+                        float *bc, float *br, long long vol, const FrameStrides &fr, int rlog, cudaStream_t st) {
   static_assert(kBpPad >= KB, "a straddling window must stay inside the zero planes");
   const size_t smem = (size_t)g.bp_splanes * sizeof(float4);
   auto k = fr.n > 1 ? bp_kernel<KB, false, true, NT> : bp_kernel<KB, false, false, NT>;
@@ -1287,7 +1314,7 @@ cudaError_t launch_bp_t(const DevGeom &g, const float *in, long long in_pair_str
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   k<<<(unsigned)nwork * fr.n, NT, smem, st>>>(g, reinterpret_cast<const float4 *>(in), in_pair_stride / 4, work, bc,
-                                              br, vol, fr, 0, 0);
+                                              br, vol, fr, 0, 0, rlog);
   return cudaGetLastError();
 }
 
@@ -1299,10 +1326,12 @@ cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_strid
   // 384 threads (two CTAs of 80 registers per SM) measured faster than 256
   // (three CTAs) at span 3 and 9 on B200: 1.58 vs 1.74 ms and 0.71 vs 0.74 ms
   const int nt = tune.bp_threads > 0 ? tune.bp_threads : 384;
-  if (kb == 8 && nt == 256) return launch_bp_t<8, 256>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, st);
-  if (kb == 8 && nt == 384) return launch_bp_t<8, 384>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, st);
-  if (kb == 4 && nt == 256) return launch_bp_t<4, 256>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, st);
-  if (kb == 4 && nt == 384) return launch_bp_t<4, 384>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, st);
+  const int rl = bp_tile_log2(g, tune);
+  if (rl < 0) return cudaErrorInvalidValue;
+  if (kb == 8 && nt == 256) return launch_bp_t<8, 256>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, rl, st);
+  if (kb == 8 && nt == 384) return launch_bp_t<8, 384>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, rl, st);
+  if (kb == 4 && nt == 256) return launch_bp_t<4, 256>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, rl, st);
+  if (kb == 4 && nt == 384) return launch_bp_t<4, 384>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, rl, st);
   return cudaErrorInvalidValue;
 }
 
@@ -1348,7 +1377,7 @@ cudaError_t launch_bp_sum(const DevGeom &g, const float *quad, int view, int x0,
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
   k<<<nquads, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(quad), 0, nullptr, out, out, 0, one_frame(), view,
-                               x0);
+                               x0, bp_tile_log2(g, default_tune()));
   return cudaGetLastError();
 }
 

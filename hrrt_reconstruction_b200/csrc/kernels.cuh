@@ -116,8 +116,11 @@ struct ProjTune {
   int fp_pwarps;  // producer warps of the forward projector (0: as many as fit, 2..6)
   int bp_planes;  // planes per back-projection task: 4 or 8 (0: kBpZ)
   int bp_threads; // threads per back-projection CTA: 256 or 384 (0: 384)
+  int bp_tile;    // back projection: plane runs side by side in a warp's 32 tasks, a power of 2
+                  // up to 32 (the rest of the warp takes consecutive rows; 0: 2 above 12
+                  // segment groups, else 4)
 };
-inline ProjTune default_tune() { return ProjTune{0, 0, 0, 0}; }
+inline ProjTune default_tune() { return ProjTune{0, 0, 0, 0, 0}; }
 constexpr int kFpPlaneVariants[3] = {7, 9, 11};
 // warps per forward-projection CTA for each plane variant (register budget)
 constexpr int kFpVariantWarps[3] = {32, 32, 24};

@@ -269,6 +269,9 @@ typedef struct hrrt_tuning {
   int fp_producer_warps;  /* sampling warps of the forward projector: 2..6 (0: as many as fit) */
   int bp_planes;          /* planes per back-projection task: 4 or 8 (0: 8) */
   int bp_threads;         /* threads per back-projection CTA: 256 or 384 (0: 384) */
+  int bp_tile;            /* back projection: plane runs side by side in a warp, a power of 2 up to 32;
+                             the warp's other tasks take consecutive rows (0: 2 above 12 segment
+                             groups, else 4) */
   double fp_ms, bp_ms;    /* filled by the tuners: the chosen shapes' device time per launch */
 } hrrt_tuning;
 

@@ -129,7 +129,13 @@ def _shapes(ctx):
                         ctx.set_tuning(pl, pw, kb, nt)
                     except H.HrrtError:
                         continue
-                    out.append((pl, pw, kb, nt))
+                    out.append((pl, pw, kb, nt, 0))
+    # the back projector's tile width (tasks side by side along the planes)
+    for kb, nt in ((8, 0), (4, 256)):
+        for r in (1, 2, 4, 8, 16, 32):
+            out.append((9, 0, kb, nt, r))
+    with pytest.raises(H.HrrtError):
+        ctx.set_tuning(9, 0, 8, 0, 3)
     ctx.set_tuning()
     return out
 
@@ -148,7 +154,7 @@ def test_launch_shapes_bit_identical(name):
         ctx.osem_subsets(0, 1)
         img0 = ctx.get_image_xyz()
         shapes = _shapes(ctx)
-        assert (9, 0, 8, 0) in shapes and len(shapes) >= 24, shapes
+        assert (9, 0, 8, 0, 0) in shapes and len(shapes) >= 32, shapes
         want = None
         for t in shapes:
             ctx.set_tuning(*t)
