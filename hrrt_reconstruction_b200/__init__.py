@@ -150,6 +150,7 @@ def _load():
         "hrrt_lm_crystal_counts": (i, [vp, vp]),
         "hrrt_lm_histogram_at": (i, [vp, vp, ctypes.c_longlong, ctypes.c_longlong, i, i, i, vp, vp, vp]),
         "hrrt_lm_seek": (i, [vp, vp, ctypes.c_longlong, ctypes.c_longlong, i, i, vp]),
+        "hrrt_lm_set_chunk": (i, [vp, ctypes.c_longlong]),
         "hrrt_lm_convert_span9": (ctypes.c_longlong, [vp, vp, vp, i]),
         "hrrt_lm_trues_span9_device": (i, [vp, vp, vp, vp, vp]),
         "hrrt_lm_block_singles": (i, [vp, vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
@@ -629,6 +630,12 @@ class Listmode:
         self._check(lib.hrrt_lm_histogram_at(self._h, _ptr(w), w.size, offset, mode, duration, flags, _ptr(sino),
                                              _ptr(dly), ctypes.byref(st)), "lm_histogram")
         return sino, dly, st.as_dict()
+
+    def set_chunk(self, words=0):
+        """Host words longer than `words` (a multiple of 2 Mi; 0: 64 Mi) are
+        histogrammed in chunks whose upload overlaps the previous chunk's
+        histogram; < 0 turns streaming off."""
+        self._check(lib.hrrt_lm_set_chunk(self._h, words), "lm_set_chunk")
 
     def seek(self, words, target, offset=0, flags=0):
         """goto_event: words consumed up to the time tag reaching `target` s

@@ -751,6 +751,13 @@ struct hrrt_lm {
   void *scratch = nullptr;
   size_t scratch_bytes = 0;
   uint32_t *h_words_dev = nullptr;  // host-API staging
+  // host API, streamed: two chunk buffers filled on their own stream while
+  // the previous chunk is histogrammed (chunk_words: 0 default, < 0 never)
+  long long chunk_words = 0;
+  uint32_t *chunk_dev[2] = {nullptr, nullptr};
+  long long chunk_cap = 0;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_copied[2] = {nullptr, nullptr};
   size_t h_words_cap = 0;
   uint16_t *h_sino_dev = nullptr;   // host-API sinograms (prompts, delayed)
   longlong2 *tagbuf = nullptr;      // ordered time tags (position, value)
@@ -786,6 +793,11 @@ struct hrrt_lm {
     if (ccounts) cudaFree(ccounts);
     if (span9_src) cudaFree(span9_src);
     if (h_words_dev) cudaFree(h_words_dev);
+    for (int b = 0; b < 2; b++) {
+      if (chunk_dev[b]) cudaFree(chunk_dev[b]);
+      if (ev_copied[b]) cudaEventDestroy(ev_copied[b]);
+    }
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     if (h_sino_dev) cudaFree(h_sino_dev);
     if (stream) cudaStreamDestroy(stream);
     cudaSetDevice(cur);
@@ -965,8 +977,18 @@ int hrrt_lm_reset_clock(hrrt_lm *h) {
   return HRRT_OK;
 }
 
-int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwords, int mode, int duration, int flags,
-                             uint16_t *d_sino, uint16_t *d_delayed, hrrt_lm_stats *out, void *stream) {
+}  // extern "C"
+
+namespace {
+
+// One histogram call over d_words.  *frame_start_io carries the frame's start
+// (s, -1 before the first time tag) into and out of the call, so that the
+// chunks of one frame can be histogrammed call by call; `last`: the words end
+// the stream here, so an unterminated frame takes its rounded end time
+// (histogram_mp.cpp:1390-1396).
+int lm_hist_call(hrrt_lm *h, const uint32_t *d_words, long long nwords, int mode, int duration, int flags,
+                 uint16_t *d_sino, uint16_t *d_delayed, hrrt_lm_stats *out, void *stream, long long *frame_start_io,
+                 bool last) {
   if (!h) return HRRT_ERR_ARG;
   if (nwords < 0 || (nwords > 0 && !d_words) || !d_sino || !out)
     return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_histogram: null buffer or negative length");
@@ -980,7 +1002,7 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
   cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
   cudaError_t e = cudaSetDevice(h->device);
   if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_histogram");
-  long long frame_start = h->current_time >= 0 ? h->current_time : -1;
+  long long frame_start = *frame_start_io;
   if (nwords == 0) {
     out->frame_start = frame_start;
     return HRRT_OK;
@@ -1231,12 +1253,24 @@ int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwor
   out->resyncs = (long long)hs[kStResync];
   out->terminated = end_tag >= 0;
   out->words_used = end_tag >= 0 ? limit + 2 : nwords;
-  if (end_tag < 0) h->current_time = (h->current_time_msec + 500) / 1000;
+  if (end_tag < 0 && last) h->current_time = (h->current_time_msec + 500) / 1000;
+  *frame_start_io = frame_start;
   out->frame_start = frame_start;
   out->duration = h->current_time - frame_start;
   out->ms = ms;
   if (hc) build_head_curve(h, clock0, frame_start0, htags, end_tag, hivl, std::move(hsing), duration, flags, limit);
   return HRRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hrrt_lm_histogram_device(hrrt_lm *h, const uint32_t *d_words, long long nwords, int mode, int duration, int flags,
+                             uint16_t *d_sino, uint16_t *d_delayed, hrrt_lm_stats *out, void *stream) {
+  if (!h) return HRRT_ERR_ARG;
+  long long frame_start = h->current_time >= 0 ? h->current_time : -1;
+  return lm_hist_call(h, d_words, nwords, mode, duration, flags, d_sino, d_delayed, out, stream, &frame_start, true);
 }
 
 int hrrt_lm_head_curve(hrrt_lm *h, hrrt_lm_second *out, int capacity) {
@@ -1298,6 +1332,116 @@ long long hrrt_lm_table(int span, int maxrd, const char *name, void *out, size_t
   return (long long)n;
 }
 
+}  // extern "C"
+
+namespace {
+
+constexpr long long kDefaultChunkWords = 32 * kPacketWords;  // 64 Mi words, 256 MB
+
+// hrrt_lm_histogram_at over a long host stream, streamed: chunks of whole
+// packets (the first one led by the packet-phase filler) go up on a copy
+// stream into two device buffers while the previous chunk is histogrammed.
+// The chunks of one frame share its start and the clock; only the chunk that
+// ends the stream rounds an unterminated frame's end time, so the result is
+// that of one call over the whole stream.
+int lm_histogram_chunked(hrrt_lm *h, const uint32_t *words, long long nwords, long long phase, long long C, int mode,
+                         int duration, int flags, uint16_t *sino, uint16_t *delayed, hrrt_lm_stats *out) {
+  const long long S = h->tab.sino_size();
+  cudaError_t e = cudaSuccess;
+  if (h->chunk_cap < C) {
+    for (int b = 0; b < 2; b++) {
+      if (h->chunk_dev[b]) cudaFree(h->chunk_dev[b]);
+      h->chunk_dev[b] = nullptr;
+    }
+    h->chunk_cap = 0;
+    for (int b = 0; b < 2 && e == cudaSuccess; b++) e = cudaMalloc(&h->chunk_dev[b], sizeof(uint32_t) * (size_t)C);
+    if (e != cudaSuccess) return lm_fail(h, HRRT_ERR_NOMEM, "hrrt_lm_histogram: event chunks");
+    h->chunk_cap = C;
+  }
+  if (!h->copy_stream) {
+    e = cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking);
+    for (int b = 0; b < 2 && e == cudaSuccess; b++)
+      e = cudaEventCreateWithFlags(&h->ev_copied[b], cudaEventDisableTiming);
+    if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_histogram: copy stream");
+  }
+  cudaStream_t st = h->stream, cs = h->copy_stream;
+  e = cudaMemsetAsync(h->h_sino_dev, 0, sizeof(uint16_t) * 2 * (size_t)S, st);
+  if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_histogram");
+  // chunk k holds the caller's words [lo(k), hi(k)); chunk 0 after `phase`
+  // filler words
+  const long long first = C - phase;
+  const int nchunks = (int)(1 + (nwords - first + C - 1) / C);
+  auto lo = [&](int k) { return k == 0 ? 0 : first + (long long)(k - 1) * C; };
+  auto hi = [&](int k) { return std::min(nwords, k == 0 ? first : first + (long long)k * C); };
+  auto issue = [&](int k) {
+    const int b = k & 1;
+    cudaError_t r = cudaSuccess;
+    uint32_t *dst = h->chunk_dev[b];
+    if (k == 0 && phase > 0) {
+      r = cudaMemsetAsync(dst, 0x80, sizeof(uint32_t) * phase, cs);
+      dst += phase;
+    }
+    if (r == cudaSuccess)
+      r = cudaMemcpyAsync(dst, words + lo(k), sizeof(uint32_t) * (hi(k) - lo(k)), cudaMemcpyHostToDevice, cs);
+    if (r == cudaSuccess) r = cudaEventRecord(h->ev_copied[b], cs);
+    return r;
+  };
+  memset(out, 0, sizeof(*out));
+  long long frame_start = h->current_time >= 0 ? h->current_time : -1;
+  int rc = HRRT_OK;
+  e = issue(0);
+  for (int k = 0; k < nchunks && e == cudaSuccess && rc == HRRT_OK; k++) {
+    // the buffer of chunk k + 1 held chunk k - 1, whose call has returned
+    if (k + 1 < nchunks) e = issue(k + 1);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, h->ev_copied[k & 1], 0);
+    if (e != cudaSuccess) break;
+    const long long n = hi(k) - lo(k) + (k == 0 ? phase : 0);
+    hrrt_lm_stats c;
+    rc = lm_hist_call(h, h->chunk_dev[k & 1], n, mode, duration, flags, h->h_sino_dev, h->h_sino_dev + S, &c, st,
+                      &frame_start, k + 1 == nchunks);
+    if (rc != HRRT_OK) break;
+    out->prompts += c.prompts;
+    out->delayed += c.delayed;
+    out->timetags += c.timetags;
+    out->tags += c.tags;
+    out->invalid += c.invalid;
+    out->unmapped += c.unmapped;
+    out->doi_other += c.doi_other;
+    out->doi7 += c.doi7;
+    out->resyncs += c.resyncs - (k == 0 ? phase : 0);
+    out->ms += c.ms;
+    out->frame_start = c.frame_start;
+    out->duration = c.duration;
+    if (c.terminated) {
+      out->terminated = 1;
+      out->words_used = lo(k) + c.words_used - (k == 0 ? phase : 0);
+      break;
+    }
+    out->words_used = hi(k);
+  }
+  const cudaError_t e2 = cudaStreamSynchronize(cs);
+  if (rc != HRRT_OK) return rc;
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sino, h->h_sino_dev, sizeof(uint16_t) * S, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && delayed && mode == HRRT_LM_PROMPTS_AND_DELAYED)
+    e = cudaMemcpyAsync(delayed, h->h_sino_dev + S, sizeof(uint16_t) * S, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return lm_cuda(h, e, "hrrt_lm_histogram");
+  return HRRT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hrrt_lm_set_chunk(hrrt_lm *h, long long words) {
+  if (!h) return HRRT_ERR_ARG;
+  if (words > 0 && words % kPacketWords != 0)
+    return lm_fail(h, HRRT_ERR_ARG, "hrrt_lm_set_chunk: a chunk is a whole number of 2 Mi-word packets");
+  h->chunk_words = words;
+  return HRRT_OK;
+}
+
 int hrrt_lm_histogram(hrrt_lm *h, const uint32_t *words, long long nwords, int mode, int duration, int flags,
                       uint16_t *sino, uint16_t *delayed, hrrt_lm_stats *out) {
   return hrrt_lm_histogram_at(h, words, nwords, 0, mode, duration, flags, sino, delayed, out);
@@ -1327,6 +1471,13 @@ int hrrt_lm_histogram_at(hrrt_lm *h, const uint32_t *words, long long nwords, lo
     }
   }
   const long long phase = file_offset % kPacketWords, staged = nwords + phase;
+  // streamed in chunks where every output is additive across chunks (the
+  // head curve and the coincidence histogram are per call; the wide and
+  // partitioned paths clear and fold per call)
+  const long long chunk = h->chunk_words == 0 ? kDefaultChunkWords : h->chunk_words;
+  const int whole_call = HRRT_LM_HEAD_CURVE | HRRT_LM_CRYSTAL_COUNTS | HRRT_LM_FORCE_WIDE | HRRT_LM_FORCE_PARTITIONED;
+  if (h->chunk_words >= 0 && !(flags & whole_call) && !kWideByDefault && !kPartitionedByDefault && staged > chunk)
+    return lm_histogram_chunked(h, words, nwords, phase, chunk, mode, duration, flags, sino, delayed, out);
   if ((size_t)staged > h->h_words_cap) {
     if (h->h_words_dev) cudaFree(h->h_words_dev);
     h->h_words_dev = nullptr;

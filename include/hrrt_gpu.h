@@ -426,6 +426,15 @@ int hrrt_lm_histogram(hrrt_lm *lm, const uint32_t *words, long long nwords, int 
  * call at their offsets, parse as one pass over the file does. */
 int hrrt_lm_histogram_at(hrrt_lm *lm, const uint32_t *words, long long nwords, long long file_offset, int mode,
                          int duration, int flags, uint16_t *sino, uint16_t *delayed, hrrt_lm_stats *stats);
+/* hrrt_lm_histogram[_at] streams host words longer than one chunk: chunks of
+ * whole packets go up on a copy stream while the previous chunk is
+ * histogrammed, with the same results as one pass (calls asking for the head
+ * curve, the coincidence histogram or a forced wide / partitioned path take
+ * the whole stream at once).  words: the chunk, a multiple of 2 Mi words
+ * (0: 64 Mi words, 256 MB; < 0: never stream).  No counterpart in the
+ * reference, whose reader thread overlaps its file reads the same way
+ * (LM_Reader_mp.cpp:124). */
+int hrrt_lm_set_chunk(hrrt_lm *lm, long long words);
 /* goto_event (histogram_mp.cpp:384-425, 619-623): advance over the words
  * (at `file_offset` in the file) to just past the time tag that reaches
  * `target_s` seconds -- for 0, the tag that reads 0 ms, the coincidence

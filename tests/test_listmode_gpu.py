@@ -280,3 +280,46 @@ def test_frames_at_file_offsets(pair, path):
     import hrrt_reconstruction_b200 as H
     with pytest.raises(H.HrrtError):
         D.seek(w, 10_000)
+
+
+@pytest.mark.parametrize("offset", [0, 12345])
+def test_streamed_chunks_equal_one_pass(pair, offset):
+    """Host streams longer than a chunk (here one packet, 2 Mi words) are
+    histogrammed chunk by chunk while the next chunk uploads: the whole
+    stream, and 1-s frames that straddle chunk ends, equal the oracle's one
+    pass bit for bit, counters included (file offsets with an odd packet
+    phase too)."""
+    import hrrt_reconstruction_b200 as H
+    O, D = pair
+    w = random_stream(17, 3_000_000, tag_every=1000, p_resync=1e-3)
+    assert w.size > 2 * lm.PACKET_WORDS  # three chunks
+    try:
+        D.set_chunk(lm.PACKET_WORDS)
+        with pytest.raises(H.HrrtError):
+            D.set_chunk(lm.PACKET_WORDS + 4)
+        for mode in (lm.PROMPTS_AND_DELAYED, lm.TRUES):
+            O.reset_clock()
+            D.reset_clock()
+            so, do, sto = O.histogram(w, mode=mode, offset=offset)
+            sd, dd, std = D.histogram(w, mode=mode, offset=offset)
+            assert np.array_equal(so, sd)
+            if mode == lm.PROMPTS_AND_DELAYED:
+                assert np.array_equal(do, dd)
+            for k in STAT_KEYS:
+                assert sto[k] == std[k], (mode, k, sto[k], std[k])
+        O.reset_clock()
+        D.reset_clock()
+        pos, nframes = 0, 0
+        while pos < w.size:
+            so, do, sto = O.histogram(w[pos:], duration=1, offset=offset + pos)
+            sd, dd, std = D.histogram(w[pos:], duration=1, offset=offset + pos)
+            assert np.array_equal(so, sd) and np.array_equal(do, dd), nframes
+            for k in STAT_KEYS:
+                assert sto[k] == std[k], (nframes, k, sto[k], std[k])
+            pos += sto["words_used"]
+            nframes += 1
+            if not sto["terminated"]:
+                break
+        assert nframes >= 2
+    finally:
+        D.set_chunk(0)
