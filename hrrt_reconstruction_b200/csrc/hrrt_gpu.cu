@@ -661,6 +661,8 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
     }
   }
   if (!m.empty()) return bail(fail(ctx, HRRT_ERR_ARG, m));
+  if (g.groupmax > kFpMaxGroups)
+    return bail(fail(ctx, HRRT_ERR_ARG, "fp: more segment groups than the projector stages per row"));
   if (g.zp % kBpZ != 0) return bail(fail(ctx, HRRT_ERR_ARG, "padded z must be a multiple of 8"));
   for (int x = 1; x <= g.c; x++)
     if (g.cyl0[x] != g.cyl1[x] && g.cyl0[x] < 1) return bail(fail(ctx, HRRT_ERR_ARG, "FOV reaches the grid edge"));
@@ -899,11 +901,12 @@ int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms
   if (ctx->batch) return fail(ctx, HRRT_ERR_STATE, "the context serves a batch (hrrt_batch_destroy first)");
   const Geometry &g = ctx->geo;
   if (int rc = ensure_input_buffers(ctx, storage)) return rc;
-  // pair-major staging of one subset's view pairs, two buffers
+  // pair-major staging of one subset's view pairs (the four float inputs),
+  // two buffers
   const float *srcs[4] = {randoms, norm, atten, scatter};
   const size_t P = g.segmentsize, N = g.nbins, V = g.nviews;
   const size_t pair_elems = 2 * P * N, set_elems = (size_t)ctx->npairs * pair_elems;
-  const size_t need = set_elems * (sizeof(int16_t) + 4 * sizeof(float));
+  const size_t need = set_elems * 4 * sizeof(float);
   cudaError_t e = cudaSuccess;
   if (ctx->pstage_bytes < need) {
     for (int b = 0; b < 2; b++)
@@ -976,8 +979,7 @@ int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms
         const size_t view = v + h * (V / 2), doff = j * pair_elems + h * P * N;
         for (int i = 0; i < 4 && e == cudaSuccess; i++) {
           if (!srcs[i]) continue;
-          stg[i] = reinterpret_cast<float *>(ctx->pstage[b] + set_elems * sizeof(int16_t) +
-                                             (size_t)i * set_elems * sizeof(float));
+          stg[i] = reinterpret_cast<float *>(ctx->pstage[b] + (size_t)i * set_elems * sizeof(float));
           e = cudaMemcpy2DAsync(stg[i] + doff, N * sizeof(float), srcs[i] + view * N, V * N * sizeof(float),
                                 N * sizeof(float), P, cudaMemcpyHostToDevice, ctx->copy_stream);
         }

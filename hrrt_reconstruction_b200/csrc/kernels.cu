@@ -282,6 +282,11 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
   float4 *cen = rows + 2 * kFpSlots * ZS;
   __shared__ ulonglong2 s_w[kFpSlots][4][2];
   __shared__ int s_off[kFpSlots][8];
+  // each row's middle-plane sampling entries (z, f, z2, f2 per group),
+  // copied in with the row's columns.  Twice as many slots as rows in flight:
+  // the entries of row r + S arrive while the consumers may still read those
+  // of rows r - S + 1 .. r.  (3 KB: two CTAs per SM still fit at span 9.)
+  __shared__ __align__(16) FpMid s_mid[2 * kFpSlots][kFpMaxGroups];
   __shared__ __align__(8) uint64_t s_bar[kFpSlots];
 
   const int nwork = gridDim.x / fr.n, frame = blockIdx.x / nwork, item = blockIdx.x - frame * nwork;
@@ -331,11 +336,13 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
     // outside points read the zero column pairs
     s_off[sl][l] = inside ? (sl * 8 + l) * 2 * cpair : zoff;
     const unsigned m = __ballot_sync(0xffu, inside);
+    const int G = g.groupmax, es = r % (2 * kFpSlots);
     if (l == 0) {
       fence_proxy_async();
-      mbar_arrive_tx(&s_bar[sl], (uint32_t)__popc(m) * 2u * cpair * 4u);
+      mbar_arrive_tx(&s_bar[sl], (uint32_t)__popc(m) * 2u * cpair * 4u + (uint32_t)G * 16u);
     }
     __syncwarp(0xffu);
+    if (l == 0) bulk_g2s(&s_mid[es][0], g.fpmid + (size_t)y * G, (uint32_t)G * 16u, &s_bar[sl]);
     if (inside) {
       float *dst = corners + ((size_t)(sl * 8 + l) * 2) * cpair;
       bulk_g2s(dst, image + pt.base, cpair * 4u, &s_bar[sl]);
@@ -429,12 +436,12 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
   const int gg = (tk.seg + 1) / 2 - 1;
   const bool odd = tk.seg & 1;  // segment 2k-1: pam2 at z, pam at z2
   const int pofs = tk.p0 - g.zshift;
-  const FpMid *mrow = g.fpmid + (gg < 0 ? 0 : gg);
+  const int gs = gg < 0 ? 0 : gg;
   const int ns_t = (tk.type < 0) ? 0 : g.ytop[tk.seg] - g.ybot[tk.seg] + 1;
   const int li0 = gg * 2 * g.zshift + ((tk.p0 < g.zshift) ? tk.p0 : tk.p0 - ns_t + 2 * g.zshift);
-  const int G = g.groupmax, FS = g.groupmax * 2 * g.zshift;
+  const int FS = g.groupmax * 2 * g.zshift;
   for (int r = 0; r < nrows; r++) {
-    const int sl = r % kFpSlots, y = ystart + r;
+    const int sl = r % kFpSlots, es = r % (2 * kFpSlots), y = ystart + r;
     bar_sync(kBarFull + sl, nthr);
     const float4 *pam = rows + (size_t)sl * 2 * ZS;
     const float4 *pam2 = pam + ZS;
@@ -443,7 +450,7 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
 #pragma unroll
       for (int j = 0; j < PL; j++) acc[j] = qadd(acc[j], qadd(ldq(pam + tk.p0 + j), ldq(pam2 + tk.p0 + j)));
     } else if (tk.type > 0) {
-      const FpMid m = mrow[y * G];
+      const FpMid m = s_mid[es][gs];
       if (m.z >= 0) {  // else the group is skipped for this row (sbrt:1923-1924)
         // segment 2k accumulates pam at z and pam2 at z2; segment 2k-1 the converse
         const float4 *A = odd ? pam2 : pam;

@@ -33,6 +33,7 @@ constexpr int kFpPlanes = 9;                   // default planes per forward-pro
 constexpr int kFpSlots = HRRT_FP_SLOTS;       // sampled rows in flight between producers and consumers
 constexpr int kFpZPad = 16;     // zeroed entries after each sampled row
 constexpr int kFpEndPlanes = 4; // planes per end-plane task (they cost ~2x a middle plane)
+constexpr int kFpMaxGroups = 32; // segment groups the forward projector stages per row (22 at span 3)
 constexpr int kBpZ = 8;         // z per back-projection task
 constexpr int kBpMinBlocks = HRRT_BP_MIN_BLOCKS;  // resident back-projection CTAs per SM (register budget)
 constexpr int kBpPad = 8;       // zero planes on each side of a segment in the back projector (>= kBpZ)
