@@ -252,6 +252,18 @@ def algorithmic_model(info, add_bytes=4):
     }
 
 
+DATA = "synthetic (seeded phantom study, Poisson prompts)"
+
+
+def bench_config(storage, ws):
+    """The workload both arms (ours and --impl reference) are measured on."""
+    return {"workload": "HRRT span 3 (45 segments, 6367 planes x 288 views x 256 bins), image 256x256x207, "
+                        "16 subsets, OP-OSEM (-W 3), 3e8 counts, lognormal norm 0.1, scatter 15%, randoms 25%",
+            "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+            "l2": "inputs larger than L2 (1.9 GB prompts+additive per frame; 117 MB ratio per subset)",
+            "storage": storage}
+
+
 _PINNED = []  # page-locked tensors behind the numpy views handed to the C ABI
 
 
@@ -333,12 +345,8 @@ def run_ours(args, ws, rank, local):
         "metric": METRIC, "value": ws * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if storage == H.STORE_F32 else "f32 compute, 16-bit stored inputs",
-        "data": "synthetic (seeded phantom study, Poisson prompts)",
-        "config": {"workload": "HRRT span 3 (45 segments, 6367 planes x 288 views x 256 bins), image 256x256x207, "
-                               "16 subsets, OP-OSEM (-W 3), 3e8 counts, lognormal norm 0.1, scatter 15%, randoms 25%",
-                   "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
-                   "l2": "inputs larger than L2 (1.9 GB prompts+additive per frame; 117 MB ratio per subset)",
-                   "storage": args.storage},
+        "data": DATA,
+        "config": bench_config(args.storage, ws),
         "e2e": e2e,
         "gpu_launches": launches,
         "kernels": {k: {"launches": v[0], "ms_total": v[1], "ms_avg": v[1] / max(v[0], 1)} for k, v in kstats.items()},
@@ -699,24 +707,53 @@ def ref_inputs(R, seed=0):
 
 
 def ref_threads():
+    """The reference's stock thread count: -T min(8, nproc).  Its projector
+    threads are threads[Cal1 + thr] of a 16-entry array with Cal1 = 8
+    (hrrt_osem3d_span3.cpp:189, :448, :4193), so -T cannot exceed 8."""
+    return max(1, min(8, os.cpu_count() or 1))
+
+
+def all_core_threads():
+    """Every host core up to the harness's 16 thread slots (a labelled second
+    figure: the stock binary does not run more than 8)."""
     return max(1, min(16, os.cpu_count() or 1))
 
 
-def cpu_baseline(args, subsets_in_sample=1):
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def time_ref_subsets(R, img, nf, prompts, add, order, first, count, T):
+    t0 = time.perf_counter()
+    for k in range(count):
+        R.osem_subset(img, nf, prompts, add, int(order[(first + k) % SUBSETS]), T)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(args, subsets_in_sample=2):
     from oracle import ref
     if not ref.available():
         return oracle_port_baseline(subsets_in_sample)
-    T = ref_threads()
-    R = ref.RefProjector(nthreads=T, **geom_dict())
+    T, TA = ref_threads(), all_core_threads()
+    R = ref.RefProjector(nthreads=max(T, TA), **geom_dict())
     img, nf, prompts, add = ref_inputs(R)
     order = R.order()
-    t0 = time.perf_counter()
-    for k in range(subsets_in_sample):
-        R.osem_subset(img, nf, prompts, add, int(order[k % SUBSETS]), T)
-    dt = time.perf_counter() - t0
+    dt = time_ref_subsets(R, img, nf, prompts, add, order, 0, subsets_in_sample, T)
+    dta = time_ref_subsets(R, img, nf, prompts, add, order, subsets_in_sample, subsets_in_sample, TA)
     return {"value": subsets_in_sample / dt, "unit": UNIT, "cores": T, "kind": "reference",
-            "sample": f"{subsets_in_sample} OP-OSEM subset(s) of the span-3 HRRT workload on the reference projector "
-                      f"(oracle/_ref/libhrrt_ref.so, -T {T} thread grouping of CalculateOsem3d)"}
+            "nproc": os.cpu_count(), "cpu_model": cpu_model(),
+            "sample": f"{subsets_in_sample} OP-OSEM subsets of the span-3 HRRT workload on the reference projector "
+                      f"(oracle/_ref/libhrrt_ref.so) with the stock -T {T} thread grouping of CalculateOsem3d",
+            "all_cores": {"value": subsets_in_sample / dta, "threads": TA,
+                          "note": "the same with -T = min(16, nproc), beyond the stock maximum of 8"}}
 
 
 def oracle_port_baseline(subsets_in_sample=1):
@@ -748,25 +785,125 @@ def run_reference(args, ws, rank, local):
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libhrrt_ref.so not built"}))
         return
-    T = ref_threads()
-    R = ref.RefProjector(nthreads=T, **geom_dict())
+    T, TA = ref_threads(), all_core_threads()
+    R = ref.RefProjector(nthreads=max(T, TA), **geom_dict())
     img, nf, prompts, add = ref_inputs(R)
     order = R.order()
-    for k in range(args.warmup):
-        R.osem_subset(img, nf, prompts, add, int(order[k % SUBSETS]), T)
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        R.osem_subset(img, nf, prompts, add, int(order[(args.warmup + k) % SUBSETS]), T)
-    dt = time.perf_counter() - t0
+    time_ref_subsets(R, img, nf, prompts, add, order, 0, args.warmup, T)
+    dt = time_ref_subsets(R, img, nf, prompts, add, order, args.warmup, args.steps, T)
     v = args.steps / dt
+    # the labelled second figure: all host cores (up to 16 threads), a short sample
+    na = min(args.steps, 4)
+    dta = time_ref_subsets(R, img, nf, prompts, add, order, 0, na, TA)
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": "HRRT span 3 OP-OSEM subset on the reference CPU projector", "threads": T},
-           "cpu_baseline": {"value": v, "unit": UNIT, "cores": T, "kind": "reference",
-                            "sample": "one OP-OSEM subset per step (9 view pairs), span-3 HRRT"},
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": DATA,
+           "config": bench_config(args.storage, ws),
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": T, "kind": "reference", "nproc": os.cpu_count(),
+                            "cpu_model": cpu_model(),
+                            "sample": f"one OP-OSEM subset per step (9 view pairs), span-3 HRRT, on the reference "
+                                      f"projector (oracle/_ref/libhrrt_ref.so) with the stock -T {T} thread "
+                                      "grouping of CalculateOsem3d",
+                            "all_cores": {"value": na / dta, "threads": TA, "steps": na,
+                                          "note": "the same with -T = min(16, nproc), beyond the stock maximum "
+                                                  "of 8"}},
            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Kernel cases: compact workloads that launch one group of kernels a few
+# times, for profiler captures (`--case`); they print per-kernel device times
+# and no benchmark line.
+# ---------------------------------------------------------------------------
+OSEM_KERNELS = ("prep_kernel", "scale_pairs_kernel", "fp_kernel", "bp_kernel", "adj_kernel", "adj_rotate_kernel",
+                "rotback_kernel", "post_iter_kernel", "psf_kernel", "apply_corr_kernel", "map_dpf_kernel")
+
+
+def case_osem(args):
+    """Seeded Poisson prompts, flat randoms and a lognormal normalisation at
+    the HRRT geometry of `--span`: upload (prep), sensitivity, then
+    `--subsets` OSEM subsets with the chosen back projector, PSF and MAP
+    options.  Holds the quad-layout inputs only (about 5 GB at span 3, 3 GB
+    with 16-bit terms), so single launches of its kernels suit a profiler."""
+    import hrrt_reconstruction_b200 as H
+    ctx = H.Context(H.hrrt_geometry(span=args.span))
+    rng = np.random.default_rng(7)
+    shape = ctx.sino_shape
+    prompts = rng.poisson(0.64, size=shape).astype(np.int16)
+    randoms = np.full(shape, 0.1, np.float32)
+    norm = np.exp(np.float32(0.1) * rng.standard_normal(shape, dtype=np.float32)).astype(np.float32)
+    storage = {"f32": H.STORE_F32, "16": H.STORE_16, "f16": H.STORE_F16}[args.storage]
+    if args.bp == "adjoint":
+        ctx.set_backprojector(H.BP_ADJOINT)
+    if args.psf:
+        ctx.set_psf(True)
+    ctx.set_profiling(True)
+    ctx.upload_inputs(prompts, randoms, norm, storage=storage)
+    ctx.sensitivity()
+    ctx.init_image()
+    if args.map:
+        ctx.set_map(1, 0.02, first_subset=0)
+    ctx.osem_subsets(0, args.subsets)
+    ctx.set_profiling(False)
+    for k in OSEM_KERNELS:
+        n, ms = ctx.kernel_stats(k)
+        if n:
+            print(f"{k:18s} launches {n:4d}  total {ms:9.3f} ms  avg {ms / n:8.3f} ms", flush=True)
+    ctx.close()
+
+
+LM_PATHS = (("direct", 16), ("wide", 64), ("partitioned", 32))
+
+
+def case_lm(args):
+    """`--events` synthetic l64 events (the benchmark's generator) histogrammed
+    `--reps` times through each device path into span-3 prompt and delayed
+    sinograms; `--lm-extra randoms` also smooths randoms from the stream's
+    coincidence histogram, `span9` folds the trues into span 9.  Holds the
+    words (8 B per event) and the two 16-bit sinograms (1.9 GB)."""
+    import torch
+
+    import hrrt_reconstruction_b200 as H
+    from hrrt_reconstruction_b200 import listmode_synth as LS
+    with H.Context(H.hrrt_geometry(span=3)) as c3:
+        E = LS.expected_prompts(c3, seed=0)
+    words = LS.synth_words(int(args.events), E, seed=0)
+    del E
+    torch.cuda.synchronize()
+    extra = set(args.lm_extra.split(",")) if args.lm_extra else set()
+    with H.Listmode(3) as lm:
+        ds = torch.zeros(lm.sino_size, dtype=torch.int16, device="cuda")
+        dd = torch.zeros(lm.sino_size, dtype=torch.int16, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        want = args.paths.split(",")
+        for name, flag in LM_PATHS:
+            if name not in want:
+                continue
+            ms = []
+            for r in range(args.reps + 1):
+                lm.reset_clock()
+                st = lm.histogram_device(words.data_ptr(), words.numel(), ds.data_ptr(), dd.data_ptr(), flags=flag,
+                                         stream=stream)
+                if r > 0:
+                    ms.append(st["ms"])
+            print(f"{name:12s} {int(args.events)} events  " + " ".join(f"{m:.2f}" for m in ms) + " ms", flush=True)
+        if "span9" in extra:
+            d9 = torch.zeros(2209 * 288 * 256, dtype=torch.int16, device="cuda")
+            for _ in range(args.reps + 1):
+                lm.trues_span9_device(ds.data_ptr(), dd.data_ptr(), d9.data_ptr(), stream=stream)
+            torch.cuda.synchronize()
+            print("span9 trues folded", flush=True)
+        if "randoms" in extra:
+            lm.reset_clock()
+            lm.histogram_device(words.data_ptr(), words.numel(), ds.data_ptr(), dd.data_ptr(),
+                                flags=H.LM_CRYSTAL_COUNTS, stream=stream)
+            torch.cuda.synchronize()
+            counts = lm.crystal_counts().astype(np.int32)
+            with H.Listmode(9) as l9:
+                for _ in range(args.reps):
+                    sino, it = l9.smooth_randoms(counts, scan_duration=max(1.0, args.events / 1e6 / 1e3))
+            print(f"smoothed randoms: {it} iterations, sum {float(sino.sum(dtype=np.float64)):.6g}", flush=True)
 
 
 def main():
@@ -783,7 +920,24 @@ def main():
     ap.add_argument("--dyn-frames", type=int, default=24, help="frames of the dynamic-study leg (0: skip it)")
     ap.add_argument("--no-compare-16", dest="compare_16", action="store_false",
                     help="skip the 16-bit-storage leg of the span-3 workload")
+    ap.add_argument("--case", choices=["osem", "lm"], help="run a kernel case for a profiler instead of the bench")
+    ap.add_argument("--span", type=int, default=3, choices=[3, 9], help="--case osem: span")
+    ap.add_argument("--subsets", type=int, default=2, help="--case osem: OSEM subsets after the sensitivity")
+    ap.add_argument("--case-storage", dest="case_storage", default="f32", choices=["f32", "16", "f16"],
+                    help="--case osem: storage of the sinogram terms")
+    ap.add_argument("--bp", default="ref", choices=["ref", "adjoint"], help="--case osem: back projector")
+    ap.add_argument("--psf", action="store_true", help="--case osem: PSF modelling (-B, HRRT defaults)")
+    ap.add_argument("--map", action="store_true", help="--case osem: MAP technique 1 from the first subset")
+    ap.add_argument("--events", type=float, default=1e8, help="--case lm: events")
+    ap.add_argument("--reps", type=int, default=1, help="--case lm: timed calls per path")
+    ap.add_argument("--paths", default="direct", help="--case lm: direct,wide,partitioned")
+    ap.add_argument("--lm-extra", default="", help="--case lm: randoms,span9")
     args = ap.parse_args()
+    if args.case == "osem":
+        args.storage = args.case_storage
+        return case_osem(args)
+    if args.case == "lm":
+        return case_lm(args)
     global GEOMETRY
     GEOMETRY = args.geometry
     if args.warmup < 3 and args.impl != "reference":

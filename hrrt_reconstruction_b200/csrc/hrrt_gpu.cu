@@ -1376,19 +1376,23 @@ int hrrt_bp_pair(hrrt_ctx *ctx, const float *prj, int view, float *imagebuf_xyz,
 // Back projection without allocation.
 //
 // Some callers cannot allocate device memory while they run: an acquisition
-// loop that must not stall on cudaMalloc's implicit device synchronisation,
-// a host application that hands this library a fixed memory budget at start-up,
-// or code that issues its work into a stream another component is recording.
-// hrrt_bp_pair_noalloc serves them.  Its only scratch -- the quad-layout copy
-// of the input sinogram rows, scaled by the back projector's segment weights --
-// lives in the static device array below, so the call itself never allocates;
-// the input rows and the output buffer are the caller's.
+// loop that must not stall on cudaMalloc's implicit device synchronisation, or
+// a host application that hands this library a fixed memory budget at
+// start-up and forbids allocations after it.  hrrt_bp_pair_noalloc serves
+// them.  It runs the reference back projector (the result of hrrt_bp_pair
+// with HRRT_BP_REF, whatever back projector the context has selected).  Its
+// only scratch -- the quad-layout copy of the input sinogram rows, scaled by
+// the back projector's segment weights -- lives in the static device array
+// below, so the call itself never allocates; the input rows and the output
+// buffer are the caller's.
 //
 // The array is kNoAllocScratchBytes (16 MiB: the quad layout of an HRRT span-3
 // view pair is 13.3 MB).  Every GPU on which the library is loaded holds it
-// until the process exits.  All calls share it and it keeps the last call's
-// contents, so calls that overlap on the GPU (other streams, other host
-// threads) race with each other.
+// until the process exits.  The first call on a device looks up the array's
+// device address there (cudaGetSymbolAddress), once.  All calls share the
+// array and it keeps the last call's contents, so each call clears it first,
+// and calls that overlap on the GPU (other streams, other host threads) race
+// with each other.
 // ---------------------------------------------------------------------------
 constexpr size_t kNoAllocScratchBytes = (size_t)16 << 20;
 static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchBytes / sizeof(float)];
@@ -1416,20 +1420,9 @@ cudaError_t noalloc_scratch(float **out) {
   *out = p;
   return cudaSuccess;
 }
-}  // namespace
-
-extern "C" {
-
-int hrrt_bp_pair_noalloc(hrrt_ctx *ctx, const float *d_prj, int view, float *d_imagebuf, void *stream) {
-  if (!ctx || !d_prj || !d_imagebuf) return HRRT_ERR_ARG;
+// the body of hrrt_bp_pair_noalloc, with ctx->device current
+int noalloc_bp(hrrt_ctx *ctx, const float *d_prj, int view, float *d_imagebuf, void *stream, size_t need) {
   const Geometry &g = ctx->geo;
-  if (view < 0 || view >= g.nviews / 2) return fail(ctx, HRRT_ERR_ARG, "view must be < nviews/2");
-  const size_t need = (size_t)ctx->quad_pair * sizeof(float);
-  if (need > kNoAllocScratchBytes)
-    return fail(ctx, HRRT_ERR_ARG,
-                "hrrt_bp_pair_noalloc: this geometry needs " + std::to_string(need) +
-                    " bytes of scratch; the static scratch holds " + std::to_string(kNoAllocScratchBytes));
-  CK(cudaSetDevice(ctx->device), "hrrt_bp_pair_noalloc");
   float *scratch = nullptr;
   CK(noalloc_scratch(&scratch), "hrrt_bp_pair_noalloc: cudaGetSymbolAddress");
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
@@ -1446,6 +1439,31 @@ int hrrt_bp_pair_noalloc(hrrt_ctx *ctx, const float *d_prj, int view, float *d_i
   CK(launch_rows_to_quad(ctx->dg, g.nbins, d_prj, scratch, 1, st), "hrrt_bp_pair_noalloc: pack");
   CK(launch_bp_sum(ctx->dg, scratch, view, x0, x1 - x0 + 1, d_imagebuf, st), "hrrt_bp_pair_noalloc: bp");
   return HRRT_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int hrrt_bp_pair_noalloc(hrrt_ctx *ctx, const float *d_prj, int view, float *d_imagebuf, void *stream) {
+  if (!ctx || !d_prj || !d_imagebuf) return HRRT_ERR_ARG;
+  const Geometry &g = ctx->geo;
+  if (view < 0 || view >= g.nviews / 2) return fail(ctx, HRRT_ERR_ARG, "view must be < nviews/2");
+  const size_t need = (size_t)ctx->quad_pair * sizeof(float);
+  if (need > kNoAllocScratchBytes)
+    return fail(ctx, HRRT_ERR_ARG,
+                "hrrt_bp_pair_noalloc: this geometry needs " + std::to_string(need) +
+                    " bytes of scratch; the static scratch holds " + std::to_string(kNoAllocScratchBytes));
+  // the work runs on the context's device; the caller's current device is
+  // put back on every return
+  int caller_dev = -1;
+  CK(cudaGetDevice(&caller_dev), "hrrt_bp_pair_noalloc: cudaGetDevice");
+  if (caller_dev != ctx->device) CK(cudaSetDevice(ctx->device), "hrrt_bp_pair_noalloc: cudaSetDevice");
+  const int rc = noalloc_bp(ctx, d_prj, view, d_imagebuf, stream, need);
+  if (caller_dev != ctx->device) {
+    const cudaError_t e = cudaSetDevice(caller_dev);
+    if (e != cudaSuccess && rc == HRRT_OK) return cuda_fail(ctx, e, "hrrt_bp_pair_noalloc: restore the device");
+  }
+  return rc;
 }
 
 int hrrt_rotate_add(hrrt_ctx *ctx, const float *imagebuf_xyz, int view, float *corr_xyz) {

@@ -608,8 +608,10 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(De
     }
   __syncthreads();
 
+  // ACC: both partial sums go through bc (br is unused and may be null), so
+  // the two destinations derive from one restrict pointer
   float *bcp = bc + (size_t)w.slot * vol;
-  float *brp = br + (size_t)w.slot * vol;
+  float *brp = (ACC ? bc : br) + (size_t)w.slot * vol;
   const int ystart = g.cyl0[x];
   const int nyq = c - ystart + 1, nzc = zp / KB;
   const int o0 = g.bp_soff[0];
@@ -1383,7 +1385,7 @@ cudaError_t launch_bp_sum(const DevGeom &g, const float *quad, int view, int x0,
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  k<<<nquads, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(quad), 0, nullptr, out, out, 0, one_frame(), view,
+  k<<<nquads, 256, smem, st>>>(g, reinterpret_cast<const float4 *>(quad), 0, nullptr, out, nullptr, 0, one_frame(), view,
                                x0, bp_tile_log2(g, default_tune()));
   return cudaGetLastError();
 }

@@ -192,16 +192,18 @@ int hrrt_set_backprojector(hrrt_ctx *ctx, int mode);
  * Back projection of one view pair that allocates no device memory (no
  * counterpart in the reference, whose projector works on host arrays).  For
  * callers that may not allocate while they run -- a real-time loop that cannot
- * take cudaMalloc's device synchronisation, a host that grants the library a
- * fixed memory budget at start-up, or work issued into a stream that is being
- * recorded.  Same result as hrrt_bp_pair, with the caller's device buffers:
- * d_prj rows [2*segmentsize][nbins] in, d_imagebuf [x][y][zp] out
- * (overwritten), on `stream` (a cudaStream_t; NULL = the context's stream),
- * asynchronously.  Its scratch is a static 16 MiB device array in the library
- * (held on every GPU that loads it until exit); geometries whose quad-layout
- * view pair exceeds it are rejected with HRRT_ERR_ARG.  The first call on a
- * device resolves that array's address, so make it before any stream capture.
- * All calls share the array: calls that overlap on the GPU race.
+ * take cudaMalloc's device synchronisation, or a host that grants the library
+ * a fixed memory budget at start-up and allows no allocation after it.  The
+ * result of hrrt_bp_pair(ctx, ..., HRRT_BP_REF) -- the reference back
+ * projector, whatever hrrt_set_backprojector selected -- with the caller's
+ * device buffers: d_prj rows [2*segmentsize][nbins] in, d_imagebuf [x][y][zp]
+ * out (overwritten), on `stream` (a cudaStream_t; NULL = the context's
+ * stream), asynchronously; the caller's current device is left as it was.
+ * Its scratch is a static 16 MiB device array in the library (held on every
+ * GPU that loads it until exit); geometries whose quad-layout view pair
+ * exceeds it are rejected with HRRT_ERR_ARG.  The first call on a device
+ * resolves that array's address, so make it before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU race.
  */
 int hrrt_bp_pair_noalloc(hrrt_ctx *ctx, const float *d_prj, int view, float *d_imagebuf, void *stream);
 

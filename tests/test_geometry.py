@@ -32,7 +32,8 @@ def test_tables_bit_identical(name, ref_lib):
 
 
 def test_hrrt_sizes():
-    """Segment and plane counts of lmhistogram_mp.cpp:105-116 / SURVEY appendix A."""
+    """Segment and plane counts of lmhistogram_mp.cpp:105-116 (and the segment
+    sizes of get_info, hrrt_osem3dv_sbrt_span3.cpp:159-191)."""
     for span, nseg, planes in ((9, 15, 2209), (3, 45, 6367)):
         g = H.hrrt_geometry(span=span)
         seg = H.geometry_table(g, "segments").reshape(3, -1)
