@@ -392,8 +392,12 @@ def run_ours(args, ws, rank, local):
                                            storage=H.STORE_F16)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
+    if rank == 0 and ws == 1 and args.parity:
+        out["parity"] = {"span3": run_parity(H, ctx, st, ITERATIONS, dict(seed=1, **STUDY))}
     ctx.close()
     del ctx, host, st
+    if rank == 0 and ws == 1 and args.parity:
+        out["parity"]["span9"] = run_parity_span9(H, local)
     _PINNED.clear()
     if args.dyn_frames > 0:
         out["dynamic"] = run_dynamic(args, torch, H, local, dist, ws)
@@ -434,6 +438,55 @@ def run_storage16(args, torch, H, ctx, st, host, names, img_f32, cs, dist, local
                            "16-bit-stored vs f32-stored inputs, same prompts",
             "storage": ("prompts int16, 1/(NA) and additive term " + ("fp16" if storage == H.STORE_F16 else "bf16")
                         + "; FP32 accumulation, FP64 image sum")}
+
+
+def run_parity(H, ctx, st, iterations, study_kw):
+    """Per-iteration parity of one whole study: hrrt_reconstruct from host
+    buffers with f32, bf16 and fp16 terms, against the reference's own
+    projector (oracle/_ref, stock -T) and the FP64 restatement run on the same
+    prep (oracle/study_parity.py).  Outside every timed region."""
+    from oracle import ref
+    from oracle import study_parity as SP
+    geom = dict(geom_dict(), span=int(ctx.geom.span))
+    raw = [st[k] for k in ("prompts", "randoms", "norm", "atten", "scatter")]
+    dev = {}
+    for name, storage in (("f32", H.STORE_F32), ("bf16", H.STORE_16), ("fp16", H.STORE_F16)):
+        dev[name] = [ctx.reconstruct(*raw, storage=storage, iterations=k + 1)[0] for k in range(iterations)]
+    t0 = time.perf_counter()
+    pre = SP.prep(geom, *raw)
+    host = {}
+    if ref.available():
+        host["reference"] = SP.reconstruct("reference", geom, pre, iterations)
+    host["fp64"] = SP.reconstruct("fp64", geom, pre, iterations)
+    host_s = time.perf_counter() - t0
+    res = {"workload": f"HRRT span {geom['span']}, 16 subsets x {iterations} iteration(s), phantom study "
+                       + ", ".join(f"{k}={v}" for k, v in study_kw.items()),
+           "metric": "image rel-L2 per iteration (whole [z][y][x] image)",
+           "host": {k: {"threads": v[0]["threads"], "sensitivity_s": v[0]["sens_s"],
+                        "iteration_s": [r["seconds"] for r in v], "sum_image": [r["sum"] for r in v]}
+                    for k, v in host.items()},
+           "host_s": host_s}
+    for name, imgs in dev.items():
+        d = {f"vs_{k}": v for k, v in SP.compare(imgs, host).items()}
+        if name != "f32":
+            d["vs_f32_device"] = [SP.rel_l2(a, b) for a, b in zip(imgs, dev["f32"])]
+        res[name] = d
+    if "reference" in host:
+        res["reference_vs_fp64"] = [SP.rel_l2(a["image"], b["image"]) for a, b in zip(host["reference"], host["fp64"])]
+    res["storage"] = {"f32": "prompts int16, terms f32", "bf16": "prompts int16, 1/(NA) and additive term bf16",
+                      "fp16": "prompts int16, 1/(NA) and additive term fp16"}
+    return res
+
+
+def run_parity_span9(H, local):
+    """The plain span-9 workload (seed-0 phantom, 1e8 counts, randoms 20 %,
+    norm 1, water attenuation, 16 subsets x 1 iteration) and its 16-bit-stored
+    form, through run_parity."""
+    from hrrt_reconstruction_b200 import phantom
+    kw = dict(seed=0, total_counts=1e8, randoms_frac=0.20)
+    with H.Context(H.hrrt_geometry(**dict(geom_dict(), span=9)), device=local) as c9:
+        st = phantom.study(c9, **kw)
+        return run_parity(H, c9, st, 1, kw)
 
 
 # Dynamic study: 24 span-9 frames of the config-0 phantom, sphere activity
@@ -823,8 +876,8 @@ OSEM_KERNELS = ("prep_kernel", "scale_pairs_kernel", "fp_kernel", "bp_kernel", "
 def case_osem(args):
     """Seeded Poisson prompts, flat randoms and a lognormal normalisation at
     the HRRT geometry of `--span`: upload (prep), sensitivity, then
-    `--subsets` OSEM subsets with the chosen back projector, PSF and MAP
-    options.  Holds the quad-layout inputs only (about 5 GB at span 3, 3 GB
+    `--subsets` OSEM subsets (and `--iterations` full iterations) with the
+    chosen back projector, PSF and MAP options.  Holds the quad-layout inputs only (about 5 GB at span 3, 3 GB
     with 16-bit terms), so single launches of its kernels suit a profiler."""
     import hrrt_reconstruction_b200 as H
     ctx = H.Context(H.hrrt_geometry(span=args.span))
@@ -845,6 +898,8 @@ def case_osem(args):
     if args.map:
         ctx.set_map(1, 0.02, first_subset=0)
     ctx.osem_subsets(0, args.subsets)
+    if args.iterations:
+        ctx.osem(args.iterations)
     ctx.set_profiling(False)
     for k in OSEM_KERNELS:
         n, ms = ctx.kernel_stats(k)
@@ -920,11 +975,15 @@ def main():
     ap.add_argument("--dyn-frames", type=int, default=24, help="frames of the dynamic-study leg (0: skip it)")
     ap.add_argument("--no-compare-16", dest="compare_16", action="store_false",
                     help="skip the 16-bit-storage leg of the span-3 workload")
+    ap.add_argument("--no-parity", dest="parity", action="store_false",
+                    help="skip the per-iteration parity of the span-3 and span-9 studies against the host checkers")
     ap.add_argument("--case", choices=["osem", "lm"], help="run a kernel case for a profiler instead of the bench")
     ap.add_argument("--span", type=int, default=3, choices=[3, 9], help="--case osem: span")
     ap.add_argument("--subsets", type=int, default=2, help="--case osem: OSEM subsets after the sensitivity")
     ap.add_argument("--case-storage", dest="case_storage", default="f32", choices=["f32", "16", "f16"],
                     help="--case osem: storage of the sinogram terms")
+    ap.add_argument("--iterations", type=int, default=0,
+                    help="--case osem: full iterations (every subset + the post-iteration pass) after the subsets")
     ap.add_argument("--bp", default="ref", choices=["ref", "adjoint"], help="--case osem: back projector")
     ap.add_argument("--psf", action="store_true", help="--case osem: PSF modelling (-B, HRRT defaults)")
     ap.add_argument("--map", action="store_true", help="--case osem: MAP technique 1 from the first subset")
