@@ -701,6 +701,7 @@ def run_listmode(args, torch, H, local, dist, ws, cpu=True):
     }
     if cpu:
         res["cpu_baseline"] = listmode_cpu_baseline(hwn)
+        res["parity"] = listmode_parity(H, hwn, local)
     lm.close()
     # the rest of the config-5 pipeline: OSEM (16 subsets x 2 iterations) of
     # the histogrammed prompts with the delayed sinogram as randoms, from the
@@ -745,6 +746,39 @@ def listmode_cpu_baseline(words, n_sample_words=8_000_000):
     ev = st["prompts"] + st["delayed"]
     return {"value": ev / dt, "unit": "events/s", "cores": 1, "kind": "port",
             "sample": f"first {n_sample_words} words ({ev} events) of the stream on oracle/lm_oracle.c"}
+
+
+def listmode_parity(H, words, local, npackets=4, duration=3):
+    """The first `npackets` whole reader packets of the stream (1 Mi events
+    each) histogrammed as one `duration`-second frame (prompts + delayed,
+    span 3) by the device, by the restatement (oracle/lm_oracle.c) and by the
+    reference's own histogrammer (oracle/_ref/lmhist_ref); bins that differ
+    between them.  Outside every timed region."""
+    from oracle import lm_ref
+    from oracle.lm import LMOracle
+    n = npackets * (2 << 20)
+    w = np.ascontiguousarray(words[:n])
+    with H.Listmode(3, device=local) as D:
+        D.reset_clock()
+        ds, dd, dst = D.histogram(w, duration=duration)
+    O = LMOracle(3)
+    O.reset_clock()
+    os_, od, ost = O.histogram(w, duration=duration)
+    res = {"prefix_words": n, "frame_s": duration, "events": int(ost["prompts"] + ost["delayed"]),
+           "bins": 2 * int(ds.size), "device_vs_oracle_bins_differing": int((ds != os_).sum() + (dd != od).sum())}
+    del os_, od
+    if lm_ref.available():
+        R = lm_ref.histogram(w, span=3, mode=1, duration=duration)
+        res["device_vs_reference_bins_differing"] = int((ds.view(np.int16) != R["prompts"]).sum() +
+                                                        (dd.view(np.int16) != R["delayed"]).sum())
+        res["reference_frame"] = {"start_s": R["frame_start"], "duration_s": R["duration"],
+                                  "prompts": R["total_prompts"], "randoms": R["total_randoms"]}
+        res["device_frame"] = {"start_s": int(dst["frame_start"]), "duration_s": int(dst["duration"]),
+                               "prompts": int(dst["prompts"]), "delayed": int(dst["delayed"])}
+        res["reference"] = ("oracle/_ref/lmhist_ref: histogram_mp.cpp, LM_Reader_mp.cpp, LM_Rebinner_mp.cpp, "
+                            "lor_sinogram_map.cpp, geometry_info.cpp, segment_info_fromarchive.cpp compiled "
+                            "unmodified")
+    return res
 
 
 def ref_inputs(R, seed=0):

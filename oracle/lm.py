@@ -59,6 +59,8 @@ def lib():
             getattr(L, n).argtypes = a
             getattr(L, n).restype = None
         L.lm_rebin_event.argtypes = [vp, i, i, i, i, i, i, i]
+        L.lm_rebin_events.argtypes = [vp, ctypes.c_longlong, vp, vp]
+        L.lm_rebin_events.restype = None
         L.lm_histogram.argtypes = [vp, vp, ctypes.c_longlong, i, i, i, vp, vp, vp, vp]
         f = ctypes.c_float
         L.lm_histogram_hc.argtypes = [vp, vp, ctypes.c_longlong, ctypes.c_longlong, i, i, i, vp, vp, vp, vp, vp, i,
@@ -125,6 +127,13 @@ class LMOracle:
 
     def rebin_event(self, mp, al, ax, ay, bl, bx, by):
         return self.L.lm_rebin_event(self.t, mp, al, ax, ay, bl, bx, by)
+
+    def rebin_events(self, ev):
+        """rebin_event for each row (mp, al, ax, ay, bl, bx, by) of int32 [n][7]"""
+        ev = np.ascontiguousarray(ev, np.int32)
+        out = np.empty(ev.shape[0], np.int32)
+        self.L.lm_rebin_events(self.t, ev.shape[0], _p(ev), _p(out))
+        return out
 
     def histogram(self, words, mode=PROMPTS_AND_DELAYED, duration=0, flags=0, sino=None, delayed=None, offset=0):
         """-> (sino, delayed, stats dict); adds into sino/delayed when given;

@@ -250,6 +250,13 @@ int lm_rebin_event(const lm_tables *t, int mp, int alayer, int ax, int ay, int b
   return (plane + t->segzoffset[segnum]) * NPROJS * NVIEWS + sino_addr;
 }
 
+void lm_rebin_events(const lm_tables *t, long long n, const int32_t *ev, int32_t *addr) {
+  for (long long k = 0; k < n; k++) {
+    const int32_t *e = ev + 7 * k;
+    addr[k] = lm_rebin_event(t, e[0], e[1], e[2], e[3], e[4], e[5], e[6]);
+  }
+}
+
 void lm_clock_init(lm_clock *c) {
   c->current_time = -1;
   c->current_time_msec = -1;
@@ -374,7 +381,10 @@ static int histogram_impl(const lm_tables *t, const uint32_t *w, long long n, lo
           continue;
         }
         if ((doia == 1 || doia == 0) && (doib == 1 || doib == 0) && ccounts) {
-          /* the coincidence histogram (hist:1212-1223) */
+          /* the coincidence histogram (hist:1212-1223), with a crystal row
+           * NHEADS * NXCRYS wide as in histogram_mp_fromarchive.cpp:916,
+           * :1092-1096 (the rewrite's row of NUM_CRYSTALS_X_Y, hist:1049,
+           * indexes past the map it allocates) */
           uint32_t *cc = ccounts + (type ? NXCRYS * NYCRYS * NHEADS * NDOIS : 0);
           cc[doia * NXCRYS * NYCRYS * NHEADS + HRRT_MPAIRS[mpe][0] * NXCRYS + ax + ay * NXCRYS * NHEADS]++;
           cc[doib * NXCRYS * NYCRYS * NHEADS + HRRT_MPAIRS[mpe][1] * NXCRYS + bx + by * NXCRYS * NHEADS]++;

@@ -72,6 +72,8 @@ void lm_get_crystals(const lm_tables *t, float *xyz /* [8][2][72][104][3] */);
 double lm_d_tan_theta(const lm_tables *t);
 /* rebin_event: sinogram address of one coincidence or -1 */
 int lm_rebin_event(const lm_tables *t, int mp, int alayer, int ax, int ay, int blayer, int bx, int by);
+/* the same for n rows (mp, alayer, ax, ay, blayer, bx, by) of ev */
+void lm_rebin_events(const lm_tables *t, long long n, const int32_t *ev, int32_t *addr);
 
 void lm_clock_init(lm_clock *c);
 /* histogram one frame of the word stream (32-bit words, little-endian pairs

@@ -3,8 +3,8 @@
 TEST INFRASTRUCTURE.  Only tests/, __graft_entry__.smoke() and bench.py (its
 reference arm and cpu_baseline leg) use this module, as the checker / CPU
 baseline.  The library is built by oracle/Makefile from the unmodified
-reference sources (hrrt_osem3d/hrrt_osem3dv_sbrt_span3.cpp, nr_utils.cpp) plus
-oracle/ref_harness.cpp, and travels prebuilt.
+reference sources (hrrt_osem3d/hrrt_osem3dv_sbrt_span3.cpp, nr_utils.cpp,
+psf.cpp, scanner_model.cpp) plus oracle/ref_harness.cpp, and travels prebuilt.
 """
 import ctypes
 import os
@@ -48,6 +48,10 @@ def lib():
         L.ref_get_tantheta.argtypes = [vp, vp]
         L.ref_get_flookup.argtypes = [vp, vp]
         L.ref_get_blookup.argtypes = [vp, vp, vp, vp]
+        L.ref_psf_setup.argtypes = [f, f, f, vp, i]
+        L.ref_psf_setup.restype = i
+        L.ref_psf_convolve.argtypes = [vp, vp]
+        L.ref_psf_convolve.restype = i
         L.ref_set_norm_zero_mask.argtypes = [vp]
         L.ref_get_norm_zero_mask.argtypes = [vp]
         _L = L
@@ -188,6 +192,23 @@ class RefProjector:
         f = np.zeros((self.nx, self.groupmax), np.float32)
         self.L.ref_get_blookup(_p(a[0]), _p(a[1]), _p(a[2]), _p(f))
         return a[0], a[1], a[2], f
+
+    def set_psf(self, fwhm1=0.0, fwhm2=0.0, ratio=0.0):
+        """-B fwhm1,fwhm2,ratio: the x/y/z kernels of make1d_psf_filter
+        (psf.cpp:21-70) for this geometry's voxel sizes; returns the x taps."""
+        taps = np.zeros(256, np.float32)
+        n = self.L.ref_psf_setup(fwhm1, fwhm2, ratio, _p(taps), taps.size)
+        if n < 1:
+            raise ValueError("make1d_psf_filter refused these parameters")
+        return taps[:n].copy()
+
+    def psf(self, image):
+        """convolve3d (psf.cpp:463-540) of an [x][y][zp] image (set_psf first)."""
+        im = np.ascontiguousarray(image, np.float32)
+        out = np.zeros(self.image_shape, np.float32)
+        if self.L.ref_psf_convolve(_p(im), _p(out)) != 0:
+            raise RuntimeError("ref_psf_convolve")
+        return out
 
     def set_norm_zero_mask(self, mask):
         m = np.ascontiguousarray(mask, np.int16)

@@ -2,8 +2,9 @@
  * ref_harness.cpp -- drives the reference's own projector code.
  *
  * TEST INFRASTRUCTURE.  oracle/Makefile compiles this file together with the
- * UNMODIFIED reference sources hrrt_osem3d/hrrt_osem3dv_sbrt_span3.cpp and
- * hrrt_osem3d/nr_utils.cpp into oracle/_ref/libhrrt_ref.so.  Only tests/,
+ * UNMODIFIED reference sources hrrt_osem3d/hrrt_osem3dv_sbrt_span3.cpp,
+ * hrrt_osem3d/nr_utils.cpp, hrrt_osem3d/psf.cpp and hrrt_osem3d/scanner_model.cpp
+ * into oracle/_ref/libhrrt_ref.so.  Only tests/,
  * __graft_entry__.smoke() and bench.py (its reference arm and cpu_baseline)
  * load that library, and only as the checker / CPU baseline.
  *
@@ -26,6 +27,11 @@
 
 #include "hrrt_osem3d.h"
 #include "nr_utils.h"
+#include "scanner_model.h"
+
+/* psf.cpp */
+int make1d_psf_filter(Psf1D *psf);
+void convolve3d(float ***image, float ***out, float ***buf);
 
 /* ---- globals the driver defines (hrrt_osem3d_span3.cpp:150-260) ---- */
 int nthreads = 1;
@@ -40,6 +46,8 @@ float zoom = 1.0f, newzoom = 1.0f;
 float rel_fov = 0.95f;
 int max_g = -1;
 int **vieworder = NULL;
+/* PSF kernels of -B (hrrt_osem3d_span3.cpp:454-456) */
+Psf1D *psfx = NULL, *psfy = NULL, *psfz = NULL;
 
 /* allocator hooks the reference's local mm_malloc.h declares */
 void *_mm_malloc(size_t size, size_t align) {
@@ -463,6 +471,55 @@ int ref_osem_subset(float *image, float *corr, const float *nf_inv_subset, const
 }
 
 /* post-iteration pass (drv:4288-4297): FOV, z in [z_min,z_max) */
+/*
+ * -B fwhm1,fwhm2,ratio: the three 1-D kernels as the driver builds them
+ * (hrrt_osem3d_span3.cpp:4521-4540: Gaussian shape, the HRRT scanner model
+ * for fwhm1 = 0 defaults, pixel sizes x_size, y_size, z_size) with the
+ * reference's make1d_psf_filter.  Copies the x kernel's taps into `taps`
+ * (up to cap) and returns their number, or -1.  ref_init first.
+ */
+int ref_psf_setup(float fwhm1, float fwhm2, float ratio, float *taps, int cap) {
+  if (!g_ready) return -1;
+  Psf1D **k[3] = {&psfx, &psfy, &psfz};
+  const float px[3] = {x_size, y_size, z_size};
+  for (int i = 0; i < 3; i++) {
+    if (*k[i]) {
+      free((*k[i])->kernel);
+      free(*k[i]);
+    }
+    Psf1D *p = (Psf1D *)malloc(sizeof(Psf1D));
+    p->kernel = NULL;
+    p->fwhm1 = fwhm1;
+    p->fwhm2 = fwhm2;
+    p->ratio = ratio;
+    p->model = scanner_model(999);
+    p->type = GaussShape;
+    p->pixel_size = px[i];
+    if (make1d_psf_filter(p) != 0) return -1;
+    *k[i] = p;
+  }
+  const int n = psfx->kernel_size < cap ? psfx->kernel_size : cap;
+  memcpy(taps, psfx->kernel, sizeof(float) * n);
+  return psfx->kernel_size;
+}
+
+/* convolve3d (psf.cpp:463-540) of an [x][y][zp] image with the kernels of
+ * ref_psf_setup, on the reference's own threads. */
+int ref_psf_convolve(const float *in, float *out) {
+  if (!g_ready || !psfx) return -1;
+  size_t vol = (size_t)x_pixels * y_pixels * g_zp;
+  std::vector<float> src(in, in + vol), buf(vol, 0.f);
+  memset(out, 0, sizeof(float) * vol);
+  float ***a = cube_ptrs(src.data(), x_pixels, y_pixels, g_zp);
+  float ***o = cube_ptrs(out, x_pixels, y_pixels, g_zp);
+  float ***b = cube_ptrs(buf.data(), x_pixels, y_pixels, g_zp);
+  convolve3d(a, o, b);
+  free_cube_ptrs(a);
+  free_cube_ptrs(o);
+  free_cube_ptrs(b);
+  return 0;
+}
+
 double ref_post_iteration(float *image, int zmin, int zmax) {
   double sum = 0;  /* the reference accumulates in a float global */
   float sumf = 0.f;

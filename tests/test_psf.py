@@ -1,7 +1,8 @@
 """PSF resolution modelling (-B; psf.cpp).
 
 CPU: the library's make1d_psf_filter taps (host code) are bit-identical to the
-restatement in oracle/hrrt_oracle.c.  GPU: convolve3d on the device is
+restatement in oracle/hrrt_oracle.c and to the reference's own psf.cpp, whose
+convolve3d the restatement's single-precision build equals bit for bit.  GPU: convolve3d on the device is
 bit-identical to the oracle's single-precision build on every test geometry
 (same taps, same sum order, no fused multiply-adds); the sensitivity images and
 one subset with PSF are within 2e-6 / 1e-5 of the FP64 oracle (as without PSF);
@@ -44,6 +45,41 @@ def test_psf_default_is_the_hrrt_kernel():
     import hrrt_reconstruction_b200 as H
     k = H.psf_kernel()
     assert k.size == 13 and int(np.argmax(k)) == 6 and np.allclose(k, k[::-1])
+
+
+@pytest.mark.parametrize("params", PARAMS)
+@pytest.mark.parametrize("name", ["small3", "hrrt9"])
+def test_psf_equals_reference(ref_lib, name, params):
+    """The reference's own make1d_psf_filter and convolve3d (psf.cpp compiled
+    unmodified into oracle/_ref/libhrrt_ref.so, kernels set up as
+    hrrt_osem3d_span3.cpp:4521-4540 does) against the restatement's taps and
+    single-precision convolve3d and the library's host taps, bit for bit."""
+    import hrrt_reconstruction_b200 as H
+    from oracle.oracle import Oracle
+    d = ALL[name]
+    R = ref_lib.RefProjector(nthreads=4, **d)
+    taps = R.set_psf(*params)
+    assert np.array_equal(taps.view(np.uint32), H.psf_kernel(*params, pixel_size=d["binsize"]).view(np.uint32))
+    O = Oracle(precision="f32", **d)
+    assert np.array_equal(taps.view(np.uint32), O.psf_kernel(*params, pixel_size=d["binsize"]).view(np.uint32))
+    O.set_psf(True, *params)
+    x = random_image(O.image_shape, O.cylwiny(), seed=33, zvalid=O.nz)
+    assert np.array_equal(R.psf(x).view(np.uint32), O.psf(x).view(np.uint32))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("params", PARAMS[:2])
+def test_psf_convolve_equals_reference_on_device(ref_lib, params):
+    """hrrt_psf_convolve against the reference's convolve3d, HRRT span 9."""
+    import hrrt_reconstruction_b200 as H
+    d = ALL["hrrt9"]
+    R = ref_lib.RefProjector(nthreads=8, **d)
+    R.set_psf(*params)
+    with H.Context(product_geom(d)) as ctx:
+        ctx.set_psf(True, *params)
+        x = random_image(ctx.image_shape, R.cylwiny(), seed=34, zvalid=R.nz)
+        got = ctx.psf(x)
+    assert np.array_equal(got.view(np.uint32), R.psf(x).view(np.uint32))
 
 
 @pytest.mark.gpu

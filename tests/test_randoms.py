@@ -1,8 +1,9 @@
 """Smoothed randoms from a coincidence histogram (gen_delays).
 
 CPU: the crystal-singles estimate of the library (host code, hrrt_lm_crystal_singles)
-is bit-identical to the restatement in oracle/lm_oracle.c and recovers the singles
-rates that generated the delayed counts.  GPU: hrrt_lm_smooth_randoms against the
+is bit-identical to the restatement in oracle/lm_oracle.c and to the reference's
+own compute_csings_from_drates, and recovers the singles rates that generated the
+delayed counts.  GPU: hrrt_lm_smooth_randoms against the
 oracle's compute_delays restatement (float sums in another order: rel-L2 <= 1e-6),
 and the command line with -d pointing at a .ch file."""
 import os
@@ -48,6 +49,29 @@ def test_crystal_singles_match_oracle_and_model():
     live = s > 0
     rel = np.abs(got[live] - s[live]) / s[live]
     assert np.median(rel) < 1e-2, np.median(rel)
+
+
+@pytest.mark.parametrize("seed,duration,live,noise", [(1, 60.0, 1.0, False), (2, 300.0, 0.97, True)])
+def test_crystal_singles_equal_reference(seed, duration, live, noise):
+    """The reference's own compute_csings_from_drates (gen_delays_lib.cpp
+    compiled unmodified into oracle/_ref/lmhist_ref) against the restatement
+    and the library's host estimate, bit for bit, iterations included;
+    Poisson-noisy counts make the estimator iterate."""
+    import hrrt_reconstruction_b200 as H
+    from oracle import lm_ref
+    if not lm_ref.available():
+        pytest.skip("oracle/_ref/lmhist_ref not built")
+    ch, _ = coinc_hist(seed, duration, live)
+    d = ch[NC:]
+    if noise:
+        d = np.random.default_rng(seed).poisson(d).astype(np.int32)
+    want, it = lm_ref.crystal_singles(d, duration, TAU)
+    got, it_o = lm.crystal_singles(d, duration, TAU)
+    assert it_o == it and np.array_equal(np.asarray(got, np.float32).view(np.uint32), want.view(np.uint32))
+    lib, it_l = H.crystal_singles(d, duration, TAU)
+    assert it_l == it and np.array_equal(np.asarray(lib, np.float32).view(np.uint32), want.view(np.uint32))
+    if noise:
+        assert it > 1
 
 
 def test_crystal_singles_dead_crystals_and_defaults():
