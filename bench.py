@@ -390,6 +390,7 @@ def run_ours(args, ws, rank, local):
         out["storage16"] = run_storage16(args, torch, H, ctx, st, host, names, img, cs, dist, local, ws, ms)
         out["storage_f16"] = run_storage16(args, torch, H, ctx, st, host, names, img, cs, dist, local, ws, ms,
                                            storage=H.STORE_F16)
+    out["adjoint"] = run_adjoint(args, torch, H, ctx, cs, dist, local, ws, ms)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     if rank == 0 and ws == 1 and args.parity:
@@ -487,6 +488,53 @@ def run_parity_span9(H, local):
     with H.Context(H.hrrt_geometry(**dict(geom_dict(), span=9)), device=local) as c9:
         st = phantom.study(c9, **kw)
         return run_parity(H, c9, st, 1, kw)
+
+
+def run_adjoint(args, torch, H, ctx, cs, dist, local, ws, ms_ref):
+    """The same device-resident subsets with the exact adjoint of the forward
+    projector as the back projector (hrrt_set_backprojector(HRRT_BP_ADJOINT)):
+    subset-iterations/s and each kernel's CUDA-event time, the adjoint pair
+    against HBM with its algorithmic bytes (partial sums written and read
+    back: the z-transpose reads the ratio (4 B/bin) and writes the column and
+    row partials of every pair (2 volumes); the bilinear transpose reads them
+    and reads/writes the image and reads the inverse sensitivity (2 x pairs +
+    3 volumes)).  The back projector is set back to the reference's after."""
+    ctx.set_backprojector(H.BP_ADJOINT)
+    ctx.sensitivity()
+    ctx.init_image()
+    ctx.osem_subsets(0, args.warmup)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    barrier(dist, local)
+    torch.cuda.synchronize()
+    ctx.reset_kernel_stats()
+    ctx.set_profiling(True)
+    ev[0].record(cs)
+    ctx.osem_subsets(args.warmup, args.steps)
+    ev[1].record(cs)
+    torch.cuda.synchronize()
+    ctx.set_profiling(False)
+    ms = max_over_ranks(dist, ev[0].elapsed_time(ev[1]), local)
+    ks = {k: ctx.kernel_stats(k) for k in ("fp_kernel", "adj_kernel", "adj_rotate_kernel")}
+    info = ctx.info
+    pairs = info.sviews // 2
+    bins = pairs * 2 * info.segmentsize * info.nbins
+    vol = info.nx * info.ny * info.zp * 4
+    algo = {"adj_kernel": bins * 4 + 2 * pairs * vol, "adj_rotate_kernel": 2 * pairs * vol + 3 * vol}
+    peak, _ = measured_peaks()
+    kern = {}
+    for k, (n, tot) in ks.items():
+        d = {"launches": n, "ms_total": tot, "ms_avg": tot / max(n, 1)}
+        if k in algo and n:
+            gbs = algo[k] / (tot / n / 1e3) / 1e9
+            d.update({"bytes_per_launch": algo[k], "achieved_gbs": gbs, "frac_hbm": gbs / peak})
+        kern[k] = d
+    ctx.set_backprojector(H.BP_REF)
+    ctx.sensitivity()
+    return {"value": ws * args.steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / args.steps,
+            "vs_reference_backprojector": ms_ref / ms, "kernels": kern,
+            "note": "exact adjoint of the forward projector (dot-product test to 1e-6 in tests/test_adjoint_gpu.py); "
+                    "same study and steps as the headline"}
 
 
 # Dynamic study: 24 span-9 frames of the config-0 phantom, sphere activity

@@ -26,11 +26,16 @@ namespace hrrt {
 #ifndef HRRT_FP_SLOTS
 #define HRRT_FP_SLOTS 3
 #endif
+#ifndef HRRT_FP_ROWS_MAX
+#define HRRT_FP_ROWS_MAX 8
+#endif
 #ifndef HRRT_BP_MIN_BLOCKS
 #define HRRT_BP_MIN_BLOCKS 3
 #endif
 constexpr int kFpPlanes = 9;                   // default planes per forward-projection task (odd: bank-conflict free)
-constexpr int kFpSlots = HRRT_FP_SLOTS;       // sampled rows in flight between producers and consumers
+constexpr int kFpSlots = HRRT_FP_SLOTS;       // rows whose corner columns are being copied in
+constexpr int kFpRowsMin = 3;                 // sampled rows in the ring between producers and consumers: at least
+constexpr int kFpRowsMax = HRRT_FP_ROWS_MAX;  // ... and at most (the launch picks the deepest that keeps its occupancy)
 constexpr int kFpZPad = 16;     // zeroed entries after each sampled row
 constexpr int kFpEndPlanes = 4; // planes per end-plane task (they cost ~2x a middle plane)
 constexpr int kFpMaxGroups = 32; // segment groups the forward projector stages per row (22 at span 3)
