@@ -688,6 +688,7 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
   d.eps1 = g.sp.epsilon1;
   d.eps3 = g.sp.epsilon3;
   d.image_max = g.sp.image_max;
+  d.unit = 1.0f;
   d.cyl0 = dupload(ctx, g.cyl0, &e);
   d.cyl1 = dupload(ctx, g.cyl1, &e);
   d.ybot = dupload(ctx, g.yr_bottom, &e);

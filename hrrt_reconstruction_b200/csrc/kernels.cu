@@ -6,11 +6,9 @@
 // bit-identical to the reference on the same inputs.
 #include "kernels.cuh"
 
-#include <cfloat>
-#include <map>
-#include <mutex>
-#include <tuple>
 #include <type_traits>
+
+#include <cfloat>
 
 namespace hrrt {
 
@@ -104,13 +102,17 @@ __device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
   return r;
 }
-// a + p where p is a packed product: done as two scalar adds.  The code
-// generator contracts a packed multiply that feeds a packed add into a fused
-// multiply-add (which rounds once instead of twice), even with -fmad=false and
-// explicit .rn; a scalar add of the product's halves is left alone.
-__device__ __forceinline__ uint64_t addp(uint64_t a, uint64_t p) {
-  const float2 x = upk(a), y = upk(p);
-  return pk(__fadd_rn(x.x, y.x), __fadd_rn(x.y, y.y));
+// a + p where p is a packed product.  The code generator contracts a packed
+// multiply that feeds a packed add into a fused multiply-add (which rounds once
+// instead of twice), even with -fmad=false and explicit .rn, and folds a
+// multiply by a literal 1 away; a packed fused multiply-add of p by a run-time
+// (1, 1) and a cannot absorb p's multiply and rounds p + a once, as the
+// reference's add does (measured bit-identical on B200; two scalar adds, the
+// alternative, cost one more instruction per pair).
+__device__ __forceinline__ uint64_t addp(uint64_t a, uint64_t p, uint64_t one) {
+  uint64_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(p), "l"(one), "l"(a));
+  return r;
 }
 __device__ __forceinline__ Q2 ldq(const float4 *p) {
   const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(p);
@@ -119,7 +121,7 @@ __device__ __forceinline__ Q2 ldq(const float4 *p) {
 __device__ __forceinline__ Q2 qadd(Q2 a, Q2 b) { return Q2{add2(a.lo, b.lo), add2(a.hi, b.hi)}; }
 __device__ __forceinline__ Q2 qsub(Q2 a, Q2 b) { return Q2{sub2(a.lo, b.lo), sub2(a.hi, b.hi)}; }
 __device__ __forceinline__ Q2 qmul(Q2 a, uint64_t s) { return Q2{mul2(a.lo, s), mul2(a.hi, s)}; }
-__device__ __forceinline__ Q2 qaddp(Q2 a, Q2 p) { return Q2{addp(a.lo, p.lo), addp(a.hi, p.hi)}; }
+__device__ __forceinline__ Q2 qaddp(Q2 a, Q2 p, uint64_t one) { return Q2{addp(a.lo, p.lo, one), addp(a.hi, p.hi, one)}; }
 __device__ __forceinline__ float4 q2f(Q2 q) {
   const float2 a = upk(q.lo), b = upk(q.hi);
   return make_float4(a.x, a.y, b.x, b.y);
@@ -163,29 +165,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
   }
   if (err) atomicExch(err, 1);
   return false;
-}
-
-// bounded wait that also gives up once another thread of the CTA has given up
-// (*abort set): a CTA whose pipeline stalled drains without every thread
-// spending the whole bound on every later phase
-__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t *bar, uint32_t parity, int *err, volatile int *abort) {
-  const uint32_t a = smem_u32(bar);
-  for (int i = 0; i < (1 << 22); i++) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (ok) return true;
-    if ((i & 255) == 255 && *abort) return false;
-  }
-  if (err) atomicExch(err, 1);
-  *abort = 1;
-  return false;
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // Rotated-grid sample point (sbrt:1866-1871): position of rotated-frame voxel
@@ -238,45 +217,82 @@ __device__ __forceinline__ float bilinear(const float *__restrict__ img, const S
 // (y,N-x)), then every thread accumulates its own (segment, plane-run) outputs
 // for all four lanes, row by row in the reference's order.
 // ============================================================================
-// named barrier among the producer warps (id 0 is __syncthreads); the id is
-// an immediate so the kernel reserves only the barrier it uses
+// named barriers (id 0 is __syncthreads); ids are immediates so the kernel
+// reserves only the barriers it uses
 template <int ID>
 __device__ __forceinline__ void bar_sync_id(int count) {
   asm volatile("bar.sync %0, %1;" ::"n"(ID), "r"(count) : "memory");
 }
-constexpr int kBarProd = 1;  // producers only: corner slot read by every producer
+template <int ID>
+__device__ __forceinline__ void bar_arrive_id(int count) {
+  asm volatile("bar.arrive %0, %1;" ::"n"(ID), "r"(count) : "memory");
+}
+// named barriers with immediate ids (a register id reserves all 16)
+__device__ __forceinline__ void bar_sync(int id, int count) {
+  switch (id) {
+    case 1: bar_sync_id<1>(count); break;
+    case 2: bar_sync_id<2>(count); break;
+    case 3: bar_sync_id<3>(count); break;
+    case 4: bar_sync_id<4>(count); break;
+    case 5: bar_sync_id<5>(count); break;
+    case 6: bar_sync_id<6>(count); break;
+    case 7: bar_sync_id<7>(count); break;
+    case 8: bar_sync_id<8>(count); break;
+    case 9: bar_sync_id<9>(count); break;
+    case 10: bar_sync_id<10>(count); break;
+    case 11: bar_sync_id<11>(count); break;
+    case 12: bar_sync_id<12>(count); break;
+    default: bar_sync_id<13>(count); break;
+  }
+}
+__device__ __forceinline__ void bar_arrive(int id, int count) {
+  switch (id) {
+    case 1: bar_arrive_id<1>(count); break;
+    case 2: bar_arrive_id<2>(count); break;
+    case 3: bar_arrive_id<3>(count); break;
+    case 4: bar_arrive_id<4>(count); break;
+    case 5: bar_arrive_id<5>(count); break;
+    case 6: bar_arrive_id<6>(count); break;
+    case 7: bar_arrive_id<7>(count); break;
+    case 8: bar_arrive_id<8>(count); break;
+    case 9: bar_arrive_id<9>(count); break;
+    case 10: bar_arrive_id<10>(count); break;
+    case 11: bar_arrive_id<11>(count); break;
+    default: bar_arrive_id<12>(count); break;
+  }
+}
+constexpr int kBarFull = 1;                 // + slot: sampled row ready (producers arrive, consumers wait)
+constexpr int kBarEmpty = 1 + kFpSlots;     // + slot: sampled row consumed (consumers arrive, producers wait)
+constexpr int kBarProd = 1 + 2 * kFpSlots;  // producers only: corner slot read by every producer
+static_assert(kBarProd <= 13, "named barrier ids");
 
 template <int MODE, int PL, int MW, typename PT, typename AT>
 __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *__restrict__ image,
                                                      const QuadWork *__restrict__ work,
                                                      const PT *__restrict__ prompts, const AT *__restrict__ add,
                                                      float4 *__restrict__ out, long long out_pair_stride,
-                                                     int nprod_warps, int nring, FrameStrides fr) {
+                                                     int nprod_warps, FrameStrides fr) {
   // shared memory: [S slots][8 points][2 column pairs][2*zp] staged corner
-  // columns, 2*cpair zeros (the corners of outside points), [R][2 halves][ZS]
-  // sampled rows, [ZS] centre column, [R + S][groupmax] middle-plane sampling
-  // entries (S = kFpSlots corner slots, R = nring row slots)
+  // columns, 2*cpair zeros (the corners of outside points), [S slots][2 halves]
+  // [ZS] sampled rows, [ZS] centre column (S = kFpSlots)
+  const uint64_t one = pk(g.unit, g.unit);
   extern __shared__ float4 smem[];
   const int ZS = g.zp + kFpZPad;
   const int zp = g.zp;
   const int cpair = 2 * zp;  // floats per column pair
-  const int G = g.groupmax;
-  const int nmid = nring + kFpSlots;
   float *corners = reinterpret_cast<float *>(smem);
   const int zoff = kFpSlots * 8 * 2 * cpair;
   float *zcol = corners + zoff;
-  float4 *rows = smem + (size_t)(kFpSlots * 8 * 2 + 2) * cpair / 4;  // [R][2][ZS]
-  float4 *cen = rows + 2 * nring * ZS;
-  // each row's middle-plane sampling entries (z, f, z2, f2 per group),
-  // copied in with the row's columns: the entries of row r + S arrive while
-  // the consumers may still read those of rows r - R + 1 .. r
-  FpMid *s_mid = reinterpret_cast<FpMid *>(cen + ZS);  // [R + S][G]
+  float4 *rows = smem + (size_t)(kFpSlots * 8 * 2 + 2) * cpair / 4;  // [S][2][ZS]
+  float4 *cen = rows + 2 * kFpSlots * ZS;
   __shared__ ulonglong2 s_w[kFpSlots][4][2];
   __shared__ int s_off[kFpSlots][8];
-  __shared__ __align__(8) uint64_t s_bar[kFpSlots];     // corner columns of a row landed
-  __shared__ __align__(8) uint64_t s_full[kFpRowsMax];  // sampled row ready (every producer thread arrives)
-  __shared__ __align__(8) uint64_t s_empty[kFpRowsMax]; // sampled row consumed (every consumer warp arrives)
-  __shared__ int s_abort;                               // a bounded wait gave up: the results are void
+  // each row's middle-plane sampling entries (z, f, z2, f2 per group),
+  // copied in with the row's columns.  Twice as many slots as rows in flight:
+  // the entries of row r + S arrive while the consumers may still read those
+  // of rows r - S + 1 .. r.  (3 KB: two CTAs per SM still fit at span 9.)
+  __shared__ __align__(16) FpMid s_mid[2 * kFpSlots][kFpMaxGroups];
+  __shared__ __align__(8) uint64_t s_bar[kFpSlots];
 
   const int nwork = gridDim.x / fr.n, frame = blockIdx.x / nwork, item = blockIdx.x - frame * nwork;
   const QuadWork w = work[item];
@@ -325,13 +341,13 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
     // outside points read the zero column pairs
     s_off[sl][l] = inside ? (sl * 8 + l) * 2 * cpair : zoff;
     const unsigned m = __ballot_sync(0xffu, inside);
-    const int es = r % nmid;
+    const int G = g.groupmax, es = r % (2 * kFpSlots);
     if (l == 0) {
       fence_proxy_async();
       mbar_arrive_tx(&s_bar[sl], (uint32_t)__popc(m) * 2u * cpair * 4u + (uint32_t)G * 16u);
     }
     __syncwarp(0xffu);
-    if (l == 0) bulk_g2s(s_mid + (size_t)es * G, g.fpmid + (size_t)y * G, (uint32_t)G * 16u, &s_bar[sl]);
+    if (l == 0) bulk_g2s(&s_mid[es][0], g.fpmid + (size_t)y * G, (uint32_t)G * 16u, &s_bar[sl]);
     if (inside) {
       float *dst = corners + ((size_t)(sl * 8 + l) * 2) * cpair;
       bulk_g2s(dst, image + pt.base, cpair * 4u, &s_bar[sl]);
@@ -342,25 +358,17 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
   if (tid == 0) {
 #pragma unroll
     for (int s = 0; s < kFpSlots; s++) mbar_init(&s_bar[s], 1);
-    for (int s = 0; s < nring; s++) {
-      mbar_init(&s_full[s], (uint32_t)nprod);
-      mbar_init(&s_empty[s], (uint32_t)(ncons / 32));
-    }
-    s_abort = 0;
     fence_mbar_init();
   }
-  for (int i = tid; i < (2 * nring + 1) * kFpZPad; i += nthr) {
+  for (int i = tid; i < (2 * kFpSlots + 1) * kFpZPad; i += nthr) {
     const int col = i / kFpZPad, k = i % kFpZPad;
     rows[col * ZS + zp + k] = f4(0.f);
   }
   for (int i = tid; i < 2 * cpair; i += nthr) zcol[i] = 0.f;
   __syncthreads();
-  // copies issued by the first producer warp, through row `hi`
-  int hi = -1;
   if (producer && ptid < 8) {
     for (int r = 0; r < kFpSlots && r < nrows; r++) issue_row(r);
   }
-  if (producer && ptid < 32) hi = min(kFpSlots, nrows) - 1;
 
   // centre column y = c (sbrt:1815-1853): lanes (x,c),(N-x,c),(c,x),(c,N-x)
   {
@@ -378,26 +386,19 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
   for (int z = zp + tid; z < ZS; z += nthr) cen[z] = f4(0.f);
   __syncthreads();
 
-  volatile int *abort = &s_abort;
+  bool timed_out = false;
   if (producer) {
-    // ---------------- producers: bilinear samples into the row ring ----------------
-    // Row r waits for its corner copies (slot r % S, issued S rows ahead) and
-    // for the consumers to release row slot r % R (row r - R), is sampled,
-    // and is announced on s_full; the producers then refill the corner slot
-    // with row r + S.  Nothing waits without a bound: after a wait gives up
-    // every later wait returns at once and the results are void.
+    // ---------------- producers: bilinear samples, kFpSlots rows ahead ----------------
     const int hsplit = nprod / 2;
     const int h_mine = ptid >= hsplit, z_mine = ptid - h_mine * hsplit;
-    int lastw = -1;  // last row whose copies this thread saw land
     for (int r = 0; r < nrows; r++) {
-      const int sl = r % kFpSlots, rs = r % nring;
-      bool ok = mbar_wait_or_abort(&s_bar[sl], (uint32_t)((r / kFpSlots) & 1), g.err, abort);
-      if (ok) lastw = r;
-      if (ok && r >= nring) ok = mbar_wait_or_abort(&s_empty[rs], (uint32_t)(((r / nring) - 1) & 1), g.err, abort);
-      if (ok) {
+      const int sl = r % kFpSlots;
+      if (!mbar_wait(&s_bar[sl], (uint32_t)((r / kFpSlots) & 1), g.err)) timed_out = true;
+      if (r >= kFpSlots) bar_sync(kBarEmpty + sl, nthr);  // consumers are done with row r-S
+      {
         // lanes (0,1) and (2,3) of this half share nothing but the plane: each
         // lane pair is evaluated with packed pairs, its weights pre-packed
-        float4 *rw = rows + (size_t)rs * 2 * ZS + h_mine * ZS;
+        float4 *rw = rows + (size_t)sl * 2 * ZS + h_mine * ZS;
         for (int z = z_mine; z < zp; z += hsplit) {
           uint64_t vv[2];
 #pragma unroll
@@ -408,24 +409,20 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
             // corner order of the reference: r1 (ix,iy), r2 (ix+1,iy), r3 (ix,iy+1), r4 (ix+1,iy+1)
             const uint64_t r1 = pk(qa[z], qb[z]), r2 = pk(qa[cpair + z], qb[cpair + z]);
             const uint64_t r3 = pk(qa[zp + z], qb[zp + z]), r4 = pk(qa[cpair + zp + z], qb[cpair + zp + z]);
-            vv[pp] = add2(addp(mul2(r1, wa.x), mul2(r2, wa.y)), addp(mul2(r3, wb.x), mul2(r4, wb.y)));
+            vv[pp] = add2(addp(mul2(r1, wa.x), mul2(r2, wa.y), one), addp(mul2(r3, wb.x), mul2(r4, wb.y), one));
           }
           *reinterpret_cast<ulonglong2 *>(rw + z) = make_ulonglong2(vv[0], vv[1]);
         }
       }
-      mbar_arrive(&s_full[rs]);
+      bar_arrive(kBarFull + sl, nthr);
       // every producer has finished reading corner slot sl: refill it with row r+S
-      bar_sync_id<kBarProd>(nprod);
-      if (ptid < 32) {
-        const bool go = __shfl_sync(0xffffffffu, *abort == 0, 0) && r + kFpSlots < nrows;
-        if (go && ptid < 8) issue_row(r + kFpSlots);
-        if (go) hi = r + kFpSlots;
-      }
+      bar_sync(kBarProd, nprod);
+      if (ptid < 8 && r + kFpSlots < nrows) issue_row(r + kFpSlots);
     }
-    if (ptid < 32 && *abort) {
+    if (timed_out) {
       // results are void (the host reports the status word); give copies
       // still in flight a bounded chance to land before the CTA exits
-      for (int r = max(lastw + 1, hi - kFpSlots + 1); r <= hi; r++)
+      for (int r = max(0, nrows - kFpSlots); r < nrows; r++)
         mbar_wait(&s_bar[r % kFpSlots], (uint32_t)((r / kFpSlots) & 1), nullptr);
     }
     return;
@@ -449,18 +446,16 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
   const int li0 = gg * 2 * g.zshift + ((tk.p0 < g.zshift) ? tk.p0 : tk.p0 - ns_t + 2 * g.zshift);
   const int FS = g.groupmax * 2 * g.zshift;
   for (int r = 0; r < nrows; r++) {
-    const int rs = r % nring, es = r % nmid, y = ystart + r;
-    const bool ok = mbar_wait_or_abort(&s_full[rs], (uint32_t)((r / nring) & 1), g.err, abort);
-    const float4 *pam = rows + (size_t)rs * 2 * ZS;
+    const int sl = r % kFpSlots, es = r % (2 * kFpSlots), y = ystart + r;
+    bar_sync(kBarFull + sl, nthr);
+    const float4 *pam = rows + (size_t)sl * 2 * ZS;
     const float4 *pam2 = pam + ZS;
-    if (!ok) {
-      // the pipeline stalled: the results are void
-    } else if (tk.type == 0) {
+    if (tk.type == 0) {
       // theta = 0 (sbrt:1907-1910)
 #pragma unroll
       for (int j = 0; j < PL; j++) acc[j] = qadd(acc[j], qadd(ldq(pam + tk.p0 + j), ldq(pam2 + tk.p0 + j)));
     } else if (tk.type > 0) {
-      const FpMid m = s_mid[(size_t)es * G + gs];
+      const FpMid m = s_mid[es][gs];
       if (m.z >= 0) {  // else the group is skipped for this row (sbrt:1923-1924)
         // segment 2k accumulates pam at z and pam2 at z2; segment 2k-1 the converse
         const float4 *A = odd ? pam2 : pam;
@@ -473,7 +468,7 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
 #pragma unroll
           for (int j = 0; j < PL; j++) {
             const Q2 a1 = ldq(Aw + j + 1), b1 = ldq(Bw + j + 1);
-            acc[j] = qadd(acc[j], qaddp(qmul(qadd(b1, a0), f2), qmul(qadd(a1, b0), f)));
+            acc[j] = qadd(acc[j], qaddp(qmul(qadd(b1, a0), f2), qmul(qadd(a1, b0), f), one));
             a0 = a1;
             b0 = b1;
           }
@@ -488,15 +483,13 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
               const float f = __int_as_float(e1.y), f2 = __int_as_float(e2.y);
               const uint64_t ff = pk(f, f), ff2 = pk(f2, f2);
               acc[j] = qadd(acc[j], qaddp(qmul(qadd(ldq(B + z2 + 1), ldq(A + z)), ff2),
-                                          qmul(qadd(ldq(A + z + 1), ldq(B + z2)), ff)));
+                                          qmul(qadd(ldq(A + z + 1), ldq(B + z2)), ff), one));
             }
           }
         }
       }
     }
-    // this warp is done with row slot rs
-    __syncwarp();
-    if ((tid & 31) == 0) mbar_arrive(&s_empty[rs]);
+    if (r + kFpSlots < nrows) bar_arrive(kBarEmpty + sl, nthr);
   }
 
   // scale (sbrt:1953-1975), then either store the estimate or the OP ratio
@@ -556,7 +549,7 @@ __device__ __forceinline__ int bsw(int i) { return i ^ ((i >> 3) & 7); }
 
 template <int KB>
 __device__ __forceinline__ void bp_lerp(Q2 (&s)[KB], const float4 *__restrict__ P, int pbase, const BpLut &bl,
-                                        int z0) {
+                                        int z0, uint64_t one) {
   // windows wholly outside [zs, ze] contribute nothing; a window that
   // straddles an end reads the segment's zero planes for its outside planes
   if (z0 + KB - 1 < bl.zs || z0 > bl.ze) return;
@@ -567,7 +560,7 @@ __device__ __forceinline__ void bp_lerp(Q2 (&s)[KB], const float4 *__restrict__ 
   for (int j = 0; j < KB; j++) {
     const Q2 b = ldq(P + bsw(i0 + j + 1));
     // the reference's p[yr] + f*(p[yr+1]-p[yr]) (sbrt:4312-4315)
-    s[j] = qadd(s[j], qaddp(a, qmul(qsub(b, a), f)));
+    s[j] = qadd(s[j], qaddp(a, qmul(qsub(b, a), f), one));
     a = b;
   }
 }
@@ -595,6 +588,7 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(De
                                                  const QuadWork *__restrict__ work, float *__restrict__ bc,
                                                  float *__restrict__ br, long long vol, FrameStrides fr,
                                                  int view0, int x0, int rlog) {
+  const uint64_t one = pk(g.unit, g.unit);
   extern __shared__ float4 P[];  // [bp_splanes]: segments with kBpPad zero planes each side
   // ACC: one view pair, quads x0 + blockIdx.x, both partial sums added into bc
   // (each voxel receives exactly two terms, so the atomic adds onto a zeroed
@@ -678,8 +672,8 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(De
         const int gn = (gg + 1 < G) ? gg + 1 : gg;
         const BpLut n1 = l1[(size_t)gn * N], n2 = l2[(size_t)gn * N];  // next group, in flight
         // sumt1: segment 2k at +u and 2k-1 at -u; sumt2: the converse
-        bp_lerp<KB>(s, P, half ? po : pe, b1, z0);
-        bp_lerp<KB>(s, P, half ? pe : po, b2, z0);
+        bp_lerp<KB>(s, P, half ? po : pe, b1, z0, one);
+        bp_lerp<KB>(s, P, half ? pe : po, b2, z0, one);
         b1 = n1;
         b2 = n2;
       }
@@ -1252,53 +1246,6 @@ __global__ void scale_pairs_kernel(DevGeom g, const T *__restrict__ src, const i
   dst[(size_t)slot * dst_pair_stride + i] = o;
 }
 
-// dynamic shared memory of the forward projector with a ring of `nring`
-// sampled rows (layout at the top of fp_kernel)
-size_t fp_smem_bytes(const DevGeom &g, int nring) {
-  const int ZS = g.zp + kFpZPad;
-  return (size_t)(kFpSlots * 8 * 2 + 2) * 2 * g.zp * sizeof(float) + (size_t)(2 * nring + 1) * ZS * sizeof(float4) +
-         (size_t)(nring + kFpSlots) * g.groupmax * sizeof(FpMid);
-}
-
-// The deepest row ring (kFpRowsMin..kFpRowsMax) that keeps as many CTAs per
-// SM resident as the shallowest: deeper rings let the consumer warps drift
-// further apart, fewer resident CTAs would cost more than that gains.  The
-// answer depends only on the kernel, its block size and the geometry's sizes,
-// so it is worked out once per combination.
-cudaError_t fp_ring_depth(const void *k, const DevGeom &g, int threads, int *nring) {
-  static std::mutex mu;
-  static std::map<std::tuple<const void *, int, int, int>, int> cache;
-  const auto key = std::make_tuple(k, threads, g.zp, g.groupmax);
-  {
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = cache.find(key);
-    if (it != cache.end()) {
-      *nring = it->second;
-      return cudaSuccess;
-    }
-  }
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)fp_smem_bytes(g, kFpRowsMax));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
-  if (e != cudaSuccess) return e;
-  int best = kFpRowsMin, base = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&base, k, threads, fp_smem_bytes(g, kFpRowsMin));
-  if (e != cudaSuccess) return e;
-  if (base < 1) return cudaErrorInvalidConfiguration;
-  for (int r = kFpRowsMin + 1; r <= kFpRowsMax; r++) {
-    int n = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, threads, fp_smem_bytes(g, r));
-    if (e != cudaSuccess) return e;
-    if (n < base) break;
-    best = r;
-  }
-  std::lock_guard<std::mutex> lk(mu);
-  cache[key] = best;
-  *nring = best;
-  return cudaSuccess;
-}
-
 template <int MODE, int PL, int MW, typename PT, typename AT>
 cudaError_t launch_fp_t(const DevGeom &g, const float *image, const QuadWork *work, int nwork, const void *prompts,
                         const void *add, float *out, long long out_pair_stride, int pwarps_req,
@@ -1309,13 +1256,16 @@ cudaError_t launch_fp_t(const DevGeom &g, const float *image, const QuadWork *wo
   const int pwarps = pwarps_req > 0 ? pwarps_req : min(6, max(2, MW - cwarps));
   if (pwarps < 2 || cwarps + pwarps > MW) return cudaErrorInvalidConfiguration;
   const int threads = (cwarps + pwarps) * 32;
+  const int ZS = g.zp + kFpZPad;
+  const size_t smem =
+      (size_t)(kFpSlots * 8 * 2 + 2) * 2 * g.zp * sizeof(float) + (size_t)(2 * kFpSlots + 1) * ZS * sizeof(float4);
   auto k = fp_kernel<MODE, PL, MW, PT, AT>;
-  int nring = 0;
-  cudaError_t e = fp_ring_depth(reinterpret_cast<const void *>(k), g, threads, &nring);
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
-  k<<<(unsigned)nwork * fr.n, threads, fp_smem_bytes(g, nring), st>>>(
-      g, image, work, (const PT *)prompts, (const AT *)add, reinterpret_cast<float4 *>(out), out_pair_stride / 4,
-      pwarps, nring, fr);
+  k<<<(unsigned)nwork * fr.n, threads, smem, st>>>(g, image, work, (const PT *)prompts, (const AT *)add,
+                                                   reinterpret_cast<float4 *>(out), out_pair_stride / 4, pwarps, fr);
   return cudaGetLastError();
 }
 

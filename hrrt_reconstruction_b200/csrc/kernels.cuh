@@ -26,16 +26,11 @@ namespace hrrt {
 #ifndef HRRT_FP_SLOTS
 #define HRRT_FP_SLOTS 3
 #endif
-#ifndef HRRT_FP_ROWS_MAX
-#define HRRT_FP_ROWS_MAX 8
-#endif
 #ifndef HRRT_BP_MIN_BLOCKS
 #define HRRT_BP_MIN_BLOCKS 3
 #endif
 constexpr int kFpPlanes = 9;                   // default planes per forward-projection task (odd: bank-conflict free)
-constexpr int kFpSlots = HRRT_FP_SLOTS;       // rows whose corner columns are being copied in
-constexpr int kFpRowsMin = 3;                 // sampled rows in the ring between producers and consumers: at least
-constexpr int kFpRowsMax = HRRT_FP_ROWS_MAX;  // ... and at most (the launch picks the deepest that keeps its occupancy)
+constexpr int kFpSlots = HRRT_FP_SLOTS;       // sampled rows in flight between producers and consumers
 constexpr int kFpZPad = 16;     // zeroed entries after each sampled row
 constexpr int kFpEndPlanes = 4; // planes per end-plane task (they cost ~2x a middle plane)
 constexpr int kFpMaxGroups = 32; // segment groups the forward projector stages per row (22 at span 3)
@@ -66,6 +61,7 @@ struct DevGeom {
   int nx, nz, zp, c, nseg, groupmax, zshift, segmentsize, pplanes, nviews, nquads;
   int fov_columns, z_min, z_max;
   float y_size, eps1, eps3, image_max;
+  float unit;                       // 1.0f, a run-time value (see addp in kernels.cu)
   const int16_t *cyl0, *cyl1;       // [ny]
   const int *ybot, *ytop, *poff;    // [nseg]; poff = padded offset of plane yr_bottom
   const float *rescale;             // [groupmax][nz]

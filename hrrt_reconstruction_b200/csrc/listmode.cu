@@ -484,6 +484,9 @@ template <int kEv>
 __device__ __forceinline__ void bump16_events(uint32_t *__restrict__ sino, uint32_t *__restrict__ dly,
                                               const long long (&addr)[kEv], uint32_t live, uint32_t sel,
                                               uint32_t minus) {
+  // a high-half bin's carry leaves the 32-bit word (the sum modulo 2^16 the
+  // bin keeps), so its add returns nothing; only a low-half bin's old value is
+  // needed, to take back a carry into its neighbour
   uint32_t old[kEv];
 #pragma unroll
   for (int k = 0; k < kEv; k++) {
@@ -491,7 +494,10 @@ __device__ __forceinline__ void bump16_events(uint32_t *__restrict__ sino, uint3
     if (!((live >> k) & 1)) continue;
     uint32_t *w = (((sel >> k) & 1) ? dly : sino) + (addr[k] >> 1);
     const uint32_t inc = ((minus >> k) & 1) ? 0xFFFFu : 1u;
-    old[k] = atomicAdd(w, inc << (16 * (uint32_t)(addr[k] & 1)));
+    if (addr[k] & 1)
+      atomicAdd(w, inc << 16);
+    else
+      old[k] = atomicAdd(w, inc);
   }
 #pragma unroll
   for (int k = 0; k < kEv; k++) {
@@ -507,8 +513,11 @@ __device__ __forceinline__ void bump16_events(uint32_t *__restrict__ sino, uint3
 // histogram into 32-bit counters with reductions that return nothing (no
 // carry to check, so no read-modify-write round trip per event), folded into
 // the 16-bit bins afterwards.  Statistics are counted by modes 1, 2 and 4.
+#ifndef HRRT_LM_MIN_BLOCKS
+#define HRRT_LM_MIN_BLOCKS 3  // 4 and 5 (64 and 48 registers, with spills) measured slower on B200
+#endif
 template <int kMode>
-__global__ void __launch_bounds__(kThreads) lm_hist_kernel(
+__global__ void __launch_bounds__(kThreads, HRRT_LM_MIN_BLOCKS) lm_hist_kernel(
     LmDev g, const uint32_t *__restrict__ words, long long n, const uint8_t *__restrict__ tile_entry,
     const unsigned int *__restrict__ tile_tagoff, const unsigned long long *__restrict__ packet_tagoff,
     int tiles_per_packet, long long limit, int mode, int flags, long long tag_cap, longlong2 *__restrict__ tags,
