@@ -539,7 +539,11 @@ def run_adjoint(args, torch, H, ctx, cs, dist, local, ws, ms_ref):
 
 # Dynamic study: 24 span-9 frames of the config-0 phantom, sphere activity
 # varying with time, counts log-uniform in [2e6, 2e8], 1-4 iterations each
-# (seeded), 16-bit-stored inputs, one batch (hrrt_batch_*).
+# (seeded), 16-bit-stored terms, one batch (hrrt_batch_*).  The terms are
+# stored as fp16: bf16 terms (8 bits of mantissa) miss the 1e-3 image bar on
+# the highest-count frames (1.15e-3 against the f32-stored image at 1.86e8
+# counts), fp16 terms (11 bits, range-checked on upload) hold it with 8x
+# margin at the same 2 bytes; bf16's error is still reported.
 DYN = dict(seed=4, counts=(2e6, 2e8), iterations=(1, 4), randoms_frac=0.20)
 
 
@@ -606,7 +610,7 @@ def run_dynamic(args, torch, H, local, dist, ws):
     imgs = [pinned_copy(torch, np.zeros((info.nz, info.ny, info.nx), np.float32)) for _ in range(nf)]
     cs = torch.cuda.ExternalStream(ctx.stream)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-    b = ctx.batch(nf, atten=atten, storage=H.STORE_16)
+    b = ctx.batch(nf, atten=atten, storage=H.STORE_F16)
     # untimed: prepare every frame, tune the launch shapes, capture the graphs
     for f in range(nf):
         b.set_frame(f, host_p[f], host_r[f], iterations=int(iters[f]))
@@ -634,9 +638,9 @@ def run_dynamic(args, torch, H, local, dist, ws):
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(dist, ev[0].elapsed_time(ev[1]), local)
     sums = [b.get_image(f, out=imgs[f])[1] for f in range(nf)]
-    # precision: two frames reconstructed alone with f32-stored inputs (and,
-    # for comparison, with fp16-stored terms)
-    rel, rel16 = {}, {}
+    # precision: two frames reconstructed alone with f32-stored terms (and,
+    # for comparison, with bf16-stored terms)
+    rel, rel_bf16 = {}, {}
 
     def rl2(a, b):
         a = a.astype(np.float64)
@@ -647,12 +651,12 @@ def run_dynamic(args, torch, H, local, dist, ws):
         ctx2 = H.Context(geom, device=local)
         want, _ = ctx2.reconstruct(host_p[f], host_r[f], atten=atten, storage=H.STORE_F32,
                                    iterations=int(iters[f]))
-        f16, _ = ctx2.reconstruct(host_p[f], host_r[f], atten=atten, storage=H.STORE_F16,
-                                  iterations=int(iters[f]))
+        bf, _ = ctx2.reconstruct(host_p[f], host_r[f], atten=atten, storage=H.STORE_16,
+                                 iterations=int(iters[f]))
         ctx2.close()
         key = f"frame{f} ({counts[f]:.3g} counts, {int(iters[f])} it)"
         rel[key] = rl2(imgs[f], want)
-        rel16[key] = rl2(f16, want)
+        rel_bf16[key] = rl2(bf, want)
     h2d = sum(int(a.nbytes) for a in host_p) + sum(int(a.nbytes) for a in host_r)
     d2h = sum(int(a.nbytes) for a in imgs)
     b.close()
@@ -660,6 +664,7 @@ def run_dynamic(args, torch, H, local, dist, ws):
     si = bst.subset_iterations
     return {
         "metric": "dynamic-study subset-iters/s (span 9, 24 frames, 16-bit-stored inputs)",
+        "storage": "prompts int16, 1/(NA) and additive term fp16; FP32 accumulation",
         "unit": UNIT, "value": ws * si / (run_ms / 1e3), "ms_run": run_ms, "subset_iterations": si,
         "workload": f"{nf} span-9 HRRT frames (2209 planes x 288 views x 256 bins), image 256x256x207, phantom "
                     "seed 0 with time-varying sphere activity, counts log-uniform 2e6..2e8, 16 subsets x 1-4 "
@@ -671,7 +676,7 @@ def run_dynamic(args, torch, H, local, dist, ws):
                 "h2d_bytes_per_step": h2d // max(est.subset_iterations, 1),
                 "d2h_bytes_per_step": d2h // max(est.subset_iterations, 1)},
         "rel_l2_vs_f32_stored": rel,
-        "rel_l2_vs_f32_stored_fp16_terms": rel16,
+        "rel_l2_vs_f32_stored_bf16_terms": rel_bf16,
         "clocks": clk, "data_gen_s": gen_s,
     }
 

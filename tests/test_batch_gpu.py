@@ -3,8 +3,8 @@ shapes.
 
 Every frame of a batch is bit-identical to the single-frame reconstruction of
 the same inputs (hrrt_upload_inputs + hrrt_sensitivity + hrrt_init_image +
-hrrt_osem(iterations) + hrrt_get_image), with uneven iteration counts, both
-storage types and both back projectors; its FP64 image sum equals
+hrrt_osem(iterations) + hrrt_get_image), with uneven iteration counts, the
+three storage types (f32, bf16 and fp16 terms) and both back projectors; its FP64 image sum equals
 hrrt_osem's.  Every launch shape, and the autotuner's pick, gives
 bit-identical images (the shape only regroups planes among threads)."""
 import numpy as np
@@ -43,7 +43,7 @@ def single_frame(d, norm, atten, prompts, randoms, scatter, iterations, storage,
         return ctx.get_image(), st.sum_image
 
 
-@pytest.mark.parametrize("name,storage,bp", [("small3", 0, 0), ("small9", 1, 0), ("small9", 0, 1)])
+@pytest.mark.parametrize("name,storage,bp", [("small3", 0, 0), ("small9", 1, 0), ("small9", 2, 0), ("small9", 0, 1)])
 def test_frames_match_single_frame(name, storage, bp):
     import hrrt_reconstruction_b200 as H
     d = ALL[name]
