@@ -704,6 +704,17 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
     flzf[i] = make_int2(g.fl_zzi[i], bits);
   }
   d.fl_zf = dupload(ctx, flzf, &e);
+  // the same two tables with the row fastest, for the exact adjoint
+  {
+    std::vector<FpMid> mt(mid.size());
+    for (int y = 0; y < g.c; y++)
+      for (int gg = 0; gg < g.groupmax; gg++) mt[(size_t)gg * g.c + y] = mid[(size_t)y * g.groupmax + gg];
+    d.fpmid_t = dupload(ctx, mt, &e);
+    std::vector<int2> ft(flzf.size());
+    for (int y = 0; y < g.ny; y++)
+      for (int i = 0; i < FS; i++) ft[(size_t)i * g.ny + y] = flzf[(size_t)y * FS + i];
+    d.fl_t = dupload(ctx, ft, &e);
+  }
   d.bplut = dupload(ctx, bpl, &e);
   d.sin_psi = dupload(ctx, g.sin_psi, &e);
   d.cos_psi = dupload(ctx, g.cos_psi, &e);

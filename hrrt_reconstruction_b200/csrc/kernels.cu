@@ -717,8 +717,44 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(De
 // rotation whose sample footprint (recomputed with the forward projector's own
 // float expressions) holds it, with that footprint's weight.
 // ============================================================================
+// packed a * b + c (one rounding): the exact adjoint is held to the FP64
+// oracle within its tolerance, not to a reference's rounding order
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ Q2 qfma(Q2 a, uint64_t b, Q2 c) { return Q2{fma2(a.lo, b, c.lo), fma2(a.hi, b, c.hi)}; }
+
+// One side of a segment group's middle planes transposed: for the task's
+// planes z0 + j, s[j] += w0 * P[a0 + j - d0] + w1 * P[a0 + j - d1] over the
+// window entries inside [lo, hi] (d0, d1 in {0, 1}).  Windows wholly inside
+// the middle planes slide without checks; windows that straddle an end check
+// each entry.
 template <int KB>
-__global__ void __launch_bounds__(256, 2) adj_kernel(DevGeom g, const float4 *__restrict__ in, long long in_pair_stride,
+__device__ __forceinline__ void adj_side(Q2 (&s)[KB], const float4 *__restrict__ P, int a0, int lo, int hi,
+                                         uint64_t w_at, uint64_t w_below) {
+  // w_at multiplies P[a0 + j], w_below multiplies P[a0 + j - 1]
+  if (a0 - 1 >= lo && a0 + KB - 1 <= hi) {
+    Q2 prev = ldq(P + a0 - 1);
+#pragma unroll
+    for (int j = 0; j < KB; j++) {
+      const Q2 cur = ldq(P + a0 + j);
+      s[j] = qfma(prev, w_below, qfma(cur, w_at, s[j]));
+      prev = cur;
+    }
+  } else if (a0 + KB - 1 >= lo && a0 - 1 <= hi) {
+#pragma unroll
+    for (int j = 0; j < KB; j++) {
+      const int ya = a0 + j;
+      if (ya >= lo && ya <= hi) s[j] = qfma(ldq(P + ya), w_at, s[j]);
+      if (ya - 1 >= lo && ya - 1 <= hi) s[j] = qfma(ldq(P + ya - 1), w_below, s[j]);
+    }
+  }
+}
+
+template <int KB>
+__global__ void __launch_bounds__(256, 3) adj_kernel(DevGeom g, const float4 *__restrict__ in, long long in_pair_stride,
                                                   const QuadWork *__restrict__ work, float *__restrict__ bc,
                                                   float *__restrict__ br, long long vol, FrameStrides fr) {
   extern __shared__ float4 P[];
@@ -728,7 +764,6 @@ __global__ void __launch_bounds__(256, 2) adj_kernel(DevGeom g, const float4 *__
   bc += (size_t)frame * fr.bc;
   br += (size_t)frame * fr.bc;
   const int x = w.x, N = g.nx, c = g.c, zp = g.zp, G = g.groupmax, ZS = g.zshift, nz = g.nz;
-  const int FS = G * 2 * ZS;
   const bool masked = g.nzmask[w.view * g.nquads + x] == 0 || g.cyl0[x] == g.cyl1[x];
   const float4 *src = in + (size_t)w.slot * in_pair_stride + (size_t)x * g.pplanes;
   if (!masked)
@@ -754,6 +789,8 @@ __global__ void __launch_bounds__(256, 2) adj_kernel(DevGeom g, const float4 *__
   const int ystart = g.cyl0[x];
   const int nyq = c - ystart + 1, nzc = zp / KB;
   const float4 *P0 = P + g.bp_soff[0];
+  // a warp's 32 tasks are 32 consecutive rows at one plane run: the rows'
+  // table entries ([group][row]) are contiguous, the stores whole sectors
   const int per_half = nyq * nzc;
   for (int task = threadIdx.x; task < 2 * per_half; task += blockDim.x) {
     const int half = task >= per_half;
@@ -761,12 +798,12 @@ __global__ void __launch_bounds__(256, 2) adj_kernel(DevGeom g, const float4 *__
     const int zc = t2 / nyq, yi = t2 - zc * nyq, z0 = zc * KB;
     const int y = ystart + yi;
     if (half && y == c) continue;
-    float4 s[KB];
+    Q2 s[KB];
 #pragma unroll
-    for (int j = 0; j < KB; j++) s[j] = f4(0.f);
+    for (int j = 0; j < KB; j++) s[j] = Q2{0ull, 0ull};
     if (!masked) {
 #pragma unroll
-      for (int j = 0; j < KB; j++) s[j] = P0[z0 + j];
+      for (int j = 0; j < KB; j++) s[j] = ldq(P0 + z0 + j);
       if (y == c) {
         // centre row: every plane of every segment took the centre samples
         for (int gg = 0; gg < G; gg++) {
@@ -776,45 +813,40 @@ __global__ void __launch_bounds__(256, 2) adj_kernel(DevGeom g, const float4 *__
 #pragma unroll
           for (int j = 0; j < KB; j++) {
             const int z = z0 + j;
-            if (z >= yb && z <= yt) s[j] = s[j] + (pe[z] + po[z]);
+            if (z >= yb && z <= yt) s[j] = qadd(s[j], qadd(ldq(pe + z), ldq(po + z)));
           }
         }
       } else {
+        const FpMid *mrow = g.fpmid_t + y;
+        const int2 *e1 = g.fl_t + y, *e2 = g.fl_t + (N - y);
         for (int gg = 0; gg < G; gg++) {
-          const FpMid m = g.fpmid[y * G + gg];
+          const FpMid m = mrow[(size_t)gg * c];
           if (m.z < 0) continue;  // the forward projector skipped this group for this row
           const int se = 2 * gg + 2, so = 2 * gg + 1;
           const int yb = g.ybot[se], yt = g.ytop[se], ym = yb + ZS, ye = yt - ZS;
           // A: the rows that read this sample at (z, z+1) with (f2, f); B:
           // the rows that read it at (z2+1, z2) with (f2, f)
           const float4 *A = P + g.bp_soff[half ? so : se] - yb, *B = P + g.bp_soff[half ? se : so] - yb;
-          const int a0 = z0 - m.z + ym, b0 = z0 - m.z2 + ym;
-#pragma unroll
-          for (int j = 0; j < KB; j++) {
-            const int ya = a0 + j, yb2 = b0 + j;
-            float4 t = f4(0.f);
-            if (ya >= ym && ya <= ye) t = t + A[ya] * m.f2;
-            if (ya - 1 >= ym && ya - 1 <= ye) t = t + A[ya - 1] * m.f;
-            if (yb2 - 1 >= ym && yb2 - 1 <= ye) t = t + B[yb2 - 1] * m.f2;
-            if (yb2 >= ym && yb2 <= ye) t = t + B[yb2] * m.f;
-            s[j] = s[j] + t;
-          }
+          const uint64_t f = pk(m.f, m.f), f2 = pk(m.f2, m.f2);
+          adj_side<KB>(s, A, z0 - m.z + ym, ym, ye, f2, f);
+          adj_side<KB>(s, B, z0 - m.z2 + ym, ym, ye, f, f2);
           // end planes: one position per plane
-          const int2 *e1 = g.fl_zf + (size_t)y * FS + gg * 2 * ZS, *e2 = g.fl_zf + (size_t)(N - y) * FS + gg * 2 * ZS;
+          const size_t eb = (size_t)gg * 2 * ZS * N;
           for (int i = 0; i < 2 * ZS; i++) {
-            const int yr = (i < ZS) ? yb + i : yt - 2 * ZS + 1 + i;
-            const int2 u = e1[i], v = e2[i];
+            const int2 u = __ldg(e1 + eb + (size_t)i * N), v = __ldg(e2 + eb + (size_t)i * N);
             const int za = u.x, zb = v.x;
             if ((za + 1 < z0 || za >= z0 + KB) && (zb + 1 < z0 || zb >= z0 + KB)) continue;
+            const int yr = (i < ZS) ? yb + i : yt - 2 * ZS + 1 + i;
             const float fa = __int_as_float(u.y), fb = __int_as_float(v.y);
-            const float4 a = A[yr], b = B[yr];
+            const uint64_t pfa = pk(fa, fa), pfb = pk(fb, fb);
+            const Q2 a = ldq(A + yr), b = ldq(B + yr);
 #pragma unroll
             for (int j = 0; j < KB; j++) {
               const int z = z0 + j;
-              if (z == za) s[j] = s[j] + a * fb;
-              if (z == za + 1) s[j] = s[j] + a * fa;
-              if (z == zb + 1) s[j] = s[j] + b * fb;
-              if (z == zb) s[j] = s[j] + b * fa;
+              if (z == za) s[j] = qfma(a, pfb, s[j]);
+              if (z == za + 1) s[j] = qfma(a, pfa, s[j]);
+              if (z == zb + 1) s[j] = qfma(b, pfb, s[j]);
+              if (z == zb) s[j] = qfma(b, pfa, s[j]);
             }
           }
         }
@@ -822,28 +854,21 @@ __global__ void __launch_bounds__(256, 2) adj_kernel(DevGeom g, const float4 *__
     }
 #pragma unroll
     for (int j = 0; j < KB; j++)
-      if (z0 + j >= nz) s[j] = f4(0.f);
+      if (z0 + j >= nz) s[j] = Q2{0ull, 0ull};
     const size_t cz = (size_t)z0;
-    auto put = [&](float *dst, int l) {
-      float v[KB];
-#pragma unroll
-      for (int j = 0; j < KB; j++) v[j] = l == 0 ? s[j].x : l == 1 ? s[j].y : l == 2 ? s[j].z : s[j].w;
-#pragma unroll
-      for (int j = 0; j < KB; j += 4) *reinterpret_cast<float4 *>(dst + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-    };
     if (!half) {
-      put(bcp + ((size_t)x * N + y) * zp + cz, 0);
-      put(brp + ((size_t)(N - y) * N + x) * zp + cz, 2);
+      store_lane<KB>(bcp + ((size_t)x * N + y) * zp + cz, s, 0);
+      store_lane<KB>(brp + ((size_t)(N - y) * N + x) * zp + cz, s, 2);
       if (x != c) {
-        put(bcp + ((size_t)(N - x) * N + y) * zp + cz, 1);
-        put(brp + ((size_t)(N - y) * N + N - x) * zp + cz, 3);
+        store_lane<KB>(bcp + ((size_t)(N - x) * N + y) * zp + cz, s, 1);
+        store_lane<KB>(brp + ((size_t)(N - y) * N + N - x) * zp + cz, s, 3);
       }
     } else {
-      put(bcp + ((size_t)x * N + N - y) * zp + cz, 0);
-      put(brp + ((size_t)y * N + x) * zp + cz, 2);
+      store_lane<KB>(bcp + ((size_t)x * N + N - y) * zp + cz, s, 0);
+      store_lane<KB>(brp + ((size_t)y * N + x) * zp + cz, s, 2);
       if (x != c) {
-        put(bcp + ((size_t)(N - x) * N + N - y) * zp + cz, 1);
-        put(brp + ((size_t)y * N + N - x) * zp + cz, 3);
+        store_lane<KB>(bcp + ((size_t)(N - x) * N + N - y) * zp + cz, s, 1);
+        store_lane<KB>(brp + ((size_t)y * N + N - x) * zp + cz, s, 3);
       }
     }
   }

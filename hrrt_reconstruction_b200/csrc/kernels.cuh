@@ -68,6 +68,8 @@ struct DevGeom {
   const float *bp_scale;            // [nseg]
   const FpMid *fpmid;               // [c][groupmax]
   const int2 *fl_zf;                // [ny][groupmax*2*zshift]: (zzi, bits of zzz0)
+  const FpMid *fpmid_t;             // fpmid transposed: [groupmax][c] (the exact adjoint's rows are threads)
+  const int2 *fl_t;                 // fl_zf transposed: [groupmax*2*zshift][ny]
   const BpLut *bplut;               // [groupmax][ny]
   const int16_t *nzmask;            // [nviews/2][nquads]
   const float *sin_psi, *cos_psi;   // [nviews]
