@@ -714,6 +714,10 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
     for (int y = 0; y < g.ny; y++)
       for (int i = 0; i < FS; i++) ft[(size_t)i * g.ny + y] = flzf[(size_t)y * FS + i];
     d.fl_t = dupload(ctx, ft, &e);
+    // the exact adjoint's rotate tables, rebuilt for each subset's pairs
+    d.adj_pairs = ctx->npairs;
+    d.adj_ent = dalloc<int2>(ctx, (size_t)ctx->npairs * g.nx * g.nx * kAdjCover, &e);
+    d.adj_cnt = d.adj_ent ? dalloc<int>(ctx, (size_t)ctx->npairs * g.nx * g.nx, &e) : nullptr;
   }
   d.bplut = dupload(ctx, bpl, &e);
   d.sin_psi = dupload(ctx, g.sin_psi, &e);

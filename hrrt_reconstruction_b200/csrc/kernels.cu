@@ -874,6 +874,55 @@ __global__ void __launch_bounds__(256, 3) adj_kernel(DevGeom g, const float4 *__
   }
 }
 
+// For each pair slot and voxel column (every column for MODE 2, the FOV
+// columns otherwise): the rotated-frame points (a, b) around the column's
+// inverse rotation whose forward-projection sample footprint -- recomputed
+// with the forward projector's own float expressions -- covers the column,
+// with that footprint's weight, in scan order.  One thread per (pair, column);
+// the rotate then reads these instead of every thread of a column repeating
+// the 16 candidate footprints.
+template <int MODE>
+__global__ void __launch_bounds__(256) adj_cover_kernel(DevGeom g, const int *__restrict__ pair_views, int npairs) {
+  const int N = g.nx, c = g.c;
+  const long long ncols = (MODE == 2) ? (long long)N * N : g.fov_columns;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncols * npairs) return;
+  const int p = (int)(t / ncols);
+  const int col = (int)(t - (long long)p * ncols);
+  int i, j;
+  if (MODE == 2) {
+    i = col / N;
+    j = col - i * N;
+  } else {
+    const short2 xy = g.fov_xy[col];
+    i = xy.x;
+    j = xy.y;
+  }
+  const int view = pair_views[p];
+  const float cosv = g.cos_psi[view], sinv = g.sin_psi[view];
+  const float di = (float)(i - c), dj = (float)(j - c);
+  const int qx0 = (int)floorf(di * cosv + dj * sinv + (float)c) - 1;
+  const int qy0 = (int)floorf(-di * sinv + dj * cosv + (float)c) - 1;
+  int2 *ent = g.adj_ent + t * kAdjCover;
+  int n = 0;
+  for (int a = qx0; a < qx0 + 4; a++) {
+    if (a < 0 || a >= N) continue;
+    for (int b = qy0; b < qy0 + 4; b++) {
+      if (b < 0 || b >= N) continue;
+      const SamplePt pt = sample_point(a, b, c, N, g.zp, cosv, sinv);
+      if (pt.base < 0) continue;
+      const int ix = pt.base / (N * g.zp), iy = (pt.base / g.zp) - ix * N;
+      const int dx = i - ix, dy = j - iy;
+      if (dx < 0 || dx > 1 || dy < 0 || dy > 1) continue;
+      const float wgt = dx ? (dy ? pt.c3 : pt.c1) : (dy ? pt.c2 : pt.c0);
+      if (n < kAdjCover) ent[n] = make_int2(a * N + b, __float_as_int(wgt));
+      n++;
+    }
+  }
+  if (n > kAdjCover) atomicExch(g.err, 2);  // more covering points than the table holds: results void
+  g.adj_cnt[t] = min(n, kAdjCover);
+}
+
 // MODE 0: OSEM update, 1: inverse sensitivity (both over the FOV columns, as
 // the rotate-back), 2: out += adjoint over every image column.
 template <int MODE>
@@ -882,7 +931,7 @@ __global__ void __launch_bounds__(256) adj_rotate_kernel(DevGeom g, const int *_
                                                          long long vol, float *__restrict__ image,
                                                          float *__restrict__ nf_inv, float *__restrict__ out,
                                                          FrameStrides fr) {
-  const int nq = g.zp / 4, N = g.nx, c = g.c;
+  const int nq = g.zp / 4, N = g.nx;
   if (MODE == 0) {
     image += (size_t)(fr.map ? __ldg(fr.map + blockIdx.y) : (int)blockIdx.y) * fr.image;
     bc += (size_t)blockIdx.y * fr.bc;
@@ -901,28 +950,20 @@ __global__ void __launch_bounds__(256) adj_rotate_kernel(DevGeom g, const int *_
     i = xy.x;
     j = xy.y;
   }
+  // the covering points of this column, found once per pair by
+  // adj_cover_kernel in this scan order
+  const long long ncols = (MODE == 2) ? (long long)N * N : g.fov_columns;
   float4 acc = f4(0.f);
   for (int p = 0; p < npairs; p++) {
-    const int view = pair_views[p];
-    const float cosv = g.cos_psi[view], sinv = g.sin_psi[view];
-    const float di = (float)(i - c), dj = (float)(j - c);
-    const int qx0 = (int)floorf(di * cosv + dj * sinv + (float)c) - 1;
-    const int qy0 = (int)floorf(-di * sinv + dj * cosv + (float)c) - 1;
     const float4 *Bc = reinterpret_cast<const float4 *>(bc + (size_t)p * vol);
     const float4 *Br = reinterpret_cast<const float4 *>(br + (size_t)p * vol);
-    for (int a = qx0; a < qx0 + 4; a++) {
-      if (a < 0 || a >= N) continue;
-      for (int b = qy0; b < qy0 + 4; b++) {
-        if (b < 0 || b >= N) continue;
-        const SamplePt pt = sample_point(a, b, c, N, g.zp, cosv, sinv);
-        if (pt.base < 0) continue;
-        const int ix = pt.base / (N * g.zp), iy = (pt.base / g.zp) - ix * N;
-        const int dx = i - ix, dy = j - iy;
-        if (dx < 0 || dx > 1 || dy < 0 || dy > 1) continue;
-        const float wgt = dx ? (dy ? pt.c3 : pt.c1) : (dy ? pt.c2 : pt.c0);
-        const size_t o = ((size_t)a * N + b) * nq + q;
-        acc = acc + (__ldg(Bc + o) + __ldg(Br + o)) * wgt;
-      }
+    const long long e0 = (long long)p * ncols + col;
+    const int n = __ldg(g.adj_cnt + e0);
+    const int2 *ent = g.adj_ent + e0 * kAdjCover;
+    for (int k = 0; k < n; k++) {
+      const int2 u = __ldg(ent + k);
+      const size_t o = (size_t)u.x * nq + q;
+      acc = acc + (__ldg(Bc + o) + __ldg(Br + o)) * __int_as_float(u.y);
     }
   }
   const size_t o = ((size_t)i * N + j) * nq + q;
@@ -1395,8 +1436,19 @@ cudaError_t launch_adj_rotate(const DevGeom &g, const int *pair_views, int npair
   if (fr.n <= 0) return cudaSuccess;
   if (mode != 0 && fr.n != 1) return cudaErrorInvalidValue;
   const long long cols = (mode == 2) ? (long long)g.nx * g.nx : (long long)g.fov_columns;
-  const long long n = cols * (g.zp / 4);
+  if (npairs > g.adj_pairs || !g.adj_ent || !g.adj_cnt) return cudaErrorInvalidValue;
   const int threads = 256;
+  {
+    const long long m = cols * npairs;
+    const unsigned cb = (unsigned)((m + threads - 1) / threads);
+    if (mode == 2)
+      adj_cover_kernel<2><<<cb, threads, 0, st>>>(g, pair_views, npairs);
+    else
+      adj_cover_kernel<0><<<cb, threads, 0, st>>>(g, pair_views, npairs);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  const long long n = cols * (g.zp / 4);
   const dim3 blocks((unsigned)((n + threads - 1) / threads), fr.n);
   if (mode == 0)
     adj_rotate_kernel<0><<<blocks, threads, 0, st>>>(g, pair_views, npairs, bc, br, vol, image, nf_inv, out, fr);

@@ -37,6 +37,7 @@ constexpr int kFpMaxGroups = 32; // segment groups the forward projector stages 
 constexpr int kBpZ = 8;         // z per back-projection task
 constexpr int kBpMinBlocks = HRRT_BP_MIN_BLOCKS;  // resident back-projection CTAs per SM (register budget)
 constexpr int kBpPad = 8;       // zero planes on each side of a segment in the back projector (>= kBpZ)
+constexpr int kAdjCover = 8;    // rotated-frame points whose bilinear footprint covers a voxel (at most 5 on HRRT)
 
 struct FpTask {
   int16_t seg;   // segment (internal = file order)
@@ -70,6 +71,9 @@ struct DevGeom {
   const int2 *fl_zf;                // [ny][groupmax*2*zshift]: (zzi, bits of zzz0)
   const FpMid *fpmid_t;             // fpmid transposed: [groupmax][c] (the exact adjoint's rows are threads)
   const int2 *fl_t;                 // fl_zf transposed: [groupmax*2*zshift][ny]
+  int2 *adj_ent;                    // exact adjoint's rotate: per (pair slot, column) the covering
+  int *adj_cnt;                     //   rotated-frame points (index, weight bits) [.][kAdjCover], their count
+  int adj_pairs;                    //   pair slots the two buffers hold (for every image column)
   const BpLut *bplut;               // [groupmax][ny]
   const int16_t *nzmask;            // [nviews/2][nquads]
   const float *sin_psi, *cos_psi;   // [nviews]
