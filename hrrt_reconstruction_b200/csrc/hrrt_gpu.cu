@@ -714,6 +714,25 @@ int hrrt_ctx_create(const hrrt_geom *gp, int device, hrrt_ctx **out) {
     for (int y = 0; y < g.ny; y++)
       for (int i = 0; i < FS; i++) ft[(size_t)i * g.ny + y] = flzf[(size_t)y * FS + i];
     d.fl_t = dupload(ctx, ft, &e);
+    // per (group, row y < c): the planes the end-plane entries of rows y and
+    // N - y touch (each entry z reaches z and z + 1), bottom end and top end
+    std::vector<int4> endr((size_t)g.groupmax * g.c, make_int4(1 << 30, -1, 1 << 30, -1));
+    for (int y = 1; y < g.c; y++)
+      for (int gg = 0; gg < g.groupmax; gg++) {
+        int4 &r = endr[(size_t)gg * g.c + y];
+        for (int i = 0; i < 2 * g.zshift; i++)
+          for (const int row : {y, g.ny - y}) {
+            const int z = g.fl_zzi[(size_t)row * FS + gg * 2 * g.zshift + i];
+            if (i < g.zshift) {
+              r.x = std::min(r.x, z);
+              r.y = std::max(r.y, z + 1);
+            } else {
+              r.z = std::min(r.z, z);
+              r.w = std::max(r.w, z + 1);
+            }
+          }
+      }
+    d.adj_endr = dupload(ctx, endr, &e);
     // the exact adjoint's rotate tables, rebuilt for each subset's pairs
     d.adj_pairs = ctx->npairs;
     d.adj_ent = dalloc<int2>(ctx, (size_t)ctx->npairs * g.nx * g.nx * kAdjCover, &e);

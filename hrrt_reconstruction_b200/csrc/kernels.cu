@@ -830,9 +830,12 @@ __global__ void __launch_bounds__(256, 3) adj_kernel(DevGeom g, const float4 *__
           const uint64_t f = pk(m.f, m.f), f2 = pk(m.f2, m.f2);
           adj_side<KB>(s, A, z0 - m.z + ym, ym, ye, f2, f);
           adj_side<KB>(s, B, z0 - m.z2 + ym, ym, ye, f, f2);
-          // end planes: one position per plane
+          // end planes: one position per plane; an end whose entries touch
+          // no plane of this task's run is skipped whole
           const size_t eb = (size_t)gg * 2 * ZS * N;
-          for (int i = 0; i < 2 * ZS; i++) {
+          const int4 er = __ldg(g.adj_endr + (size_t)gg * c + y);
+          const bool bot = er.x < z0 + KB && er.y >= z0, top = er.z < z0 + KB && er.w >= z0;
+          for (int i = bot ? 0 : ZS; i < (top ? 2 * ZS : ZS); i++) {
             const int2 u = __ldg(e1 + eb + (size_t)i * N), v = __ldg(e2 + eb + (size_t)i * N);
             const int za = u.x, zb = v.x;
             if ((za + 1 < z0 || za >= z0 + KB) && (zb + 1 < z0 || zb >= z0 + KB)) continue;

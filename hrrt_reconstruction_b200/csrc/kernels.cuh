@@ -71,6 +71,8 @@ struct DevGeom {
   const int2 *fl_zf;                // [ny][groupmax*2*zshift]: (zzi, bits of zzz0)
   const FpMid *fpmid_t;             // fpmid transposed: [groupmax][c] (the exact adjoint's rows are threads)
   const int2 *fl_t;                 // fl_zf transposed: [groupmax*2*zshift][ny]
+  const int4 *adj_endr;             // exact adjoint, [groupmax][c]: planes the bottom / top end-plane
+                                    //   entries of a row touch (x..y bottom, z..w top; empty: lo > hi)
   int2 *adj_ent;                    // exact adjoint's rotate: per (pair slot, column) the covering
   int *adj_cnt;                     //   rotated-frame points (index, weight bits) [.][kAdjCover], their count
   int adj_pairs;                    //   pair slots the two buffers hold (for every image column)
