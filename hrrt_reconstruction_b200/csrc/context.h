@@ -69,6 +69,7 @@ struct hrrt_ctx {
   // back projector of the OSEM loop, and the device geometry it runs with
   // (for the adjoint: segment weights of 1, the forward projector's scaling)
   int bp_mode = HRRT_BP_REF;
+  int staging = HRRT_STAGE_F32;  // shared-memory staging of the OSEM subsets' projectors
   hrrt::DevGeom dg_adj{};
   int *d_view1 = nullptr;       // one view index, for single-pair entry points
 

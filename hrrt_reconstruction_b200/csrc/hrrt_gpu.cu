@@ -215,6 +215,7 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
   float *nf = ctx->d_nfinv + (size_t)s * ctx->vol;
   const bool single = b.fr.n == 1 && !b.fr.map;
   const bool map = single && ctx->map_on && ctx->subsets_done >= ctx->map_first;
+  const bool stage16 = ctx->staging == HRRT_STAGE_BF16;
   if (single) ctx->subsets_done++;
   if (map) {
     // je_hrrt_osem3d's subset with MAP (hrrt_osem3d.cpp:4439-4463): the
@@ -228,7 +229,7 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
     {
       Launch L(ctx, "fp_kernel");
       CK(launch_fp(g, proj, fw, ctx->fp_cnt[s], 1, b.prompts, b.add, ctx->storage, b.ratio, ctx->quad_pair,
-                   ctx->tune, b.fr, ctx->stream),
+                   ctx->tune, b.fr, ctx->stream, stage16),
          "fp_kernel");
     }
     if (adj) {
@@ -242,7 +243,7 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
       {
         Launch L(ctx, "bp_kernel");
         CK(launch_bp(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, ctx->tune, b.fr,
-                     ctx->stream),
+                     ctx->stream, stage16),
            "bp_kernel");
       }
       Launch L(ctx, "rotback_kernel");
@@ -268,7 +269,7 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
     {
       Launch L(ctx, "fp_kernel");
       CK(launch_fp(g, ctx->d_image_psf, fw, ctx->fp_cnt[s], 1, b.prompts, b.add, ctx->storage, b.ratio,
-                   ctx->quad_pair, ctx->tune, b.fr, ctx->stream),
+                   ctx->quad_pair, ctx->tune, b.fr, ctx->stream, stage16),
          "fp_kernel");
     }
     if (adj) {
@@ -280,7 +281,7 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
          "adj_rotate_kernel");
     } else {
       CK(launch_bp(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, ctx->tune, b.fr,
-                   ctx->stream),
+                   ctx->stream, stage16),
          "bp_kernel");
       CK(launch_rotback(g, pv, ctx->npairs, b.bc, b.br, ctx->vol, nullptr, nullptr, ctx->d_corr, 3, b.fr,
                         ctx->stream),
@@ -293,7 +294,7 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
   {
     Launch L(ctx, "fp_kernel");
     CK(launch_fp(g, b.image, fw, ctx->fp_cnt[s], 1, b.prompts, b.add, ctx->storage, b.ratio, ctx->quad_pair,
-                 ctx->tune, b.fr, ctx->stream),
+                 ctx->tune, b.fr, ctx->stream, stage16),
        "fp_kernel");
   }
   if (adj) {
@@ -309,7 +310,8 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
   }
   {
     Launch L(ctx, "bp_kernel");
-    CK(launch_bp(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, ctx->tune, b.fr, ctx->stream),
+    CK(launch_bp(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, ctx->tune, b.fr, ctx->stream,
+                 stage16),
        "bp_kernel");
   }
   Launch L(ctx, "rotback_kernel");
@@ -1345,6 +1347,14 @@ int hrrt_set_backprojector(hrrt_ctx *ctx, int mode) {
     ctx->config_epoch++;
   }
   ctx->bp_mode = mode;
+  return HRRT_OK;
+}
+
+int hrrt_set_staging(hrrt_ctx *ctx, int mode) {
+  if (!ctx) return HRRT_ERR_ARG;
+  if (mode != HRRT_STAGE_F32 && mode != HRRT_STAGE_BF16) return fail(ctx, HRRT_ERR_ARG, "unknown staging");
+  if (mode != ctx->staging) ctx->config_epoch++;
+  ctx->staging = mode;
   return HRRT_OK;
 }
 
