@@ -390,8 +390,6 @@ def run_ours(args, ws, rank, local):
         out["storage16"] = run_storage16(args, torch, H, ctx, st, host, names, img, cs, dist, local, ws, ms)
         out["storage_f16"] = run_storage16(args, torch, H, ctx, st, host, names, img, cs, dist, local, ws, ms,
                                            storage=H.STORE_F16)
-        out["storage_f16_staged"] = run_storage16(args, torch, H, ctx, st, host, names, img, cs, dist, local, ws,
-                                                  ms, storage=H.STORE_F16, staged=True)
     out["adjoint"] = run_adjoint(args, torch, H, ctx, cs, dist, local, ws, ms)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
@@ -413,16 +411,12 @@ def run_ours(args, ws, rank, local):
         dist.destroy_process_group()
 
 
-def run_storage16(args, torch, H, ctx, st, host, names, img_f32, cs, dist, local, ws, ms_f32, storage=None,
-                  staged=False):
+def run_storage16(args, torch, H, ctx, st, host, names, img_f32, cs, dist, local, ws, ms_f32, storage=None):
     """The same study with 1/(NA) and the additive term stored in 16 bits (bf16
     by default, fp16 with storage=STORE_F16; prompts int16; FP32 arithmetic):
     device-resident subset-iterations/s over the same steps, and the rel-L2
-    of its image after the e2e reconstruction against the f32-stored image.
-    staged: the projectors of the subsets also stage bf16 samples in shared
-    memory (hrrt_set_staging(HRRT_STAGE_BF16))."""
+    of its image after the e2e reconstruction against the f32-stored image."""
     storage = H.STORE_16 if storage is None else storage
-    ctx.set_staging(H.STAGE_BF16 if staged else H.STAGE_F32)
     img16 = pinned_copy(torch, np.zeros_like(img_f32))
     ctx.reconstruct(*(host.get(k) for k in names), storage=storage, iterations=ITERATIONS, out=img16)
     a = img16.astype(np.float64)
@@ -439,13 +433,11 @@ def run_storage16(args, torch, H, ctx, st, host, names, img_f32, cs, dist, local
     ev[1].record(cs)
     torch.cuda.synchronize()
     ms = max_over_ranks(dist, ev[0].elapsed_time(ev[1]), local)
-    ctx.set_staging(H.STAGE_F32)
     return {"value": ws * args.steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / args.steps,
             "speedup_vs_f32": ms_f32 / ms, "rel_l2_vs_f32_image": rel,
             "rel_l2_note": f"image after {ITERATIONS} iterations x {SUBSETS} subsets (hrrt_reconstruct), "
                            "16-bit-stored vs f32-stored inputs, same prompts",
             "storage": ("prompts int16, 1/(NA) and additive term " + ("fp16" if storage == H.STORE_F16 else "bf16")
-                        + ("; projector samples staged as bf16 in shared memory" if staged else "")
                         + "; FP32 accumulation, FP64 image sum")}
 
 
@@ -459,11 +451,8 @@ def run_parity(H, ctx, st, iterations, study_kw):
     geom = dict(geom_dict(), span=int(ctx.geom.span))
     raw = [st[k] for k in ("prompts", "randoms", "norm", "atten", "scatter")]
     dev = {}
-    for name, storage, stage in (("f32", H.STORE_F32, H.STAGE_F32), ("bf16", H.STORE_16, H.STAGE_F32),
-                                 ("fp16", H.STORE_F16, H.STAGE_F32), ("fp16_staged", H.STORE_F16, H.STAGE_BF16)):
-        ctx.set_staging(stage)
+    for name, storage in (("f32", H.STORE_F32), ("bf16", H.STORE_16), ("fp16", H.STORE_F16)):
         dev[name] = [ctx.reconstruct(*raw, storage=storage, iterations=k + 1)[0] for k in range(iterations)]
-    ctx.set_staging(H.STAGE_F32)
     t0 = time.perf_counter()
     pre = SP.prep(geom, *raw)
     host = {}
@@ -486,9 +475,7 @@ def run_parity(H, ctx, st, iterations, study_kw):
     if "reference" in host:
         res["reference_vs_fp64"] = [SP.rel_l2(a["image"], b["image"]) for a, b in zip(host["reference"], host["fp64"])]
     res["storage"] = {"f32": "prompts int16, terms f32", "bf16": "prompts int16, 1/(NA) and additive term bf16",
-                      "fp16": "prompts int16, 1/(NA) and additive term fp16",
-                      "fp16_staged": "prompts int16, 1/(NA) and additive term fp16, projector samples staged as "
-                                     "bf16 in shared memory"}
+                      "fp16": "prompts int16, 1/(NA) and additive term fp16"}
     return res
 
 
@@ -989,8 +976,6 @@ def case_osem(args):
     storage = {"f32": H.STORE_F32, "16": H.STORE_16, "f16": H.STORE_F16}[args.storage]
     if args.bp == "adjoint":
         ctx.set_backprojector(H.BP_ADJOINT)
-    if args.stage == "bf16":
-        ctx.set_staging(H.STAGE_BF16)
     if args.psf:
         ctx.set_psf(True)
     ctx.set_profiling(True)
@@ -1010,7 +995,7 @@ def case_osem(args):
     ctx.close()
 
 
-LM_PATHS = (("direct", 16), ("wide", 64), ("partitioned", 32), ("records", 512))
+LM_PATHS = (("direct", 16), ("wide", 64), ("partitioned", 32))
 
 
 def case_lm(args):
@@ -1087,7 +1072,6 @@ def main():
     ap.add_argument("--iterations", type=int, default=0,
                     help="--case osem: full iterations (every subset + the post-iteration pass) after the subsets")
     ap.add_argument("--bp", default="ref", choices=["ref", "adjoint"], help="--case osem: back projector")
-    ap.add_argument("--stage", default="f32", choices=["f32", "bf16"], help="--case osem: projector staging")
     ap.add_argument("--psf", action="store_true", help="--case osem: PSF modelling (-B, HRRT defaults)")
     ap.add_argument("--map", action="store_true", help="--case osem: MAP technique 1 from the first subset")
     ap.add_argument("--events", type=float, default=1e8, help="--case lm: events")

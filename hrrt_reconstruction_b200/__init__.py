@@ -17,7 +17,6 @@ import os
 import numpy as np
 
 __all__ = ["Geometry", "HrrtError", "Context", "Batch", "Tuning", "Listmode", "lib", "LIB_PATH", "STORE_F32", "STORE_16", "STORE_F16", "BP_REF", "BP_ADJOINT",
-           "STAGE_F32", "STAGE_BF16",
            "geometry_table", "hrrt_geometry"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libhrrt_gpu.so")
@@ -26,8 +25,6 @@ STORE_16 = 1   # bf16 additive and multiplicative terms
 STORE_F16 = 2  # fp16 additive and multiplicative terms
 BP_REF = 0
 BP_ADJOINT = 1
-STAGE_F32 = 0   # projectors of OSEM subsets stage float samples (bit-exact)
-STAGE_BF16 = 1  # the forward projector stages bf16 samples (16-bit precision form)
 
 
 class HrrtError(RuntimeError):
@@ -88,7 +85,6 @@ class BatchStats(ctypes.Structure):
 LM_TRUES, LM_PROMPTS_AND_DELAYED, LM_PROMPTS_ONLY = 0, 1, 2
 LM_IGNORE_BORDER_CRYSTAL, LM_NO_DOI, LM_TIME_FROM_COUNT = 1, 2, 4
 LM_FORCE_DIRECT, LM_FORCE_PARTITIONED, LM_FORCE_WIDE, LM_HEAD_CURVE, LM_CRYSTAL_COUNTS = 16, 32, 64, 128, 256
-LM_FORCE_RECORDS = 512
 
 
 def _load():
@@ -121,7 +117,6 @@ def _load():
         "hrrt_forward_project": (i, [vp, vp, vp]),
         "hrrt_bp_pair_noalloc": (i, [vp, vp, i, vp, vp]),
         "hrrt_set_backprojector": (i, [vp, i]),
-        "hrrt_set_staging": (i, [vp, i]),
         "hrrt_rotate_add": (i, [vp, vp, i, vp]),
         "hrrt_geometry_table": (ctypes.c_longlong, [G, ctypes.c_char_p, vp, ctypes.c_size_t]),
         "hrrt_set_profiling": (i, [vp, i]),
@@ -383,11 +378,6 @@ class Context:
         """BP_REF (the reference's back projector) or BP_ADJOINT (the forward
         projector's exact transpose) for sensitivity() and osem()."""
         self._check(lib.hrrt_set_backprojector(self._h, mode), "set_backprojector")
-
-    def set_staging(self, mode):
-        """STAGE_F32 (default: float samples, the reference's arithmetic) or
-        STAGE_BF16 (OSEM subsets' forward projector stages bf16 samples)."""
-        self._check(lib.hrrt_set_staging(self._h, mode), "set_staging")
 
     def rotate_add(self, imagebuf, view, corr):
         ib = _c(imagebuf, np.float32)

@@ -127,7 +127,7 @@ int autotune(hrrt_ctx *ctx, const SubsetBufs &bb, int repeats, hrrt_tuning *chos
       double ms = 0;
       int rc = time_launch(ctx, repeats, [&] {
         return launch_fp(g, bb.image, fw, ctx->fp_cnt[s], 1, bb.prompts, bb.add, ctx->storage, bb.ratio,
-                         ctx->quad_pair, t, bb.fr, ctx->stream, ctx->staging == HRRT_STAGE_BF16);
+                         ctx->quad_pair, t, bb.fr, ctx->stream);
       }, &ms);
       if (rc) {
         apply_tune(ctx, saved);
@@ -150,7 +150,7 @@ int autotune(hrrt_ctx *ctx, const SubsetBufs &bb, int repeats, hrrt_tuning *chos
       double ms = 0;
       int rc = time_launch(ctx, repeats, [&] {
         return launch_bp(ctx->dg, bb.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], bb.bc, bb.br, ctx->vol, t, bb.fr,
-                         ctx->stream, ctx->staging == HRRT_STAGE_BF16);
+                         ctx->stream);
       }, &ms);
       if (rc) return rc;
       if (ms < best_bp) {

@@ -58,6 +58,9 @@ struct hrrt_ctx {
   // copy of one chunk overlapping the prep of the previous one
   cudaStream_t copy_stream = nullptr;
   cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+  // hrrt_reconstruct: further streams that share each subset's strided copies
+  cudaStream_t copy_side[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t ev_side[3][2] = {};
   char *stage[2] = {nullptr, nullptr};
   size_t stage_bytes = 0;
   // pipelined reconstruction: the view pairs of one subset staged pair-major
@@ -69,7 +72,6 @@ struct hrrt_ctx {
   // back projector of the OSEM loop, and the device geometry it runs with
   // (for the adjoint: segment weights of 1, the forward projector's scaling)
   int bp_mode = HRRT_BP_REF;
-  int staging = HRRT_STAGE_F32;  // shared-memory staging of the OSEM subsets' projectors
   hrrt::DevGeom dg_adj{};
   int *d_view1 = nullptr;       // one view index, for single-pair entry points
 
@@ -110,6 +112,11 @@ struct hrrt_ctx {
       if (ev_free[b]) cudaEventDestroy(ev_free[b]);
     }
     if (copy_stream) cudaStreamDestroy(copy_stream);
+    for (int i = 0; i < 3; i++) {
+      if (copy_side[i]) cudaStreamDestroy(copy_side[i]);
+      for (int b = 0; b < 2; b++)
+        if (ev_side[i][b]) cudaEventDestroy(ev_side[i][b]);
+    }
     if (stream) cudaStreamDestroy(stream);
   }
 };

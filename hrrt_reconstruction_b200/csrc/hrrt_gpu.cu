@@ -215,7 +215,6 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
   float *nf = ctx->d_nfinv + (size_t)s * ctx->vol;
   const bool single = b.fr.n == 1 && !b.fr.map;
   const bool map = single && ctx->map_on && ctx->subsets_done >= ctx->map_first;
-  const bool stage16 = ctx->staging == HRRT_STAGE_BF16;
   if (single) ctx->subsets_done++;
   if (map) {
     // je_hrrt_osem3d's subset with MAP (hrrt_osem3d.cpp:4439-4463): the
@@ -229,7 +228,7 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
     {
       Launch L(ctx, "fp_kernel");
       CK(launch_fp(g, proj, fw, ctx->fp_cnt[s], 1, b.prompts, b.add, ctx->storage, b.ratio, ctx->quad_pair,
-                   ctx->tune, b.fr, ctx->stream, stage16),
+                   ctx->tune, b.fr, ctx->stream),
          "fp_kernel");
     }
     if (adj) {
@@ -243,7 +242,7 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
       {
         Launch L(ctx, "bp_kernel");
         CK(launch_bp(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, ctx->tune, b.fr,
-                     ctx->stream, stage16),
+                     ctx->stream),
            "bp_kernel");
       }
       Launch L(ctx, "rotback_kernel");
@@ -269,7 +268,7 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
     {
       Launch L(ctx, "fp_kernel");
       CK(launch_fp(g, ctx->d_image_psf, fw, ctx->fp_cnt[s], 1, b.prompts, b.add, ctx->storage, b.ratio,
-                   ctx->quad_pair, ctx->tune, b.fr, ctx->stream, stage16),
+                   ctx->quad_pair, ctx->tune, b.fr, ctx->stream),
          "fp_kernel");
     }
     if (adj) {
@@ -281,7 +280,7 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
          "adj_rotate_kernel");
     } else {
       CK(launch_bp(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, ctx->tune, b.fr,
-                   ctx->stream, stage16),
+                   ctx->stream),
          "bp_kernel");
       CK(launch_rotback(g, pv, ctx->npairs, b.bc, b.br, ctx->vol, nullptr, nullptr, ctx->d_corr, 3, b.fr,
                         ctx->stream),
@@ -294,7 +293,7 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
   {
     Launch L(ctx, "fp_kernel");
     CK(launch_fp(g, b.image, fw, ctx->fp_cnt[s], 1, b.prompts, b.add, ctx->storage, b.ratio, ctx->quad_pair,
-                 ctx->tune, b.fr, ctx->stream, stage16),
+                 ctx->tune, b.fr, ctx->stream),
        "fp_kernel");
   }
   if (adj) {
@@ -310,8 +309,7 @@ int run_subset(hrrt_ctx *ctx, int s, const SubsetBufs &b) {
   }
   {
     Launch L(ctx, "bp_kernel");
-    CK(launch_bp(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, ctx->tune, b.fr, ctx->stream,
-                 stage16),
+    CK(launch_bp(g, b.ratio, ctx->quad_pair, bw, ctx->bp_cnt[s], b.bc, b.br, ctx->vol, ctx->tune, b.fr, ctx->stream),
        "bp_kernel");
   }
   Launch L(ctx, "rotback_kernel");
@@ -928,6 +926,12 @@ int hrrt_osem(hrrt_ctx *ctx, int iterations, hrrt_stats *stats) {
   return HRRT_OK;
 }
 
+#ifndef HRRT_COPY_STREAMS
+#define HRRT_COPY_STREAMS 1
+#endif
+constexpr int kCopyStreams = HRRT_COPY_STREAMS;  // 1..4
+static_assert(kCopyStreams >= 1 && kCopyStreams <= 4, "copy streams");
+
 int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms, const float *norm,
                      const float *atten, const float *scatter, int storage, const float *init_image_zyx,
                      int iterations, float *image_zyx, hrrt_stats *stats) {
@@ -994,6 +998,8 @@ int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms
   CK(cudaEventCreate(&tb), "event");
   auto bail = [&](int rc) {
     cudaStreamSynchronize(ctx->copy_stream);
+    for (int i = 0; i < 3; i++)
+      if (ctx->copy_side[i]) cudaStreamSynchronize(ctx->copy_side[i]);
     cudaStreamSynchronize(ctx->stream);
     cudaEventDestroy(ta);
     cudaEventDestroy(tb);
@@ -1006,10 +1012,22 @@ int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms
   CK(cudaMemcpyAsync(ctx->pflat, prompts, sizeof(int16_t) * pelems, cudaMemcpyHostToDevice, ctx->copy_stream),
      "reconstruct prompts");
   const int S = g.sp.subsets;
+  // a subset's strided copies are dealt out over kCopyStreams streams
+  cudaStream_t cst[kCopyStreams];
+  cst[0] = ctx->copy_stream;
+  for (int i = 1; i < kCopyStreams; i++) {
+    if (!ctx->copy_side[i - 1]) {
+      CK(cudaStreamCreateWithFlags(&ctx->copy_side[i - 1], cudaStreamNonBlocking), "copy stream");
+      for (int b = 0; b < 2; b++)
+        CK(cudaEventCreateWithFlags(&ctx->ev_side[i - 1][b], cudaEventDisableTiming), "event");
+    }
+    cst[i] = ctx->copy_side[i - 1];
+  }
   for (int k = 0; k < S; k++) {
     const int s = g.order[k], b = k & 1;
     float *stg[4] = {nullptr, nullptr, nullptr, nullptr};
-    e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_free[b], 0);
+    for (int c = 0; c < kCopyStreams && e == cudaSuccess; c++) e = cudaStreamWaitEvent(cst[c], ctx->ev_free[b], 0);
+    int nc = 0;
     for (int j = 0; j < ctx->npairs && e == cudaSuccess; j++) {
       const int v = g.vieworder[(size_t)s * g.sviews + j];
       for (int h = 0; h < 2 && e == cudaSuccess; h++) {
@@ -1018,9 +1036,13 @@ int hrrt_reconstruct(hrrt_ctx *ctx, const int16_t *prompts, const float *randoms
           if (!srcs[i]) continue;
           stg[i] = reinterpret_cast<float *>(ctx->pstage[b] + (size_t)i * set_elems * sizeof(float));
           e = cudaMemcpy2DAsync(stg[i] + doff, N * sizeof(float), srcs[i] + view * N, V * N * sizeof(float),
-                                N * sizeof(float), P, cudaMemcpyHostToDevice, ctx->copy_stream);
+                                N * sizeof(float), P, cudaMemcpyHostToDevice, cst[nc++ % kCopyStreams]);
         }
       }
+    }
+    for (int c = 1; c < kCopyStreams && e == cudaSuccess; c++) {
+      e = cudaEventRecord(ctx->ev_side[c - 1][b], cst[c]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_side[c - 1][b], 0);
     }
     if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_copied[b], ctx->copy_stream);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_copied[b], 0);
@@ -1347,14 +1369,6 @@ int hrrt_set_backprojector(hrrt_ctx *ctx, int mode) {
     ctx->config_epoch++;
   }
   ctx->bp_mode = mode;
-  return HRRT_OK;
-}
-
-int hrrt_set_staging(hrrt_ctx *ctx, int mode) {
-  if (!ctx) return HRRT_ERR_ARG;
-  if (mode != HRRT_STAGE_F32 && mode != HRRT_STAGE_BF16) return fail(ctx, HRRT_ERR_ARG, "unknown staging");
-  if (mode != ctx->staging) ctx->config_epoch++;
-  ctx->staging = mode;
   return HRRT_OK;
 }
 

@@ -118,21 +118,6 @@ __device__ __forceinline__ Q2 ldq(const float4 *p) {
   const ulonglong2 v = *reinterpret_cast<const ulonglong2 *>(p);
   return Q2{v.x, v.y};
 }
-// a staged entry of four bf16 lanes (lanes 0,1 in .x, low half first),
-// widened to float exactly (a bf16 is the top half of a float)
-__device__ __forceinline__ uint64_t bf2f2(uint32_t w) {
-  return pk(__uint_as_float(w << 16), __uint_as_float(w & 0xFFFF0000u));
-}
-__device__ __forceinline__ Q2 ldq(const uint2 *p) {
-  const uint2 u = *p;
-  return Q2{bf2f2(u.x), bf2f2(u.y)};
-}
-// four float lanes (two packed pairs) rounded to bf16 (nearest, ties to even)
-__device__ __forceinline__ uint2 f2bf4(uint64_t lo, uint64_t hi) {
-  const float2 a = upk(lo), b = upk(hi);
-  const __nv_bfloat162 x = __floats2bfloat162_rn(a.x, a.y), y = __floats2bfloat162_rn(b.x, b.y);
-  return make_uint2(*reinterpret_cast<const uint32_t *>(&x), *reinterpret_cast<const uint32_t *>(&y));
-}
 __device__ __forceinline__ Q2 qadd(Q2 a, Q2 b) { return Q2{add2(a.lo, b.lo), add2(a.hi, b.hi)}; }
 __device__ __forceinline__ Q2 qsub(Q2 a, Q2 b) { return Q2{sub2(a.lo, b.lo), sub2(a.hi, b.hi)}; }
 __device__ __forceinline__ Q2 qmul(Q2 a, uint64_t s) { return Q2{mul2(a.lo, s), mul2(a.hi, s)}; }
@@ -231,6 +216,13 @@ __device__ __forceinline__ float bilinear(const float *__restrict__ img, const S
 // (pam: lanes (x,y),(N-x,y),(N-y,x),(N-y,N-x); pam2: (x,N-y),(N-x,N-y),(y,x),
 // (y,N-x)), then every thread accumulates its own (segment, plane-run) outputs
 // for all four lanes, row by row in the reference's order.
+// The consumers are bound by instruction issue and shared-load latency (64
+// registers a thread at 1024 threads), not by shared-memory bandwidth.
+// Measured on B200 at span 3 and not used: rows staged as bf16 (half the
+// shared bytes, plus the widening: 1.89 -> 1.89 ms), consumer warps split
+// into two or three groups with a row-ready barrier each (2.12, 2.23 ms), and
+// two CTAs per quad with half the tasks each, two CTAs or one of 128
+// registers per SM (2.01, 3.27 ms).
 // ============================================================================
 // named barriers (id 0 is __syncthreads); ids are immediates so the kernel
 // reserves only the barriers it uses
@@ -257,9 +249,7 @@ __device__ __forceinline__ void bar_sync(int id, int count) {
     case 10: bar_sync_id<10>(count); break;
     case 11: bar_sync_id<11>(count); break;
     case 12: bar_sync_id<12>(count); break;
-    case 13: bar_sync_id<13>(count); break;
-    case 14: bar_sync_id<14>(count); break;
-    default: bar_sync_id<15>(count); break;
+    default: bar_sync_id<13>(count); break;
   }
 }
 __device__ __forceinline__ void bar_arrive(int id, int count) {
@@ -275,27 +265,15 @@ __device__ __forceinline__ void bar_arrive(int id, int count) {
     case 9: bar_arrive_id<9>(count); break;
     case 10: bar_arrive_id<10>(count); break;
     case 11: bar_arrive_id<11>(count); break;
-    case 12: bar_arrive_id<12>(count); break;
-    case 13: bar_arrive_id<13>(count); break;
-    default: bar_arrive_id<14>(count); break;
+    default: bar_arrive_id<12>(count); break;
   }
 }
-// + group * slots + slot: sampled row ready for one consumer group (producers
-// arrive, the group's consumers wait).  Groups of consumer warps wait for a
-// row independently, so a group that finishes a row early starts the next
-// one while the others finish theirs (within the rows in flight).
-constexpr int kBarFull = 1;
-constexpr int kBarEmpty = 1 + kFpGroups * kFpSlots;  // + slot: sampled row consumed (consumers arrive, producers wait)
-constexpr int kBarProd = kBarEmpty + kFpSlots;       // producers only: corner slot read by every producer
-static_assert(kBarProd <= 15, "named barrier ids");
-// consumer warps [fp_group_lo(gi), fp_group_lo(gi + 1)) form group gi
-__device__ __forceinline__ int fp_group_lo(int gi, int cwarps, int ng) { return (gi * cwarps + ng - 1) / ng; }
+constexpr int kBarFull = 1;                 // + slot: sampled row ready (producers arrive, consumers wait)
+constexpr int kBarEmpty = 1 + kFpSlots;     // + slot: sampled row consumed (consumers arrive, producers wait)
+constexpr int kBarProd = 1 + 2 * kFpSlots;  // producers only: corner slot read by every producer
+static_assert(kBarProd <= 13, "named barrier ids");
 
-// RT: the staged row entry, float4 (four float lanes: the reference's
-// arithmetic, bit for bit) or uint2 (four bf16 lanes: half the shared-memory
-// bytes per sample, for the OSEM subsets of the 16-bit precision form; the
-// samples are rounded once, the arithmetic and the sums stay float)
-template <int MODE, int PL, int MW, typename PT, typename AT, typename RT = float4>
+template <int MODE, int PL, int MW, typename PT, typename AT>
 __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *__restrict__ image,
                                                      const QuadWork *__restrict__ work,
                                                      const PT *__restrict__ prompts, const AT *__restrict__ add,
@@ -312,8 +290,8 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
   float *corners = reinterpret_cast<float *>(smem);
   const int zoff = kFpSlots * 8 * 2 * cpair;
   float *zcol = corners + zoff;
-  RT *rows = reinterpret_cast<RT *>(smem + (size_t)(kFpSlots * 8 * 2 + 2) * cpair / 4);  // [S][2][ZS]
-  float4 *cen = reinterpret_cast<float4 *>(rows + 2 * kFpSlots * ZS);
+  float4 *rows = smem + (size_t)(kFpSlots * 8 * 2 + 2) * cpair / 4;  // [S][2][ZS]
+  float4 *cen = rows + 2 * kFpSlots * ZS;
   __shared__ ulonglong2 s_w[kFpSlots][4][2];
   __shared__ int s_off[kFpSlots][8];
   // each row's middle-plane sampling entries (z, f, z2, f2 per group),
@@ -342,12 +320,6 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
   const int ncons = nthr - nprod;        // consumer threads: one task each
   const bool producer = tid >= ncons;
   const int ptid = tid - ncons;
-  const int cwarps = ncons / 32, ngroups = min(kFpGroups, cwarps);
-  int my_group = 0;
-  if (!producer)
-    while (my_group + 1 < ngroups && tid / 32 >= fp_group_lo(my_group + 1, cwarps, ngroups)) my_group++;
-  const int my_full_count =
-      (fp_group_lo(my_group + 1, cwarps, ngroups) - fp_group_lo(my_group, cwarps, ngroups)) * 32 + nprod;
 
   // TMA issue (producer lanes 0-7, one sample point each): the two contiguous
   // column pairs (ix, iy..iy+1) and (ix+1, iy..iy+1) of each inside point
@@ -395,9 +367,9 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
     for (int s = 0; s < kFpSlots; s++) mbar_init(&s_bar[s], 1);
     fence_mbar_init();
   }
-  for (int i = tid; i < 2 * kFpSlots * kFpZPad; i += nthr) {
+  for (int i = tid; i < (2 * kFpSlots + 1) * kFpZPad; i += nthr) {
     const int col = i / kFpZPad, k = i % kFpZPad;
-    rows[col * ZS + zp + k] = RT{};
+    rows[col * ZS + zp + k] = f4(0.f);
   }
   for (int i = tid; i < 2 * cpair; i += nthr) zcol[i] = 0.f;
   __syncthreads();
@@ -433,7 +405,7 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
       {
         // lanes (0,1) and (2,3) of this half share nothing but the plane: each
         // lane pair is evaluated with packed pairs, its weights pre-packed
-        RT *rw = rows + (size_t)sl * 2 * ZS + h_mine * ZS;
+        float4 *rw = rows + (size_t)sl * 2 * ZS + h_mine * ZS;
         for (int z = z_mine; z < zp; z += hsplit) {
           uint64_t vv[2];
 #pragma unroll
@@ -446,15 +418,10 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
             const uint64_t r3 = pk(qa[zp + z], qb[zp + z]), r4 = pk(qa[cpair + zp + z], qb[cpair + zp + z]);
             vv[pp] = add2(addp(mul2(r1, wa.x), mul2(r2, wa.y), one), addp(mul2(r3, wb.x), mul2(r4, wb.y), one));
           }
-          if constexpr (std::is_same<RT, float4>::value)
-            *reinterpret_cast<ulonglong2 *>(rw + z) = make_ulonglong2(vv[0], vv[1]);
-          else
-            rw[z] = f2bf4(vv[0], vv[1]);
+          *reinterpret_cast<ulonglong2 *>(rw + z) = make_ulonglong2(vv[0], vv[1]);
         }
       }
-      for (int gi = 0; gi < ngroups; gi++)
-        bar_arrive(kBarFull + gi * kFpSlots + sl,
-                   (fp_group_lo(gi + 1, cwarps, ngroups) - fp_group_lo(gi, cwarps, ngroups)) * 32 + nprod);
+      bar_arrive(kBarFull + sl, nthr);
       // every producer has finished reading corner slot sl: refill it with row r+S
       bar_sync(kBarProd, nprod);
       if (ptid < 8 && r + kFpSlots < nrows) issue_row(r + kFpSlots);
@@ -487,9 +454,9 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
   const int FS = g.groupmax * 2 * g.zshift;
   for (int r = 0; r < nrows; r++) {
     const int sl = r % kFpSlots, es = r % (2 * kFpSlots), y = ystart + r;
-    bar_sync(kBarFull + my_group * kFpSlots + sl, my_full_count);
-    const RT *pam = rows + (size_t)sl * 2 * ZS;
-    const RT *pam2 = pam + ZS;
+    bar_sync(kBarFull + sl, nthr);
+    const float4 *pam = rows + (size_t)sl * 2 * ZS;
+    const float4 *pam2 = pam + ZS;
     if (tk.type == 0) {
       // theta = 0 (sbrt:1907-1910)
 #pragma unroll
@@ -498,11 +465,11 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
       const FpMid m = s_mid[es][gs];
       if (m.z >= 0) {  // else the group is skipped for this row (sbrt:1923-1924)
         // segment 2k accumulates pam at z and pam2 at z2; segment 2k-1 the converse
-        const RT *A = odd ? pam2 : pam;
-        const RT *B = odd ? pam : pam2;
+        const float4 *A = odd ? pam2 : pam;
+        const float4 *B = odd ? pam : pam2;
         if (tk.type == 1) {
           // middle planes: z, z2 advance with the plane (sbrt:1933-1947)
-          const RT *Aw = A + m.z + pofs, *Bw = B + m.z2 + pofs;
+          const float4 *Aw = A + m.z + pofs, *Bw = B + m.z2 + pofs;
           const uint64_t f = pk(m.f, m.f), f2 = pk(m.f2, m.f2);
           Q2 a0 = ldq(Aw), b0 = ldq(Bw);
 #pragma unroll
@@ -586,25 +553,19 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
 // different 16-byte bank groups without the shared memory a padding would
 // cost.
 __device__ __forceinline__ int bsw(int i) { return i ^ ((i >> 3) & 7); }
-// bf16 lanes (8 bytes a plane): the same rule on 128-byte lines of 16 planes
-// (the plane's position within its line XORed with the line's index), which
-// keeps the swizzle inside aligned groups of 8 planes
-__device__ __forceinline__ int bsw16(int i) { return i ^ ((i >> 4) & 7); }
-__device__ __forceinline__ int bsw_of(const float4 *, int i) { return bsw(i); }
-__device__ __forceinline__ int bsw_of(const uint2 *, int i) { return bsw16(i); }
 
-template <int KB, typename RT>
-__device__ __forceinline__ void bp_lerp(Q2 (&s)[KB], const RT *__restrict__ P, int pbase, const BpLut &bl,
+template <int KB>
+__device__ __forceinline__ void bp_lerp(Q2 (&s)[KB], const float4 *__restrict__ P, int pbase, const BpLut &bl,
                                         int z0, uint64_t one) {
   // windows wholly outside [zs, ze] contribute nothing; a window that
   // straddles an end reads the segment's zero planes for its outside planes
   if (z0 + KB - 1 < bl.zs || z0 > bl.ze) return;
   const int i0 = pbase + z0 + bl.d;
   const uint64_t f = pk(bl.f, bl.f);
-  Q2 a = ldq(P + bsw_of(P, i0));
+  Q2 a = ldq(P + bsw(i0));
 #pragma unroll
   for (int j = 0; j < KB; j++) {
-    const Q2 b = ldq(P + bsw_of(P, i0 + j + 1));
+    const Q2 b = ldq(P + bsw(i0 + j + 1));
     // the reference's p[yr] + f*(p[yr+1]-p[yr]) (sbrt:4312-4315)
     s[j] = qadd(s[j], qaddp(a, qmul(qsub(b, a), f), one));
     a = b;
@@ -629,16 +590,13 @@ __device__ __forceinline__ void store_lane(float *__restrict__ dst, const Q2 (&s
   }
 }
 
-// ST: the staged plane of a quad, float4 (the reference's arithmetic) or
-// uint2 (four bf16 lanes, the 16-bit precision form's OSEM subsets)
-template <int KB, bool ACC = false, bool MULTI = false, int NT = 256, typename ST = float4>
+template <int KB, bool ACC = false, bool MULTI = false, int NT = 256>
 __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(DevGeom g, const float4 *__restrict__ in, long long in_pair_stride,
                                                  const QuadWork *__restrict__ work, float *__restrict__ bc,
                                                  float *__restrict__ br, long long vol, FrameStrides fr,
                                                  int view0, int x0, int rlog) {
   const uint64_t one = pk(g.unit, g.unit);
-  extern __shared__ float4 P_raw[];
-  ST *P = reinterpret_cast<ST *>(P_raw);  // [bp_splanes]: segments with kBpPad zero planes each side
+  extern __shared__ float4 P[];  // [bp_splanes]: segments with kBpPad zero planes each side
   // ACC: one view pair, quads x0 + blockIdx.x, both partial sums added into bc
   // (each voxel receives exactly two terms, so the atomic adds onto a zeroed
   // buffer give a + b whatever their order)
@@ -659,12 +617,7 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(De
   if (!masked)
     for (int i = threadIdx.x; i < g.bp_splanes; i += blockDim.x) {
       const int q = __ldg(g.bp_src + i);
-      if constexpr (std::is_same<ST, float4>::value) {
-        P[bsw(i)] = (q >= 0) ? src[q] : f4(0.f);
-      } else {
-        const float4 v = (q >= 0) ? src[q] : f4(0.f);
-        P[bsw16(i)] = f2bf4(pk(v.x, v.y), pk(v.z, v.w));
-      }
+      P[bsw(i)] = (q >= 0) ? src[q] : f4(0.f);
     }
   __syncthreads();
 
@@ -702,7 +655,7 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(De
     } else if (y == c) {
       // centre row (sbrt:4260-4284): rays pass plane yr = z exactly
 #pragma unroll
-      for (int j = 0; j < KB; j++) s[j] = ldq(P + bsw_of(P, o0 + z0 + j));
+      for (int j = 0; j < KB; j++) s[j] = ldq(P + bsw(o0 + z0 + j));
       for (int gg = 0; gg < G; gg++) {
         const int se = 2 * gg + 2, so = 2 * gg + 1;
         const int yb = g.ybot[se], yt = g.ytop[se];
@@ -710,12 +663,12 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(De
 #pragma unroll
         for (int j = 0; j < KB; j++) {
           const int z = z0 + j;
-          if (z >= yb && z <= yt) s[j] = qadd(s[j], qadd(ldq(P + bsw_of(P, pe + z)), ldq(P + bsw_of(P, po + z))));
+          if (z >= yb && z <= yt) s[j] = qadd(s[j], qadd(ldq(P + bsw(pe + z)), ldq(P + bsw(po + z))));
         }
       }
     } else {
 #pragma unroll
-      for (int j = 0; j < KB; j++) s[j] = ldq(P + bsw_of(P, o0 + z0 + j));
+      for (int j = 0; j < KB; j++) s[j] = ldq(P + bsw(o0 + z0 + j));
       // bplut is [group][row]: the threads of a row read the same entries
       const BpLut *l1 = g.bplut + y, *l2 = g.bplut + (N - y);
       BpLut b1 = l1[0], b2 = l2[0];
@@ -1369,7 +1322,7 @@ __global__ void scale_pairs_kernel(DevGeom g, const T *__restrict__ src, const i
   dst[(size_t)slot * dst_pair_stride + i] = o;
 }
 
-template <int MODE, int PL, int MW, typename PT, typename AT, typename RT>
+template <int MODE, int PL, int MW, typename PT, typename AT>
 cudaError_t launch_fp_t(const DevGeom &g, const float *image, const QuadWork *work, int nwork, const void *prompts,
                         const void *add, float *out, long long out_pair_stride, int pwarps_req,
                         const FrameStrides &fr, cudaStream_t st) {
@@ -1380,9 +1333,9 @@ cudaError_t launch_fp_t(const DevGeom &g, const float *image, const QuadWork *wo
   if (pwarps < 2 || cwarps + pwarps > MW) return cudaErrorInvalidConfiguration;
   const int threads = (cwarps + pwarps) * 32;
   const int ZS = g.zp + kFpZPad;
-  const size_t smem = (size_t)(kFpSlots * 8 * 2 + 2) * 2 * g.zp * sizeof(float) +
-                      (size_t)2 * kFpSlots * ZS * sizeof(RT) + (size_t)ZS * sizeof(float4);
-  auto k = fp_kernel<MODE, PL, MW, PT, AT, RT>;
+  const size_t smem =
+      (size_t)(kFpSlots * 8 * 2 + 2) * 2 * g.zp * sizeof(float) + (size_t)(2 * kFpSlots + 1) * ZS * sizeof(float4);
+  auto k = fp_kernel<MODE, PL, MW, PT, AT>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
@@ -1392,53 +1345,39 @@ cudaError_t launch_fp_t(const DevGeom &g, const float *image, const QuadWork *wo
   return cudaGetLastError();
 }
 
-template <int PL, int MW, typename RT>
-cudaError_t launch_fp_rt(const DevGeom &g, const float *image, const QuadWork *work, int nwork, int mode,
-                         const void *prompts, const void *add, int storage, float *out, long long stride, int pwarps,
-                         const FrameStrides &fr, cudaStream_t st) {
-  if (mode == 0)
-    return launch_fp_t<0, PL, MW, int16_t, float, RT>(g, image, work, nwork, nullptr, nullptr, out, stride, pwarps, fr,
-                                                      st);
-  if (storage == 0)
-    return launch_fp_t<1, PL, MW, int16_t, float, RT>(g, image, work, nwork, prompts, add, out, stride, pwarps, fr,
-                                                      st);
-  if (storage == 1)
-    return launch_fp_t<1, PL, MW, int16_t, __nv_bfloat16, RT>(g, image, work, nwork, prompts, add, out, stride,
-                                                              pwarps, fr, st);
-  return launch_fp_t<1, PL, MW, int16_t, __half, RT>(g, image, work, nwork, prompts, add, out, stride, pwarps, fr,
-                                                     st);
-}
-
 template <int PL, int MW>
 cudaError_t launch_fp_pl(const DevGeom &g, const float *image, const QuadWork *work, int nwork, int mode,
                          const void *prompts, const void *add, int storage, float *out, long long stride, int pwarps,
-                         const FrameStrides &fr, bool stage16, cudaStream_t st) {
-  // bf16 staging only where it is asked for: the ratio of an OSEM subset
-  if (stage16 && mode == 1)
-    return launch_fp_rt<PL, MW, uint2>(g, image, work, nwork, mode, prompts, add, storage, out, stride, pwarps, fr,
-                                       st);
-  return launch_fp_rt<PL, MW, float4>(g, image, work, nwork, mode, prompts, add, storage, out, stride, pwarps, fr,
-                                      st);
+                         const FrameStrides &fr, cudaStream_t st) {
+  if (mode == 0)
+    return launch_fp_t<0, PL, MW, int16_t, float>(g, image, work, nwork, nullptr, nullptr, out, stride, pwarps, fr,
+                                                  st);
+  if (storage == 0)
+    return launch_fp_t<1, PL, MW, int16_t, float>(g, image, work, nwork, prompts, add, out, stride, pwarps, fr, st);
+  if (storage == 1)
+    return launch_fp_t<1, PL, MW, int16_t, __nv_bfloat16>(g, image, work, nwork, prompts, add, out, stride, pwarps,
+                                                          fr, st);
+  return launch_fp_t<1, PL, MW, int16_t, __half>(g, image, work, nwork, prompts, add, out, stride, pwarps, fr, st);
 }
 
 }  // namespace
 
 cudaError_t launch_fp(const DevGeom &g, const float *image, const QuadWork *work, int nwork, int mode,
                       const void *prompts, const void *add, int storage, float *out, long long out_pair_stride,
-                      const ProjTune &tune, const FrameStrides &fr, cudaStream_t st, bool stage16) {
+                      const ProjTune &tune, const FrameStrides &fr, cudaStream_t st) {
   if (nwork <= 0 || fr.n <= 0) return cudaSuccess;
   static_assert(kFpPlaneVariants[0] == 7 && kFpPlaneVariants[1] == 9 && kFpPlaneVariants[2] == 11, "variants");
   const int pl = tune.fp_planes > 0 ? tune.fp_planes : kFpPlanes;
   switch (pl) {
     case 7:
       return launch_fp_pl<7, kFpVariantWarps[0]>(g, image, work, nwork, mode, prompts, add, storage, out,
-                                                 out_pair_stride, tune.fp_pwarps, fr, stage16, st);
+                                                 out_pair_stride, tune.fp_pwarps, fr, st);
     case 9:
       return launch_fp_pl<9, kFpVariantWarps[1]>(g, image, work, nwork, mode, prompts, add, storage, out,
-                                                 out_pair_stride, tune.fp_pwarps, fr, stage16, st);
+                                                 out_pair_stride, tune.fp_pwarps, fr, st);
     case 11:
       return launch_fp_pl<11, kFpVariantWarps[2]>(g, image, work, nwork, mode, prompts, add, storage, out,
-                                                  out_pair_stride, tune.fp_pwarps, fr, stage16, st);
+                                                  out_pair_stride, tune.fp_pwarps, fr, st);
     default:
       return cudaErrorInvalidValue;
   }
@@ -1455,12 +1394,12 @@ int bp_tile_log2(const DevGeom &g, const ProjTune &t) {
   return -1;
 }
 
-template <int KB, int NT, typename RT = float4>
+template <int KB, int NT>
 cudaError_t launch_bp_t(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
                         float *bc, float *br, long long vol, const FrameStrides &fr, int rlog, cudaStream_t st) {
   static_assert(kBpPad >= KB, "a straddling window must stay inside the zero planes");
-  const size_t smem = (size_t)g.bp_splanes * sizeof(RT);
-  auto k = fr.n > 1 ? bp_kernel<KB, false, true, NT, RT> : bp_kernel<KB, false, false, NT, RT>;
+  const size_t smem = (size_t)g.bp_splanes * sizeof(float4);
+  auto k = fr.n > 1 ? bp_kernel<KB, false, true, NT> : bp_kernel<KB, false, false, NT>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
@@ -1472,7 +1411,7 @@ cudaError_t launch_bp_t(const DevGeom &g, const float *in, long long in_pair_str
 
 cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
                       float *bc, float *br, long long vol, const ProjTune &tune, const FrameStrides &fr,
-                      cudaStream_t st, bool stage16) {
+                      cudaStream_t st) {
   if (nwork <= 0 || fr.n <= 0) return cudaSuccess;
   const int kb = tune.bp_planes > 0 ? tune.bp_planes : kBpZ;
   // 384 threads (two CTAs of 80 registers per SM) measured faster than 256
@@ -1480,17 +1419,6 @@ cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_strid
   const int nt = tune.bp_threads > 0 ? tune.bp_threads : 384;
   const int rl = bp_tile_log2(g, tune);
   if (rl < 0) return cudaErrorInvalidValue;
-  if (stage16) {
-    if (kb == 8 && nt == 256)
-      return launch_bp_t<8, 256, uint2>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, rl, st);
-    if (kb == 8 && nt == 384)
-      return launch_bp_t<8, 384, uint2>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, rl, st);
-    if (kb == 4 && nt == 256)
-      return launch_bp_t<4, 256, uint2>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, rl, st);
-    if (kb == 4 && nt == 384)
-      return launch_bp_t<4, 384, uint2>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, rl, st);
-    return cudaErrorInvalidValue;
-  }
   if (kb == 8 && nt == 256) return launch_bp_t<8, 256>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, rl, st);
   if (kb == 8 && nt == 384) return launch_bp_t<8, 384>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, rl, st);
   if (kb == 4 && nt == 256) return launch_bp_t<4, 256>(g, in, in_pair_stride, work, nwork, bc, br, vol, fr, rl, st);

@@ -29,11 +29,7 @@ namespace hrrt {
 #ifndef HRRT_BP_MIN_BLOCKS
 #define HRRT_BP_MIN_BLOCKS 3
 #endif
-#ifndef HRRT_FP_GROUPS
-#define HRRT_FP_GROUPS 1
-#endif
-constexpr int kFpGroups = HRRT_FP_GROUPS;      // consumer warp groups, each with its own row-ready barrier
-constexpr int kFpPlanes = 9;                  // default planes per forward-projection task (odd: bank-conflict free)
+constexpr int kFpPlanes = 9;                   // default planes per forward-projection task (odd: bank-conflict free)
 constexpr int kFpSlots = HRRT_FP_SLOTS;       // sampled rows in flight between producers and consumers
 constexpr int kFpZPad = 16;     // zeroed entries after each sampled row
 constexpr int kFpEndPlanes = 4; // planes per end-plane task (they cost ~2x a middle plane)
@@ -145,14 +141,11 @@ constexpr int kFpVariantWarps[3] = {32, 32, 24};
 // `g.fptasks` must be the task list built for tune.fp_planes.
 cudaError_t launch_fp(const DevGeom &g, const float *image, const QuadWork *work, int nwork, int mode,
                       const void *prompts, const void *add, int storage, float *out, long long out_pair_stride,
-                      const ProjTune &tune, const FrameStrides &fr, cudaStream_t st, bool stage16 = false);
-// stage16 (mode 1 only): the sampled rows are staged in shared memory as bf16
-// (half the bytes per sample; float arithmetic and sums) instead of float;
-// in launch_bp the quad's planes are.
+                      const ProjTune &tune, const FrameStrides &fr, cudaStream_t st);
 // back projection of quad-layout input into the column (Bc) / row (Br) partials
 cudaError_t launch_bp(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,
                       float *bc, float *br, long long vol, const ProjTune &tune, const FrameStrides &fr,
-                      cudaStream_t st, bool stage16 = false);
+                      cudaStream_t st);
 // exact adjoint of the forward projector: z-transpose into the column / row
 // partials (rows scaled as the forward projector scales them)
 cudaError_t launch_adj(const DevGeom &g, const float *in, long long in_pair_stride, const QuadWork *work, int nwork,

@@ -59,13 +59,15 @@ constexpr int kSinoPlane = 256 * 288;
 // partition by partition in L2.  On B200, for 2.5e8 events: direct 14.3 ms,
 // wide 17.0 ms (the random read-modify-write of a DRAM sector per event bounds
 // both; the wide path adds a clear and a fold of 4-byte counters), partitioned
-// 21.0 ms (two extra parses), so the other two run only when asked for.
+// 21.0 ms (two extra parses), so the other two run only when asked for.  A
+// fourth way, rebinning every event into a 4-byte record in stream order and
+// adding the records in a separate pass with 30 registers a thread (eight
+// blocks per SM, more adds in flight), measured 19.1 ms: the adds are bound
+// by the DRAM sectors they read and write, not by how many are in flight.
 constexpr bool kPartitionedByDefault = false;
 constexpr long long kPartitionMinWords = 1LL << 24;
 constexpr bool kWideByDefault = false;
 constexpr long long kWideMinWords = 1LL << 26;
-constexpr bool kRecordsByDefault = false;
-constexpr long long kRecordsMinWords = 1LL << 24;
 // EWTYPES (geometry_info.h:76) packed two bits per entry: index =
 // (ew1 >> 30) << 2 | (ew2 >> 30); 0 prompt, 1 delayed, 2 tag, 3 out of sync
 constexpr uint32_t kEwTypes = (3u << 0) | (3u << 2) | (1u << 4) | (0u << 6) | (3u << 8) | (3u << 10) | (2u << 12) |
@@ -212,24 +214,46 @@ __global__ void __launch_bounds__(kThreads) lm_map_kernel(const uint32_t *__rest
                            ((unsigned long long)incl.c1 << 40);
 }
 
-// One thread per packet: tile entries and tag offsets within the packet.
-__global__ void lm_entry_kernel(const unsigned long long *__restrict__ tile_sum, long long ntiles, int tiles_per_packet,
-                                long long npackets, uint8_t *__restrict__ tile_entry,
-                                unsigned int *__restrict__ tile_tagoff, unsigned long long *__restrict__ packet_tags) {
-  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per packet: tile entries and tag offsets within the packet.  Each
+// lane composes the summaries of its run of tiles, a warp scan gives every
+// run its entry (a packet is parsed from its first word: entry 0) and tag
+// offset, and the lane walks its run again to write them.
+constexpr int kEntryThreads = 128;
+__global__ void __launch_bounds__(kEntryThreads) lm_entry_kernel(const unsigned long long *__restrict__ tile_sum,
+                                                                 long long ntiles, int tiles_per_packet,
+                                                                 long long npackets, uint8_t *__restrict__ tile_entry,
+                                                                 unsigned int *__restrict__ tile_tagoff,
+                                                                 unsigned long long *__restrict__ packet_tags) {
+  const long long p = ((long long)blockIdx.x * kEntryThreads + threadIdx.x) >> 5;  // the same in the whole warp
+  const int lane = threadIdx.x & 31;
   if (p >= npackets) return;
   const long long t_begin = p * tiles_per_packet;
   const long long t_end = min(t_begin + tiles_per_packet, ntiles);
-  uint32_t e = 0;
-  unsigned long long off = 0;
-  for (long long t = t_begin; t < t_end; t++) {
+  const int per = (tiles_per_packet + 31) / 32;
+  const long long lb = min(t_begin + (long long)lane * per, t_end), le = min(lb + per, t_end);
+  auto tile = [](unsigned long long s) {
+    return Sub{(uint32_t)(s & 3u), (uint32_t)((s >> 16) & 0xFFFFFF), (uint32_t)((s >> 40) & 0xFFFFFF)};
+  };
+  Sub run{2u, 0u, 0u};  // identity: 0 -> 0, 1 -> 1
+  for (long long t = lb; t < le; t++) run = compose(run, tile(tile_sum[t]));
+  Sub incl = run;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const Sub o = shfl_up_sub(incl, d);
+    if (lane >= d) incl = compose(o, incl);
+  }
+  const Sub prev = shfl_up_sub(incl, 1);
+  const Sub excl = lane > 0 ? prev : Sub{2u, 0u, 0u};
+  uint32_t e = excl.map & 1u;  // entering the packet at offset 0
+  unsigned long long off = excl.c0;
+  for (long long t = lb; t < le; t++) {
     const unsigned long long s = tile_sum[t];
     tile_entry[t] = (uint8_t)e;
     tile_tagoff[t] = (unsigned int)off;
     off += e ? ((s >> 40) & 0xFFFFFF) : ((s >> 16) & 0xFFFFFF);
     e = (uint32_t)((s >> e) & 1);
   }
-  packet_tags[p] = off;
+  if (lane == 31) packet_tags[p] = incl.c0;
 }
 
 // Exclusive scan of the per-packet tag counts (one block).
@@ -298,7 +322,6 @@ __device__ __forceinline__ long long rebin_address(const LmDev &g, const LmShare
 // 16-bit bins) each, prompts-side partitions first.
 constexpr int kPartShift = 25;
 constexpr int kMaxParts = 64;
-constexpr uint32_t kRecNone = 0xFFFFFFFFu;  // an empty record slot (bit 31 set: no sinogram address)
 
 // Walk one thread's words from its entry offset: count the statistics (kStats),
 // record time tags in stream order (when tags != null), and hand every
@@ -515,9 +538,7 @@ __device__ __forceinline__ void bump16_events(uint32_t *__restrict__ sino, uint3
 // records (address | sinogram << 29 | subtract << 30) partition-major; 4:
 // histogram into 32-bit counters with reductions that return nothing (no
 // carry to check, so no read-modify-write round trip per event), folded into
-// the 16-bit bins afterwards; 5: the same packed records in stream order,
-// kSub/2 slots per thread (kRecNone where a slot holds no event), added by
-// lm_rec_hist_kernel.  Statistics are counted by modes 1, 2, 4 and 5.
+// the 16-bit bins afterwards.  Statistics are counted by modes 1, 2 and 4.
 #ifndef HRRT_LM_MIN_BLOCKS
 #define HRRT_LM_MIN_BLOCKS 3  // 4 and 5 (64 and 48 registers, with spills) measured slower on B200
 #endif
@@ -576,27 +597,6 @@ __global__ void __launch_bounds__(kThreads, HRRT_LM_MIN_BLOCKS) lm_hist_kernel(
                       [&](const long long (&a)[kSub / 2], uint32_t live, uint32_t sel, uint32_t minus) {
                         bump16_events<kSub / 2>(sino, dly, a, live, sel, minus);
                       });
-  } else if (kMode == 5) {
-    // this thread's kSub/2 record slots, written whole (two 16-byte stores)
-    uint4 *slot = reinterpret_cast<uint4 *>(records + ((size_t)tile * kThreads + threadIdx.x) * (kSub / 2));
-    bool written = false;
-    walk_events<true>(g, tb, w, s, e, pend, t0, limit, mode, flags, c, tagpos, tag_cap, tg,
-                      [&](long long addr, int sel, bool minus) { bump16(sel ? dly : sino, addr, minus); },
-                      [&](const long long (&a)[kSub / 2], uint32_t live, uint32_t sel, uint32_t minus) {
-                        uint32_t r[kSub / 2];
-#pragma unroll
-                        for (int k = 0; k < kSub / 2; k++)
-                          r[k] = ((live >> k) & 1) ? ((uint32_t)a[k] | (((sel >> k) & 1) << 29) |
-                                                      (((minus >> k) & 1) << 30))
-                                                   : kRecNone;
-                        slot[0] = make_uint4(r[0], r[1], r[2], r[3]);
-                        slot[1] = make_uint4(r[4], r[5], r[6], r[7]);
-                        written = true;
-                      });
-    if (!written) {
-      slot[0] = make_uint4(kRecNone, kRecNone, kRecNone, kRecNone);
-      slot[1] = slot[0];
-    }
   } else if (kMode == 4) {
     int *cs = reinterpret_cast<int *>(records), *cd = cs + g.sino_size;
     auto wide = [&](long long addr, int sel, bool minus) { atomicAdd((sel ? cd : cs) + addr, minus ? -1 : 1); };
@@ -625,7 +625,7 @@ __global__ void __launch_bounds__(kThreads, HRRT_LM_MIN_BLOCKS) lm_hist_kernel(
     walk_events<false>(g, tb, w, s, e, pend, t0, limit, mode, flags, c, tagpos, 0, nullptr, scatter,
                        each(scatter));
   }
-  if (kMode == 1 || kMode == 2 || kMode == 4 || kMode == 5) {
+  if (kMode == 1 || kMode == 2 || kMode == 4) {
     // block reduction of the counters
 #pragma unroll
     for (int k = 0; k < kStCount; k++) {
@@ -668,29 +668,6 @@ __global__ void __launch_bounds__(kThreads) lm_part_hist_kernel(const uint32_t *
     const uint32_t r = __ldg(records + i);
     bump16(((r >> 29) & 1) ? dly : sino, r & 0x1FFFFFFFu, ((r >> 30) & 1) != 0);
   }
-}
-
-// The stream-order records of mode 5 added to the 16-bit bins: kSub/2
-// records (two 16-byte loads) per thread, every add issued before any carry
-// is checked; nothing else to do, so many threads (and adds) per SM.
-static_assert(kSub / 2 == 8, "two uint4 of records per thread");
-__global__ void __launch_bounds__(kThreads) lm_rec_hist_kernel(const uint4 *__restrict__ records, long long nthreads,
-                                                               uint32_t *__restrict__ sino, uint32_t *__restrict__ dly) {
-  const long long t = (long long)blockIdx.x * kThreads + threadIdx.x;
-  if (t >= nthreads) return;
-  const uint4 v0 = __ldcs(records + 2 * t), v1 = __ldcs(records + 2 * t + 1);
-  const uint32_t r[8] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y, v1.z, v1.w};
-  long long addr[8];
-  uint32_t live = 0, sel = 0, minus = 0;
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    addr[k] = r[k] & 0x1FFFFFFFu;
-    if (r[k] == kRecNone) continue;
-    live |= 1u << k;
-    sel |= ((r[k] >> 29) & 1u) << k;
-    minus |= ((r[k] >> 30) & 1u) << k;
-  }
-  if (live) bump16_events<8>(sino, dly, addr, live, sel, minus);
 }
 
 // Smoothed randoms: compute_delays (gen_delays_lib/gen_delays_lib.cpp:89-153)
@@ -1096,8 +1073,8 @@ int lm_hist_call(hrrt_lm *h, const uint32_t *d_words, long long nwords, int mode
   e = cudaMemsetAsync(stats, 0, 8 * (kStCount + 1), st);
   if (e == cudaSuccess) {
     lm_map_kernel<<<(unsigned)ntiles, kThreads, 0, st>>>(d_words, nwords, tile_sum);
-    lm_entry_kernel<<<(unsigned)((npackets + 127) / 128), 128, 0, st>>>(tile_sum, ntiles, tpp, npackets, tile_entry,
-                                                                       tile_tagoff, pk);
+    lm_entry_kernel<<<(unsigned)((npackets * 32 + kEntryThreads - 1) / kEntryThreads), kEntryThreads, 0, st>>>(
+        tile_sum, ntiles, tpp, npackets, tile_entry, tile_tagoff, pk);
     lm_scan_kernel<<<1, 1024, 0, st>>>(pk, npackets, stats + kStCount);
     e = cudaGetLastError();
   }
@@ -1135,20 +1112,13 @@ int lm_hist_call(hrrt_lm *h, const uint32_t *d_words, long long nwords, int mode
     wide = true;
     partitioned = false;
   }
-  bool recs = kRecordsByDefault && nwords >= kRecordsMinWords && !partitioned && !wide &&
-              !(flags & HRRT_LM_FORCE_DIRECT);
-  if (flags & HRRT_LM_FORCE_RECORDS) {
-    recs = true;
-    partitioned = wide = false;
-  }
   if (2 * pps > kMaxParts) partitioned = false;
   unsigned long long *cursor = stats + kStCount + 1;          // [kMaxParts]
   unsigned long long *starts = cursor + kMaxParts;            // [kMaxParts + 1]
-  if ((partitioned || wide || recs) && e == cudaSuccess) {
+  if ((partitioned || wide) && e == cudaSuccess) {
     // partitioned: one packed record per event; wide: 32-bit counters for
-    // both sinograms; records: kSub/2 slots per thread of every tile
-    const long long cap = recs ? (long long)ntiles * kTileWords / 2
-                               : partitioned ? nwords / 2 + 1 : 2 * h->dev.sino_size;
+    // both sinograms
+    const long long cap = partitioned ? nwords / 2 + 1 : 2 * h->dev.sino_size;
     if (cap > h->rec_cap) {
       if (h->records) cudaFree(h->records);
       h->records = nullptr;
@@ -1156,7 +1126,7 @@ int lm_hist_call(hrrt_lm *h, const uint32_t *d_words, long long nwords, int mode
       e = cudaMalloc(&h->records, sizeof(uint32_t) * (size_t)cap);
       if (e != cudaSuccess) {
         h->records = nullptr;
-        partitioned = wide = recs = false;  // not enough memory: fall back to the direct path
+        partitioned = wide = false;  // not enough memory: fall back to the direct path
         e = cudaSuccess;
         cudaGetLastError();
       } else {
@@ -1186,14 +1156,6 @@ int lm_hist_call(hrrt_lm *h, const uint32_t *d_words, long long nwords, int mode
       case 4:
         lm_hist_kernel<4><<<nb, kThreads, 0, st>>>(dv, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
                                                    mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
-        break;
-      case 5:
-        lm_hist_kernel<5><<<nb, kThreads, 0, st>>>(dv, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
-                                                   mode, flags, tcap, tags, sn, dl, stats, cursor, h->records, pps);
-        if (cudaPeekAtLastError() == cudaSuccess) {
-          const long long nth = (long long)nb * kThreads;
-          lm_rec_hist_kernel<<<nb, kThreads, 0, st>>>(reinterpret_cast<const uint4 *>(h->records), nth, sn, dl);
-        }
         break;
       default:
         lm_hist_kernel<3><<<nb, kThreads, 0, st>>>(dv, d_words, nwords, tile_entry, tile_tagoff, pk, tpp, lim,
@@ -1230,7 +1192,7 @@ int lm_hist_call(hrrt_lm *h, const uint32_t *d_words, long long nwords, int mode
     if (e == cudaSuccess) e = cudaMemsetAsync(h->ccounts, 0, sizeof(unsigned int) * 2 * hrrt::kCrystals, st);
   }
   const bool one_pass = duration <= 0 && !hc;
-  const int hist_mode = partitioned ? 2 : (wide ? 4 : (recs ? 5 : 1));
+  const int hist_mode = partitioned ? 2 : (wide ? 4 : 1);
   if (one_pass && (flags & HRRT_LM_CRYSTAL_COUNTS)) dv.ccounts = h->ccounts;
   if (e == cudaSuccess) e = launch(one_pass ? hist_mode : 0, one_pass ? nwords : -1, tag_cap);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);

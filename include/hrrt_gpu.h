@@ -188,19 +188,6 @@ int hrrt_bp_pair(hrrt_ctx *ctx, const float *prj, int view, float *imagebuf_xyz,
  * Clears the sensitivity images.  No counterpart in the reference. */
 int hrrt_set_backprojector(hrrt_ctx *ctx, int mode);
 
-/* Shared-memory staging of the projectors in OSEM subsets (hrrt_osem,
- * hrrt_osem_subsets, hrrt_reconstruct, batches).  HRRT_STAGE_F32 (default):
- * the forward projector's sampled rows are staged as float -- the reference's
- * arithmetic, bit for bit.  HRRT_STAGE_BF16: they are staged as bf16 (each
- * bilinear sample rounded once to an 8-bit significand; the z interpolation,
- * the line integrals and everything after stay float), which halves the
- * shared-memory bytes the forward projector reads per sample -- its bound.
- * Part of the 16-bit precision form beside HRRT_STORE_16 / HRRT_STORE_F16.
- * The sensitivity images, hrrt_fp_pair, hrrt_bp_pair and hrrt_forward_project
- * always run in float.  No counterpart in the reference. */
-enum { HRRT_STAGE_F32 = 0, HRRT_STAGE_BF16 = 1 };
-int hrrt_set_staging(hrrt_ctx *ctx, int mode);
-
 /*
  * Back projection of one view pair that allocates no device memory (no
  * counterpart in the reference, whose projector works on host arrays).  For
@@ -375,10 +362,6 @@ int hrrt_batch_get_image(hrrt_batch *b, int frame, float *image_zyx, double *sum
 #define HRRT_LM_HEAD_CURVE 128
 /* also count the coincidence histogram (hrrt_lm_crystal_counts) */
 #define HRRT_LM_CRYSTAL_COUNTS 256
-/* implementation choice (same result): rebin every event into a 4-byte
- * record in stream order first, then add the records to the 16-bit bins in
- * a separate pass that does nothing else (more atomics in flight per SM) */
-#define HRRT_LM_FORCE_RECORDS 512
 
 /* one line of the head curve (.hc, process_tagword histogram_mp.cpp:241-258):
  * at each change of second, the time, the prompt and delayed events since the

@@ -225,49 +225,3 @@ def test_reconstruct_full_size(hrrt3_inputs):
     with H.Context(product_geom(HRRT3)) as ctx:
         got, st = ctx.reconstruct(*raw, iterations=1)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
-
-
-@pytest.mark.parametrize("storage", [0, 2])
-def test_bf16_staging_vs_fp64_oracle(hrrt3_inputs, storage):
-    """HRRT_STAGE_BF16 (the forward projector stages bf16 samples in OSEM
-    subsets), with float or fp16 terms: two subsets within 1e-3 rel-L2 of the
-    FP64 oracle and of the float-staged path; the sensitivity images are
-    untouched by the staging (bit-identical)."""
-    import hrrt_reconstruction_b200 as H
-    O, raw, (p, a, m) = hrrt3_inputs
-    imgs, sens = [], []
-    for stage in (H.STAGE_F32, H.STAGE_BF16):
-        with H.Context(product_geom(HRRT3)) as ctx:
-            ctx.set_staging(stage)
-            ctx.upload_inputs(*raw, storage=storage)
-            ctx.sensitivity()
-            sens.append(ctx.get_sensitivity(0))
-            ctx.init_image()
-            ctx.osem_subsets(0, 2)
-            imgs.append(ctx.get_image_xyz())
-    assert np.array_equal(sens[0].view(np.uint32), sens[1].view(np.uint32))
-    nf = O.sensitivity(m)
-    want = O.init_image()
-    for s in [int(v) for v in O.order()[:2]]:
-        O.osem_subset(want, nf[s], p, a, s)
-    e_oracle = rel_l2(imgs[1], want)
-    e_f32 = rel_l2(imgs[1], imgs[0])
-    assert e_oracle <= 1e-3, e_oracle
-    assert e_f32 <= 1e-3, e_f32
-
-
-def test_bf16_staging_leaves_projector_entry_points_exact():
-    """The staging applies to OSEM subsets only: hrrt_fp_pair stays
-    bit-identical to the oracle's single-precision forward projection."""
-    import hrrt_reconstruction_b200 as H
-    from oracle.oracle import Oracle
-    d = ALL["small3"]
-    O = Oracle(precision="f32", **d)
-    rng = np.random.default_rng(3)
-    with H.Context(product_geom(d)) as ctx:
-        ctx.set_staging(H.STAGE_BF16)
-        img = rng.random(ctx.image_shape, dtype=np.float32)
-        for view in (0, 7):
-            want = O.fp_pair(img, view)
-            got = ctx.fp_pair(img, view)
-            assert np.array_equal(want.view(np.uint32), got.view(np.uint32))
