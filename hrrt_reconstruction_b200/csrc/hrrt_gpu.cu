@@ -926,8 +926,11 @@ int hrrt_osem(hrrt_ctx *ctx, int iterations, hrrt_stats *stats) {
   return HRRT_OK;
 }
 
+// Each subset's strided copies (1 KB rows) are dealt out over kCopyStreams
+// streams: measured on B200 for the span-3 reconstruction with the projectors
+// running, 271 ms with one stream, 267 with two, 262 with four.
 #ifndef HRRT_COPY_STREAMS
-#define HRRT_COPY_STREAMS 1
+#define HRRT_COPY_STREAMS 4
 #endif
 constexpr int kCopyStreams = HRRT_COPY_STREAMS;  // 1..4
 static_assert(kCopyStreams >= 1 && kCopyStreams <= 4, "copy streams");

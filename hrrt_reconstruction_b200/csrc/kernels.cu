@@ -583,6 +583,12 @@ __device__ __forceinline__ void store_lane(float *__restrict__ dst, const Q2 (&s
   if (ACC) {
 #pragma unroll
     for (int j = 0; j < KB; j++) atomicAdd(dst + j, v[j]);
+  } else if constexpr (KB == 8) {
+    // one 32-byte store (sm_100): a whole sector per lane, one line touched
+    // per row of the warp's task tile instead of two stores to each
+    asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(dst), "f"(v[0]), "f"(v[1]), "f"(v[2]),
+                 "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+                 : "memory");
   } else {
 #pragma unroll
     for (int j = 0; j < KB; j += 4)
