@@ -92,11 +92,6 @@ __device__ __forceinline__ uint64_t add2(uint64_t a, uint64_t b) {
   asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
   return r;
 }
-__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
-  uint64_t r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-  return r;
-}
 __device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
   uint64_t r;
   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
@@ -119,9 +114,18 @@ __device__ __forceinline__ Q2 ldq(const float4 *p) {
   return Q2{v.x, v.y};
 }
 __device__ __forceinline__ Q2 qadd(Q2 a, Q2 b) { return Q2{add2(a.lo, b.lo), add2(a.hi, b.hi)}; }
-__device__ __forceinline__ Q2 qsub(Q2 a, Q2 b) { return Q2{sub2(a.lo, b.lo), sub2(a.hi, b.hi)}; }
 __device__ __forceinline__ Q2 qmul(Q2 a, uint64_t s) { return Q2{mul2(a.lo, s), mul2(a.hi, s)}; }
 __device__ __forceinline__ Q2 qaddp(Q2 a, Q2 p, uint64_t one) { return Q2{addp(a.lo, p.lo, one), addp(a.hi, p.hi, one)}; }
+// packed a * b + c (one rounding), where no reference rounding order is to
+// be kept: the back projector (held to the reference within 2e-6, its sums
+// being incremental there and direct here) and the exact adjoint (held to
+// the FP64 oracle)
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ Q2 qfma(Q2 a, uint64_t b, Q2 c) { return Q2{fma2(a.lo, b, c.lo), fma2(a.hi, b, c.hi)}; }
 __device__ __forceinline__ float4 q2f(Q2 q) {
   const float2 a = upk(q.lo), b = upk(q.hi);
   return make_float4(a.x, a.y, b.x, b.y);
@@ -556,18 +560,19 @@ __device__ __forceinline__ int bsw(int i) { return i ^ ((i >> 3) & 7); }
 
 template <int KB>
 __device__ __forceinline__ void bp_lerp(Q2 (&s)[KB], const float4 *__restrict__ P, int pbase, const BpLut &bl,
-                                        int z0, uint64_t one) {
+                                        int z0) {
   // windows wholly outside [zs, ze] contribute nothing; a window that
   // straddles an end reads the segment's zero planes for its outside planes
   if (z0 + KB - 1 < bl.zs || z0 > bl.ze) return;
   const int i0 = pbase + z0 + bl.d;
-  const uint64_t f = pk(bl.f, bl.f);
+  // the reference's p[yr] + f*(p[yr+1]-p[yr]) (sbrt:4312-4315) as
+  // (1-f) p[yr] + f p[yr+1], added with two fused multiply-adds
+  const uint64_t f = pk(bl.f, bl.f), g = pk(1.0f - bl.f, 1.0f - bl.f);
   Q2 a = ldq(P + bsw(i0));
 #pragma unroll
   for (int j = 0; j < KB; j++) {
     const Q2 b = ldq(P + bsw(i0 + j + 1));
-    // the reference's p[yr] + f*(p[yr+1]-p[yr]) (sbrt:4312-4315)
-    s[j] = qadd(s[j], qaddp(a, qmul(qsub(b, a), f), one));
+    s[j] = qfma(b, f, qfma(a, g, s[j]));
     a = b;
   }
 }
@@ -601,7 +606,6 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(De
                                                  const QuadWork *__restrict__ work, float *__restrict__ bc,
                                                  float *__restrict__ br, long long vol, FrameStrides fr,
                                                  int view0, int x0, int rlog) {
-  const uint64_t one = pk(g.unit, g.unit);
   extern __shared__ float4 P[];  // [bp_splanes]: segments with kBpPad zero planes each side
   // ACC: one view pair, quads x0 + blockIdx.x, both partial sums added into bc
   // (each voxel receives exactly two terms, so the atomic adds onto a zeroed
@@ -685,8 +689,8 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(De
         const int gn = (gg + 1 < G) ? gg + 1 : gg;
         const BpLut n1 = l1[(size_t)gn * N], n2 = l2[(size_t)gn * N];  // next group, in flight
         // sumt1: segment 2k at +u and 2k-1 at -u; sumt2: the converse
-        bp_lerp<KB>(s, P, half ? po : pe, b1, z0, one);
-        bp_lerp<KB>(s, P, half ? pe : po, b2, z0, one);
+        bp_lerp<KB>(s, P, half ? po : pe, b1, z0);
+        bp_lerp<KB>(s, P, half ? pe : po, b2, z0);
         b1 = n1;
         b2 = n2;
       }
@@ -730,14 +734,7 @@ __global__ void __launch_bounds__(NT, NT >= 384 ? 2 : kBpMinBlocks) bp_kernel(De
 // rotation whose sample footprint (recomputed with the forward projector's own
 // float expressions) holds it, with that footprint's weight.
 // ============================================================================
-// packed a * b + c (one rounding): the exact adjoint is held to the FP64
-// oracle within its tolerance, not to a reference's rounding order
-__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
-  uint64_t r;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
-  return r;
-}
-__device__ __forceinline__ Q2 qfma(Q2 a, uint64_t b, Q2 c) { return Q2{fma2(a.lo, b, c.lo), fma2(a.hi, b, c.hi)}; }
+
 
 // One side of a segment group's middle planes transposed: for the task's
 // planes z0 + j, s[j] += w0 * P[a0 + j - d0] + w1 * P[a0 + j - d1] over the
