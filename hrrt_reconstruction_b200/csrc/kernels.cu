@@ -6,9 +6,11 @@
 // bit-identical to the reference on the same inputs.
 #include "kernels.cuh"
 
-#include <type_traits>
+#include <cuda.h>  // CUtensorMap (the encoder is reached through the runtime's driver entry point)
 
 #include <cfloat>
+#include <cstring>
+#include <type_traits>
 
 namespace hrrt {
 
@@ -155,6 +157,16 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
+// one box of a 4-D tensor (coordinates innermost first) into shared memory,
+// completing on the mbarrier; the map is a __grid_constant__ kernel parameter
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+      : "memory");
+}
 // bounded wait on an mbarrier phase; on timeout records the error and returns false
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
   const uint32_t a = smem_u32(bar);
@@ -282,16 +294,20 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
                                                      const QuadWork *__restrict__ work,
                                                      const PT *__restrict__ prompts, const AT *__restrict__ add,
                                                      float4 *__restrict__ out, long long out_pair_stride,
-                                                     int nprod_warps, FrameStrides fr) {
+                                                     int nprod_warps, FrameStrides fr,
+                                                     const __grid_constant__ CUtensorMap cols, int use_cols) {
   // shared memory: [S slots][8 points][2 column pairs][2*zp] staged corner
   // columns, 2*cpair zeros (the corners of outside points), [S slots][2 halves]
   // [ZS] sampled rows, [ZS] centre column (S = kFpSlots)
   const uint64_t one = pk(g.unit, g.unit);
-  extern __shared__ float4 smem[];
+  extern __shared__ __align__(128) float4 smem[];
   const int ZS = g.zp + kFpZPad;
   const int zp = g.zp;
   const int cpair = 2 * zp;  // floats per column pair
   float *corners = reinterpret_cast<float *>(smem);
+  // the four corner columns of a point arrive as one box of the image's
+  // tensor map where the map is there and the slots are 128-byte aligned
+  const bool box4 = use_cols && (smem_u32(corners) & 127u) == 0;
   const int zoff = kFpSlots * 8 * 2 * cpair;
   float *zcol = corners + zoff;
   float4 *rows = smem + (size_t)(kFpSlots * 8 * 2 + 2) * cpair / 4;  // [S][2][ZS]
@@ -361,8 +377,17 @@ __global__ void __launch_bounds__(MW * 32, 1) fp_kernel(DevGeom g, const float *
     if (l == 0) bulk_g2s(&s_mid[es][0], g.fpmid + (size_t)y * G, (uint32_t)G * 16u, &s_bar[sl]);
     if (inside) {
       float *dst = corners + ((size_t)(sl * 8 + l) * 2) * cpair;
-      bulk_g2s(dst, image + pt.base, cpair * 4u, &s_bar[sl]);
-      bulk_g2s(dst + cpair, image + pt.base + (size_t)N * zp, cpair * 4u, &s_bar[sl]);
+      const int ix = pt.base / (N * zp), iy = pt.base / zp - ix * N;
+      if (box4 && iy + 1 < N) {
+        // columns (ix, iy..iy+1) and (ix+1, iy..iy+1): box {zp, 2, 2} at
+        // (0, iy, ix, stored frame), laid out as the two pairs below
+        tma_load_4d(dst, &cols, 0, iy, ix, fs, &s_bar[sl]);
+      } else {
+        // the pair (ix, N-1..N) runs on into column (ix+1, 0) in the
+        // contiguous image, as the reference's flat addressing reads it
+        bulk_g2s(dst, image + pt.base, cpair * 4u, &s_bar[sl]);
+        bulk_g2s(dst + cpair, image + pt.base + (size_t)N * zp, cpair * 4u, &s_bar[sl]);
+      }
     }
   };
 
@@ -1325,6 +1350,44 @@ __global__ void scale_pairs_kernel(DevGeom g, const T *__restrict__ src, const i
   dst[(size_t)slot * dst_pair_stride + i] = o;
 }
 
+// The images the forward projector samples as a 4-D tensor (z, y, x, stored
+// frame) with a box of the four corner columns of one sample point, {zp, 2,
+// 2, 1}: one bulk tensor copy instead of two per point (the projector's row
+// pipeline is bound by the number of copies, not their bytes).  Returns 0 (the
+// kernel then copies column pairs) where the encoder is unavailable or
+// refuses the shape.
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+int image_column_map(const DevGeom &g, const float *image, const FrameStrides &fr, CUtensorMap *map) {
+  static EncodeTiledFn encode = [] {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return (EncodeTiledFn) nullptr;
+    }
+    return reinterpret_cast<EncodeTiledFn>(fn);
+  }();
+  std::memset(map, 0, sizeof(*map));
+  if (!encode || !image || (reinterpret_cast<uintptr_t>(image) & 15)) return 0;
+  const cuuint64_t N = (cuuint64_t)g.nx, zp = (cuuint64_t)g.zp;
+  const cuuint64_t fstride = fr.image > 0 ? (cuuint64_t)fr.image : N * N * zp;
+  // stored frames: every frame a launch may name (the map bounds no access the
+  // kernel makes; coordinates stay inside the frames that exist)
+  const cuuint64_t frames = fr.image > 0 ? (cuuint64_t)1 << 16 : 1;
+  const cuuint64_t dim[4] = {zp, N, N, frames};
+  const cuuint64_t stride[3] = {zp * 4, N * zp * 4, fstride * 4};
+  const cuuint32_t box[4] = {(cuuint32_t)zp, 2, 2, 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  if (zp > 256 || (zp * 4) % 16 || (fstride * 4) % 16) return 0;
+  const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float *>(image), dim, stride, box, es,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? 1 : 0;
+}
+
 template <int MODE, int PL, int MW, typename PT, typename AT>
 cudaError_t launch_fp_t(const DevGeom &g, const float *image, const QuadWork *work, int nwork, const void *prompts,
                         const void *add, float *out, long long out_pair_stride, int pwarps_req,
@@ -1343,8 +1406,11 @@ cudaError_t launch_fp_t(const DevGeom &g, const float *image, const QuadWork *wo
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   if (e != cudaSuccess) return e;
+  CUtensorMap cols;
+  const int use_cols = image_column_map(g, image, fr, &cols);
   k<<<(unsigned)nwork * fr.n, threads, smem, st>>>(g, image, work, (const PT *)prompts, (const AT *)add,
-                                                   reinterpret_cast<float4 *>(out), out_pair_stride / 4, pwarps, fr);
+                                                   reinterpret_cast<float4 *>(out), out_pair_stride / 4, pwarps, fr,
+                                                   cols, use_cols);
   return cudaGetLastError();
 }
 
